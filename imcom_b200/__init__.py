@@ -1,0 +1,12 @@
+"""imcom_b200: the IMCOM solve path on one B200 (sm_100a).
+
+The compute lives in ``libimcom_gpu.so`` (hand-written CUDA behind the C-ABI of
+``include/imcom_gpu.h``).  This package holds the ctypes binding
+(``_lib``), a host-side mirror of the reference's solve-path routines
+(``api.Solver``), the problem model (``problem``) and the seeded synthetic
+inputs (``synth``).
+"""
+from .api import (EIGH_DC, EIGH_JACOBI, EIGH_LIBRARY, EPS, ImcomError, SolveResult,  # noqa: F401
+                  Solver)
+
+__all__ = ["Solver", "SolveResult", "ImcomError", "EIGH_DC", "EIGH_JACOBI", "EIGH_LIBRARY", "EPS"]

@@ -1,0 +1,158 @@
+// common.cuh -- shared definitions of the sm_100a IMCOM solve path.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "../../include/imcom_gpu.h"
+
+namespace imcom {
+
+// Device matrix: column-major, leading dimension ld >= rows (rounded up so
+// that every column starts on a 256-byte boundary).
+struct DMat {
+  double* p = nullptr;
+  long long rows = 0, cols = 0, ld = 0;
+  size_t bytes() const { return (size_t)ld * (size_t)cols * sizeof(double); }
+};
+
+inline long long pad_ld(long long rows) { return (rows + 31) / 32 * 32; }
+
+enum Stage { ST_SPECTRA = 0, ST_A, ST_EIG, ST_B, ST_P, ST_BISECT, ST_T, ST_EPI, ST_N };
+
+struct MlpWeights {
+  float* w = nullptr;  // packed device weights (see kappa.cu)
+  bool set = false;
+};
+
+struct EigWork;  // eigen.cu
+
+}  // namespace imcom
+
+struct imcom_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int eig_mode = IMCOM_EIGH_DC;
+  long long eig_maxiter = 0;
+
+  // geometry
+  int n = 0, m = 0;
+  double psfx = 0, psfy = 0;
+  double *x = nullptr, *y = nullptr, *X = nullptr, *Y = nullptr;
+  double *I = nullptr, *Nd = nullptr;
+  int* exp_i = nullptr;  // 1-based
+  bool have_I = false, have_N = false;
+
+  // PSFs
+  int nps = 0, nexppsf = 0, psfconst = 0;
+  double* G = nullptr;       // (nps, nps, E) real
+  double* Gamma = nullptr;   // (nps, nps)
+  double* rot = nullptr;     // host copy of angles (E)
+  double2* Gt = nullptr;     // (nps, nps, E) complex
+  double2* Gammat = nullptr; // (nps, nps)
+  bool have_psf = false, have_spectra = false;
+  double C_a = 0;
+
+  // system
+  imcom::DMat A, Q, B, P, T, Pt;  // Pt = P / (L + K_a), the T GEMM operand
+  double* L = nullptr;
+  double *K = nullptr, *US = nullptr, *H = nullptr, *S = nullptr, *U = nullptr;
+  int* nev = nullptr;
+  int* flags = nullptr;  // device status word(s)
+  bool have_A = false, have_QL = false, have_B = false, have_P = false,
+       have_K = false, have_T = false, have_Pt = false;
+  int max_exp = 0;  // largest exp_i
+
+  // tables and FFT scratch (kept between calls of the same size)
+  double* tables = nullptr;
+  size_t tables_bytes = 0;
+  double2* fftbuf = nullptr;
+  size_t fftbuf_bytes = 0;
+  cufftHandle plan_big = 0;
+  int plan_big_L = 0, plan_big_batch = 0;
+  cufftHandle plan_r2c = 0;
+  int plan_r2c_n = 0, plan_r2c_batch = 0;
+
+  imcom::EigWork* eig = nullptr;
+  imcom::MlpWeights mlp;
+  float* feat = nullptr;
+
+  cudaEvent_t ev0[imcom::ST_N] = {}, ev1[imcom::ST_N] = {};
+  bool ev_used[imcom::ST_N] = {};
+};
+
+namespace imcom {
+
+int set_err(imcom_ctx* c, int code, const char* fmt, ...);
+
+#define IMC_CUDA(call)                                                        \
+  do {                                                                        \
+    cudaError_t e_ = (call);                                                  \
+    if (e_ != cudaSuccess)                                                    \
+      return ::imcom::set_err(ctx, IMCOM_ERR_CUDA, "%s: %s (%s:%d)", #call,   \
+                              cudaGetErrorString(e_), __FILE__, __LINE__);    \
+  } while (0)
+
+extern unsigned long long g_launches;
+
+#define IMC_LAUNCH()                                                          \
+  do {                                                                        \
+    __atomic_fetch_add(&::imcom::g_launches, 1ULL, __ATOMIC_RELAXED);         \
+    cudaError_t e_ = cudaGetLastError();                                      \
+    if (e_ != cudaSuccess)                                                    \
+      return ::imcom::set_err(ctx, IMCOM_ERR_CUDA, "kernel launch: %s (%s:%d)",\
+                              cudaGetErrorString(e_), __FILE__, __LINE__);    \
+  } while (0)
+
+#define IMC_CUFFT(call)                                                       \
+  do {                                                                        \
+    cufftResult r_ = (call);                                                  \
+    if (r_ != CUFFT_SUCCESS)                                                  \
+      return ::imcom::set_err(ctx, IMCOM_ERR_LIBRARY, "%s: cufft status %d",  \
+                              #call, (int)r_);                                \
+  } while (0)
+
+#define IMC_TRY(expr)                                                         \
+  do {                                                                        \
+    int s_ = (expr);                                                          \
+    if (s_ != 0) return s_;                                                   \
+  } while (0)
+
+// (Re)allocate a device matrix of the given shape; keeps the buffer when it
+// is already large enough.
+int ensure_mat(imcom_ctx* ctx, DMat& M, long long rows, long long cols);
+int ensure_buf(imcom_ctx* ctx, void** p, size_t& have, size_t need);
+template <class T>
+int ensure_vec(imcom_ctx* ctx, T** p, size_t count);
+
+int upload_mat(imcom_ctx* ctx, DMat& M, const double* host, long long rows,
+               long long cols);
+int download_mat(imcom_ctx* ctx, const DMat& M, double* host);
+
+void stage_begin(imcom_ctx* ctx, Stage s);
+void stage_end(imcom_ctx* ctx, Stage s);
+
+// Number of SMs of the context's device (cached).
+int sm_count(imcom_ctx* ctx);
+
+// ---- kernels exported between translation units ----
+// FP64 GEMM: C (M x N) = alpha * op(A) * op(B) + beta * C, column-major.
+// transA: 'N' (A is M x K, ld lda) or 'T' (A is K x M).  transB: 'N' (B is
+// K x N) or 'T' (B is N x K).
+int dgemm(imcom_ctx* ctx, char transA, char transB, long long M, long long N,
+          long long K, double alpha, const double* A, long long lda,
+          const double* B, long long ldb, double beta, double* C,
+          long long ldc);
+
+int eigen_dc(imcom_ctx* ctx, const DMat& A, DMat& W, double* w);
+int eigen_jacobi(imcom_ctx* ctx, const DMat& A, DMat& Q, double* L);
+int eigen_library(imcom_ctx* ctx, const DMat& A, DMat& Q, double* L);
+void eig_free(imcom_ctx* ctx);
+
+}  // namespace imcom

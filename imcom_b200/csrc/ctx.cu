@@ -1,0 +1,451 @@
+// ctx.cu -- context, module state upload/download and the cache-read branches
+// of the reference's imcom_get_* routines.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+
+namespace imcom {
+
+unsigned long long g_launches = 0;
+
+int set_err(imcom_ctx* c, int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+int ensure_buf(imcom_ctx* ctx, void** p, size_t& have, size_t need) {
+  if (*p && have >= need) return 0;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  have = 0;
+  if (need == 0) return 0;
+  cudaError_t e = cudaMalloc(p, need);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return set_err(ctx, IMCOM_ERR_ALLOC, "cudaMalloc(%zu bytes): %s", need,
+                   cudaGetErrorString(e));
+  }
+  have = need;
+  return 0;
+}
+
+int ensure_mat(imcom_ctx* ctx, DMat& M, long long rows, long long cols) {
+  long long ld = pad_ld(rows);
+  size_t need = (size_t)ld * (size_t)cols * sizeof(double);
+  if (M.p && M.ld == ld && M.cols == cols && M.rows == rows) return 0;
+  if (M.p && M.bytes() >= need) {
+    M.rows = rows;
+    M.cols = cols;
+    M.ld = ld;
+    return 0;
+  }
+  if (M.p) cudaFree(M.p);
+  M.p = nullptr;
+  cudaError_t e = cudaMalloc(&M.p, need);
+  if (e != cudaSuccess) {
+    M.p = nullptr;
+    cudaGetLastError();
+    return set_err(ctx, IMCOM_ERR_ALLOC, "cudaMalloc(%zu bytes) for %lldx%lld matrix: %s",
+                   need, rows, cols, cudaGetErrorString(e));
+  }
+  M.rows = rows;
+  M.cols = cols;
+  M.ld = ld;
+  return 0;
+}
+
+template <class T>
+int ensure_vec(imcom_ctx* ctx, T** p, size_t count) {
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T) + 256);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return set_err(ctx, IMCOM_ERR_ALLOC, "cudaMalloc(%zu): %s", count * sizeof(T),
+                   cudaGetErrorString(e));
+  }
+  return 0;
+}
+template int ensure_vec<double>(imcom_ctx*, double**, size_t);
+template int ensure_vec<int>(imcom_ctx*, int**, size_t);
+template int ensure_vec<float>(imcom_ctx*, float**, size_t);
+template int ensure_vec<double2>(imcom_ctx*, double2**, size_t);
+
+int upload_mat(imcom_ctx* ctx, DMat& M, const double* host, long long rows,
+               long long cols) {
+  IMC_TRY(ensure_mat(ctx, M, rows, cols));
+  IMC_CUDA(cudaMemcpy2DAsync(M.p, M.ld * sizeof(double), host, rows * sizeof(double),
+                             rows * sizeof(double), cols, cudaMemcpyHostToDevice,
+                             ctx->stream));
+  return 0;
+}
+
+int download_mat(imcom_ctx* ctx, const DMat& M, double* host) {
+  IMC_CUDA(cudaMemcpy2DAsync(host, M.rows * sizeof(double), M.p, M.ld * sizeof(double),
+                             M.rows * sizeof(double), M.cols, cudaMemcpyDeviceToHost,
+                             ctx->stream));
+  return 0;
+}
+
+void stage_begin(imcom_ctx* ctx, Stage s) {
+  if (!ctx->ev0[s]) {
+    cudaEventCreate(&ctx->ev0[s]);
+    cudaEventCreate(&ctx->ev1[s]);
+  }
+  cudaEventRecord(ctx->ev0[s], ctx->stream);
+}
+
+void stage_end(imcom_ctx* ctx, Stage s) {
+  cudaEventRecord(ctx->ev1[s], ctx->stream);
+  ctx->ev_used[s] = true;
+}
+
+int sm_count(imcom_ctx* ctx) {
+  static int cached[64] = {0};
+  int d = ctx->device;
+  if (d >= 0 && d < 64 && cached[d]) return cached[d];
+  int v = 148;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, d);
+  if (d >= 0 && d < 64) cached[d] = v;
+  return v;
+}
+
+}  // namespace imcom
+
+using namespace imcom;
+
+static int check_finite(imcom_ctx* ctx, const double* p, long long count, const char* what) {
+  if (!p) return 0;
+  for (long long k = 0; k < count; ++k)
+    if (!std::isfinite(p[k]))
+      return set_err(ctx, IMCOM_ERR_NOT_FINITE, "non-finite value in %s at index %lld", what, k);
+  return 0;
+}
+
+extern "C" {
+
+int imcom_gpu_create(int device, imcom_ctx** out) {
+  if (!out) return -2;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return IMCOM_ERR_CUDA;
+  }
+  if (device < 0 || device >= ndev) return -1;
+  imcom_ctx* ctx = new imcom_ctx();
+  ctx->device = device;
+  if (cudaSetDevice(device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    delete ctx;
+    return IMCOM_ERR_CUDA;
+  }
+  if (cudaMalloc(&ctx->flags, 64 * sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return IMCOM_ERR_ALLOC;
+  }
+  cudaMemset(ctx->flags, 0, 64 * sizeof(int));
+  *out = ctx;
+  return 0;
+}
+
+int imcom_gpu_destroy(imcom_ctx* ctx) {
+  if (!ctx) return 0;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  eig_free(ctx);
+  void* ptrs[] = {ctx->x, ctx->y, ctx->X, ctx->Y, ctx->I, ctx->Nd, ctx->exp_i, ctx->G,
+                  ctx->Gamma, ctx->Gt, ctx->Gammat, ctx->A.p, ctx->Q.p, ctx->B.p, ctx->P.p,
+                  ctx->T.p, ctx->Pt.p, ctx->L, ctx->K, ctx->US, ctx->H, ctx->S, ctx->U,
+                  ctx->nev, ctx->flags, ctx->tables, ctx->fftbuf, ctx->mlp.w, ctx->feat};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  delete[] ctx->rot;
+  if (ctx->plan_big) cufftDestroy(ctx->plan_big);
+  if (ctx->plan_r2c) cufftDestroy(ctx->plan_r2c);
+  for (int s = 0; s < ST_N; ++s) {
+    if (ctx->ev0[s]) cudaEventDestroy(ctx->ev0[s]);
+    if (ctx->ev1[s]) cudaEventDestroy(ctx->ev1[s]);
+  }
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return 0;
+}
+
+const char* imcom_gpu_last_error(const imcom_ctx* ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+int imcom_gpu_synchronize(imcom_ctx* ctx) {
+  if (!ctx) return -1;
+  cudaSetDevice(ctx->device);
+  IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  IMC_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int imcom_gpu_set_option(imcom_ctx* ctx, int option, long long value) {
+  if (!ctx) return -1;
+  switch (option) {
+    case IMCOM_OPT_EIGENSOLVER:
+      if (value != IMCOM_EIGH_DC && value != IMCOM_EIGH_JACOBI && value != IMCOM_EIGH_LIBRARY)
+        return -3;
+      ctx->eig_mode = (int)value;
+      return 0;
+    case IMCOM_OPT_EIGEN_MAXITER:
+      if (value < 0) return -3;
+      ctx->eig_maxiter = value;
+      return 0;
+    default:
+      return -2;
+  }
+}
+
+int imcom_gpu_set_inputs(imcom_ctx* ctx, int n, int m, const double* x_i, const double* y_i,
+                         const int* exp_i, const double* X_a, const double* Y_a,
+                         const double* I_i, const double* Ndiag, double psfxscale,
+                         double psfyscale) {
+  if (!ctx) return -1;
+  if (n <= 0) return -2;
+  if (m <= 0) return -3;
+  if (!x_i) return -4;
+  if (!y_i) return -5;
+  if (!exp_i) return -6;
+  if (!X_a) return -7;
+  if (!Y_a) return -8;
+  if (!(psfxscale > 0)) return -11;
+  if (!(psfyscale > 0)) return -12;
+  for (int i = 0; i < n; ++i)
+    if (exp_i[i] < 1) return set_err(ctx, -6, "exp_i(%d) = %d < 1", i + 1, exp_i[i]);
+  for (int i = 1; i < n; ++i)
+    if (exp_i[i] < exp_i[i - 1])
+      return set_err(ctx, -6, "exp_i must be non-decreasing (exposure-major order)");
+  IMC_TRY(check_finite(ctx, x_i, n, "x_i"));
+  IMC_TRY(check_finite(ctx, y_i, n, "y_i"));
+  IMC_TRY(check_finite(ctx, X_a, m, "X_a"));
+  IMC_TRY(check_finite(ctx, Y_a, m, "Y_a"));
+  IMC_TRY(check_finite(ctx, I_i, n, "I_i"));
+  IMC_TRY(check_finite(ctx, Ndiag, n, "Ndiag"));
+  cudaSetDevice(ctx->device);
+  if (n != ctx->n || m != ctx->m) {
+    ctx->have_A = ctx->have_QL = ctx->have_B = ctx->have_P = ctx->have_K = ctx->have_T = false;
+  }
+  ctx->n = n;
+  ctx->m = m;
+  ctx->psfx = psfxscale;
+  ctx->psfy = psfyscale;
+  IMC_TRY(ensure_vec(ctx, &ctx->x, n));
+  IMC_TRY(ensure_vec(ctx, &ctx->y, n));
+  IMC_TRY(ensure_vec(ctx, &ctx->I, n));
+  IMC_TRY(ensure_vec(ctx, &ctx->Nd, n));
+  IMC_TRY(ensure_vec(ctx, &ctx->exp_i, n));
+  IMC_TRY(ensure_vec(ctx, &ctx->X, m));
+  IMC_TRY(ensure_vec(ctx, &ctx->Y, m));
+  IMC_TRY(ensure_vec(ctx, &ctx->L, n));
+  IMC_TRY(ensure_vec(ctx, &ctx->K, m));
+  IMC_TRY(ensure_vec(ctx, &ctx->US, m));
+  IMC_TRY(ensure_vec(ctx, &ctx->H, m));
+  IMC_TRY(ensure_vec(ctx, &ctx->S, m));
+  IMC_TRY(ensure_vec(ctx, &ctx->U, m));
+  IMC_TRY(ensure_vec(ctx, &ctx->nev, m));
+  ctx->max_exp = 0;
+  for (int i = 0; i < n; ++i) ctx->max_exp = exp_i[i] > ctx->max_exp ? exp_i[i] : ctx->max_exp;
+  IMC_CUDA(cudaMemcpyAsync(ctx->x, x_i, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  IMC_CUDA(cudaMemcpyAsync(ctx->y, y_i, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  IMC_CUDA(cudaMemcpyAsync(ctx->exp_i, exp_i, n * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  IMC_CUDA(cudaMemcpyAsync(ctx->X, X_a, m * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  IMC_CUDA(cudaMemcpyAsync(ctx->Y, Y_a, m * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  ctx->have_I = I_i != nullptr;
+  ctx->have_N = Ndiag != nullptr;
+  if (I_i)
+    IMC_CUDA(cudaMemcpyAsync(ctx->I, I_i, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  if (Ndiag)
+    IMC_CUDA(cudaMemcpyAsync(ctx->Nd, Ndiag, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int imcom_gpu_set_psfs(imcom_ctx* ctx, int nps, int nexppsf, int psfconst,
+                       const double* G_unrot, const double* rotangdeg, const double* Gamma) {
+  if (!ctx) return -1;
+  if (nps < 2) return -2;
+  if (nexppsf < 1) return -3;
+  if (psfconst != 0 && psfconst != 1)
+    return set_err(ctx, -4, "IMCOM ERROR: PSFCONST must be 1 or 0!");
+  if (psfconst == 1 && nexppsf != 1) return -3;
+  if (!G_unrot) return -5;
+  if (!rotangdeg) return -6;
+  if (!Gamma) return -7;
+  size_t ps2 = (size_t)nps * nps;
+  IMC_TRY(check_finite(ctx, G_unrot, (long long)(ps2 * nexppsf), "G_unrot"));
+  IMC_TRY(check_finite(ctx, Gamma, (long long)ps2, "Gamma"));
+  IMC_TRY(check_finite(ctx, rotangdeg, nexppsf, "rotangdeg"));
+  cudaSetDevice(ctx->device);
+  ctx->nps = nps;
+  ctx->nexppsf = nexppsf;
+  ctx->psfconst = psfconst;
+  IMC_TRY(ensure_vec(ctx, &ctx->G, ps2 * nexppsf));
+  IMC_TRY(ensure_vec(ctx, &ctx->Gamma, ps2));
+  IMC_TRY(ensure_vec(ctx, &ctx->Gt, ps2 * nexppsf));
+  IMC_TRY(ensure_vec(ctx, &ctx->Gammat, ps2));
+  delete[] ctx->rot;
+  ctx->rot = new double[nexppsf];
+  std::memcpy(ctx->rot, rotangdeg, nexppsf * sizeof(double));
+  IMC_CUDA(cudaMemcpyAsync(ctx->G, G_unrot, ps2 * nexppsf * sizeof(double),
+                           cudaMemcpyHostToDevice, ctx->stream));
+  IMC_CUDA(cudaMemcpyAsync(ctx->Gamma, Gamma, ps2 * sizeof(double), cudaMemcpyHostToDevice,
+                           ctx->stream));
+  IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->have_psf = true;
+  ctx->have_spectra = false;
+  return 0;
+}
+
+int imcom_gpu_load_A(imcom_ctx* ctx, const double* A) {
+  if (!ctx) return -1;
+  if (!A) return -2;
+  if (ctx->n <= 0) return set_err(ctx, IMCOM_ERR_STATE, "imcom_gpu_set_inputs has not run");
+  cudaSetDevice(ctx->device);
+  IMC_TRY(upload_mat(ctx, ctx->A, A, ctx->n, ctx->n));
+  IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->have_A = true;
+  return 0;
+}
+
+int imcom_gpu_load_QL(imcom_ctx* ctx, const double* Q, const double* L) {
+  if (!ctx) return -1;
+  if (!Q) return -2;
+  if (!L) return -3;
+  if (ctx->n <= 0) return set_err(ctx, IMCOM_ERR_STATE, "imcom_gpu_set_inputs has not run");
+  cudaSetDevice(ctx->device);
+  IMC_TRY(upload_mat(ctx, ctx->Q, Q, ctx->n, ctx->n));
+  IMC_CUDA(cudaMemcpyAsync(ctx->L, L, ctx->n * sizeof(double), cudaMemcpyHostToDevice,
+                           ctx->stream));
+  IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->have_QL = true;
+  return 0;
+}
+
+int imcom_gpu_load_B(imcom_ctx* ctx, const double* B) {
+  if (!ctx) return -1;
+  if (!B) return -2;
+  if (ctx->n <= 0) return set_err(ctx, IMCOM_ERR_STATE, "imcom_gpu_set_inputs has not run");
+  cudaSetDevice(ctx->device);
+  IMC_TRY(upload_mat(ctx, ctx->B, B, ctx->n, ctx->m));
+  IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->have_B = true;
+  return 0;
+}
+
+int imcom_gpu_load_P(imcom_ctx* ctx, const double* P) {
+  if (!ctx) return -1;
+  if (!P) return -2;
+  if (ctx->n <= 0) return set_err(ctx, IMCOM_ERR_STATE, "imcom_gpu_set_inputs has not run");
+  cudaSetDevice(ctx->device);
+  IMC_TRY(upload_mat(ctx, ctx->P, P, ctx->n, ctx->m));
+  IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->have_P = true;
+  return 0;
+}
+
+int imcom_gpu_load_T(imcom_ctx* ctx, const double* T) {
+  if (!ctx) return -1;
+  if (!T) return -2;
+  if (ctx->n <= 0) return set_err(ctx, IMCOM_ERR_STATE, "imcom_gpu_set_inputs has not run");
+  cudaSetDevice(ctx->device);
+  IMC_TRY(upload_mat(ctx, ctx->T, T, ctx->n, ctx->m));
+  IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->have_T = true;
+  return 0;
+}
+
+int imcom_gpu_load_K(imcom_ctx* ctx, const double* K) {
+  if (!ctx) return -1;
+  if (!K) return -2;
+  if (ctx->m <= 0) return set_err(ctx, IMCOM_ERR_STATE, "imcom_gpu_set_inputs has not run");
+  cudaSetDevice(ctx->device);
+  IMC_CUDA(cudaMemcpyAsync(ctx->K, K, ctx->m * sizeof(double), cudaMemcpyHostToDevice,
+                           ctx->stream));
+  IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->have_K = true;
+  ctx->have_Pt = false;
+  ctx->have_T = false;
+  return 0;
+}
+
+int imcom_gpu_free_AB(imcom_ctx* ctx) {
+  if (!ctx) return -1;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->A.p) cudaFree(ctx->A.p);
+  if (ctx->B.p) cudaFree(ctx->B.p);
+  ctx->A = DMat();
+  ctx->B = DMat();
+  ctx->have_A = ctx->have_B = false;
+  return 0;
+}
+
+int imcom_gpu_device_buffer(imcom_ctx* ctx, char which, void** dptr, long long* ld) {
+  if (!ctx) return -1;
+  if (!dptr) return -3;
+  long long l = 0;
+  void* p = nullptr;
+  switch (which) {
+    case 'A': p = ctx->A.p; l = ctx->A.ld; break;
+    case 'Q': p = ctx->Q.p; l = ctx->Q.ld; break;
+    case 'B': p = ctx->B.p; l = ctx->B.ld; break;
+    case 'P': p = ctx->P.p; l = ctx->P.ld; break;
+    case 'T': p = ctx->T.p; l = ctx->T.ld; break;
+    case 'L': p = ctx->L; l = ctx->n; break;
+    case 'K': p = ctx->K; l = ctx->m; break;
+    case 'H': p = ctx->H; l = ctx->m; break;
+    case 'S': p = ctx->S; l = ctx->m; break;
+    case 'U': p = ctx->U; l = ctx->m; break;
+    default: return -2;
+  }
+  *dptr = p;
+  if (ld) *ld = l;
+  return p ? 0 : set_err(ctx, IMCOM_ERR_STATE, "buffer %c not allocated", which);
+}
+
+int imcom_gpu_launch_count(imcom_ctx* ctx, long long* count) {
+  if (!ctx) return -1;
+  if (!count) return -2;
+  *count = (long long)__atomic_load_n(&g_launches, __ATOMIC_RELAXED);
+  return 0;
+}
+
+int imcom_gpu_get_stream(imcom_ctx* ctx, void** stream) {
+  if (!ctx) return -1;
+  if (!stream) return -2;
+  *stream = (void*)ctx->stream;
+  return 0;
+}
+
+int imcom_gpu_stage_times(imcom_ctx* ctx, double* ms) {
+  if (!ctx) return -1;
+  if (!ms) return -2;
+  cudaSetDevice(ctx->device);
+  IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (int s = 0; s < ST_N; ++s) {
+    float t = 0.f;
+    if (ctx->ev_used[s] && cudaEventElapsedTime(&t, ctx->ev0[s], ctx->ev1[s]) == cudaSuccess)
+      ms[s] = t;
+    else
+      ms[s] = 0.0;
+  }
+  cudaGetLastError();
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,201 @@
+// dgemm.cu -- FP64 GEMM on the B200 double-precision tensor path.
+//
+// C (M x N) = alpha * op(A) op(B) + beta * C, column-major, any M, N, K.
+// Used for P = Q^T B (imcom_build_P, imcom_matrix.f90:699, DGEMM 'T','N'),
+// T = Q P~ (imcom_build_T, :732-744, m DGEMVs fused into one GEMM) and the
+// eigensolver's blocked updates.
+//
+// sm_100a has no tcgen05 kind for f64, so the FP64 tensor instruction is the
+// warp-level DMMA  mma.sync.m16n8k4.f64.  CTA tile 128 x 128 x 16, 8 warps
+// as 2 (M) x 4 (N), warp tile 64 x 32 = 4 x 4 MMAs per k-step of 4.
+// Operands stream through a 3-stage cp.async shared-memory pipeline; the
+// shared layouts are padded so every fragment load is bank-conflict free
+// (stride 20 doubles for k-contiguous tiles, 132 for m/n-contiguous ones).
+#include "common.cuh"
+
+namespace imcom {
+namespace {
+
+constexpr int BM = 128, BN = 128, BK = 16, STAGES = 3, THREADS = 256;
+constexpr int SKC = BK + 4;   // stride of a k-contiguous tile row
+constexpr int SMC = BM + 4;   // stride of an m/n-contiguous tile row
+constexpr int TILE_DBL = (BM * SKC > BK * SMC) ? BM * SKC : BK * SMC;  // 2560
+constexpr int STAGE_DBL = 2 * TILE_DBL;
+constexpr size_t SMEM_BYTES = (size_t)STAGES * STAGE_DBL * sizeof(double);
+
+__device__ __forceinline__ void cp_async(double* dst, const double* src, int bytes, int vec) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  if (vec == 2)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(src), "r"(bytes));
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(src), "r"(bytes));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// Load one operand tile.  KCONTIG: element (r, k) at P[k + r * ld] (r = m or
+// n), stored S[r][k] (stride SKC).  Otherwise element (r, k) at P[r + k * ld],
+// stored S[k][r] (stride SMC).  Out-of-range elements are zero-filled.
+template <bool KCONTIG, int VEC>
+__device__ __forceinline__ void load_tile(double* S, const double* __restrict__ P, long long ld,
+                                          long long r0, long long k0, long long R, long long K) {
+  constexpr int CHUNKS = BM * BK / VEC;
+  for (int c = threadIdx.x; c < CHUNKS; c += THREADS) {
+    long long r, k;
+    double* dst;
+    int valid;
+    const double* src;
+    if (KCONTIG) {
+      constexpr int PER = BK / VEC;
+      int rr = c / PER, kk = (c % PER) * VEC;
+      r = r0 + rr;
+      k = k0 + kk;
+      dst = S + rr * SKC + kk;
+      valid = (r < R) ? (int)min((long long)VEC, max(0LL, K - k)) : 0;
+      src = valid ? P + k + r * ld : P;
+    } else {
+      constexpr int PER = BM / VEC;
+      int kk = c / PER, rr = (c % PER) * VEC;
+      r = r0 + rr;
+      k = k0 + kk;
+      dst = S + kk * SMC + rr;
+      valid = (k < K) ? (int)min((long long)VEC, max(0LL, R - r)) : 0;
+      src = valid ? P + r + k * ld : P;
+    }
+    cp_async(dst, src, valid * 8, VEC);
+  }
+}
+
+template <bool AK, bool BKC, int VEC>
+__global__ void __launch_bounds__(THREADS, 1)
+dgemm_kernel(long long M, long long N, long long K, double alpha, const double* __restrict__ A,
+             long long lda, const double* __restrict__ B, long long ldb, double beta,
+             double* __restrict__ C, long long ldc) {
+  extern __shared__ __align__(16) double smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wm = warp & 1, wn = warp >> 1;  // 2 x 4 warps
+  const int g = lane >> 2, t = lane & 3;
+  const long long m0 = (long long)blockIdx.x * BM, n0 = (long long)blockIdx.y * BN;
+  const int nk = (int)((K + BK - 1) / BK);
+
+  double acc[4][4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0;
+
+  auto stageA = [&](int s) { return smem + s * STAGE_DBL; };
+  auto stageB = [&](int s) { return smem + s * STAGE_DBL + TILE_DBL; };
+
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < nk) {
+      load_tile<AK, VEC>(stageA(s), A, lda, m0, (long long)s * BK, M, K);
+      load_tile<BKC, VEC>(stageB(s), B, ldb, n0, (long long)s * BK, N, K);
+    }
+    cp_commit();
+  }
+
+  for (int kt = 0; kt < nk; ++kt) {
+    cp_wait<STAGES - 2>();
+    __syncthreads();
+    const double* As = stageA(kt % STAGES);
+    const double* Bs = stageB(kt % STAGES);
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 4) {
+      double af[4][2], bf[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        int mr = wm * 64 + i * 16 + g;
+        if (AK) {
+          af[i][0] = As[mr * SKC + kk + t];
+          af[i][1] = As[(mr + 8) * SKC + kk + t];
+        } else {
+          af[i][0] = As[(kk + t) * SMC + mr];
+          af[i][1] = As[(kk + t) * SMC + mr + 8];
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        int nc = wn * 32 + j * 8 + g;
+        bf[j] = BKC ? Bs[nc * SKC + kk + t] : Bs[(kk + t) * SMC + nc];
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          asm volatile(
+              "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+              "{%0,%1,%2,%3};\n"
+              : "+d"(acc[i][j][0]), "+d"(acc[i][j][1]), "+d"(acc[i][j][2]), "+d"(acc[i][j][3])
+              : "d"(af[i][0]), "d"(af[i][1]), "d"(bf[j]));
+    }
+    int nxt = kt + STAGES - 1;
+    if (nxt < nk) {
+      load_tile<AK, VEC>(stageA(nxt % STAGES), A, lda, m0, (long long)nxt * BK, M, K);
+      load_tile<BKC, VEC>(stageB(nxt % STAGES), B, ldb, n0, (long long)nxt * BK, N, K);
+    }
+    cp_commit();
+  }
+  cp_wait<0>();
+
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        long long row = m0 + wm * 64 + i * 16 + g + ((r >> 1) ? 8 : 0);
+        long long col = n0 + wn * 32 + j * 8 + 2 * t + (r & 1);
+        if (row < M && col < N) {
+          double* cp = C + row + col * ldc;
+          double v = alpha * acc[i][j][r];
+          if (beta != 0.0) v += beta * *cp;
+          *cp = v;
+        }
+      }
+}
+
+template <bool AK, bool BKC>
+int launch(imcom_ctx* ctx, long long M, long long N, long long K, double alpha, const double* A,
+           long long lda, const double* B, long long ldb, double beta, double* C, long long ldc,
+           int vec) {
+  dim3 grd((unsigned)((M + BM - 1) / BM), (unsigned)((N + BN - 1) / BN));
+  if (vec == 2) {
+    auto k = dgemm_kernel<AK, BKC, 2>;
+    IMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES));
+    k<<<grd, THREADS, SMEM_BYTES, ctx->stream>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+  } else {
+    auto k = dgemm_kernel<AK, BKC, 1>;
+    IMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES));
+    k<<<grd, THREADS, SMEM_BYTES, ctx->stream>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+  }
+  IMC_LAUNCH();
+  return 0;
+}
+
+}  // namespace
+
+int dgemm(imcom_ctx* ctx, char transA, char transB, long long M, long long N, long long K,
+          double alpha, const double* A, long long lda, const double* B, long long ldb,
+          double beta, double* C, long long ldc) {
+  if (M <= 0 || N <= 0) return 0;
+  if (K <= 0) {
+    if (beta == 1.0) return 0;
+    // C = beta * C through a K = 0 GEMM with zero-filled operands.
+    K = 0;
+  }
+  bool ak = (transA == 'T' || transA == 't');
+  bool bk = !(transB == 'T' || transB == 't');
+  auto al16 = [](const void* p) { return ((uintptr_t)p & 15) == 0; };
+  int vec = (al16(A) && al16(B) && (lda % 2 == 0) && (ldb % 2 == 0)) ? 2 : 1;
+  if (ak && bk) return launch<true, true>(ctx, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, vec);
+  if (ak && !bk) return launch<true, false>(ctx, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, vec);
+  if (!ak && bk) return launch<false, true>(ctx, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, vec);
+  return launch<false, false>(ctx, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, vec);
+}
+
+}  // namespace imcom

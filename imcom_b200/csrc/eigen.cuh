@@ -1,0 +1,34 @@
+// eigen.cuh -- shared state of the eigensolvers.
+#pragma once
+
+#include "common.cuh"
+
+namespace imcom {
+
+struct EigWork {
+  DMat W;   // ascending eigenvectors (solver output)
+  DMat Z;   // scratch matrices
+  DMat V;
+  double* w = nullptr;  // ascending eigenvalues
+  size_t w_cap = 0;
+  void* buf = nullptr;  // general scratch
+  size_t buf_bytes = 0;
+  void* solver = nullptr;  // cuSOLVER handle (comparison baseline only)
+};
+
+EigWork* eig_work(imcom_ctx* ctx);
+int eig_buf(imcom_ctx* ctx, size_t bytes);
+int copy_mat(imcom_ctx* ctx, const double* A, long long lda, double* B, long long ldb, int rows,
+             int cols);
+
+// Keep-if-large-enough vector allocation.
+template <class T>
+inline int ensure_vec_keep(imcom_ctx* ctx, T** p, size_t& cap, size_t count) {
+  size_t bytes = count * sizeof(T);
+  void* v = *p;
+  int s = ensure_buf(ctx, &v, cap, bytes);
+  *p = (T*)v;
+  return s;
+}
+
+}  // namespace imcom

@@ -1,0 +1,299 @@
+// solve.cu -- P = Q^T B, per-pixel kappa bisection, T and the output maps.
+//
+//   imcom_gpu_build_P      imcom_build_P       imcom_matrix.f90:682-712
+//   bisect_kernel          imcom_bisect_kappa  imcom_bisect.f90:78-170
+//                          imcom_bisect_by_U   imcom_bisect.f90:174-222
+//                          imcom_bisect_by_S   imcom_bisect.f90:226-267
+//   imcom_gpu_build_T      imcom_build_T       imcom_matrix.f90:716-750
+//   image_s_kernel         imcom_build_image   imcom_matrix.f90:754-790
+//                          imcom_build_S       imcom_matrix.f90:839-877
+//   eval_kernel            imcom_build_U       imcom_matrix.f90:795-835
+//
+// The bisection runs one warp per output pixel; the eigenvalues and the
+// pixel's P column are staged in shared memory and every U/S evaluation is a
+// warp-wide sum (usum.cuh).  Its epilogue also writes the T operand
+// P~(:, a) = P(:, a) / (L + K_a) (the DGEMV argument of imcom_matrix.f90:734),
+// so T = -1/2 Q P~ is a single FP64 GEMM.
+#include <cmath>
+
+#include "common.cuh"
+#include "solve.cuh"
+#include "usum.cuh"
+
+namespace imcom {
+
+namespace {
+
+__global__ void bisect_kernel(BisectArgs a, PixelSmem plan) {
+  extern __shared__ __align__(16) double smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const double* lam = a.L;
+  if (plan.lam_smem) {
+    for (int p = threadIdx.x; p < a.n; p += blockDim.x) smem[p] = a.L[p];
+    __syncthreads();
+    lam = smem;
+  }
+  double* mycol = plan.col_smem ? smem + (size_t)a.n * (1 + warp) : nullptr;
+  for (int pix = blockIdx.x * plan.warps + warp; pix < a.m; pix += gridDim.x * plan.warps) {
+    const double* col = a.P + (size_t)pix * a.ldp;
+    if (mycol) {
+      for (int p = lane; p < a.n; p += 32) mycol[p] = col[p];
+      __syncwarp();
+      col = mycol;
+    }
+    int nev;
+    double k, us;
+    bisect_pixel(a, lam, col, lane, &nev, &k, &us);
+    write_pixel(a, lam, col, pix, lane, nev, k, us);
+    __syncwarp();
+  }
+}
+
+// U_a or S_a at the given K_a (one evaluation per pixel).
+__global__ void eval_kernel(BisectArgs a, PixelSmem plan, double* __restrict__ out) {
+  extern __shared__ __align__(16) double smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const double* lam = a.L;
+  if (plan.lam_smem) {
+    for (int p = threadIdx.x; p < a.n; p += blockDim.x) smem[p] = a.L[p];
+    __syncthreads();
+    lam = smem;
+  }
+  for (int pix = blockIdx.x * plan.warps + warp; pix < a.m; pix += gridDim.x * plan.warps) {
+    const double* col = a.P + (size_t)pix * a.ldp;
+    double v = warp_us(a.UnotS != 0, lam, col, a.Nd, a.n, a.K[pix], a.C, lane);
+    if (lane == 0) out[pix] = v;
+  }
+}
+
+// H_a = sum_i T_ia I_i and S_a = sum_i T_ia (T_ia Ndiag_i), one warp per a.
+__global__ void image_s_kernel(const double* __restrict__ T, long long ldt,
+                               const double* __restrict__ I, const double* __restrict__ Nd,
+                               int n, int m, double* __restrict__ H, double* __restrict__ S) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  for (int a = blockIdx.x * wpb + warp; a < m; a += gridDim.x * wpb) {
+    const double* col = T + (size_t)a * ldt;
+    double h = 0.0, s = 0.0;
+    for (int i = lane; i < n; i += 32) {
+      double t = col[i];
+      if (H) h += t * I[i];
+      if (S) s = __dadd_rn(s, __dmul_rn(t, __dmul_rn(t, Nd[i])));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      h += __shfl_xor_sync(0xffffffffu, h, o);
+      s += __shfl_xor_sync(0xffffffffu, s, o);
+    }
+    if (lane == 0) {
+      if (H) H[a] = h;
+      if (S) S[a] = s;
+    }
+  }
+}
+
+}  // namespace
+
+int fill_bisect_args(imcom_ctx* ctx, BisectArgs& a, int UnotS, double US_max, double k_min,
+                     double k_max, double tol, int maxnits, double C_a) {
+  if (!ctx->have_P) return set_err(ctx, IMCOM_ERR_STATE, "P has not been built or loaded");
+  if (!ctx->have_QL) return set_err(ctx, IMCOM_ERR_STATE, "L has not been built or loaded");
+  if (!UnotS && !ctx->have_N)
+    return set_err(ctx, IMCOM_ERR_STATE, "S-mode bisection needs Ndiag (imcom_gpu_set_inputs)");
+  if (!(k_min > 0.0)) return -4;
+  if (!(k_max > 0.0)) return -5;
+  if (maxnits < 0) return -7;
+  if (!(C_a > 0.0) || !std::isfinite(C_a)) return -8;
+  a.L = ctx->L;
+  a.P = ctx->P.p;
+  a.ldp = ctx->P.ld;
+  a.Nd = ctx->Nd;
+  a.Pt = ctx->Pt.p;
+  a.ldt = ctx->Pt.ld;
+  a.K = ctx->K;
+  a.US = ctx->US;
+  a.nev = ctx->nev;
+  a.n = ctx->n;
+  a.m = ctx->m;
+  a.UnotS = UnotS ? 1 : 0;
+  a.US_max = US_max;
+  a.k_min = k_min;
+  a.k_max = k_max;
+  a.tol = tol;
+  a.C = C_a;
+  a.eps = 1.1102230246251565e-16;  // DLAMCH('Espilon') (imcom_bisect.f90:187)
+  a.lg_min = std::log10(k_min);
+  a.lg_max = std::log10(k_max);
+  a.maxnits = maxnits;
+  return 0;
+}
+
+int pixel_grid(imcom_ctx* ctx, const PixelSmem& plan, int m) {
+  int blocks = (m + plan.warps - 1) / plan.warps;
+  return blocks;
+}
+
+int copy_pixel_outputs(imcom_ctx* ctx, double* K_out, double* US_out, int* nev_out) {
+  int m = ctx->m;
+  if (K_out)
+    IMC_CUDA(cudaMemcpyAsync(K_out, ctx->K, m * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  if (US_out)
+    IMC_CUDA(cudaMemcpyAsync(US_out, ctx->US, m * sizeof(double), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+  if (nev_out)
+    IMC_CUDA(cudaMemcpyAsync(nev_out, ctx->nev, m * sizeof(int), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+  if (K_out || US_out || nev_out) IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+}  // namespace imcom
+
+using namespace imcom;
+
+extern "C" int imcom_gpu_build_P(imcom_ctx* ctx, double* P_out) {
+  if (!ctx) return -1;
+  if (!ctx->have_QL) return set_err(ctx, IMCOM_ERR_STATE, "Q has not been built or loaded");
+  if (!ctx->have_B) return set_err(ctx, IMCOM_ERR_STATE, "B has not been built or loaded");
+  cudaSetDevice(ctx->device);
+  stage_begin(ctx, ST_P);
+  IMC_TRY(ensure_mat(ctx, ctx->P, ctx->n, ctx->m));
+  // P = Q^T B (DGEMM 'T', 'N', n, m, n)
+  IMC_TRY(dgemm(ctx, 'T', 'N', ctx->n, ctx->m, ctx->n, 1.0, ctx->Q.p, ctx->Q.ld, ctx->B.p,
+                ctx->B.ld, 0.0, ctx->P.p, ctx->P.ld));
+  stage_end(ctx, ST_P);
+  ctx->have_P = true;
+  ctx->have_K = ctx->have_T = ctx->have_Pt = false;
+  if (P_out) {
+    IMC_TRY(download_mat(ctx, ctx->P, P_out));
+    IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  }
+  return 0;
+}
+
+extern "C" int imcom_gpu_bisect_kappa(imcom_ctx* ctx, int UnotS, double US_max, double k_min,
+                                      double k_max, double tol, int maxnits, double C_a,
+                                      double* K_out, double* US_out, int* nevals_out) {
+  if (!ctx) return -1;
+  BisectArgs a;
+  IMC_TRY(fill_bisect_args(ctx, a, UnotS, US_max, k_min, k_max, tol, maxnits, C_a));
+  cudaSetDevice(ctx->device);
+  stage_begin(ctx, ST_BISECT);
+  IMC_TRY(ensure_mat(ctx, ctx->Pt, ctx->n, ctx->m));
+  a.Pt = ctx->Pt.p;
+  a.ldt = ctx->Pt.ld;
+  PixelSmem plan = plan_pixel_smem(ctx->n);
+  IMC_CUDA(cudaFuncSetAttribute(bisect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)plan.bytes));
+  bisect_kernel<<<pixel_grid(ctx, plan, ctx->m), plan.warps * 32, plan.bytes, ctx->stream>>>(a, plan);
+  IMC_LAUNCH();
+  stage_end(ctx, ST_BISECT);
+  ctx->have_K = true;
+  ctx->have_Pt = true;
+  ctx->have_T = false;
+  return copy_pixel_outputs(ctx, K_out, US_out, nevals_out);
+}
+
+extern "C" int imcom_gpu_build_T(imcom_ctx* ctx, double* T_out) {
+  if (!ctx) return -1;
+  if (!ctx->have_K) return set_err(ctx, IMCOM_ERR_STATE, "kappa has not been solved or loaded");
+  if (!ctx->have_QL || !ctx->have_P)
+    return set_err(ctx, IMCOM_ERR_STATE, "Q, L and P are needed for T");
+  cudaSetDevice(ctx->device);
+  stage_begin(ctx, ST_T);
+  if (!ctx->have_Pt) {
+    IMC_TRY(make_Pt(ctx));
+    ctx->have_Pt = true;
+  }
+  IMC_TRY(ensure_mat(ctx, ctx->T, ctx->n, ctx->m));
+  // T = -1/2 Q P~ with P~(:, a) = P(:, a) / (L + K_a) written by the bisection.
+  IMC_TRY(dgemm(ctx, 'N', 'N', ctx->n, ctx->m, ctx->n, -0.5, ctx->Q.p, ctx->Q.ld, ctx->Pt.p,
+                ctx->Pt.ld, 0.0, ctx->T.p, ctx->T.ld));
+  stage_end(ctx, ST_T);
+  ctx->have_T = true;
+  if (T_out) {
+    IMC_TRY(download_mat(ctx, ctx->T, T_out));
+    IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  }
+  return 0;
+}
+
+// P~ from a loaded K (used when kappa came from imcom_gpu_load_K).
+namespace imcom {
+namespace {
+__global__ void scale_cols_kernel(const double* __restrict__ P, long long ldp,
+                                  const double* __restrict__ L, const double* __restrict__ K,
+                                  double* __restrict__ Pt, long long ldt, int n, int m) {
+  int a = blockIdx.y;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
+    Pt[p + (size_t)a * ldt] = __ddiv_rn(P[p + (size_t)a * ldp], __dadd_rn(L[p], K[a]));
+}
+}  // namespace
+
+int make_Pt(imcom_ctx* ctx) {
+  IMC_TRY(ensure_mat(ctx, ctx->Pt, ctx->n, ctx->m));
+  dim3 grd((ctx->n + 255) / 256, ctx->m);
+  scale_cols_kernel<<<grd, 256, 0, ctx->stream>>>(ctx->P.p, ctx->P.ld, ctx->L, ctx->K, ctx->Pt.p,
+                                                  ctx->Pt.ld, ctx->n, ctx->m);
+  IMC_LAUNCH();
+  return 0;
+}
+}  // namespace imcom
+
+extern "C" int imcom_gpu_build_image(imcom_ctx* ctx, double* H_out) {
+  if (!ctx) return -1;
+  if (!ctx->have_T) return set_err(ctx, IMCOM_ERR_STATE, "T has not been built or loaded");
+  if (!ctx->have_I) return set_err(ctx, IMCOM_ERR_STATE, "I_i was not given to set_inputs");
+  cudaSetDevice(ctx->device);
+  stage_begin(ctx, ST_EPI);
+  int blocks = (ctx->m + 7) / 8;
+  image_s_kernel<<<blocks, 256, 0, ctx->stream>>>(ctx->T.p, ctx->T.ld, ctx->I, ctx->Nd, ctx->n,
+                                                  ctx->m, ctx->H, nullptr);
+  IMC_LAUNCH();
+  stage_end(ctx, ST_EPI);
+  if (H_out) {
+    IMC_CUDA(cudaMemcpyAsync(H_out, ctx->H, ctx->m * sizeof(double), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  }
+  return 0;
+}
+
+extern "C" int imcom_gpu_build_S(imcom_ctx* ctx, double* S_out) {
+  if (!ctx) return -1;
+  if (!ctx->have_T) return set_err(ctx, IMCOM_ERR_STATE, "T has not been built or loaded");
+  if (!ctx->have_N) return set_err(ctx, IMCOM_ERR_STATE, "Ndiag was not given to set_inputs");
+  cudaSetDevice(ctx->device);
+  int blocks = (ctx->m + 7) / 8;
+  image_s_kernel<<<blocks, 256, 0, ctx->stream>>>(ctx->T.p, ctx->T.ld, ctx->I, ctx->Nd, ctx->n,
+                                                  ctx->m, nullptr, ctx->S);
+  IMC_LAUNCH();
+  if (S_out) {
+    IMC_CUDA(cudaMemcpyAsync(S_out, ctx->S, ctx->m * sizeof(double), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  }
+  return 0;
+}
+
+extern "C" int imcom_gpu_build_U(imcom_ctx* ctx, double C_a, double* U_out) {
+  if (!ctx) return -1;
+  if (!ctx->have_K) return set_err(ctx, IMCOM_ERR_STATE, "kappa has not been solved or loaded");
+  BisectArgs a;
+  IMC_TRY(fill_bisect_args(ctx, a, 1, 0.0, 1.0, 1.0, 0.0, 0, C_a));
+  cudaSetDevice(ctx->device);
+  PixelSmem plan = plan_pixel_smem(ctx->n);
+  plan.col_smem = false;
+  plan.bytes = plan.lam_smem ? (size_t)ctx->n * sizeof(double) : 0;
+  IMC_CUDA(cudaFuncSetAttribute(eval_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)plan.bytes));
+  eval_kernel<<<pixel_grid(ctx, plan, ctx->m), plan.warps * 32, plan.bytes, ctx->stream>>>(
+      a, plan, ctx->U);
+  IMC_LAUNCH();
+  if (U_out) {
+    IMC_CUDA(cudaMemcpyAsync(U_out, ctx->U, ctx->m * sizeof(double), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  }
+  return 0;
+}

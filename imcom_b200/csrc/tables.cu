@@ -1,0 +1,380 @@
+// tables.cu -- PSF rotation, PSF spectra and the FFT-built lookup tables.
+//
+// Compiled with --fmad=false: every expression here rounds as written, like
+// the reference's gfortran build, so rotation indices and table values follow
+// imcom_proc.f90 / imcom_matrix.f90 operation by operation.  The FFTs are
+// cuFFT (the reference calls FFTW for the same transforms).
+//
+//   rotate_psf_kernel     imcom_rotate_image   imcom_proc.f90:184-250
+//   hermitian_fill_kernel imcom_ft_r2c         imcom_proc.f90:433-475
+//   csum_kernel           imcom_calc_C         imcom_matrix.f90:546-552
+//   embed_kernel          imcom_build_Alookup  imcom_matrix.f90:395-411
+//                         imcom_build_Blookup  imcom_matrix.f90:468-476
+//   shift_scale_kernel    (same, :412-413, :427-429 / :477-478, :490-492)
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+
+namespace imcom {
+namespace {
+
+// Neville on at most 16 points: imcom_polint (imcom_proc.f90:351-394),
+// step for step.  Returns nonzero on the duplicate-abscissa trap.
+__device__ int polint_dev(const double* xa, const double* ya, int n, double x,
+                          double* y, double eps) {
+  double c[16], d[16], den[16], ho[16];
+  for (int i = 0; i < n; ++i) {
+    c[i] = ya[i];
+    d[i] = ya[i];
+    ho[i] = xa[i] - x;
+  }
+  int ns = 1;
+  double best = fabs(x - xa[0]);
+  for (int i = 1; i < n; ++i) {
+    double v = fabs(x - xa[i]);
+    if (v < best) {
+      best = v;
+      ns = i + 1;
+    }
+  }
+  double yy = ya[ns - 1], dy;
+  ns = ns - 1;
+  for (int m = 1; m <= n - 1; ++m) {
+    for (int i = 1; i <= n - m; ++i) den[i - 1] = ho[i - 1] - ho[i + m - 1];
+    for (int i = 1; i <= n - m; ++i)
+      if (fabs(den[i - 1]) <= eps) return 1;
+    for (int i = 1; i <= n - m; ++i) den[i - 1] = (c[i] - d[i - 1]) / den[i - 1];
+    for (int i = 1; i <= n - m; ++i) {
+      d[i - 1] = ho[i + m - 1] * den[i - 1];
+      c[i - 1] = ho[i - 1] * den[i - 1];
+    }
+    if (2 * ns < n - m) {
+      dy = c[ns];
+    } else {
+      dy = d[ns - 1];
+      ns = ns - 1;
+    }
+    yy = yy + dy;
+  }
+  *y = yy;
+  return 0;
+}
+
+// One output pixel of imcom_rotate_image per thread.  cost/sint come from
+// the host (same libm as the reference's runtime), so the source coordinate
+// and its floor/ceiling are bit-identical.
+__global__ void rotate_psf_kernel(const double* __restrict__ in, double* __restrict__ out,
+                                  int nim, int npm, double cost, double sint,
+                                  double eps, int* flags) {
+  int iout = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  int jout = blockIdx.y + 1;
+  if (iout > nim) return;
+  double x_cent = (double)(nim + 1) / 2.0, y_cent = x_cent;
+  double xout = (double)iout - x_cent;
+  double yout = (double)jout - y_cent;
+  double xs = xout * cost + yout * sint + x_cent;
+  double ys = -xout * sint + yout * cost + y_cent;
+  int is_floor = (int)floor(xs), js_floor = (int)floor(ys);
+  int is_ceil = (int)ceil(xs), js_ceil = (int)ceil(ys);
+  double f = 0.0;
+  if (is_floor >= 1 && js_floor >= 1 && is_ceil <= nim && js_ceil <= nim) {
+    int imin = max(1, is_floor - npm), jmin = max(1, js_floor - npm);
+    int imax = min(nim, is_ceil + npm), jmax = min(nim, js_ceil + npm);
+    int m1 = imax - imin + 1, m2 = jmax - jmin + 1;
+    double x1a[16], x2a[16], ymtmp[16], yntmp[16];
+    for (int ii = 0; ii < m1; ++ii) x1a[ii] = (double)(imin + ii);
+    for (int jj = 0; jj < m2; ++jj) x2a[jj] = (double)(jmin + jj);
+    int bad = 0;
+    for (int j = 0; j < m1; ++j) {
+      for (int k = 0; k < m2; ++k)
+        yntmp[k] = in[(size_t)(imin - 1 + j) + (size_t)(jmin - 1 + k) * nim];
+      bad |= polint_dev(x2a, yntmp, m2, ys, &ymtmp[j], eps);
+    }
+    bad |= polint_dev(x1a, ymtmp, m1, xs, &f, eps);
+    if (bad) atomicOr(flags, 1);
+  }
+  out[(size_t)(iout - 1) + (size_t)(jout - 1) * nim] = f;
+}
+
+// Block sums of a real array (tree order); the host finishes the sum.
+__global__ void partial_sum_kernel(const double* __restrict__ a, size_t count,
+                                   double* __restrict__ partial) {
+  __shared__ double sh[256];
+  double s = 0.0;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < count;
+       k += (size_t)gridDim.x * blockDim.x)
+    s += a[k];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
+}
+
+__global__ void finish_sum_kernel(const double* __restrict__ partial, int np, double* out) {
+  __shared__ double sh[256];
+  double s = 0.0;
+  for (int k = threadIdx.x; k < np; k += blockDim.x) s += partial[k];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sh[0];
+}
+
+// im_out = sum(im_in) * im_out / sum(im_out)  (imcom_proc.f90:249)
+__global__ void flux_scale_kernel(double* __restrict__ out, size_t count,
+                                  const double* __restrict__ sums) {
+  double sin_ = sums[0], sout = sums[1];
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < count;
+       k += (size_t)gridDim.x * blockDim.x)
+    out[k] = sin_ * out[k] / sout;
+}
+
+// Full spectrum from the r2c half spectrum with the reference's fill:
+// Ft(k, j) = half(k, j) for k <= n1/2, else conj(half(n1 - k, (n2 - j) mod n2)).
+// half is [b][j][0..n1/2], full is [b][j][0..n1-1] (x fastest).
+__global__ void hermitian_fill_kernel(const double2* __restrict__ half, double2* __restrict__ full,
+                                      int n1, int n2) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y;
+  int b = blockIdx.z;
+  if (k >= n1) return;
+  int nh = n1 / 2 + 1;
+  const double2* hb = half + (size_t)b * nh * n2;
+  double2 v;
+  if (k <= n1 / 2) {
+    v = hb[(size_t)j * nh + k];
+  } else {
+    double2 s = hb[(size_t)((n2 - j) % n2) * nh + (n1 - k)];
+    v = make_double2(s.x, -s.y);
+  }
+  full[(size_t)b * n1 * n2 + (size_t)j * n1 + k] = v;
+}
+
+// Partial sums of |z|^2 computed as a*a - b*(-b) (Re(z conj(z))).
+__global__ void abs2_partial_kernel(const double2* __restrict__ z, size_t count,
+                                    double* __restrict__ partial) {
+  __shared__ double sh[256];
+  double s = 0.0;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < count;
+       k += (size_t)gridDim.x * blockDim.x) {
+    double2 v = z[k];
+    s += v.x * v.x - v.y * (-v.y);
+  }
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
+}
+
+// Fortran CSHIFT source index (1-based): cshift(X, s)(i) = X(1 + mod(i-1+s, n)).
+__device__ __forceinline__ int cshift_src(int i1, int s, int n) {
+  return 1 + ((i1 - 1 + s) % n + n) % n;
+}
+
+// Embedding of conj(Gt_e) * Gt_f (A) or conj(Gammat) * Gt_e (B) into the
+// npad-times larger frequency grid, with both cshifts of the reference
+// composed into one gather.  Output grid [t][q][p], p fastest.
+__global__ void embed_kernel(const double2* __restrict__ Gt, const double2* __restrict__ Gammat,
+                             const int2* __restrict__ pairs, double2* __restrict__ grid,
+                             int nps, int nbig) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x + 1;  // 1-based
+  int q = blockIdx.y + 1;
+  int t = blockIdx.z;
+  if (p > nbig) return;
+  int nmin = (nbig - nps) / 2 + 1, nmax = (nbig + nps) / 2;
+  int sp = cshift_src(p, nbig / 2, nbig), sq = cshift_src(q, nbig / 2, nbig);
+  double2 v = make_double2(0.0, 0.0);
+  if (sp >= nmin && sp <= nmax && sq >= nmin && sq <= nmax) {
+    int si = cshift_src(sp - nmin + 1, nps / 2, nps);
+    int sj = cshift_src(sq - nmin + 1, nps / 2, nps);
+    size_t s = (size_t)(si - 1) + (size_t)(sj - 1) * nps;
+    int2 pr = pairs[t];
+    double2 a, b;
+    if (pr.y > 0) {  // A: conj(Gt_e) * Gt_f
+      a = Gt[s + (size_t)(pr.x - 1) * nps * nps];
+      b = Gt[s + (size_t)(pr.y - 1) * nps * nps];
+    } else {  // B: conj(Gammat) * Gt_e
+      a = Gammat[s];
+      b = Gt[s + (size_t)(pr.x - 1) * nps * nps];
+    }
+    double ar = a.x, ai = -a.y;  // conj(a)
+    double xr = ar * b.x - ai * b.y;
+    double xi = ar * b.y + ai * b.x;
+    // times imcom_upsilon2D(ux, uy, 1) = (1, 0)
+    v = make_double2(xr * 1.0 - xi * 0.0, xr * 0.0 + xi * 1.0);
+  }
+  grid[(size_t)t * nbig * nbig + (size_t)(q - 1) * nbig + (p - 1)] = v;
+}
+
+// table(p, q) = Re(tmp(cshift(p), cshift(q))) / nps / nps   (A)
+//             = (-2 * Re(...)) / nps / nps                   (B)
+__global__ void shift_scale_kernel(const double2* __restrict__ grid, double* __restrict__ tab,
+                                   int nbig, int nps, int isB) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  int q = blockIdx.y + 1;
+  int t = blockIdx.z;
+  if (p > nbig) return;
+  int sp = cshift_src(p, nbig / 2, nbig), sq = cshift_src(q, nbig / 2, nbig);
+  double v = grid[(size_t)t * nbig * nbig + (size_t)(sq - 1) * nbig + (sp - 1)].x;
+  if (isB) v = -2.0 * v;
+  tab[(size_t)t * nbig * nbig + (size_t)(q - 1) * nbig + (p - 1)] = v / (double)nps / (double)nps;
+}
+
+int sum_device(imcom_ctx* ctx, const double* a, size_t count, double* dst, double* scratch) {
+  partial_sum_kernel<<<256, 256, 0, ctx->stream>>>(a, count, scratch);
+  IMC_LAUNCH();
+  finish_sum_kernel<<<1, 256, 0, ctx->stream>>>(scratch, 256, dst);
+  IMC_LAUNCH();
+  return 0;
+}
+
+}  // namespace
+
+// Build the lookup tables for A (isB = 0: all pairs e <= f, packed index
+// ial = e + f(f-1)/2) or B (isB = 1: one per exposure) into ctx->tables.
+int build_tables(imcom_ctx* ctx, int npad, int isB) {
+  int nps = ctx->nps, E = ctx->nexppsf;
+  int nbig = nps * npad;
+  std::vector<int2> pairs;
+  if (!isB) {
+    pairs.resize(E * (E + 1) / 2);
+    for (int iexp = 1; iexp <= E; ++iexp)
+      for (int jexp = iexp; jexp <= E; ++jexp) pairs[iexp + jexp * (jexp - 1) / 2 - 1] = make_int2(iexp, jexp);
+  } else {
+    for (int iexp = 1; iexp <= E; ++iexp) pairs.push_back(make_int2(iexp, 0));
+  }
+  int ntab = (int)pairs.size();
+  size_t big2 = (size_t)nbig * nbig;
+  IMC_TRY(ensure_buf(ctx, (void**)&ctx->fftbuf, ctx->fftbuf_bytes,
+                     big2 * ntab * sizeof(double2) + 4096));
+  IMC_TRY(ensure_buf(ctx, (void**)&ctx->tables, ctx->tables_bytes, big2 * ntab * sizeof(double)));
+  int2* dpairs = reinterpret_cast<int2*>(reinterpret_cast<char*>(ctx->fftbuf) +
+                                         big2 * ntab * sizeof(double2));
+  IMC_CUDA(cudaMemcpyAsync(dpairs, pairs.data(), ntab * sizeof(int2), cudaMemcpyHostToDevice,
+                           ctx->stream));
+  if (!ctx->plan_big || ctx->plan_big_L != nbig || ctx->plan_big_batch != ntab) {
+    if (ctx->plan_big) cufftDestroy(ctx->plan_big);
+    ctx->plan_big = 0;
+    int dims[2] = {nbig, nbig};
+    IMC_CUFFT(cufftPlanMany(&ctx->plan_big, 2, dims, nullptr, 1, (int)big2, nullptr, 1,
+                            (int)big2, CUFFT_Z2Z, ntab));
+    ctx->plan_big_L = nbig;
+    ctx->plan_big_batch = ntab;
+  }
+  IMC_CUFFT(cufftSetStream(ctx->plan_big, ctx->stream));
+  dim3 blk(128), grd((nbig + 127) / 128, nbig, ntab);
+  embed_kernel<<<grd, blk, 0, ctx->stream>>>(ctx->Gt, ctx->Gammat, dpairs, ctx->fftbuf, nps, nbig);
+  IMC_LAUNCH();
+  IMC_CUFFT(cufftExecZ2Z(ctx->plan_big, (cufftDoubleComplex*)ctx->fftbuf,
+                         (cufftDoubleComplex*)ctx->fftbuf, CUFFT_INVERSE));
+  shift_scale_kernel<<<grd, blk, 0, ctx->stream>>>(ctx->fftbuf, ctx->tables, nbig, nps, isB);
+  IMC_LAUNCH();
+  return 0;
+}
+
+}  // namespace imcom
+
+using namespace imcom;
+
+extern "C" int imcom_gpu_psf_spectra(imcom_ctx* ctx, int npoly_in, double* C_out, double* Gt_out,
+                                     double* Gammat_out) {
+  if (!ctx) return -1;
+  if (!ctx->have_psf) return set_err(ctx, IMCOM_ERR_STATE, "imcom_gpu_set_psfs has not run");
+  cudaSetDevice(ctx->device);
+  int npoly = npoly_in;
+  if (npoly % 2 == 0) npoly = npoly - 1;  // imcom_proc.f90:201-205
+  if (npoly < 1 || npoly > 15) return set_err(ctx, -2, "npoly must be in 1..16");
+  int npm = npoly / 2;
+  int nps = ctx->nps, E = ctx->nexppsf;
+  size_t ps2 = (size_t)nps * nps;
+  int nh = nps / 2 + 1;
+  // scratch: real inputs (E+1) ps2 | half spectra (E+1) nh nps | sums
+  size_t real_b = (E + 1) * ps2 * sizeof(double);
+  size_t half_b = (size_t)(E + 1) * nh * nps * sizeof(double2);
+  size_t need = real_b + half_b + 8192;
+  stage_begin(ctx, ST_SPECTRA);
+  IMC_TRY(ensure_buf(ctx, (void**)&ctx->fftbuf, ctx->fftbuf_bytes, need));
+  double* rin = reinterpret_cast<double*>(ctx->fftbuf);
+  double2* half = reinterpret_cast<double2*>(reinterpret_cast<char*>(ctx->fftbuf) + real_b);
+  double* sums = reinterpret_cast<double*>(reinterpret_cast<char*>(ctx->fftbuf) + real_b + half_b);
+  double* scratch = sums + 16;
+  const double pi = 3.141592653589793;  // imcom_data.f90 parameter
+  const double eps = 1.1102230246251565e-16;  // DLAMCH('Epsilon')
+  IMC_CUDA(cudaMemsetAsync(ctx->flags, 0, sizeof(int), ctx->stream));
+  for (int e = 0; e < E; ++e) {
+    const double* src = ctx->G + (size_t)e * ps2;
+    double* dst = rin + (size_t)e * ps2;
+    double ang = ctx->rot[e];
+    if (fabs(ang) > 2.0 * pi * eps) {  // imcom.f90:102
+      double theta_rad = std::fmod(ang, 360.0) * pi / 180.0;
+      double cost = std::cos(theta_rad), sint = std::sin(theta_rad);
+      dim3 blk(128), grd((nps + 127) / 128, nps);
+      rotate_psf_kernel<<<grd, blk, 0, ctx->stream>>>(src, dst, nps, npm, cost, sint, eps,
+                                                       ctx->flags);
+      IMC_LAUNCH();
+      IMC_TRY(sum_device(ctx, src, ps2, sums + 0, scratch));
+      IMC_TRY(sum_device(ctx, dst, ps2, sums + 1, scratch + 256));
+      flux_scale_kernel<<<296, 256, 0, ctx->stream>>>(dst, ps2, sums);
+      IMC_LAUNCH();
+    } else {
+      IMC_CUDA(cudaMemcpyAsync(dst, src, ps2 * sizeof(double), cudaMemcpyDeviceToDevice,
+                               ctx->stream));
+    }
+  }
+  IMC_CUDA(cudaMemcpyAsync(rin + (size_t)E * ps2, ctx->Gamma, ps2 * sizeof(double),
+                           cudaMemcpyDeviceToDevice, ctx->stream));
+  if (!ctx->plan_r2c || ctx->plan_r2c_n != nps || ctx->plan_r2c_batch != E + 1) {
+    if (ctx->plan_r2c) cufftDestroy(ctx->plan_r2c);
+    ctx->plan_r2c = 0;
+    int dims[2] = {nps, nps};
+    IMC_CUFFT(cufftPlanMany(&ctx->plan_r2c, 2, dims, nullptr, 1, (int)ps2, nullptr, 1,
+                            nh * nps, CUFFT_D2Z, E + 1));
+    ctx->plan_r2c_n = nps;
+    ctx->plan_r2c_batch = E + 1;
+  }
+  IMC_CUFFT(cufftSetStream(ctx->plan_r2c, ctx->stream));
+  IMC_CUFFT(cufftExecD2Z(ctx->plan_r2c, rin, (cufftDoubleComplex*)half));
+  {
+    dim3 blk(128), grd((nps + 127) / 128, nps, E);
+    hermitian_fill_kernel<<<grd, blk, 0, ctx->stream>>>(half, ctx->Gt, nps, nps);
+    IMC_LAUNCH();
+    dim3 grd1((nps + 127) / 128, nps, 1);
+    hermitian_fill_kernel<<<grd1, blk, 0, ctx->stream>>>(half + (size_t)E * nh * nps,
+                                                         ctx->Gammat, nps, nps);
+    IMC_LAUNCH();
+  }
+  abs2_partial_kernel<<<256, 256, 0, ctx->stream>>>(ctx->Gammat, ps2, scratch);
+  IMC_LAUNCH();
+  finish_sum_kernel<<<1, 256, 0, ctx->stream>>>(scratch, 256, sums + 2);
+  IMC_LAUNCH();
+  double hs[3];
+  int flag = 0;
+  IMC_CUDA(cudaMemcpyAsync(hs, sums, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  IMC_CUDA(cudaMemcpyAsync(&flag, ctx->flags, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  if (Gt_out)
+    IMC_CUDA(cudaMemcpyAsync(Gt_out, ctx->Gt, ps2 * E * sizeof(double2), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+  if (Gammat_out)
+    IMC_CUDA(cudaMemcpyAsync(Gammat_out, ctx->Gammat, ps2 * sizeof(double2),
+                             cudaMemcpyDeviceToHost, ctx->stream));
+  stage_end(ctx, ST_SPECTRA);
+  IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (flag)
+    return set_err(ctx, IMCOM_ERR_NEVILLE,
+                   "IMCOM ERROR: Two or more identical x input locations to IMCOM_POLINT");
+  // C_a = sum(real(Gammat * conj(Gammat))) / n1psf / n2psf
+  ctx->C_a = hs[2] / (double)nps / (double)nps;
+  if (C_out) *C_out = ctx->C_a;
+  ctx->have_spectra = true;
+  return 0;
+}

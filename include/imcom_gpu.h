@@ -1,0 +1,201 @@
+/*
+ * imcom_gpu.h -- C-ABI of the B200 (sm_100a) IMCOM solve path.
+ *
+ * Drop-in boundary for the solve path of IMCOM (barnabytprowe/imcom,
+ * Fortran 95).  The Fortran driver (imcom.f90) and I/O module (imcom_io.f90)
+ * keep reading configs and FITS files; their "build" branches call these
+ * functions through ISO_C_BINDING instead of the Fortran routines named on
+ * each declaration.  The Fortran module state (imcom_data.f90:24-135) becomes
+ * device buffers owned by an opaque context.
+ *
+ * Conventions
+ *  - Every array is a plain host pointer to Fortran-ordered (column-major)
+ *    storage with leading dimension = number of rows, exactly as the Fortran
+ *    side allocates it.  double = real(KIND=8), int = default integer,
+ *    complex arrays are interleaved (re, im) pairs = complex(KIND=8).
+ *  - Indices passed in (exp_i) are 1-based, as in the reference.
+ *  - Output pointers may be NULL: the result then stays on the device only
+ *    (the reference's "None" filename / save=0 case) and the call returns
+ *    without waiting for the GPU.  A call with a non-NULL host output waits
+ *    for the GPU before it returns.
+ *  - Return value: 0 on success; < 0 an invalid argument (-k = argument k,
+ *    the LAPACK convention); > 0 a device, library or convergence error.
+ *    imcom_gpu_last_error() gives the message.  Errors reached by the
+ *    reference's `write + stop` paths come back as status codes so the
+ *    Fortran shim can print "IMCOM ERROR: ..." and stop.
+ *  - One context per host thread; calls on one context are serialised on its
+ *    CUDA stream.
+ */
+#ifndef IMCOM_GPU_H
+#define IMCOM_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct imcom_ctx imcom_ctx;
+
+/* Status codes (> 0). */
+#define IMCOM_ERR_CUDA 1        /* CUDA runtime / kernel launch error        */
+#define IMCOM_ERR_LIBRARY 2     /* cuFFT error                                */
+#define IMCOM_ERR_STATE 3       /* a prerequisite stage has not run           */
+#define IMCOM_ERR_NEVILLE 4     /* imcom_polint duplicate-abscissa trap       */
+#define IMCOM_ERR_EIGEN 5       /* eigensolver did not converge (DSYEVR info) */
+#define IMCOM_ERR_ALLOC 6       /* device allocation failed                   */
+#define IMCOM_ERR_NOT_FINITE 7  /* non-finite input                           */
+
+/* Eigensolver selection for imcom_gpu_set_option(IMCOM_OPT_EIGENSOLVER). */
+#define IMCOM_EIGH_DC 0         /* own tridiagonalisation + divide & conquer  */
+#define IMCOM_EIGH_JACOBI 1     /* own one-sided Jacobi (small n)             */
+#define IMCOM_EIGH_LIBRARY 2    /* cuSOLVER syevd: comparison baseline only   */
+
+/* Options for imcom_gpu_set_option. */
+#define IMCOM_OPT_EIGENSOLVER 1
+#define IMCOM_OPT_EIGEN_MAXITER 2 /* iteration cap of the iterative solvers  */
+
+/* ---- context ---------------------------------------------------------- */
+
+/* Create a context on CUDA device `device`.  No reference counterpart (the
+ * reference keeps module globals, imcom_data.f90:18-216). */
+int imcom_gpu_create(int device, imcom_ctx** ctx);
+int imcom_gpu_destroy(imcom_ctx* ctx);
+/* Last error message of this context ("" if none). */
+const char* imcom_gpu_last_error(const imcom_ctx* ctx);
+/* Wait for all queued work; returns the first asynchronous error. */
+int imcom_gpu_synchronize(imcom_ctx* ctx);
+int imcom_gpu_set_option(imcom_ctx* ctx, int option, long long value);
+
+/* ---- inputs (module state) -------------------------------------------- */
+
+/* Input and output geometry, image and noise vectors: the arrays built by
+ * imcom_alloc_gims / imcom_build_xy / imcom_alloc_xy / imcom_build_XaYa /
+ * imcom_build_Ndiag (imcom_io.f90:36-240, imcom_proc.f90:56-119,
+ * imcom_matrix.f90:556-582).  x_i, y_i, I_i, Ndiag, exp_i: length n;
+ * X_a, Y_a: length m.  I_i and Ndiag may be NULL (then H, S and S-mode
+ * bisection are unavailable until set). */
+int imcom_gpu_set_inputs(imcom_ctx* ctx, int n, int m, const double* x_i,
+                         const double* y_i, const int* exp_i,
+                         const double* X_a, const double* Y_a,
+                         const double* I_i, const double* Ndiag,
+                         double psfxscale, double psfyscale);
+
+/* PSFs as padded and normalised by imcom_alloc_psfs (imcom_io.f90:244-335):
+ * G_unrot (nps, nps, nexppsf), Gamma (nps, nps), rotangdeg (nexppsf).
+ * psfconst is the value of imcom_test_psfconst (imcom_proc.f90:582-599). */
+int imcom_gpu_set_psfs(imcom_ctx* ctx, int nps, int nexppsf, int psfconst,
+                       const double* G_unrot, const double* rotangdeg,
+                       const double* Gamma);
+
+/* ---- solve path ------------------------------------------------------- */
+
+/* Rotate each PSF (imcom_rotate_image, imcom_proc.f90:184-250, when
+ * |angle| > 2 pi eps), Fourier transform it and Gamma with the reference's
+ * Hermitian fill (imcom_ft_r2c, imcom_proc.f90:433-475; call site
+ * imcom.f90:90-116), and compute C (imcom_calc_C, imcom_matrix.f90:546-552).
+ * Gt_out (nps, nps, nexppsf) and Gammat_out (nps, nps) are complex and may
+ * be NULL. */
+int imcom_gpu_psf_spectra(imcom_ctx* ctx, int npoly, double* C_out,
+                          double* Gt_out, double* Gammat_out);
+
+/* Lookup tables for A (imcom_build_Alookup, imcom_matrix.f90:361-430) and
+ * A assembly by 7th-order interpolation (imcom_lookup_A, :206-284).  This is
+ * the build branch of imcom_get_A (:41-73).  A_out (n, n) may be NULL. */
+int imcom_gpu_build_A(imcom_ctx* ctx, int npoly, int npad, double* A_out);
+/* Cache-read branch of imcom_get_A (:49-68): A read from FITS by the caller. */
+int imcom_gpu_load_A(imcom_ctx* ctx, const double* A);
+
+/* Eigendecomposition of A in FP64, eigenvalues descending (imcom_eigen_A,
+ * imcom_matrix.f90:586-678; build branch of imcom_get_QL, :155-202).
+ * Q_out (n, n), L_out (n) may be NULL; cond_out receives max(L)/min(L). */
+int imcom_gpu_eigen_A(imcom_ctx* ctx, double* Q_out, double* L_out,
+                      double* cond_out);
+/* Cache-read branch of imcom_get_QL (:164-198). */
+int imcom_gpu_load_QL(imcom_ctx* ctx, const double* Q, const double* L);
+
+/* Lookup tables for B (imcom_build_Blookup, :434-493) and B assembly
+ * (imcom_lookup_B, :288-357): build branch of imcom_get_B (:77-109). */
+int imcom_gpu_build_B(imcom_ctx* ctx, int npoly, int npad, double* B_out);
+int imcom_gpu_load_B(imcom_ctx* ctx, const double* B);
+
+/* P = Q^T B in FP64 (imcom_build_P, :682-712; build branch of imcom_get_P,
+ * :113-151).  P2 = P*P is formed where it is used, bit-identical. */
+int imcom_gpu_build_P(imcom_ctx* ctx, double* P_out);
+int imcom_gpu_load_P(imcom_ctx* ctx, const double* P);
+
+/* Release A and B (imcom.f90:159). */
+int imcom_gpu_free_AB(imcom_ctx* ctx);
+
+/* Per-pixel kappa bisection (imcom_bisect_kappa, imcom_bisect.f90:78-170,
+ * with imcom_bisect_by_U :174-222 / imcom_bisect_by_S :226-267 and
+ * imcom_U_from_kappa / imcom_S_from_kappa, imcom_matrix.f90:904-970).
+ * UnotS != 0 solves U_a < US_max, else S_a < US_max.  K_out, US_out (m)
+ * and nevals_out (m; evaluations per pixel) may be NULL. */
+int imcom_gpu_bisect_kappa(imcom_ctx* ctx, int UnotS, double US_max,
+                           double k_min, double k_max, double tol,
+                           int maxnits, double C_a, double* K_out,
+                           double* US_out, int* nevals_out);
+
+/* Same contract and bit-identical K as imcom_gpu_bisect_kappa, with the
+ * learned-kappa bracket: an MLP (imcom_gpu_mlp_set_weights) predicts
+ * log10(kappa) and a bracket half-width per pixel; the bracket is verified
+ * with two evaluations and the bisection steps it decides are skipped.
+ * Pixels whose bracket fails run the plain bisection.  No reference
+ * counterpart; replaces imcom_bisect_kappa (imcom_bisect.f90:78-170). */
+int imcom_gpu_bisect_kappa_learned(imcom_ctx* ctx, int UnotS, double US_max,
+                                   double k_min, double k_max, double tol,
+                                   int maxnits, double C_a, double* K_out,
+                                   double* US_out, int* nevals_out,
+                                   int* fallback_out);
+
+/* T(:,a) = -1/2 Q (P(:,a) / (L + K_a)) (imcom_build_T,
+ * imcom_matrix.f90:716-750).  Needs the bisection to have run (or
+ * imcom_gpu_load_K).  T_out (n, m) may be NULL. */
+int imcom_gpu_build_T(imcom_ctx* ctx, double* T_out);
+/* T-reuse path (imcom_bisect.f90:47-62): T read from FITS by the caller. */
+int imcom_gpu_load_T(imcom_ctx* ctx, const double* T);
+/* Kappa map from a previous solve (K_a, imcom_data.f90:104). */
+int imcom_gpu_load_K(imcom_ctx* ctx, const double* K);
+
+/* H = T^T I (imcom_build_image, imcom_matrix.f90:754-790). */
+int imcom_gpu_build_image(imcom_ctx* ctx, double* H_out);
+/* S_a = sum_i T_ia^2 Ndiag_i (imcom_build_S, imcom_matrix.f90:839-877). */
+int imcom_gpu_build_S(imcom_ctx* ctx, double* S_out);
+/* U_a = U(K_a) (imcom_build_U, imcom_matrix.f90:795-835). */
+int imcom_gpu_build_U(imcom_ctx* ctx, double C_a, double* U_out);
+
+/* ---- learned kappa (no reference counterpart) -------------------------- */
+
+/* Per-pixel features (12 per pixel, feature-major (12, m)): input-pixel
+ * density near X_a, hit count, 8 log-moments of P2 weighted by L, and the
+ * U/S target.  Needs P and L on the device. */
+int imcom_gpu_kappa_features(imcom_ctx* ctx, int UnotS, double US_max,
+                             double C_a, float* feat_out);
+/* Install MLP weights (12 -> 64 -> 64 -> 2, fp32 host arrays, row-major
+ * [out][in]) and the feature normalisation (mean/std, 12 each). */
+int imcom_gpu_mlp_set_weights(imcom_ctx* ctx, const float* W1,
+                              const float* b1, const float* W2,
+                              const float* b2, const float* W3,
+                              const float* b3, const float* feat_mean,
+                              const float* feat_std);
+
+/* ---- device views (for callers that keep data on the GPU) -------------- */
+
+/* Device pointer and leading dimension of an internal buffer:
+ * which = 'A','Q','L','B','P','T','K','H','S','U' (column-major, ld rows). */
+int imcom_gpu_device_buffer(imcom_ctx* ctx, char which, void** dptr,
+                            long long* ld);
+/* Number of this library's own kernel launches since the process started
+ * (library calls such as cuFFT are not counted). */
+int imcom_gpu_launch_count(imcom_ctx* ctx, long long* count);
+/* The context's CUDA stream (cudaStream_t), for callers that order their
+ * own work or events against the library's. */
+int imcom_gpu_get_stream(imcom_ctx* ctx, void** stream);
+/* Milliseconds spent on the GPU by the last call of each stage (CUDA
+ * events): [spectra, build_A, eigen_A, build_B, build_P, bisect, build_T,
+ * epilogue]. */
+int imcom_gpu_stage_times(imcom_ctx* ctx, double* ms8);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IMCOM_GPU_H */
