@@ -1,0 +1,208 @@
+!    IMCOM_GPU_IFACE.F90 - ISO_C_BINDING interface of the B200 solve path
+!
+!    Binds the C-ABI declared in include/imcom_gpu.h so the reference's
+!    Fortran driver (imcom.f90) and matrix module can call the GPU solve path
+!    in their "build" branches.  Arrays are passed as the Fortran arrays the
+!    module already allocates (column-major, leading dimension = rows); the
+!    C side receives plain pointers.  Every function returns an integer
+!    status (0 = success, < 0 bad argument, > 0 device or convergence
+!    error); imcom_gpu_check turns a failure into the reference's
+!    "IMCOM ERROR: ..." + STOP behaviour.
+!
+!    Link with -L<repo>/imcom_b200 -limcom_gpu.
+!
+MODULE imcom_gpu_iface
+
+USE ISO_C_BINDING
+implicit none
+
+INTERFACE
+
+  INTEGER(C_INT) FUNCTION imcom_gpu_create(device, ctx) BIND(C, NAME="imcom_gpu_create")
+    IMPORT :: C_INT, C_PTR
+    INTEGER(C_INT), VALUE :: device
+    TYPE(C_PTR) :: ctx
+  END FUNCTION
+
+  INTEGER(C_INT) FUNCTION imcom_gpu_destroy(ctx) BIND(C, NAME="imcom_gpu_destroy")
+    IMPORT :: C_INT, C_PTR
+    TYPE(C_PTR), VALUE :: ctx
+  END FUNCTION
+
+  TYPE(C_PTR) FUNCTION imcom_gpu_last_error(ctx) BIND(C, NAME="imcom_gpu_last_error")
+    IMPORT :: C_PTR
+    TYPE(C_PTR), VALUE :: ctx
+  END FUNCTION
+
+  ! imcom_data module state: x_i, y_i, exp_i, X_a, Y_a, I_i, Ndiag
+  INTEGER(C_INT) FUNCTION imcom_gpu_set_inputs(ctx, n, m, x_i, y_i, exp_i, X_a, Y_a, I_i, &
+                                               Ndiag, psfxscale, psfyscale) &
+                                               BIND(C, NAME="imcom_gpu_set_inputs")
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: ctx
+    INTEGER(C_INT), VALUE :: n, m
+    REAL(C_DOUBLE), DIMENSION(*), INTENT(IN) :: x_i, y_i, X_a, Y_a, I_i, Ndiag
+    INTEGER(C_INT), DIMENSION(*), INTENT(IN) :: exp_i
+    REAL(C_DOUBLE), VALUE :: psfxscale, psfyscale
+  END FUNCTION
+
+  ! G_unrot(n1psf, n2psf, nexppsf), rotangdeg(nexppsf), Gamma(n1psf, n2psf)
+  INTEGER(C_INT) FUNCTION imcom_gpu_set_psfs(ctx, nps, nexppsf, psfconst, G_unrot, &
+                                             rotangdeg, Gamma) BIND(C, NAME="imcom_gpu_set_psfs")
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: ctx
+    INTEGER(C_INT), VALUE :: nps, nexppsf, psfconst
+    REAL(C_DOUBLE), DIMENSION(*), INTENT(IN) :: G_unrot, rotangdeg, Gamma
+  END FUNCTION
+
+  ! imcom.f90:90-122 (rotation, r2c FFTs, imcom_calc_C)
+  INTEGER(C_INT) FUNCTION imcom_gpu_psf_spectra(ctx, npoly, C_out, Gt_out, Gammat_out) &
+                                                BIND(C, NAME="imcom_gpu_psf_spectra")
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: ctx
+    INTEGER(C_INT), VALUE :: npoly
+    REAL(C_DOUBLE) :: C_out
+    TYPE(C_PTR), VALUE :: Gt_out, Gammat_out   ! C_NULL_PTR or C_LOC(complex arrays)
+  END FUNCTION
+
+  ! imcom_get_A build branch (imcom_build_Alookup + imcom_lookup_A)
+  INTEGER(C_INT) FUNCTION imcom_gpu_build_A(ctx, npoly, npad, A_out) &
+                                            BIND(C, NAME="imcom_gpu_build_A")
+    IMPORT :: C_INT, C_PTR
+    TYPE(C_PTR), VALUE :: ctx
+    INTEGER(C_INT), VALUE :: npoly, npad
+    TYPE(C_PTR), VALUE :: A_out                 ! C_LOC(A_aij) when saveA, else C_NULL_PTR
+  END FUNCTION
+
+  INTEGER(C_INT) FUNCTION imcom_gpu_load_A(ctx, A) BIND(C, NAME="imcom_gpu_load_A")
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: ctx
+    REAL(C_DOUBLE), DIMENSION(*), INTENT(IN) :: A
+  END FUNCTION
+
+  ! imcom_eigen_A (DSYEVR + reversal)
+  INTEGER(C_INT) FUNCTION imcom_gpu_eigen_A(ctx, Q_out, L_out, cond_out) &
+                                            BIND(C, NAME="imcom_gpu_eigen_A")
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: ctx
+    TYPE(C_PTR), VALUE :: Q_out, L_out
+    REAL(C_DOUBLE) :: cond_out
+  END FUNCTION
+
+  INTEGER(C_INT) FUNCTION imcom_gpu_load_QL(ctx, Q, L) BIND(C, NAME="imcom_gpu_load_QL")
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: ctx
+    REAL(C_DOUBLE), DIMENSION(*), INTENT(IN) :: Q, L
+  END FUNCTION
+
+  ! imcom_get_B build branch (imcom_build_Blookup + imcom_lookup_B)
+  INTEGER(C_INT) FUNCTION imcom_gpu_build_B(ctx, npoly, npad, B_out) &
+                                            BIND(C, NAME="imcom_gpu_build_B")
+    IMPORT :: C_INT, C_PTR
+    TYPE(C_PTR), VALUE :: ctx
+    INTEGER(C_INT), VALUE :: npoly, npad
+    TYPE(C_PTR), VALUE :: B_out
+  END FUNCTION
+
+  INTEGER(C_INT) FUNCTION imcom_gpu_load_B(ctx, B) BIND(C, NAME="imcom_gpu_load_B")
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: ctx
+    REAL(C_DOUBLE), DIMENSION(*), INTENT(IN) :: B
+  END FUNCTION
+
+  ! imcom_build_P (DGEMM 'T','N')
+  INTEGER(C_INT) FUNCTION imcom_gpu_build_P(ctx, P_out) BIND(C, NAME="imcom_gpu_build_P")
+    IMPORT :: C_INT, C_PTR
+    TYPE(C_PTR), VALUE :: ctx
+    TYPE(C_PTR), VALUE :: P_out
+  END FUNCTION
+
+  INTEGER(C_INT) FUNCTION imcom_gpu_load_P(ctx, P) BIND(C, NAME="imcom_gpu_load_P")
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: ctx
+    REAL(C_DOUBLE), DIMENSION(*), INTENT(IN) :: P
+  END FUNCTION
+
+  INTEGER(C_INT) FUNCTION imcom_gpu_free_AB(ctx) BIND(C, NAME="imcom_gpu_free_AB")
+    IMPORT :: C_INT, C_PTR
+    TYPE(C_PTR), VALUE :: ctx
+  END FUNCTION
+
+  ! imcom_bisect_kappa (USB -> UnotS)
+  INTEGER(C_INT) FUNCTION imcom_gpu_bisect_kappa(ctx, UnotS, US_max, k_min, k_max, tol, &
+                                                 maxnits, C_a, K_out, US_out, nevals_out) &
+                                                 BIND(C, NAME="imcom_gpu_bisect_kappa")
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: ctx
+    INTEGER(C_INT), VALUE :: UnotS, maxnits
+    REAL(C_DOUBLE), VALUE :: US_max, k_min, k_max, tol, C_a
+    REAL(C_DOUBLE), DIMENSION(*) :: K_out, US_out
+    TYPE(C_PTR), VALUE :: nevals_out
+  END FUNCTION
+
+  ! imcom_build_T
+  INTEGER(C_INT) FUNCTION imcom_gpu_build_T(ctx, T_out) BIND(C, NAME="imcom_gpu_build_T")
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: ctx
+    REAL(C_DOUBLE), DIMENSION(*) :: T_out
+  END FUNCTION
+
+  INTEGER(C_INT) FUNCTION imcom_gpu_load_T(ctx, T) BIND(C, NAME="imcom_gpu_load_T")
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: ctx
+    REAL(C_DOUBLE), DIMENSION(*), INTENT(IN) :: T
+  END FUNCTION
+
+  ! imcom_build_image / imcom_build_S / imcom_build_U
+  INTEGER(C_INT) FUNCTION imcom_gpu_build_image(ctx, H_out) BIND(C, NAME="imcom_gpu_build_image")
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: ctx
+    REAL(C_DOUBLE), DIMENSION(*) :: H_out
+  END FUNCTION
+
+  INTEGER(C_INT) FUNCTION imcom_gpu_build_S(ctx, S_out) BIND(C, NAME="imcom_gpu_build_S")
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: ctx
+    REAL(C_DOUBLE), DIMENSION(*) :: S_out
+  END FUNCTION
+
+  INTEGER(C_INT) FUNCTION imcom_gpu_build_U(ctx, C_a, U_out) BIND(C, NAME="imcom_gpu_build_U")
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: ctx
+    REAL(C_DOUBLE), VALUE :: C_a
+    REAL(C_DOUBLE), DIMENSION(*) :: U_out
+  END FUNCTION
+
+END INTERFACE
+
+TYPE(C_PTR), SAVE :: imcom_gpu_ctx = C_NULL_PTR
+
+CONTAINS
+
+SUBROUTINE imcom_gpu_check(status, what)
+! Reference error behaviour (write + stop) for a failed C-ABI call.
+implicit none
+integer(C_INT), intent(IN) :: status
+character(LEN=*), intent(IN) :: what
+character(KIND=C_CHAR), dimension(:), pointer :: msg
+integer :: i
+interface
+  integer(C_SIZE_T) function c_strlen(s) bind(C, name="strlen")
+    import :: C_SIZE_T, C_PTR
+    type(C_PTR), value :: s
+  end function
+end interface
+type(C_PTR) :: p
+if (status.eq.0) return
+p = imcom_gpu_last_error(imcom_gpu_ctx)
+call c_f_pointer(p, msg, [c_strlen(p)])
+write(*, FMT='(A, I4)') "IMCOM ERROR: "//what//" failed with status ", status
+write(*, FMT='(A)', ADVANCE='NO') "IMCOM ERROR: "
+do i = 1, size(msg)
+  write(*, FMT='(A)', ADVANCE='NO') msg(i)
+end do
+write(*, *)
+stop
+END SUBROUTINE imcom_gpu_check
+
+END MODULE imcom_gpu_iface

@@ -21,7 +21,8 @@ from ._lib import ImcomError
 
 EIGH_DC, EIGH_JACOBI, EIGH_LIBRARY = 0, 1, 2
 OPT_EIGENSOLVER, OPT_EIGEN_MAXITER = 1, 2
-STAGES = ("spectra", "build_A", "eigen_A", "build_B", "build_P", "bisect", "build_T", "epilogue")
+STAGES = ("spectra", "build_A", "eigen_A", "build_B", "build_P", "bisect", "build_T", "epilogue",
+          "eig_tridiag", "eig_dc", "eig_backtransform")
 EPS = 1.1102230246251565e-16  # DLAMCH('Epsilon')
 
 
@@ -81,7 +82,7 @@ class Solver:
         self.set_option(OPT_EIGENSOLVER, mode)
 
     def stage_times(self) -> dict:
-        ms = np.zeros(8)
+        ms = np.zeros(len(STAGES))
         self._call("imcom_gpu_stage_times", _ptr(ms))
         return dict(zip(STAGES, ms.tolist()))
 

@@ -23,7 +23,10 @@ struct DMat {
 
 inline long long pad_ld(long long rows) { return (rows + 31) / 32 * 32; }
 
-enum Stage { ST_SPECTRA = 0, ST_A, ST_EIG, ST_B, ST_P, ST_BISECT, ST_T, ST_EPI, ST_N };
+enum Stage {
+  ST_SPECTRA = 0, ST_A, ST_EIG, ST_B, ST_P, ST_BISECT, ST_T, ST_EPI,
+  ST_EIG_TRD, ST_EIG_DC, ST_EIG_BT, ST_N
+};
 
 struct MlpWeights {
   float* w = nullptr;  // packed device weights (see kappa.cu)
@@ -78,6 +81,9 @@ struct imcom_ctx {
   int plan_big_L = 0, plan_big_batch = 0;
   cufftHandle plan_r2c = 0;
   int plan_r2c_n = 0, plan_r2c_batch = 0;
+
+  void* gemm_ws = nullptr;  // split-K partial sums
+  size_t gemm_ws_bytes = 0;
 
   imcom::EigWork* eig = nullptr;
   imcom::MlpWeights mlp;

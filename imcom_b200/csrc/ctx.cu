@@ -169,7 +169,8 @@ int imcom_gpu_destroy(imcom_ctx* ctx) {
   void* ptrs[] = {ctx->x, ctx->y, ctx->X, ctx->Y, ctx->I, ctx->Nd, ctx->exp_i, ctx->G,
                   ctx->Gamma, ctx->Gt, ctx->Gammat, ctx->A.p, ctx->Q.p, ctx->B.p, ctx->P.p,
                   ctx->T.p, ctx->Pt.p, ctx->L, ctx->K, ctx->US, ctx->H, ctx->S, ctx->U,
-                  ctx->nev, ctx->flags, ctx->tables, ctx->fftbuf, ctx->mlp.w, ctx->feat};
+                  ctx->nev, ctx->flags, ctx->tables, ctx->fftbuf, ctx->mlp.w, ctx->feat,
+                  ctx->gemm_ws};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete[] ctx->rot;

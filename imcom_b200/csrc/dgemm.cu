@@ -11,6 +11,8 @@
 // Operands stream through a 3-stage cp.async shared-memory pipeline; the
 // shared layouts are padded so every fragment load is bank-conflict free
 // (stride 20 doubles for k-contiguous tiles, 132 for m/n-contiguous ones).
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace imcom {
@@ -71,13 +73,17 @@ template <bool AK, bool BKC, int VEC>
 __global__ void __launch_bounds__(THREADS, 1)
 dgemm_kernel(long long M, long long N, long long K, double alpha, const double* __restrict__ A,
              long long lda, const double* __restrict__ B, long long ldb, double beta,
-             double* __restrict__ C, long long ldc) {
+             double* __restrict__ C, long long ldc, long long kchunk) {
   extern __shared__ __align__(16) double smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wm = warp & 1, wn = warp >> 1;  // 2 x 4 warps
   const int g = lane >> 2, t = lane & 3;
   const long long m0 = (long long)blockIdx.x * BM, n0 = (long long)blockIdx.y * BN;
-  const int nk = (int)((K + BK - 1) / BK);
+  // split-K: this CTA covers k in [kb, ke); partial sums go to slice z of C
+  const long long kb = (long long)blockIdx.z * kchunk;
+  const long long ke = min(K, kb + kchunk);
+  if (gridDim.z > 1) C += (size_t)blockIdx.z * (size_t)ldc * (size_t)N;
+  const int nk = ke > kb ? (int)((ke - kb + BK - 1) / BK) : 0;
 
   double acc[4][4][4];
 #pragma unroll
@@ -93,8 +99,8 @@ dgemm_kernel(long long M, long long N, long long K, double alpha, const double* 
 #pragma unroll
   for (int s = 0; s < STAGES - 1; ++s) {
     if (s < nk) {
-      load_tile<AK, VEC>(stageA(s), A, lda, m0, (long long)s * BK, M, K);
-      load_tile<BKC, VEC>(stageB(s), B, ldb, n0, (long long)s * BK, N, K);
+      load_tile<AK, VEC>(stageA(s), A, lda, m0, kb + (long long)s * BK, M, ke);
+      load_tile<BKC, VEC>(stageB(s), B, ldb, n0, kb + (long long)s * BK, N, ke);
     }
     cp_commit();
   }
@@ -135,8 +141,8 @@ dgemm_kernel(long long M, long long N, long long K, double alpha, const double* 
     }
     int nxt = kt + STAGES - 1;
     if (nxt < nk) {
-      load_tile<AK, VEC>(stageA(nxt % STAGES), A, lda, m0, (long long)nxt * BK, M, K);
-      load_tile<BKC, VEC>(stageB(nxt % STAGES), B, ldb, n0, (long long)nxt * BK, N, K);
+      load_tile<AK, VEC>(stageA(nxt % STAGES), A, lda, m0, kb + (long long)nxt * BK, M, ke);
+      load_tile<BKC, VEC>(stageB(nxt % STAGES), B, ldb, n0, kb + (long long)nxt * BK, N, ke);
     }
     cp_commit();
   }
@@ -153,27 +159,69 @@ dgemm_kernel(long long M, long long N, long long K, double alpha, const double* 
         if (row < M && col < N) {
           double* cp = C + row + col * ldc;
           double v = alpha * acc[i][j][r];
-          if (beta != 0.0) v += beta * *cp;
+          if (gridDim.z == 1 && beta != 0.0) v += beta * *cp;
           *cp = v;
         }
       }
+}
+
+// C = alpha * sum_z part[z] + beta * C
+__global__ void splitk_reduce_kernel(const double* __restrict__ part, long long ldp, int splits,
+                                     long long M, long long N, double alpha, double beta,
+                                     double* __restrict__ C, long long ldc) {
+  long long col = blockIdx.y;
+  for (long long row = blockIdx.x * (long long)blockDim.x + threadIdx.x; row < M;
+       row += (long long)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int z = 0; z < splits; ++z) s += part[(size_t)z * ldp * N + row + col * ldp];
+    double* cp = C + row + col * ldc;
+    s = alpha * s;
+    *cp = (beta != 0.0) ? s + beta * *cp : s;
+  }
 }
 
 template <bool AK, bool BKC>
 int launch(imcom_ctx* ctx, long long M, long long N, long long K, double alpha, const double* A,
            long long lda, const double* B, long long ldb, double beta, double* C, long long ldc,
            int vec) {
-  dim3 grd((unsigned)((M + BM - 1) / BM), (unsigned)((N + BN - 1) / BN));
+  long long gm = (M + BM - 1) / BM, gn = (N + BN - 1) / BN;
+  int sms = sm_count(ctx);
+  // Split K when the output tiles cannot fill the GPU and K is long.
+  int splits = 1;
+  if (gm * gn < sms && K >= 8 * BK) {
+    splits = (int)std::min<long long>((2LL * sms + gm * gn - 1) / (gm * gn), K / (4 * BK));
+    splits = std::max(1, std::min(splits, 16));
+  }
+  long long kchunk = (K + splits - 1) / splits;
+  kchunk = (kchunk + BK - 1) / BK * BK;
+  if (kchunk <= 0) kchunk = BK;
+  splits = (int)std::max<long long>(1, (K + kchunk - 1) / kchunk);
+  double* out = C;
+  long long ldo = ldc;
+  if (splits > 1) {
+    ldo = pad_ld(M);
+    size_t need = (size_t)splits * (size_t)ldo * (size_t)N * sizeof(double);
+    IMC_TRY(ensure_buf(ctx, &ctx->gemm_ws, ctx->gemm_ws_bytes, need));
+    out = (double*)ctx->gemm_ws;
+  }
+  dim3 grd((unsigned)gm, (unsigned)gn, (unsigned)splits);
+  double a1 = splits > 1 ? 1.0 : alpha;
   if (vec == 2) {
     auto k = dgemm_kernel<AK, BKC, 2>;
     IMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES));
-    k<<<grd, THREADS, SMEM_BYTES, ctx->stream>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+    k<<<grd, THREADS, SMEM_BYTES, ctx->stream>>>(M, N, K, a1, A, lda, B, ldb, beta, out, ldo, kchunk);
   } else {
     auto k = dgemm_kernel<AK, BKC, 1>;
     IMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES));
-    k<<<grd, THREADS, SMEM_BYTES, ctx->stream>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+    k<<<grd, THREADS, SMEM_BYTES, ctx->stream>>>(M, N, K, a1, A, lda, B, ldb, beta, out, ldo, kchunk);
   }
   IMC_LAUNCH();
+  if (splits > 1) {
+    dim3 g2((unsigned)std::min<long long>((M + 255) / 256, 64), (unsigned)N);
+    splitk_reduce_kernel<<<g2, 256, 0, ctx->stream>>>(out, ldo, splits, M, N, alpha, beta, C,
+                                                      ldc);
+    IMC_LAUNCH();
+  }
   return 0;
 }
 

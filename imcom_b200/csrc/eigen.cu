@@ -58,6 +58,7 @@ void eig_free(imcom_ctx* ctx) {
   if (w->w) cudaFree(w->w);
   if (w->Z.p) cudaFree(w->Z.p);
   if (w->V.p) cudaFree(w->V.p);
+  if (w->U.p) cudaFree(w->U.p);
   if (w->buf) cudaFree(w->buf);
   if (w->solver) cusolverDnDestroy((cusolverDnHandle_t)w->solver);
   delete w;

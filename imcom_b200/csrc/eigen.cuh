@@ -9,6 +9,7 @@ struct EigWork {
   DMat W;   // ascending eigenvectors (solver output)
   DMat Z;   // scratch matrices
   DMat V;
+  DMat U;   // divide-and-conquer node blocks (U | G | OUT)
   double* w = nullptr;  // ascending eigenvalues
   size_t w_cap = 0;
   void* buf = nullptr;  // general scratch

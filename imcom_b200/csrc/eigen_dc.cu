@@ -1,12 +1,1052 @@
-// eigen_dc.cu -- placeholder entry points of the own eigensolvers.
+// eigen_dc.cu -- FP64 symmetric eigensolver: blocked Householder
+// tridiagonalisation, divide and conquer on the tridiagonal matrix, and
+// blocked back-transformation.  Replaces LAPACK DSYEVR in imcom_eigen_A
+// (imcom_matrix.f90:617-643); results are returned in ascending order and
+// reversed by the caller (imcom_matrix.f90:656-662).
+//
+// 1. Tridiagonalisation (LAPACK dsytrd/dlatrd, lower).  Panels of NB = 32
+//    columns.  Inside a panel every column needs the trailing symmetric
+//    matrix-vector product y0 = A22 v and the panel corrections
+//    y = y0 - V (W^T v) - W (V^T v).  One persistent cooperative kernel per
+//    panel runs the whole panel with two grid-wide barriers per column:
+//      phase A: y0 tiles over the trailing matrix (all SMs), plus the panel
+//               dot products W^T v, V^T v and v^T y0 (atomics);
+//      phase B: w = tau (y - 1/2 tau (y^T v) v) row by row, using
+//               v^T y = v^T y0 - 2 (V^T v).(W^T v), the update of the next
+//               column and its norm (atomics).
+//    The trailing update A22 -= V W^T + W V^T runs on the DMMA GEMM.
+//    Grid barriers spin with a bound and report a timeout instead of hanging.
+// 2. Divide and conquer (LAPACK dstedc / dlaed0-4 structure).  Leaves of at
+//    most 32 rows are diagonalised by a cyclic Jacobi sweep in one CTA each.
+//    Each merge level runs batched over all nodes: z vector and sort (merge
+//    ranks), deflation scan (one thread per node, LAPACK dlaed2 tests and
+//    Givens rotations), the secular equation roots (one warp per root,
+//    safeguarded Newton in the shifted variable tau = lambda - d_org), the
+//    Gu-Eisenstat z-hat (dlaed3) and the eigenvector columns (one warp each),
+//    then Q_node = Q_old(:, nondeflated) U as one DMMA GEMM per node.
+// 3. Back-transformation (dormtr): Z <- (I - V T V^T) Z over blocks of 128
+//    reflectors, T built from V^T V (dlarft), three GEMMs per block.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
 #include "common.cuh"
 #include "eigen.cuh"
 
 namespace imcom {
 
-int eigen_dc(imcom_ctx* ctx, const DMat& A, DMat& W, double* w) {
-  (void)A; (void)W; (void)w;
-  return set_err(ctx, IMCOM_ERR_STATE, "divide-and-conquer eigensolver not built");
+namespace {
+
+constexpr int NB = 32;            // tridiagonalisation panel width
+constexpr int TRD_THREADS = 256;  // threads per CTA of the panel kernel
+constexpr int CW = 256;           // columns per symv tile
+constexpr int LEAF = 32;          // largest leaf of the divide-and-conquer tree
+constexpr int NBB = 128;          // reflectors per back-transformation block
+constexpr double EPS = 1.1102230246251565e-16;
+constexpr size_t LARFT_SMEM = (size_t)NBB * (NBB + 1) * sizeof(double);
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ double ld_cg(const double* p) {
+  double v;
+  asm volatile("ld.global.cg.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+
+// ---------------------------------------------------------------------------
+// Bounded grid barrier (cooperative launch guarantees co-residency).
+// ---------------------------------------------------------------------------
+struct GridSync {
+  unsigned count;
+  unsigned gen;
+  int err;
+  int pad;
+};
+
+__device__ __forceinline__ bool grid_barrier(GridSync* s, long long limit) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* vgen = &s->gen;
+    unsigned g = *vgen;
+    __threadfence();
+    unsigned arrived = atomicAdd(&s->count, 1u) + 1u;
+    int ok = 1;
+    if (arrived == gridDim.x) {
+      atomicExch(&s->count, 0u);
+      __threadfence();
+      atomicAdd(&s->gen, 1u);
+    } else {
+      long long it = 0;
+      volatile int* verr = &s->err;
+      while (*vgen == g) {
+        if (*verr) {
+          ok = 0;
+          break;
+        }
+        if (++it > limit) {
+          atomicExch(&s->err, 1);
+          ok = 0;
+          break;
+        }
+      }
+    }
+    __threadfence();
+    if (*(volatile int*)&s->err) ok = 0;
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// ---------------------------------------------------------------------------
+// 1. Tridiagonalisation
+// ---------------------------------------------------------------------------
+struct TrdAcc {
+  double pq[2 * NB];  // p = W^T v (0..NB-1), q = V^T v (NB..2NB-1)
+  double vty0;        // v^T y0
+  double nrm;         // squared norm of the next column below its subdiagonal
+};
+
+struct TrdArgs {
+  double* A;
+  long long lda;
+  double* V;  // n x n: column j holds v_j (zero above row j+1, 1 at row j+1)
+  long long ldv;
+  double* W;  // n x NB panel
+  long long ldw;
+  double *d, *e, *tau;
+  double* ypart;  // [chunk][ldy]
+  long long ldy;
+  TrdAcc* acc;  // [2] by column parity
+  GridSync* sync;
+  int n, k, b;
+  long long spin;
+};
+
+__global__ void __launch_bounds__(TRD_THREADS) trd_panel_kernel(TrdArgs a) {
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int WPB = TRD_THREADS / 32;
+  const long long gw = (long long)blockIdx.x * WPB + wib;
+  const long long GW = (long long)gridDim.x * WPB;
+  const int n = a.n, k = a.k;
+  double* A = a.A;
+  const long long lda = a.lda, ldv = a.ldv, ldw = a.ldw;
+  __shared__ double s_pq[2 * NB];
+  __shared__ double s_rowV[NB], s_rowW[NB];
+  if (*(volatile int*)&a.sync->err) return;  // an earlier panel failed
+
+  // Column k: d(k) and the norm of A(k+2:n, k).
+  for (long long r0 = k + 2 + gw * 32; r0 < n; r0 += GW * 32) {
+    long long r = r0 + lane;
+    double v = (r < n) ? A[r + k * lda] : 0.0;
+    double s = warp_sum(v * v);
+    if (lane == 0) atomicAdd(&a.acc[0].nrm, s);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) a.d[k] = A[k + k * lda];
+  if (!grid_barrier(a.sync, a.spin)) return;
+
+  for (int i = 0; i < a.b; ++i) {
+    const int j = k + i;
+    const int par = i & 1;
+    TrdAcc* cur = a.acc + par;
+    TrdAcc* nxt = a.acc + (par ^ 1);
+    // Householder reflector of x = A(j+1:n, j) (LAPACK dlarfg)
+    const double alpha = ld_cg(A + (j + 1) + j * lda);
+    const double xn2 = ld_cg(&cur->nrm);
+    double beta, t, scl;
+    if (xn2 == 0.0) {
+      t = 0.0;
+      beta = alpha;
+      scl = 0.0;
+    } else {
+      beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+      t = (beta - alpha) / beta;
+      scl = 1.0 / (alpha - beta);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      a.e[j] = beta;
+      a.tau[j] = t;
+    }
+    if (blockIdx.x == 0 && threadIdx.x < 2 * NB + 2) {
+      // clear the other parity's accumulators (last read one phase ago)
+      if (threadIdx.x < 2 * NB) nxt->pq[threadIdx.x] = 0.0;
+      else if (threadIdx.x == 2 * NB) nxt->vty0 = 0.0;
+      else nxt->nrm = 0.0;
+    }
+    const double* colj = A + j * lda;
+    auto vcol = [&](long long c) -> double {
+      return (c == j + 1) ? 1.0 : ld_cg(colj + c) * scl;
+    };
+
+    // ---- phase A: y0 = A22 v by 32-row x CW-column tiles ----
+    const long long R = n - j - 1;
+    const long long RB = (R + 31) / 32, NC = (R + CW - 1) / CW;
+    for (long long tile = gw; tile < RB * NC; tile += GW) {
+      const long long rb = tile % RB, ch = tile / RB;
+      const long long r = j + 1 + rb * 32 + lane;
+      const long long c0 = j + 1 + ch * CW, c1 = min((long long)n, c0 + CW);
+      double acc = 0.0;
+      if (r < n) {
+        const double* Ar = A + r;
+        long long c = c0;
+        for (; c + 8 <= c1; c += 8) {
+          double av[8], vv[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            av[u] = Ar[(c + u) * lda];
+            vv[u] = vcol(c + u);
+          }
+#pragma unroll
+          for (int u = 0; u < 8; ++u) acc = fma(av[u], vv[u], acc);
+        }
+        for (; c < c1; ++c) acc = fma(Ar[c * lda], vcol(c), acc);
+        a.ypart[ch * a.ldy + r] = acc;
+      }
+      const double vr = (r < n) ? vcol(r) : 0.0;
+      double s = warp_sum(vr * acc);
+      if (lane == 0) atomicAdd(&cur->vty0, s);
+      if (ch == 0) {
+        for (int p = 0; p < i; ++p) {
+          double wv = (r < n) ? ld_cg(a.W + r + p * ldw) * vr : 0.0;
+          double vv = (r < n) ? ld_cg(a.V + r + (k + p) * ldv) * vr : 0.0;
+          wv = warp_sum(wv);
+          vv = warp_sum(vv);
+          if (lane == 0) {
+            atomicAdd(&cur->pq[p], wv);
+            atomicAdd(&cur->pq[NB + p], vv);
+          }
+        }
+      }
+    }
+    if (!grid_barrier(a.sync, a.spin)) return;
+
+    // ---- phase B: w, the next column and its norm ----
+    if (threadIdx.x < 2 * NB) {
+      int p = threadIdx.x % NB;
+      s_pq[threadIdx.x] = (p < i) ? ld_cg(&cur->pq[threadIdx.x]) : 0.0;
+    }
+    __syncthreads();
+    double qp = 0.0;
+    for (int p = 0; p < i; ++p) qp += s_pq[NB + p] * s_pq[p];
+    const double vty = ld_cg(&cur->vty0) - 2.0 * qp;
+    const double alpha2 = -0.5 * t * t * vty;
+    const bool next = (i + 1 < a.b);
+    if (next) {
+      if (wib == 0) {
+        // w(j+1) for row j+1 of the panel (every CTA needs it)
+        double y = 0.0;
+        for (long long ch = lane; ch < NC; ch += 32) y += ld_cg(a.ypart + ch * a.ldy + (j + 1));
+        y = warp_sum(y);
+        double corr = 0.0;
+        for (int p = lane; p < i; p += 32)
+          corr += ld_cg(a.V + (j + 1) + (k + p) * ldv) * s_pq[p] +
+                  ld_cg(a.W + (j + 1) + p * ldw) * s_pq[NB + p];
+        corr = warp_sum(corr);
+        const double wj1 = t * (y - corr) + alpha2;
+        if (lane <= i) {
+          s_rowV[lane] = (lane < i) ? ld_cg(a.V + (j + 1) + (k + lane) * ldv) : 1.0;
+          s_rowW[lane] = (lane < i) ? ld_cg(a.W + (j + 1) + lane * ldw) : wj1;
+        }
+      }
+      __syncthreads();
+    }
+    for (long long r0 = j + 1 + gw * 32; r0 < n; r0 += GW * 32) {
+      const long long r = r0 + lane;
+      double nrm = 0.0;
+      if (r < n) {
+        double y0 = 0.0;
+        for (long long ch = 0; ch < NC; ++ch) y0 += ld_cg(a.ypart + ch * a.ldy + r);
+        const double vr = vcol(r);
+        double corr = 0.0;
+        for (int p = 0; p < i; ++p)
+          corr += ld_cg(a.V + r + (k + p) * ldv) * s_pq[p] + ld_cg(a.W + r + p * ldw) * s_pq[NB + p];
+        const double wr = t * (y0 - corr) + alpha2 * vr;
+        a.V[r + j * ldv] = vr;
+        a.W[r + i * ldw] = wr;
+        if (next) {
+          double upd = vr * s_rowW[i] + wr * s_rowV[i];
+          for (int p = 0; p < i; ++p)
+            upd += ld_cg(a.V + r + (k + p) * ldv) * s_rowW[p] + ld_cg(a.W + r + p * ldw) * s_rowV[p];
+          const double anew = ld_cg(A + r + (j + 1) * lda) - upd;
+          A[r + (j + 1) * lda] = anew;
+          if (r == j + 1) a.d[j + 1] = anew;
+          if (r >= j + 3) nrm = anew * anew;
+        }
+      }
+      if (next) {
+        nrm = warp_sum(nrm);
+        if (lane == 0) atomicAdd(&nxt->nrm, nrm);
+      }
+    }
+    if (!grid_barrier(a.sync, a.spin)) return;
+  }
+}
+
+__global__ void set_last_diag_kernel(const double* A, long long lda, int n, double* d) {
+  d[n - 1] = A[(n - 1) + (long long)(n - 1) * lda];
+}
+
+// ---------------------------------------------------------------------------
+// 2. Divide and conquer
+// ---------------------------------------------------------------------------
+struct Node {
+  int s, n1, nm;  // first row, left child size, node size
+};
+
+// Tearing: d(s-1) -= |e(s-1)|, d(s) -= |e(s-1)| at every split point.
+__global__ void tear_kernel(double* dt, const double* e, const int* splits, int nsplit) {
+  if (blockIdx.x == 0 && threadIdx.x == 0)
+    for (int q = 0; q < nsplit; ++q) {
+      int s = splits[q];
+      double b = fabs(e[s - 1]);
+      dt[s - 1] -= b;
+      dt[s] -= b;
+    }
+}
+
+// Cyclic Jacobi on one leaf (tridiagonal block), sorted ascending output.
+__global__ void __launch_bounds__(256) leaf_jacobi_kernel(const Node* nodes, const double* dt,
+                                                          const double* e, double* w, double* Z,
+                                                          long long ldz, int max_sweeps,
+                                                          int* err) {
+  const Node nd = nodes[blockIdx.x];
+  const int m = nd.nm, s0 = nd.s;
+  __shared__ double Am[LEAF][LEAF + 1];
+  __shared__ double Zm[LEAF][LEAF + 1];
+  __shared__ double cs[LEAF / 2][2];
+  __shared__ int pr[LEAF / 2][2];
+  __shared__ int s_done;
+  __shared__ double s_val[LEAF];
+  __shared__ int s_idx[LEAF];
+  const int tid = threadIdx.x;
+  for (int q = tid; q < LEAF * LEAF; q += blockDim.x) {
+    int r = q % LEAF, c = q / LEAF;
+    double v = 0.0;
+    if (r < m && c < m) {
+      if (r == c) v = dt[s0 + r];
+      else if (r == c + 1) v = e[s0 + c];
+      else if (c == r + 1) v = e[s0 + r];
+    }
+    Am[r][c] = v;
+    Zm[r][c] = (r == c) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  const int mp = (m + 1) & ~1;  // even number of players (a dummy when m is odd)
+  for (int sweep = 0; sweep < max_sweeps; ++sweep) {
+    // convergence: off-diagonal mass below eps^2 of the total
+    if (tid == 0) {
+      double off = 0.0, tot = 0.0;
+      for (int r = 0; r < m; ++r)
+        for (int c = 0; c < m; ++c) {
+          double v = Am[r][c] * Am[r][c];
+          tot += v;
+          if (r != c) off += v;
+        }
+      s_done = (off <= 64.0 * EPS * EPS * tot) ? 1 : 0;
+    }
+    __syncthreads();
+    if (s_done) break;
+    for (int rnd = 0; rnd < mp - 1; ++rnd) {
+      if (tid < mp / 2) {
+        auto idx = [&](int x) { return x == 0 ? 0 : 1 + (x - 1 + rnd) % (mp - 1); };
+        int p = idx(tid), q = idx(mp - 1 - tid);
+        if (p > q) { int tt = p; p = q; q = tt; }
+        double c = 1.0, sn = 0.0;
+        if (q < m) {
+          double apq = Am[p][q];
+          if (apq != 0.0) {
+            double theta = (Am[q][q] - Am[p][p]) / (2.0 * apq);
+            double tt = copysign(1.0, theta) / (fabs(theta) + sqrt(1.0 + theta * theta));
+            c = 1.0 / sqrt(1.0 + tt * tt);
+            sn = tt * c;
+          }
+        }
+        pr[tid][0] = p;
+        pr[tid][1] = q;
+        cs[tid][0] = c;
+        cs[tid][1] = sn;
+      }
+      __syncthreads();
+      // columns: A <- A J, Z <- Z J
+      for (int item = tid; item < (mp / 2) * LEAF; item += blockDim.x) {
+        int pi = item / LEAF, r = item % LEAF;
+        int p = pr[pi][0], q = pr[pi][1];
+        if (q >= m || r >= m) continue;
+        double c = cs[pi][0], sn = cs[pi][1];
+        double ap = Am[r][p], aq = Am[r][q];
+        Am[r][p] = c * ap - sn * aq;
+        Am[r][q] = sn * ap + c * aq;
+        double zp = Zm[r][p], zq = Zm[r][q];
+        Zm[r][p] = c * zp - sn * zq;
+        Zm[r][q] = sn * zp + c * zq;
+      }
+      __syncthreads();
+      // rows: A <- J^T A
+      for (int item = tid; item < (mp / 2) * LEAF; item += blockDim.x) {
+        int pi = item / LEAF, col = item % LEAF;
+        int p = pr[pi][0], q = pr[pi][1];
+        if (q >= m || col >= m) continue;
+        double c = cs[pi][0], sn = cs[pi][1];
+        double ap = Am[p][col], aq = Am[q][col];
+        Am[p][col] = c * ap - sn * aq;
+        Am[q][col] = sn * ap + c * aq;
+      }
+      __syncthreads();
+      // the rotation annihilates a_pq exactly in exact arithmetic
+      if (tid < mp / 2 && pr[tid][1] < m && cs[tid][1] != 0.0) {
+        Am[pr[tid][0]][pr[tid][1]] = 0.0;
+        Am[pr[tid][1]][pr[tid][0]] = 0.0;
+      }
+      __syncthreads();
+    }
+    if (sweep == max_sweeps - 1 && tid == 0) atomicOr(err, 2);
+    __syncthreads();
+  }
+  // sort ascending (insertion sort of m values)
+  if (tid == 0) {
+    for (int c = 0; c < m; ++c) {
+      s_val[c] = Am[c][c];
+      s_idx[c] = c;
+    }
+    for (int c = 1; c < m; ++c) {
+      double v = s_val[c];
+      int ix = s_idx[c], p = c - 1;
+      while (p >= 0 && s_val[p] > v) {
+        s_val[p + 1] = s_val[p];
+        s_idx[p + 1] = s_idx[p];
+        --p;
+      }
+      s_val[p + 1] = v;
+      s_idx[p + 1] = ix;
+    }
+  }
+  __syncthreads();
+  for (int q = tid; q < m * m; q += blockDim.x) {
+    int r = q % m, c = q / m;
+    Z[(s0 + r) + (long long)(s0 + c) * ldz] = Zm[r][s_idx[c]];
+  }
+  for (int c = tid; c < m; c += blockDim.x) w[s0 + c] = s_val[c];
+}
+
+struct DcWork {
+  // per element (offset by node start s)
+  double *ds, *zs, *dl, *zz, *defd, *tau, *lam, *zhat;
+  int *perm, *ndcol, *defcol, *org, *rank;
+  // rotations (offset s): columns and (c, s)
+  int2* rcol;
+  double2* rcs;
+  // per node
+  int *kcnt, *ndef, *nrot;
+  double* rho;
+};
+
+// z, merge ranks of the two sorted child lists, scatter into sorted order.
+__global__ void dc_prep_kernel(const Node* nodes, const double* w, const double* Z, long long ldz,
+                               const double* e, DcWork wk) {
+  const Node nd = nodes[blockIdx.y];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nd.nm) return;
+  const int s = nd.s, n1 = nd.n1, n2 = nd.nm - nd.n1;
+  const double beta = e[s + n1 - 1];
+  const double sq = 0.70710678118654752440;  // 1/sqrt(2)
+  double v = w[s + i], z;
+  int pos;
+  if (i < n1) {
+    z = Z[(s + n1 - 1) + (long long)(s + i) * ldz] * sq;
+    // number of right-list values strictly below v
+    int lo = 0, hi = n2;
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (w[s + n1 + mid] < v) lo = mid + 1; else hi = mid;
+    }
+    pos = i + lo;
+  } else {
+    int jj = i - n1;
+    z = copysign(1.0, beta) * Z[(s + n1) + (long long)(s + i) * ldz] * sq;
+    // number of left-list values <= v
+    int lo = 0, hi = n1;
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (w[s + mid] <= v) lo = mid + 1; else hi = mid;
+    }
+    pos = jj + lo;
+  }
+  wk.ds[s + pos] = v;
+  wk.zs[s + pos] = z;
+  wk.perm[s + pos] = i;
+  if (i == 0) wk.rho[blockIdx.y] = 2.0 * fabs(beta);
+}
+
+// Deflation (LAPACK dlaed2): one CTA per node; reductions in parallel, the
+// scan by thread 0.
+__global__ void __launch_bounds__(256) dc_deflate_kernel(const Node* nodes, DcWork wk) {
+  const Node nd = nodes[blockIdx.x];
+  const int s = nd.s, nm = nd.nm;
+  const double rho = wk.rho[blockIdx.x];
+  __shared__ double sh_d[256], sh_z[256];
+  double md = 0.0, mz = 0.0;
+  for (int q = threadIdx.x; q < nm; q += blockDim.x) {
+    md = fmax(md, fabs(wk.ds[s + q]));
+    mz = fmax(mz, fabs(wk.zs[s + q]));
+  }
+  sh_d[threadIdx.x] = md;
+  sh_z[threadIdx.x] = mz;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      sh_d[threadIdx.x] = fmax(sh_d[threadIdx.x], sh_d[threadIdx.x + o]);
+      sh_z[threadIdx.x] = fmax(sh_z[threadIdx.x], sh_z[threadIdx.x + o]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  const double tol = 8.0 * EPS * fmax(sh_d[0], rho * sh_z[0]);
+  double* d = wk.ds + s;
+  double* z = wk.zs + s;
+  const int* perm = wk.perm + s;
+  int k = 0, ndef = 0, nrot = 0, prev = -1;
+  for (int jj = 0; jj < nm; ++jj) {
+    if (rho * fabs(z[jj]) <= tol) {
+      wk.defd[s + ndef] = d[jj];
+      wk.defcol[s + ndef] = perm[jj];
+      ++ndef;
+      continue;
+    }
+    if (prev < 0) {
+      prev = jj;
+      continue;
+    }
+    double sv = z[prev], cv = z[jj];
+    double tau = hypot(cv, sv);
+    double t = d[jj] - d[prev];
+    cv /= tau;
+    sv = -sv / tau;
+    if (fabs(t * cv * sv) <= tol) {
+      z[jj] = tau;
+      z[prev] = 0.0;
+      wk.rcol[s + nrot] = make_int2(perm[prev], perm[jj]);
+      wk.rcs[s + nrot] = make_double2(cv, sv);
+      ++nrot;
+      double tt = d[prev] * cv * cv + d[jj] * sv * sv;
+      d[jj] = d[prev] * sv * sv + d[jj] * cv * cv;
+      d[prev] = tt;
+      wk.defd[s + ndef] = d[prev];
+      wk.defcol[s + ndef] = perm[prev];
+      ++ndef;
+      prev = jj;
+    } else {
+      wk.dl[s + k] = d[prev];
+      wk.zz[s + k] = z[prev];
+      wk.ndcol[s + k] = perm[prev];
+      ++k;
+      prev = jj;
+    }
+  }
+  if (prev >= 0) {
+    wk.dl[s + k] = d[prev];
+    wk.zz[s + k] = z[prev];
+    wk.ndcol[s + k] = perm[prev];
+    ++k;
+  }
+  wk.kcnt[blockIdx.x] = k;
+  wk.ndef[blockIdx.x] = ndef;
+  wk.nrot[blockIdx.x] = nrot;
+}
+
+// Apply each node's deflation rotations, in order, to its columns of Z.
+__global__ void dc_rotate_kernel(const Node* nodes, double* Z, long long ldz, DcWork wk) {
+  const Node nd = nodes[blockIdx.y];
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nd.nm) return;
+  const int s = nd.s, nrot = wk.nrot[blockIdx.y];
+  double* row = Z + (s + r);
+  for (int q = 0; q < nrot; ++q) {
+    int2 cc = wk.rcol[s + q];
+    double2 t = wk.rcs[s + q];
+    double* pp = row + (long long)(s + cc.x) * ldz;
+    double* pj = row + (long long)(s + cc.y) * ldz;
+    double a = *pp, b = *pj;
+    *pp = t.x * a + t.y * b;
+    *pj = t.x * b - t.y * a;
+  }
+}
+
+// Secular equation 1 + rho sum z_i^2 / (d_i - lambda) = 0: root j of each node.
+__global__ void dc_secular_kernel(const Node* nodes, DcWork wk, int maxit, int* err) {
+  const int lane = threadIdx.x & 31;
+  const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int b = blockIdx.y;
+  const int k = wk.kcnt[b];
+  if (j >= k) return;
+  const int s = nodes[b].s;
+  const double rho = wk.rho[b];
+  const double* dl = wk.dl + s;
+  const double* zz = wk.zz + s;
+  int org;
+  double lo, hi;
+  if (j < k - 1) {
+    const double mid = 0.5 * (dl[j + 1] - dl[j]);
+    double f = 0.0;
+    for (int q = lane; q < k; q += 32) f += zz[q] * zz[q] / ((dl[q] - dl[j]) - mid);
+    f = 1.0 + rho * warp_sum(f);
+    if (f > 0.0) {
+      org = j;
+      lo = 0.0;
+      hi = mid;
+    } else {
+      org = j + 1;
+      lo = -mid;
+      hi = 0.0;
+    }
+  } else {
+    org = k - 1;
+    double z2 = 0.0;
+    for (int q = lane; q < k; q += 32) z2 += zz[q] * zz[q];
+    lo = 0.0;
+    hi = rho * warp_sum(z2) * (1.0 + 8.0 * EPS) + 1e-300;
+  }
+  const double dorg = dl[org];
+  const double zo = rho * zz[org] * zz[org];
+  double tau = 0.5 * (lo + hi);
+  int it = 0;
+  for (; it < maxit; ++it) {
+    // g = 1 + rho sum z_i^2 / (s_i - tau); the org pole is treated exactly:
+    // 1 + phi + phi' (t - tau) - zo / t = 0 is solved for the next t.
+    double g = 0.0, gabs = 0.0, phi = 0.0, dphi = 0.0;
+    for (int q = lane; q < k; q += 32) {
+      double del = (dl[q] - dorg) - tau;
+      double r = zz[q] / del;
+      double term = zz[q] * r;
+      g += term;
+      gabs += fabs(term);
+      if (q != org) {
+        phi += term;
+        dphi += r * r;
+      }
+    }
+    g = 1.0 + rho * warp_sum(g);
+    gabs = 1.0 + rho * warp_sum(gabs);
+    phi = rho * warp_sum(phi);
+    dphi = rho * warp_sum(dphi);
+    if (fabs(g) <= 4.0 * k * EPS * gabs) break;  // at the rounding level of g
+    if (g > 0.0) hi = tau; else lo = tau;
+    const double qa = dphi, qb = 1.0 + phi - dphi * tau, qc = -zo;
+    double tn;
+    if (qa == 0.0) {
+      tn = -qc / qb;
+    } else {
+      const double sq = sqrt(fmax(qb * qb - 4.0 * qa * qc, 0.0));
+      const double qq = -0.5 * (qb + copysign(sq, qb));
+      const double r1 = qq != 0.0 ? qq / qa : 0.0;
+      const double r2 = qq != 0.0 ? qc / qq : 0.0;
+      const bool ok1 = r1 > lo && r1 < hi, ok2 = r2 > lo && r2 < hi;
+      if (ok1 && ok2) tn = fabs(r1 - tau) < fabs(r2 - tau) ? r1 : r2;
+      else if (ok1) tn = r1;
+      else if (ok2) tn = r2;
+      else tn = 0.5 * (lo + hi);
+    }
+    if (!(tn > lo && tn < hi)) tn = 0.5 * (lo + hi);
+    if (fabs(tn - tau) <= 2.0 * EPS * fabs(tn) ||
+        hi - lo <= 2.0 * EPS * fmax(fabs(lo), fabs(hi))) {
+      tau = tn;
+      break;
+    }
+    tau = tn;
+  }
+  if (lane == 0) {
+    wk.org[s + j] = org;
+    wk.tau[s + j] = tau;
+    wk.lam[s + j] = dorg + tau;
+    if (it >= maxit) atomicOr(err, 4);
+  }
+}
+
+// Gu-Eisenstat z-hat (LAPACK dlaed3): zhat_i^2 = -delta_ii prod_{j!=i}
+// delta_ij / (d_i - d_j) / rho, with delta_ij = (d_i - d_org_j) - tau_j.
+__global__ void dc_zhat_kernel(const Node* nodes, DcWork wk, int* err) {
+  const int lane = threadIdx.x & 31;
+  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int b = blockIdx.y;
+  const int k = wk.kcnt[b];
+  if (i >= k) return;
+  const int s = nodes[b].s;
+  const double* dl = wk.dl + s;
+  const double di = dl[i];
+  double prod = 1.0;
+  for (int q = lane; q < k; q += 32) {
+    double del = (di - dl[wk.org[s + q]]) - wk.tau[s + q];
+    prod *= (q == i) ? -del : del / (di - dl[q]);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) prod *= __shfl_xor_sync(0xffffffffu, prod, o);
+  if (lane == 0) {
+    double v = prod / wk.rho[b];
+    if (!isfinite(v)) atomicOr(err, 8);
+    wk.zhat[s + i] = copysign(sqrt(fmax(v, 0.0)), wk.zz[s + i]);
+  }
+}
+
+// Eigenvector j of D + rho zhat zhat^T: U(:, j) = zhat / delta(:, j), normalised.
+__global__ void dc_vectors_kernel(const Node* nodes, DcWork wk, double* U, long long ldu) {
+  const int lane = threadIdx.x & 31;
+  const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int b = blockIdx.y;
+  const int k = wk.kcnt[b];
+  if (j >= k) return;
+  const int s = nodes[b].s;
+  const double* dl = wk.dl + s;
+  const double dorg = dl[wk.org[s + j]], tau = wk.tau[s + j];
+  double* col = U + s + (long long)(s + j) * ldu;
+  double nrm = 0.0;
+  for (int q = lane; q < k; q += 32) {
+    double v = wk.zhat[s + q] / ((dl[q] - dorg) - tau);
+    col[q] = v;
+    nrm += v * v;
+  }
+  nrm = sqrt(warp_sum(nrm));
+  __syncwarp();
+  for (int q = lane; q < k; q += 32) col[q] = col[q] / nrm;
+}
+
+// G(:, jj) = Z(node rows, ndcol(jj)) for the non-deflated columns.
+__global__ void dc_gather_kernel(const Node* nodes, const double* Z, long long ldz, DcWork wk,
+                                 double* G, long long ldg) {
+  const Node nd = nodes[blockIdx.z];
+  const int jj = blockIdx.y;
+  if (jj >= wk.kcnt[blockIdx.z]) return;
+  const int s = nd.s;
+  const int col = wk.ndcol[s + jj];
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nd.nm; r += gridDim.x * blockDim.x)
+    G[(s + r) + (long long)(s + jj) * ldg] = Z[(s + r) + (long long)(s + col) * ldz];
+}
+
+// Rank of each new eigenvalue within its node (stable, O(nm) per element).
+__global__ void dc_rank_kernel(const Node* nodes, DcWork wk) {
+  const Node nd = nodes[blockIdx.y];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nd.nm) return;
+  const int s = nd.s, k = wk.kcnt[blockIdx.y];
+  auto val = [&](int q) { return q < k ? wk.lam[s + q] : wk.defd[s + (q - k)]; };
+  const double v = val(i);
+  int rank = 0;
+  for (int q = 0; q < nd.nm; ++q) {
+    double u = val(q);
+    rank += (u < v) || (u == v && q < i);
+  }
+  wk.rank[s + i] = rank;
+}
+
+// New node block: column rank(q) <- OUT(:, q) (q < k) or Z_old(:, defcol).
+__global__ void dc_assemble_kernel(const Node* nodes, DcWork wk, const double* OUT, long long ldo,
+                                   const double* Zold, long long ldz, double* Znew,
+                                   long long ldn, double* w) {
+  const Node nd = nodes[blockIdx.z];
+  const int q = blockIdx.y;
+  if (q >= nd.nm) return;
+  const int s = nd.s, k = wk.kcnt[blockIdx.z];
+  const int dst = wk.rank[s + q];
+  const double* src = (q < k) ? OUT + s + (long long)(s + q) * ldo
+                              : Zold + s + (long long)(s + wk.defcol[s + (q - k)]) * ldz;
+  double* out = Znew + s + (long long)(s + dst) * ldn;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nd.nm; r += gridDim.x * blockDim.x)
+    out[r] = src[r];
+  if (blockIdx.x == 0 && threadIdx.x == 0)
+    w[s + dst] = (q < k) ? wk.lam[s + q] : wk.defd[s + (q - k)];
+}
+
+// ---------------------------------------------------------------------------
+// 3. Back-transformation: T factor of a block of reflectors (dlarft)
+// ---------------------------------------------------------------------------
+// T(i,i) = tau_i, T(0:i, i) = -tau_i T(0:i, 0:i) G(0:i, i), G = V^T V.
+__global__ void __launch_bounds__(NBB) larft_kernel(const double* G, long long ldg,
+                                                    const double* tau, int jb, double* T,
+                                                    long long ldt) {
+  extern __shared__ double smem_t[];
+  double(*Ts)[NBB + 1] = reinterpret_cast<double(*)[NBB + 1]>(smem_t);
+  __shared__ double col[NBB];
+  const int r = threadIdx.x;
+  for (int c = 0; c < jb; ++c) Ts[r][c] = 0.0;
+  __syncthreads();
+  for (int i = 0; i < jb; ++i) {
+    const double ti = tau[i];
+    if (r < i) col[r] = G[r + (long long)i * ldg];
+    __syncthreads();
+    if (r < i) {
+      double s = 0.0;
+      for (int c = r; c < i; ++c) s += Ts[r][c] * col[c];
+      Ts[r][i] = -ti * s;
+    }
+    if (r == i) Ts[i][i] = ti;
+    __syncthreads();
+  }
+  for (int c = 0; c < jb; ++c)
+    if (r < jb) T[r + (long long)c * ldt] = Ts[r][c];
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Host driver
+// ---------------------------------------------------------------------------
+struct DcBuffers {
+  double* base = nullptr;
+  size_t bytes = 0;
+};
+
+static int sytrd_gpu(imcom_ctx* ctx, DMat& Aw, DMat& Vall, double* d, double* e, double* tau,
+                     double* W, long long ldw, double* ypart, long long ldy, void* accbuf,
+                     long long spin) {
+  const int n = (int)Aw.rows;
+  int dev = ctx->device, coop = 0;
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+  if (!coop) return set_err(ctx, IMCOM_ERR_CUDA, "device lacks cooperative launch");
+  int per_sm = 0;
+  IMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trd_panel_kernel, TRD_THREADS, 0));
+  if (per_sm < 1) return set_err(ctx, IMCOM_ERR_CUDA, "panel kernel does not fit on an SM");
+  int grid = sm_count(ctx);  // one CTA per SM: the cheapest grid barrier
+  TrdAcc* acc = (TrdAcc*)accbuf;
+  GridSync* sync = (GridSync*)((char*)accbuf + 2 * sizeof(TrdAcc) + 64);
+  int* flag = &sync->err;
+  IMC_CUDA(cudaMemsetAsync(sync, 0, sizeof(GridSync), ctx->stream));
+  for (int k = 0; k < n - 1; k += NB) {
+    const int b = std::min(NB, n - 1 - k);
+    IMC_CUDA(cudaMemsetAsync(accbuf, 0, 2 * sizeof(TrdAcc), ctx->stream));
+    TrdArgs a{Aw.p, Aw.ld, Vall.p, Vall.ld, W, ldw, d, e, tau, ypart, ldy, acc, sync, n, k, b,
+              spin};
+    void* args[] = {&a};
+    IMC_CUDA(cudaLaunchCooperativeKernel((void*)trd_panel_kernel, grid, TRD_THREADS, args, 0,
+                                         ctx->stream));
+    IMC_LAUNCH();
+    const int t0 = k + b, rem = n - t0;
+    if (rem > 0) {
+      // A22 -= V W^T + W V^T
+      const double* Vp = Vall.p + t0 + (long long)k * Vall.ld;
+      IMC_TRY(dgemm(ctx, 'N', 'T', rem, rem, b, -1.0, Vp, Vall.ld, W + t0, ldw, 1.0,
+                    Aw.p + t0 + (long long)t0 * Aw.ld, Aw.ld));
+      IMC_TRY(dgemm(ctx, 'N', 'T', rem, rem, b, -1.0, W + t0, ldw, Vp, Vall.ld, 1.0,
+                    Aw.p + t0 + (long long)t0 * Aw.ld, Aw.ld));
+    }
+    // a timed-out barrier ends the factorisation with an error
+    if ((k / NB) % 16 == 15 || k + NB >= n - 1) {
+      int h = 0;
+      IMC_CUDA(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+      IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+      if (h) return set_err(ctx, IMCOM_ERR_EIGEN, "tridiagonalisation grid barrier timed out");
+    }
+  }
+  set_last_diag_kernel<<<1, 1, 0, ctx->stream>>>(Aw.p, Aw.ld, n, d);
+  IMC_LAUNCH();
+  return 0;
+}
+
+int eigen_dc(imcom_ctx* ctx, const DMat& A, DMat& Wout, double* wout) {
+  EigWork* ew = eig_work(ctx);
+  const int n = (int)A.rows;
+  if (n == 1) {
+    IMC_CUDA(cudaMemcpyAsync(wout, A.p, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    double one = 1.0;
+    IMC_CUDA(cudaMemcpyAsync(Wout.p, &one, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+    return 0;
+  }
+  const long long spin = ctx->eig_maxiter > 0 ? ctx->eig_maxiter : 20000000LL;
+  // Buffers: Aw (copy of A, ld), Vall (n x n), Z (ping-pong with Wout), G, U, OUT.
+  IMC_TRY(ensure_mat(ctx, ew->Z, n, n));
+  IMC_TRY(ensure_mat(ctx, ew->V, n, n));
+  DMat& Aw = ew->Z;     // first the working copy of A, later a D&C buffer
+  DMat& Vall = ew->V;   // reflectors; later reused as the GEMM output block
+  const long long ld = Wout.ld;
+  const size_t nn = (size_t)ld * n;
+  // scratch vectors and small matrices in one allocation
+  const long long ldw = pad_ld(n), ldy = pad_ld(n);
+  const long long nch = (n + CW - 1) / CW + 1;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t o = off;
+    off += (bytes + 255) / 256 * 256;
+    return o;
+  };
+  size_t o_d = take(n * 8), o_e = take(n * 8), o_tau = take(n * 8), o_dt = take(n * 8);
+  size_t o_W = take((size_t)ldw * NB * 8), o_y = take((size_t)ldy * nch * 8);
+  size_t o_acc = take(4096);
+  size_t o_split = take((size_t)n * 4), o_nodes = take((size_t)n * sizeof(Node));
+  size_t o_wk = take(((size_t)n * 8 + 16) * 9 + ((size_t)n * 4 + 16) * 8 + ((size_t)n * 24 + 32) +
+                     4096);
+  size_t o_T = take((size_t)NBB * NBB * 8), o_G = take((size_t)NBB * NBB * 8);
+  size_t o_X = take((size_t)NBB * ld * 8 * 2);
+  size_t o_err = take(64);
+  IMC_TRY(eig_buf(ctx, off + 256));
+  char* base = (char*)ew->buf;
+  double* d = (double*)(base + o_d);
+  double* e = (double*)(base + o_e);
+  double* tau = (double*)(base + o_tau);
+  double* dt = (double*)(base + o_dt);
+  double* Wp = (double*)(base + o_W);
+  double* yp = (double*)(base + o_y);
+  int* dsplit = (int*)(base + o_split);
+  Node* dnodes = (Node*)(base + o_nodes);
+  double* Tb = (double*)(base + o_T);
+  double* Gb = (double*)(base + o_G);
+  double* Xb = (double*)(base + o_X);
+  int* derr = (int*)(base + o_err);
+  IMC_CUDA(cudaMemsetAsync(derr, 0, 64, ctx->stream));
+
+  // ---- 1. tridiagonalisation ----
+  stage_begin(ctx, ST_EIG_TRD);
+  IMC_TRY(copy_mat(ctx, A.p, A.ld, Aw.p, Aw.ld, n, n));
+  IMC_CUDA(cudaMemsetAsync(Vall.p, 0, Vall.bytes(), ctx->stream));
+  IMC_CUDA(cudaMemsetAsync(Wp, 0, (size_t)ldw * NB * 8, ctx->stream));
+  IMC_TRY(sytrd_gpu(ctx, Aw, Vall, d, e, tau, Wp, ldw, yp, ldy, base + o_acc, spin));
+  stage_end(ctx, ST_EIG_TRD);
+  stage_begin(ctx, ST_EIG_DC);
+
+  // ---- 2. divide and conquer on (d, e) ----
+  // tree of nodes: split ranges in halves until they hold at most LEAF rows
+  std::vector<std::vector<Node>> levels;
+  levels.push_back({Node{0, n / 2, n}});
+  while (true) {
+    const auto& last = levels.back();
+    if (last[0].nm <= LEAF && std::all_of(last.begin(), last.end(), [](const Node& x) { return x.nm <= LEAF; }))
+      break;
+    std::vector<Node> nxt;
+    for (const Node& x : last) {
+      int l = x.nm / 2, r = x.nm - l;
+      nxt.push_back(Node{x.s, l / 2, l});
+      nxt.push_back(Node{x.s + l, r / 2, r});
+    }
+    levels.push_back(nxt);
+  }
+  std::vector<int> splits;
+  for (size_t L = 0; L + 1 < levels.size(); ++L)
+    for (const Node& x : levels[L]) splits.push_back(x.s + x.n1);
+  IMC_CUDA(cudaMemcpyAsync(dt, d, n * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+  if (!splits.empty()) {
+    IMC_CUDA(cudaMemcpyAsync(dsplit, splits.data(), splits.size() * 4, cudaMemcpyHostToDevice,
+                             ctx->stream));
+    tear_kernel<<<1, 1, 0, ctx->stream>>>(dt, e, dsplit, (int)splits.size());
+    IMC_LAUNCH();
+  }
+  // Z buffers: ZA = Wout, ZB = Aw (the A copy is no longer needed after sytrd...
+  // but Aw holds nothing the back-transformation needs: the reflectors are in Vall)
+  double* ZA = Wout.p;
+  double* ZB = Aw.p;
+  IMC_CUDA(cudaMemsetAsync(ZA, 0, nn * 8, ctx->stream));
+  IMC_CUDA(cudaMemsetAsync(ZB, 0, nn * 8, ctx->stream));
+  // D&C work arrays
+  DcWork wk;
+  {
+    // every array starts on a 16-byte boundary whatever n is
+    char* p = base + o_wk;
+    auto adv = [&](size_t bytes) { p += (bytes + 15) / 16 * 16; };
+    auto dv = [&](void) { double* r = (double*)p; adv((size_t)n * 8); return r; };
+    auto iv = [&](void) { int* r = (int*)p; adv((size_t)n * 4); return r; };
+    wk.ds = dv(); wk.zs = dv(); wk.dl = dv(); wk.zz = dv(); wk.defd = dv(); wk.tau = dv();
+    wk.lam = dv(); wk.zhat = dv();
+    wk.perm = iv(); wk.ndcol = iv(); wk.defcol = iv(); wk.org = iv(); wk.rank = iv();
+    wk.rcs = (double2*)p; adv((size_t)n * 16);
+    wk.rcol = (int2*)p; adv((size_t)n * 8);
+    wk.kcnt = iv(); wk.ndef = iv(); wk.nrot = iv();
+    wk.rho = dv();
+  }
+  double* w = wout;
+  // leaves
+  {
+    const auto& leaves = levels.back();
+    IMC_CUDA(cudaMemcpyAsync(dnodes, leaves.data(), leaves.size() * sizeof(Node),
+                             cudaMemcpyHostToDevice, ctx->stream));
+    leaf_jacobi_kernel<<<(unsigned)leaves.size(), 256, 0, ctx->stream>>>(dnodes, dt, e, w, ZA, ld,
+                                                                         60, derr);
+    IMC_LAUNCH();
+  }
+  // merges, deepest level first
+  double* Zcur = ZA;
+  double* Znxt = ZB;
+  // node blocks of U (k x k), G (gathered columns) and OUT = G U, each n x n
+  DMat& UO = ew->U;
+  IMC_TRY(ensure_mat(ctx, UO, n, 3 * (long long)n));
+  double* Ub = UO.p;
+  double* Gm = UO.p + (size_t)UO.ld * n;
+  double* OUT = UO.p + 2 * (size_t)UO.ld * n;
+  for (int L = (int)levels.size() - 2; L >= 0; --L) {
+    const auto& nodes = levels[L];
+    const int nn_ = (int)nodes.size();
+    int maxnm = 0;
+    for (const Node& x : nodes) maxnm = std::max(maxnm, x.nm);
+    IMC_CUDA(cudaMemcpyAsync(dnodes, nodes.data(), nn_ * sizeof(Node), cudaMemcpyHostToDevice,
+                             ctx->stream));
+    dim3 ge((maxnm + 255) / 256, nn_);
+    dc_prep_kernel<<<ge, 256, 0, ctx->stream>>>(dnodes, w, Zcur, ld, e, wk);
+    IMC_LAUNCH();
+    dc_deflate_kernel<<<nn_, 256, 0, ctx->stream>>>(dnodes, wk);
+    IMC_LAUNCH();
+    dc_rotate_kernel<<<ge, 256, 0, ctx->stream>>>(dnodes, Zcur, ld, wk);
+    IMC_LAUNCH();
+    dim3 gw((maxnm + 7) / 8, nn_);
+    dc_secular_kernel<<<gw, 256, 0, ctx->stream>>>(dnodes, wk, 100, derr);
+    IMC_LAUNCH();
+    dc_zhat_kernel<<<gw, 256, 0, ctx->stream>>>(dnodes, wk, derr);
+    IMC_LAUNCH();
+    dc_vectors_kernel<<<gw, 256, 0, ctx->stream>>>(dnodes, wk, Ub, UO.ld);
+    IMC_LAUNCH();
+    dim3 gg((maxnm + 255) / 256, maxnm, nn_);
+    dc_gather_kernel<<<gg, 256, 0, ctx->stream>>>(dnodes, Zcur, ld, wk, Gm, UO.ld);
+    IMC_LAUNCH();
+    std::vector<int> kh(nn_);
+    IMC_CUDA(cudaMemcpyAsync(kh.data(), wk.kcnt, nn_ * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+    // OUT(node) = G(node) U(node): the new non-deflated eigenvectors
+    for (int b = 0; b < nn_; ++b) {
+      const Node& x = nodes[b];
+      if (kh[b] == 0) continue;
+      IMC_TRY(dgemm(ctx, 'N', 'N', x.nm, kh[b], kh[b], 1.0, Gm + x.s + (size_t)x.s * UO.ld,
+                    UO.ld, Ub + x.s + (size_t)x.s * UO.ld, UO.ld, 0.0,
+                    OUT + x.s + (size_t)x.s * UO.ld, UO.ld));
+    }
+    dc_rank_kernel<<<ge, 256, 0, ctx->stream>>>(dnodes, wk);
+    IMC_LAUNCH();
+    // Znxt(node) = [OUT | rotated deflated columns of Zcur] in eigenvalue order
+    dim3 ga((maxnm + 255) / 256, maxnm, nn_);
+    dc_assemble_kernel<<<ga, 256, 0, ctx->stream>>>(dnodes, wk, OUT, UO.ld, Zcur, ld, Znxt, ld, w);
+    IMC_LAUNCH();
+    std::swap(Zcur, Znxt);
+  }
+  {
+    int h = 0;
+    IMC_CUDA(cudaMemcpyAsync(&h, derr, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (h) return set_err(ctx, IMCOM_ERR_EIGEN, "divide and conquer did not converge (flags %d)", h);
+  }
+
+  stage_end(ctx, ST_EIG_DC);
+  // ---- 3. back-transformation Z <- Q_T Z (Q_T = H_0 H_1 ... H_{n-2}) ----
+  stage_begin(ctx, ST_EIG_BT);
+  const int nref = n - 1;
+  const int nblk = (nref + NBB - 1) / NBB;
+  IMC_CUDA(cudaFuncSetAttribute(larft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)LARFT_SMEM));
+  double* X = Xb;
+  double* X2 = Xb + (size_t)NBB * ld;
+  for (int bi = nblk - 1; bi >= 0; --bi) {
+    const int j0 = bi * NBB, jb = std::min(NBB, nref - j0);
+    // rows from j0: row j0 of the block's reflectors is zero, and an even
+    // first row keeps the GEMM operands 16-byte aligned
+    const int r0 = j0, K = n - r0;
+    const double* Vb = Vall.p + r0 + (size_t)j0 * Vall.ld;
+    IMC_TRY(dgemm(ctx, 'T', 'N', jb, jb, K, 1.0, Vb, Vall.ld, Vb, Vall.ld, 0.0, Gb, NBB));
+    larft_kernel<<<1, NBB, LARFT_SMEM, ctx->stream>>>(Gb, NBB, tau + j0, jb, Tb, NBB);
+    IMC_LAUNCH();
+    IMC_TRY(dgemm(ctx, 'T', 'N', jb, n, K, 1.0, Vb, Vall.ld, Zcur + r0, ld, 0.0, X, NBB));
+    IMC_TRY(dgemm(ctx, 'N', 'N', jb, n, jb, 1.0, Tb, NBB, X, NBB, 0.0, X2, NBB));
+    IMC_TRY(dgemm(ctx, 'N', 'N', K, n, jb, -1.0, Vb, Vall.ld, X2, NBB, 1.0, Zcur + r0, ld));
+  }
+  if (Zcur != Wout.p) IMC_TRY(copy_mat(ctx, Zcur, ld, Wout.p, Wout.ld, n, n));
+  stage_end(ctx, ST_EIG_BT);
+  return 0;
 }
 
 int eigen_jacobi(imcom_ctx* ctx, const DMat& A, DMat& W, double* w) {

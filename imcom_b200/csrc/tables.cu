@@ -299,8 +299,9 @@ extern "C" int imcom_gpu_psf_spectra(imcom_ctx* ctx, int npoly_in, double* C_out
   size_t ps2 = (size_t)nps * nps;
   int nh = nps / 2 + 1;
   // scratch: real inputs (E+1) ps2 | half spectra (E+1) nh nps | sums
-  size_t real_b = (E + 1) * ps2 * sizeof(double);
-  size_t half_b = (size_t)(E + 1) * nh * nps * sizeof(double2);
+  // each region starts on a 256-byte boundary (complex data needs 16 bytes)
+  size_t real_b = ((E + 1) * ps2 * sizeof(double) + 255) / 256 * 256;
+  size_t half_b = ((size_t)(E + 1) * nh * nps * sizeof(double2) + 255) / 256 * 256;
   size_t need = real_b + half_b + 8192;
   stage_begin(ctx, ST_SPECTRA);
   IMC_TRY(ensure_buf(ctx, (void**)&ctx->fftbuf, ctx->fftbuf_bytes, need));

@@ -192,8 +192,9 @@ int imcom_gpu_launch_count(imcom_ctx* ctx, long long* count);
 int imcom_gpu_get_stream(imcom_ctx* ctx, void** stream);
 /* Milliseconds spent on the GPU by the last call of each stage (CUDA
  * events): [spectra, build_A, eigen_A, build_B, build_P, bisect, build_T,
- * epilogue]. */
-int imcom_gpu_stage_times(imcom_ctx* ctx, double* ms8);
+ * epilogue, eigen tridiagonalisation, eigen divide and conquer, eigen
+ * back-transformation] (11 values). */
+int imcom_gpu_stage_times(imcom_ctx* ctx, double* ms11);
 
 #ifdef __cplusplus
 }

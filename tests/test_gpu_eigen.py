@@ -1,0 +1,59 @@
+"""The own FP64 eigensolver (tridiagonalisation + divide and conquer +
+back-transformation) on matrices with IMCOM-like spectra: decades of decay,
+near-degenerate clusters, exact multiplicities and tiny sizes.  Reference:
+LAPACK through numpy; parity bars as for imcom_eigen_A: eigenvalues within
+1e-12 * lambda_max, orthonormal vectors, residual ||AQ - QL|| <= 1e-12 ||A||."""
+import numpy as np
+import pytest
+
+from imcom_b200 import EIGH_DC, EIGH_LIBRARY
+
+pytestmark = pytest.mark.gpu
+
+
+def spectrum_matrix(n, kind, seed):
+    rng = np.random.default_rng(seed)
+    Q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    if kind == "decay":
+        lam = np.logspace(-1, -16, n)
+    elif kind == "cluster":
+        lam = np.concatenate([np.logspace(-1, -13, n - n // 2),
+                              1e-3 * (1 + 1e-13 * rng.standard_normal(n // 2))])
+    elif kind == "multiple":
+        lam = np.repeat(rng.random(max(1, n // 8)), 8)[:n]
+        lam = np.concatenate([lam, np.ones(n - len(lam))])
+    else:
+        lam = rng.standard_normal(n)
+    A = (Q * lam) @ Q.T
+    return np.asfortranarray(0.5 * (A + A.T))
+
+
+def run_eigen(solver, A, mode):
+    n = A.shape[0]
+    x = np.arange(n, dtype=float)
+    solver.set_inputs(x, x, np.ones(n, dtype=np.int32), x[:1], x[:1], None, None, 1.0, 1.0)
+    solver.set_eigensolver(mode)
+    solver.load_A(A)
+    return solver.eigen_A()
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 31, 33, 72, 257, 1000])
+@pytest.mark.parametrize("kind", ["decay", "cluster", "multiple", "random"])
+def test_eigen_dc(solver, n, kind):
+    A = spectrum_matrix(n, kind, seed=n)
+    Q, L, cond = run_eigen(solver, A, EIGH_DC)
+    ref = np.linalg.eigvalsh(A)[::-1]
+    scale = max(np.abs(ref).max(), 1e-300)
+    assert np.all(np.diff(L) <= 0)
+    assert np.max(np.abs(L - ref)) < 1e-12 * scale
+    assert np.max(np.abs(Q.T @ Q - np.eye(n))) < 1e-12
+    assert np.max(np.abs(A @ Q - Q * L)) < 1e-12 * scale
+
+
+def test_eigen_dc_matches_library_n2048(solver):
+    A = spectrum_matrix(2048, "cluster", seed=7)
+    Q1, L1, _ = run_eigen(solver, A, EIGH_DC)
+    Q2, L2, _ = run_eigen(solver, A, EIGH_LIBRARY)
+    assert np.max(np.abs(L1 - L2)) < 1e-12 * L2.max()
+    assert np.max(np.abs(A @ Q1 - Q1 * L1)) < 1e-12 * L2.max()
+    assert np.max(np.abs(Q1.T @ Q1 - np.eye(2048))) < 1e-12

@@ -9,7 +9,7 @@ import sys
 import numpy as np
 import pytest
 
-from imcom_b200 import EIGH_LIBRARY, EPS, synth
+from imcom_b200 import EIGH_DC, EIGH_LIBRARY, EPS, synth
 from oracle import oracle as O
 
 sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
@@ -17,7 +17,7 @@ import make_golden  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
-EIG_MODE = int(os.environ.get("IMCOM_TEST_EIGH", EIGH_LIBRARY))
+EIG_MODE = int(os.environ.get("IMCOM_TEST_EIGH", EIGH_DC))
 
 
 def rel(a, b):
