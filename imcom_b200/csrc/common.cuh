@@ -77,8 +77,8 @@ struct imcom_ctx {
   size_t tables_bytes = 0;
   double2* fftbuf = nullptr;
   size_t fftbuf_bytes = 0;
-  cufftHandle plan_big = 0;
-  int plan_big_L = 0, plan_big_batch = 0;
+  cufftHandle plan_big[2] = {0, 0};  // [0] A tables, [1] B tables
+  int plan_big_L[2] = {0, 0}, plan_big_batch[2] = {0, 0};
   cufftHandle plan_r2c = 0;
   int plan_r2c_n = 0, plan_r2c_batch = 0;
 

@@ -174,7 +174,8 @@ int imcom_gpu_destroy(imcom_ctx* ctx) {
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete[] ctx->rot;
-  if (ctx->plan_big) cufftDestroy(ctx->plan_big);
+  for (int q = 0; q < 2; ++q)
+    if (ctx->plan_big[q]) cufftDestroy(ctx->plan_big[q]);
   if (ctx->plan_r2c) cufftDestroy(ctx->plan_r2c);
   for (int s = 0; s < ST_N; ++s) {
     if (ctx->ev0[s]) cudaEventDestroy(ctx->ev0[s]);

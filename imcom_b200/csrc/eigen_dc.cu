@@ -38,8 +38,8 @@ namespace imcom {
 namespace {
 
 constexpr int NB = 32;            // tridiagonalisation panel width
-constexpr int TRD_THREADS = 256;  // threads per CTA of the panel kernel
-constexpr int CW = 256;           // columns per symv tile
+constexpr int TRD_THREADS = 512;  // threads per CTA of the panel kernel
+constexpr int CW = 16;            // columns per symv tile
 constexpr int LEAF = 32;          // largest leaf of the divide-and-conquer tree
 constexpr int NBB = 128;          // reflectors per back-transformation block
 constexpr double EPS = 1.1102230246251565e-16;
@@ -61,42 +61,41 @@ __device__ __forceinline__ double ld_cg(const double* p) {
 // Bounded grid barrier (cooperative launch guarantees co-residency).
 // ---------------------------------------------------------------------------
 struct GridSync {
-  unsigned count;
-  unsigned gen;
+  unsigned count;  // arrivals so far (monotonic; one barrier = gridDim.x arrivals)
+  unsigned pad0;
   int err;
-  int pad;
+  int pad1;
 };
 
+// Arrive with a release add, wait with acquire loads until every CTA of this
+// barrier generation has arrived.  The wait gives up after `limit` polls and
+// sets the error word instead of spinning forever.
 __device__ __forceinline__ bool grid_barrier(GridSync* s, long long limit) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned* vgen = &s->gen;
-    unsigned g = *vgen;
-    __threadfence();
-    unsigned arrived = atomicAdd(&s->count, 1u) + 1u;
+    const unsigned nb = gridDim.x;
+    unsigned old;
+    asm volatile("atom.add.release.gpu.u32 %0, [%1], 1;" : "=r"(old) : "l"(&s->count) : "memory");
+    const unsigned target = (old / nb + 1) * nb;
     int ok = 1;
-    if (arrived == gridDim.x) {
-      atomicExch(&s->count, 0u);
-      __threadfence();
-      atomicAdd(&s->gen, 1u);
-    } else {
-      long long it = 0;
-      volatile int* verr = &s->err;
-      while (*vgen == g) {
-        if (*verr) {
+    long long it = 0;
+    while (true) {
+      unsigned cur;
+      asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(cur) : "l"(&s->count) : "memory");
+      if ((int)(cur - target) >= 0) break;
+      if ((++it & 31) == 0) {
+        if (*(volatile int*)&s->err) {
           ok = 0;
           break;
         }
-        if (++it > limit) {
+        if (it > limit) {
           atomicExch(&s->err, 1);
           ok = 0;
           break;
         }
       }
     }
-    __threadfence();
-    if (*(volatile int*)&s->err) ok = 0;
     s_ok = ok;
   }
   __syncthreads();
@@ -107,9 +106,10 @@ __device__ __forceinline__ bool grid_barrier(GridSync* s, long long limit) {
 // 1. Tridiagonalisation
 // ---------------------------------------------------------------------------
 struct TrdAcc {
-  double pq[2 * NB];  // p = W^T v (0..NB-1), q = V^T v (NB..2NB-1)
-  double vty0;        // v^T y0
-  double nrm;         // squared norm of the next column below its subdiagonal
+  double SW[NB];  // sum_{r >= j+2} A(r, j) W(r, p) for the column j this parity serves
+  double SV[NB];  // sum_{r >= j+2} A(r, j) V(r, p)
+  double vty0;    // v^T y0
+  double nrm;     // squared norm of the column below its subdiagonal
 };
 
 struct TrdArgs {
@@ -130,14 +130,15 @@ struct TrdArgs {
 
 __global__ void __launch_bounds__(TRD_THREADS) trd_panel_kernel(TrdArgs a) {
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int WPB = TRD_THREADS / 32;
+  constexpr int WPB = TRD_THREADS / 32;
   const long long gw = (long long)blockIdx.x * WPB + wib;
   const long long GW = (long long)gridDim.x * WPB;
   const int n = a.n, k = a.k;
   double* A = a.A;
   const long long lda = a.lda, ldv = a.ldv, ldw = a.ldw;
-  __shared__ double s_pq[2 * NB];
-  __shared__ double s_rowV[NB], s_rowW[NB];
+  __shared__ double s_pq[2 * NB];            // p = W^T v, q = V^T v of the current column
+  __shared__ double s_rowV[NB], s_rowW[NB];  // row j+1 of V and W
+  __shared__ double sm_y[WPB][32], sm_c[WPB][32], sm_u[WPB][32];
   if (*(volatile int*)&a.sync->err) return;  // an earlier panel failed
 
   // Column k: d(k) and the norm of A(k+2:n, k).
@@ -156,8 +157,8 @@ __global__ void __launch_bounds__(TRD_THREADS) trd_panel_kernel(TrdArgs a) {
     TrdAcc* cur = a.acc + par;
     TrdAcc* nxt = a.acc + (par ^ 1);
     // Householder reflector of x = A(j+1:n, j) (LAPACK dlarfg)
-    const double alpha = ld_cg(A + (j + 1) + j * lda);
-    const double xn2 = ld_cg(&cur->nrm);
+    const double alpha = __ldcg(A + (j + 1) + (long long)j * lda);
+    const double xn2 = __ldcg(&cur->nrm);
     double beta, t, scl;
     if (xn2 == 0.0) {
       t = 0.0;
@@ -174,114 +175,168 @@ __global__ void __launch_bounds__(TRD_THREADS) trd_panel_kernel(TrdArgs a) {
     }
     if (blockIdx.x == 0 && threadIdx.x < 2 * NB + 2) {
       // clear the other parity's accumulators (last read one phase ago)
-      if (threadIdx.x < 2 * NB) nxt->pq[threadIdx.x] = 0.0;
+      if (threadIdx.x < NB) nxt->SW[threadIdx.x] = 0.0;
+      else if (threadIdx.x < 2 * NB) nxt->SV[threadIdx.x - NB] = 0.0;
       else if (threadIdx.x == 2 * NB) nxt->vty0 = 0.0;
       else nxt->nrm = 0.0;
     }
-    const double* colj = A + j * lda;
-    auto vcol = [&](long long c) -> double {
-      return (c == j + 1) ? 1.0 : ld_cg(colj + c) * scl;
+    // Row j+1 of V and W, and p = W^T v = W(j+1, :) + scl * SW, q = V^T v
+    // likewise (sums from the previous column's phase B).
+    if (wib == 0 && lane < i) {
+      const double wr1 = __ldcg(a.W + (j + 1) + lane * ldw);
+      const double vr1 = __ldcg(a.V + (j + 1) + (k + lane) * ldv);
+      s_rowW[lane] = wr1;
+      s_rowV[lane] = vr1;
+      s_pq[lane] = wr1 + scl * __ldcg(&cur->SW[lane]);
+      s_pq[NB + lane] = vr1 + scl * __ldcg(&cur->SV[lane]);
+    }
+    const double* colj = A + (long long)j * lda;
+    // v(r): 0 above row j+1, 1 at j+1, A(r, j) * scl below
+    auto vrow = [&](long long r) -> double {
+      return (r <= j || r >= n) ? 0.0 : (r == j + 1 ? 1.0 : __ldcg(colj + r) * scl);
     };
+    // rows handled in pairs from an even base row so the loads are 16-byte
+    const long long rbase = (j + 1) & ~1LL;
+    const long long R = n - (j + 1);
+    const long long RB = (n - rbase + 63) / 64, NC = (R + CW - 1) / CW;
 
-    // ---- phase A: y0 = A22 v by 32-row x CW-column tiles ----
-    const long long R = n - j - 1;
-    const long long RB = (R + 31) / 32, NC = (R + CW - 1) / CW;
+    // ---- phase A: y0 = A22 v by 64-row x CW-column tiles; every load of a
+    // tile is issued before the first use ----
     for (long long tile = gw; tile < RB * NC; tile += GW) {
       const long long rb = tile % RB, ch = tile / RB;
-      const long long r = j + 1 + rb * 32 + lane;
+      const long long r = rbase + rb * 64 + 2 * lane;
       const long long c0 = j + 1 + ch * CW, c1 = min((long long)n, c0 + CW);
-      double acc = 0.0;
-      if (r < n) {
-        const double* Ar = A + r;
-        long long c = c0;
-        for (; c + 8 <= c1; c += 8) {
-          double av[8], vv[8];
+      const long long cl = c0 + lane;
+      const double vreg = (cl < c1) ? vrow(cl) : 0.0;
+      const double v0 = vrow(r), v1 = vrow(r + 1);
+      const bool pair = (r + 1 < n), single = (r < n);
+      const double* Ar = A + r;
+      double2 av[CW];
 #pragma unroll
-          for (int u = 0; u < 8; ++u) {
-            av[u] = Ar[(c + u) * lda];
-            vv[u] = vcol(c + u);
-          }
-#pragma unroll
-          for (int u = 0; u < 8; ++u) acc = fma(av[u], vv[u], acc);
+      for (int u = 0; u < CW; ++u) {
+        const long long c = c0 + u;
+        av[u] = make_double2(0.0, 0.0);
+        if (c < c1) {
+          if (pair) av[u] = *reinterpret_cast<const double2*>(Ar + c * lda);
+          else if (single) av[u].x = Ar[c * lda];
         }
-        for (; c < c1; ++c) acc = fma(Ar[c * lda], vcol(c), acc);
-        a.ypart[ch * a.ldy + r] = acc;
       }
-      const double vr = (r < n) ? vcol(r) : 0.0;
-      double s = warp_sum(vr * acc);
+      double acc0 = 0.0, acc1 = 0.0;
+#pragma unroll
+      for (int u = 0; u < CW; ++u) {
+        const double vc = __shfl_sync(0xffffffffu, vreg, u);
+        acc0 = fma(av[u].x, vc, acc0);
+        acc1 = fma(av[u].y, vc, acc1);
+      }
+      if (r >= j + 1 && r < n) a.ypart[ch * a.ldy + r] = acc0;
+      if (r + 1 >= j + 1 && r + 1 < n) a.ypart[ch * a.ldy + r + 1] = acc1;
+      double s = warp_sum(v0 * acc0 + v1 * acc1);
       if (lane == 0) atomicAdd(&cur->vty0, s);
-      if (ch == 0) {
-        for (int p = 0; p < i; ++p) {
-          double wv = (r < n) ? ld_cg(a.W + r + p * ldw) * vr : 0.0;
-          double vv = (r < n) ? ld_cg(a.V + r + (k + p) * ldv) * vr : 0.0;
-          wv = warp_sum(wv);
-          vv = warp_sum(vv);
-          if (lane == 0) {
-            atomicAdd(&cur->pq[p], wv);
-            atomicAdd(&cur->pq[NB + p], vv);
-          }
-        }
-      }
     }
     if (!grid_barrier(a.sync, a.spin)) return;
 
-    // ---- phase B: w, the next column and its norm ----
-    if (threadIdx.x < 2 * NB) {
-      int p = threadIdx.x % NB;
-      s_pq[threadIdx.x] = (p < i) ? ld_cg(&cur->pq[threadIdx.x]) : 0.0;
-    }
-    __syncthreads();
-    double qp = 0.0;
-    for (int p = 0; p < i; ++p) qp += s_pq[NB + p] * s_pq[p];
-    const double vty = ld_cg(&cur->vty0) - 2.0 * qp;
-    const double alpha2 = -0.5 * t * t * vty;
+    // ---- phase B: w, the next column, its norm and dot products ----
     const bool next = (i + 1 < a.b);
-    if (next) {
-      if (wib == 0) {
-        // w(j+1) for row j+1 of the panel (every CTA needs it)
-        double y = 0.0;
-        for (long long ch = lane; ch < NC; ch += 32) y += ld_cg(a.ypart + ch * a.ldy + (j + 1));
-        y = warp_sum(y);
-        double corr = 0.0;
-        for (int p = lane; p < i; p += 32)
-          corr += ld_cg(a.V + (j + 1) + (k + p) * ldv) * s_pq[p] +
-                  ld_cg(a.W + (j + 1) + p * ldw) * s_pq[NB + p];
-        corr = warp_sum(corr);
-        const double wj1 = t * (y - corr) + alpha2;
-        if (lane <= i) {
-          s_rowV[lane] = (lane < i) ? ld_cg(a.V + (j + 1) + (k + lane) * ldv) : 1.0;
-          s_rowW[lane] = (lane < i) ? ld_cg(a.W + (j + 1) + lane * ldw) : wj1;
+    double alpha2 = 0.0;
+    bool have_w1 = false;
+    // one 32-row block per CTA at a time; the warps split the chunk partials
+    // and the panel columns, then reduce through shared memory
+    for (long long rb = blockIdx.x; j + 1 + rb * 32 < n; rb += gridDim.x) {
+      const long long r = j + 1 + rb * 32 + lane;
+      const bool valid = r < n;
+      // issue every load of the row block first
+      double ys = 0.0, vp[2] = {0.0, 0.0}, wp[2] = {0.0, 0.0};
+      double vr = 0.0, aold = 0.0;
+      const double vty0 = __ldcg(&cur->vty0);
+      if (valid) {
+#pragma unroll 8
+        for (long long ch = wib; ch < NC; ch += WPB) ys += __ldcg(a.ypart + ch * a.ldy + r);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int p = wib + WPB * h;
+          if (p < i) {
+            vp[h] = __ldcg(a.V + r + (k + p) * ldv);
+            wp[h] = __ldcg(a.W + r + p * ldw);
+          }
+        }
+        vr = vrow(r);
+        if (next) aold = __ldcg(A + r + (long long)(j + 1) * lda);
+      }
+      if (!have_w1) {
+        double qp = 0.0;
+        for (int p = 0; p < i; ++p) qp += s_pq[NB + p] * s_pq[p];
+        alpha2 = -0.5 * t * t * (vty0 - 2.0 * qp);
+        if (next && wib == 0) {
+          // w(j+1) (the new entry of row j+1 of W)
+          double y = 0.0;
+#pragma unroll 8
+          for (long long ch = lane; ch < NC; ch += 32) y += __ldcg(a.ypart + ch * a.ldy + (j + 1));
+          y = warp_sum(y);
+          double corr = (lane < i) ? s_rowV[lane] * s_pq[lane] + s_rowW[lane] * s_pq[NB + lane] : 0.0;
+          corr = warp_sum(corr);
+          if (lane == 0) {
+            s_rowW[i] = t * (y - corr) + alpha2;
+            s_rowV[i] = 1.0;
+          }
+        }
+        have_w1 = true;
+      }
+      double cs = 0.0, us = 0.0;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int p = wib + WPB * h;
+        if (p < i) {
+          cs += vp[h] * s_pq[p] + wp[h] * s_pq[NB + p];
+          us += vp[h] * s_rowW[p] + wp[h] * s_rowV[p];
+        }
+      }
+      sm_y[wib][lane] = ys;
+      sm_c[wib][lane] = cs;
+      sm_u[wib][lane] = us;
+      __syncthreads();
+      double y0 = 0.0, corr = 0.0, upd = 0.0;
+#pragma unroll
+      for (int w = 0; w < WPB; ++w) {
+        y0 += sm_y[w][lane];
+        corr += sm_c[w][lane];
+        upd += sm_u[w][lane];
+      }
+      const double wr = t * (y0 - corr) + alpha2 * vr;
+      if (valid && wib == 0) {
+        a.V[r + (long long)j * ldv] = vr;
+        a.W[r + i * ldw] = wr;
+      }
+      if (next) {
+        double anew = 0.0;
+        if (valid) {
+          upd += vr * s_rowW[i] + wr * s_rowV[i];
+          anew = aold - upd;
+          if (wib == 0) {
+            A[r + (long long)(j + 1) * lda] = anew;
+            if (r == j + 1) a.d[j + 1] = anew;
+          }
+        }
+        // column j+1's dot products with W, V over rows >= j+3 and its norm
+        const double am = (valid && r >= j + 3) ? anew : 0.0;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int p = wib + WPB * h;
+          if (p <= i) {
+            const double wv = (p == i) ? wr : wp[h];
+            const double vv = (p == i) ? vr : vp[h];
+            const double sw = warp_sum(am * wv), sv = warp_sum(am * vv);
+            if (lane == 0) {
+              atomicAdd(&nxt->SW[p], sw);
+              atomicAdd(&nxt->SV[p], sv);
+            }
+          }
+        }
+        if (wib == 0) {
+          const double nr = warp_sum(am * am);
+          if (lane == 0) atomicAdd(&nxt->nrm, nr);
         }
       }
       __syncthreads();
-    }
-    for (long long r0 = j + 1 + gw * 32; r0 < n; r0 += GW * 32) {
-      const long long r = r0 + lane;
-      double nrm = 0.0;
-      if (r < n) {
-        double y0 = 0.0;
-        for (long long ch = 0; ch < NC; ++ch) y0 += ld_cg(a.ypart + ch * a.ldy + r);
-        const double vr = vcol(r);
-        double corr = 0.0;
-        for (int p = 0; p < i; ++p)
-          corr += ld_cg(a.V + r + (k + p) * ldv) * s_pq[p] + ld_cg(a.W + r + p * ldw) * s_pq[NB + p];
-        const double wr = t * (y0 - corr) + alpha2 * vr;
-        a.V[r + j * ldv] = vr;
-        a.W[r + i * ldw] = wr;
-        if (next) {
-          double upd = vr * s_rowW[i] + wr * s_rowV[i];
-          for (int p = 0; p < i; ++p)
-            upd += ld_cg(a.V + r + (k + p) * ldv) * s_rowW[p] + ld_cg(a.W + r + p * ldw) * s_rowV[p];
-          const double anew = ld_cg(A + r + (j + 1) * lda) - upd;
-          A[r + (j + 1) * lda] = anew;
-          if (r == j + 1) a.d[j + 1] = anew;
-          if (r >= j + 3) nrm = anew * anew;
-        }
-      }
-      if (next) {
-        nrm = warp_sum(nrm);
-        if (lane == 0) atomicAdd(&nxt->nrm, nrm);
-      }
     }
     if (!grid_barrier(a.sync, a.spin)) return;
   }
@@ -816,6 +871,7 @@ static int sytrd_gpu(imcom_ctx* ctx, DMat& Aw, DMat& Vall, double* d, double* e,
   for (int k = 0; k < n - 1; k += NB) {
     const int b = std::min(NB, n - 1 - k);
     IMC_CUDA(cudaMemsetAsync(accbuf, 0, 2 * sizeof(TrdAcc), ctx->stream));
+    static_assert(2 * sizeof(TrdAcc) + 64 + sizeof(GridSync) <= 4096, "panel scratch");
     TrdArgs a{Aw.p, Aw.ld, Vall.p, Vall.ld, W, ldw, d, e, tau, ypart, ldy, acc, sync, n, k, b,
               spin};
     void* args[] = {&a};

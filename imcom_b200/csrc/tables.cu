@@ -262,20 +262,22 @@ int build_tables(imcom_ctx* ctx, int npad, int isB) {
                                          big2 * ntab * sizeof(double2));
   IMC_CUDA(cudaMemcpyAsync(dpairs, pairs.data(), ntab * sizeof(int2), cudaMemcpyHostToDevice,
                            ctx->stream));
-  if (!ctx->plan_big || ctx->plan_big_L != nbig || ctx->plan_big_batch != ntab) {
-    if (ctx->plan_big) cufftDestroy(ctx->plan_big);
-    ctx->plan_big = 0;
+  // one cached plan per table kind (the A and B passes have different batches)
+  cufftHandle& plan = ctx->plan_big[isB ? 1 : 0];
+  if (!plan || ctx->plan_big_L[isB] != nbig || ctx->plan_big_batch[isB] != ntab) {
+    if (plan) cufftDestroy(plan);
+    plan = 0;
     int dims[2] = {nbig, nbig};
-    IMC_CUFFT(cufftPlanMany(&ctx->plan_big, 2, dims, nullptr, 1, (int)big2, nullptr, 1,
-                            (int)big2, CUFFT_Z2Z, ntab));
-    ctx->plan_big_L = nbig;
-    ctx->plan_big_batch = ntab;
+    IMC_CUFFT(cufftPlanMany(&plan, 2, dims, nullptr, 1, (int)big2, nullptr, 1, (int)big2,
+                            CUFFT_Z2Z, ntab));
+    ctx->plan_big_L[isB] = nbig;
+    ctx->plan_big_batch[isB] = ntab;
   }
-  IMC_CUFFT(cufftSetStream(ctx->plan_big, ctx->stream));
+  IMC_CUFFT(cufftSetStream(plan, ctx->stream));
   dim3 blk(128), grd((nbig + 127) / 128, nbig, ntab);
   embed_kernel<<<grd, blk, 0, ctx->stream>>>(ctx->Gt, ctx->Gammat, dpairs, ctx->fftbuf, nps, nbig);
   IMC_LAUNCH();
-  IMC_CUFFT(cufftExecZ2Z(ctx->plan_big, (cufftDoubleComplex*)ctx->fftbuf,
+  IMC_CUFFT(cufftExecZ2Z(plan, (cufftDoubleComplex*)ctx->fftbuf,
                          (cufftDoubleComplex*)ctx->fftbuf, CUFFT_INVERSE));
   shift_scale_kernel<<<grd, blk, 0, ctx->stream>>>(ctx->fftbuf, ctx->tables, nbig, nps, isB);
   IMC_LAUNCH();
