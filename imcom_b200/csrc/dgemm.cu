@@ -16,7 +16,6 @@
 #include "common.cuh"
 
 namespace imcom {
-namespace {
 
 constexpr int BM = 128, BN = 128, BK = 16, STAGES = 3, THREADS = 256;
 constexpr int SKC = BK + 4;   // stride of a k-contiguous tile row
@@ -225,8 +224,6 @@ int launch(imcom_ctx* ctx, long long M, long long N, long long K, double alpha, 
   return 0;
 }
 
-}  // namespace
-
 int dgemm(imcom_ctx* ctx, char transA, char transB, long long M, long long N, long long K,
           double alpha, const double* A, long long lda, const double* B, long long ldb,
           double beta, double* C, long long ldc) {
@@ -247,3 +244,97 @@ int dgemm(imcom_ctx* ctx, char transA, char transB, long long M, long long N, lo
 }
 
 }  // namespace imcom
+
+// ---------------------------------------------------------------------------
+// Allocation-free P = Q^T B for callers that must not allocate device memory.
+//
+// The split-K partial sums live in this fixed array instead of a cudaMalloc'd
+// buffer.  It is 32 MiB, allocated when the module loads and held by every
+// GPU that loads the library until the process exits.  Host code may not use
+// the array's name as a device address; the first call on each device looks
+// the address up with cudaGetSymbolAddress (and sets the kernel's shared-
+// memory limit), so that first call should come before any stream capture.
+// Each call writes every partial-sum element it later reads, so nothing needs
+// clearing between calls; calls whose GPU work overlaps (different streams or
+// threads) share the array and race.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr long long kNoAllocDoubles = 4LL * 1024 * 1024;  // 32 MiB of partial sums
+constexpr int kNoAllocSplits = 2;                         // K slices per call
+}  // namespace
+
+static __device__ __align__(256) double g_noalloc_partials[kNoAllocDoubles];
+
+#include <mutex>
+
+namespace {
+std::mutex g_noalloc_mu;
+double* g_noalloc_addr[64] = {};
+
+int noalloc_setup(int dev, double** out) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess || !p) {
+      cudaGetLastError();
+      return IMCOM_ERR_CUDA;
+    }
+    auto k2 = imcom::dgemm_kernel<true, true, 2>;
+    auto k1 = imcom::dgemm_kernel<true, true, 1>;
+    if (cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)imcom::SMEM_BYTES) != cudaSuccess ||
+        cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)imcom::SMEM_BYTES) != cudaSuccess) {
+      cudaGetLastError();
+      return IMCOM_ERR_CUDA;
+    }
+    g_noalloc_addr[dev] = (double*)p;
+  }
+  *out = g_noalloc_addr[dev];
+  return 0;
+}
+}  // namespace
+
+extern "C" int imcom_gpu_build_P_noalloc(const double* dQ, long long ldq, const double* dB,
+                                         long long ldb, double* dP, long long ldp, int n, int m,
+                                         void* stream) {
+  if (!dQ) return -1;
+  if (ldq < n || ldq < 1) return -2;
+  if (!dB) return -3;
+  if (ldb < n || ldb < 1) return -4;
+  if (!dP) return -5;
+  if (ldp < n || ldp < 1) return -6;
+  if (n <= 0) return -7;
+  if (m <= 0) return -8;
+  const long long ldo = imcom::pad_ld(n);
+  if ((long long)kNoAllocSplits * ldo * (long long)m > kNoAllocDoubles)
+    return IMCOM_ERR_NOALLOC_SIZE;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return IMCOM_ERR_CUDA;
+  }
+  double* part = nullptr;
+  int st = noalloc_setup(dev, &part);
+  if (st) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  const long long gm = (n + imcom::BM - 1) / imcom::BM, gn = (m + imcom::BN - 1) / imcom::BN;
+  long long kchunk = ((long long)n + kNoAllocSplits - 1) / kNoAllocSplits;
+  kchunk = (kchunk + imcom::BK - 1) / imcom::BK * imcom::BK;
+  const int splits = (int)std::max<long long>(1, (n + kchunk - 1) / kchunk);
+  dim3 grd((unsigned)gm, (unsigned)gn, (unsigned)splits);
+  auto al16 = [](const void* p) { return ((uintptr_t)p & 15) == 0; };
+  if (al16(dQ) && al16(dB) && ldq % 2 == 0 && ldb % 2 == 0)
+    imcom::dgemm_kernel<true, true, 2><<<grd, imcom::THREADS, imcom::SMEM_BYTES, s>>>(
+        n, m, n, 1.0, dQ, ldq, dB, ldb, 0.0, part, ldo, kchunk);
+  else
+    imcom::dgemm_kernel<true, true, 1><<<grd, imcom::THREADS, imcom::SMEM_BYTES, s>>>(
+        n, m, n, 1.0, dQ, ldq, dB, ldb, 0.0, part, ldo, kchunk);
+  __atomic_fetch_add(&imcom::g_launches, 1ULL, __ATOMIC_RELAXED);
+  if (cudaGetLastError() != cudaSuccess) return IMCOM_ERR_CUDA;
+  dim3 g2((unsigned)std::min<long long>((n + 255) / 256, 64), (unsigned)m);
+  imcom::splitk_reduce_kernel<<<g2, 256, 0, s>>>(part, ldo, splits, n, m, 1.0, 0.0, dP, ldp);
+  __atomic_fetch_add(&imcom::g_launches, 1ULL, __ATOMIC_RELAXED);
+  if (cudaGetLastError() != cudaSuccess) return IMCOM_ERR_CUDA;
+  return 0;
+}

@@ -43,6 +43,7 @@ typedef struct imcom_ctx imcom_ctx;
 #define IMCOM_ERR_EIGEN 5       /* eigensolver did not converge (DSYEVR info) */
 #define IMCOM_ERR_ALLOC 6       /* device allocation failed                   */
 #define IMCOM_ERR_NOT_FINITE 7  /* non-finite input                           */
+#define IMCOM_ERR_NOALLOC_SIZE 8 /* problem too large for imcom_gpu_build_P_noalloc */
 
 /* Eigensolver selection for imcom_gpu_set_option(IMCOM_OPT_EIGENSOLVER). */
 #define IMCOM_EIGH_DC 0         /* own tridiagonalisation + divide & conquer  */
@@ -177,6 +178,33 @@ int imcom_gpu_mlp_set_weights(imcom_ctx* ctx, const float* W1,
                               const float* b2, const float* W3,
                               const float* b3, const float* feat_mean,
                               const float* feat_std);
+
+/* ---- allocation-free projection ---------------------------------------- */
+
+/* P = Q^T B (the product imcom_gpu_build_P forms) without allocating any
+ * device memory, for callers that cannot call cudaMalloc or cudaFree: for
+ * example a host application or framework that reserves the GPU's memory up
+ * front in its own allocator, where allocating or freeing mid-run would
+ * synchronise the device, fragment the reserved pool or fail outright.
+ * No counterpart in the reference (which calls DGEMM, imcom_matrix.f90:699).
+ *
+ * dQ (n x n, leading dimension ldq), dB (n x m, ldb) and dP (n x m, ldp) are
+ * DEVICE pointers owned by the caller, column-major; stream is a
+ * cudaStream_t (NULL = the default stream).  The call only queues work: it
+ * returns without waiting for the GPU.
+ *
+ * Scratch: the split-K partial sums live in a fixed 32 MiB device array that
+ * every GPU loading the library holds until the process exits.  Limit:
+ * 2 * round_up(n, 32) * m <= 4,194,304 (e.g. n = 2048 with m <= 1024); larger
+ * problems return IMCOM_ERR_NOALLOC_SIZE without touching the GPU.  The
+ * first call on each device looks the array up and sets the kernel's
+ * shared-memory limit, so make that first call before any stream capture.
+ * All calls share the array: calls whose GPU work overlaps race.
+ * Returns 0, -k for a bad argument k, IMCOM_ERR_NOALLOC_SIZE or
+ * IMCOM_ERR_CUDA. */
+int imcom_gpu_build_P_noalloc(const double* dQ, long long ldq, const double* dB,
+                              long long ldb, double* dP, long long ldp, int n, int m,
+                              void* stream);
 
 /* ---- device views (for callers that keep data on the GPU) -------------- */
 

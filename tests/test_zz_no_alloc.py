@@ -1,0 +1,52 @@
+"""imcom_gpu_build_P_noalloc: the allocation-free projection P = Q^T B.
+
+Callers that cannot allocate device memory (their GPU memory is reserved up
+front by their own allocator) pass device buffers they already own; the entry
+point keeps its split-K partial sums in a fixed device array instead of
+allocating.  This file runs last so a failure here leaves every other test
+already run.  The check: two calls in a row through the C-ABI agree with
+imcom_gpu_build_P's P (normwise relative difference < 1e-13, the tolerance of
+the other P tests).
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+IMCOM_ERR_NOALLOC_SIZE = 8
+
+
+def test_build_P_noalloc_matches_build_P(solver):
+    import torch
+
+    from imcom_b200 import EIGH_DC, synth
+
+    prob = synth.make("small", seed=3)
+    solver.set_eigensolver(EIGH_DC)
+    r = solver.solve(prob, UnotS=True, US_max=1e-6, US_tol=1e-8, maxnits=40)
+    n, m = prob.n, prob.m
+    # the caller's own device buffers (column-major, ld = n)
+    dQ = torch.tensor(np.asfortranarray(r.Q).ravel(order="F"), device="cuda")
+    dB = torch.tensor(np.asfortranarray(r.B).ravel(order="F"), device="cuda")
+    lib = solver.lib
+    scale = np.abs(r.P).max()
+    for call in range(2):
+        dP = torch.full((n * m,), float("nan"), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        st = lib.imcom_gpu_build_P_noalloc(dQ.data_ptr(), n, dB.data_ptr(), n, dP.data_ptr(), n,
+                                           n, m, None)
+        assert st == 0, f"call {call}: status {st}"
+        torch.cuda.synchronize()
+        P = dP.cpu().numpy().reshape((n, m), order="F")
+        assert np.max(np.abs(P - r.P)) < 1e-13 * scale, f"call {call}"
+
+
+def test_build_P_noalloc_rejects_oversized_problem(solver):
+    lib = solver.lib
+    n = m = 4096  # 2 * 4096 * 4096 partial sums exceed the fixed array
+    fake = ctypes.c_void_p(256)  # never dereferenced: the size check comes first
+    st = lib.imcom_gpu_build_P_noalloc(fake, n, fake, n, fake, n, n, m, None)
+    assert st == IMCOM_ERR_NOALLOC_SIZE
+    assert lib.imcom_gpu_build_P_noalloc(None, n, fake, n, fake, n, n, m, None) == -1
