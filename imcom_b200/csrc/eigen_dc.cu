@@ -9,19 +9,21 @@
 //    matrix-vector product y0 = A22 v and the panel corrections
 //    y = y0 - V (W^T v) - W (V^T v).  One persistent cooperative kernel per
 //    panel runs the whole panel with two grid-wide barriers per column:
-//      phase A: y0 tiles over the trailing matrix (all SMs), plus the panel
-//               dot products W^T v, V^T v and v^T y0 (atomics);
+//      phase A: y0 tiles over the trailing matrix (all SMs) and v^T y0
+//               (summed per CTA, one atomic per CTA);
 //      phase B: w = tau (y - 1/2 tau (y^T v) v) row by row, using
 //               v^T y = v^T y0 - 2 (V^T v).(W^T v), the update of the next
-//               column and its norm (atomics).
+//               column, its norm and its dot products with the panel's
+//               W and V (the rows already hold them in registers).
 //    The trailing update A22 -= V W^T + W V^T runs on the DMMA GEMM.
 //    Grid barriers spin with a bound and report a timeout instead of hanging.
 // 2. Divide and conquer (LAPACK dstedc / dlaed0-4 structure).  Leaves of at
 //    most 32 rows are diagonalised by a cyclic Jacobi sweep in one CTA each.
 //    Each merge level runs batched over all nodes: z vector and sort (merge
 //    ranks), deflation scan (one thread per node, LAPACK dlaed2 tests and
-//    Givens rotations), the secular equation roots (one warp per root,
-//    safeguarded Newton in the shifted variable tau = lambda - d_org), the
+//    Givens rotations), the secular equation roots (one warp per root; in
+//    tau = lambda - d_org the nearest pole is kept exact and the rest
+//    linearised, so each step solves a quadratic), the
 //    Gu-Eisenstat z-hat (dlaed3) and the eigenvector columns (one warp each),
 //    then Q_node = Q_old(:, nondeflated) U as one DMMA GEMM per node.
 // 3. Back-transformation (dormtr): Z <- (I - V T V^T) Z over blocks of 128
@@ -141,12 +143,22 @@ __global__ void __launch_bounds__(TRD_THREADS) trd_panel_kernel(TrdArgs a) {
   __shared__ double sm_y[WPB][32], sm_c[WPB][32], sm_u[WPB][32];
   if (*(volatile int*)&a.sync->err) return;  // an earlier panel failed
 
-  // Column k: d(k) and the norm of A(k+2:n, k).
-  for (long long r0 = k + 2 + gw * 32; r0 < n; r0 += GW * 32) {
-    long long r = r0 + lane;
-    double v = (r < n) ? A[r + k * lda] : 0.0;
-    double s = warp_sum(v * v);
-    if (lane == 0) atomicAdd(&a.acc[0].nrm, s);
+  // Column k: d(k) and the norm of A(k+2:n, k) (one atomic per CTA).
+  {
+    double part = 0.0;
+    for (long long r0 = k + 2 + gw * 32; r0 < n; r0 += GW * 32) {
+      long long r = r0 + lane;
+      double v = (r < n) ? A[r + k * lda] : 0.0;
+      part += v * v;
+    }
+    part = warp_sum(part);
+    if (lane == 0) sm_y[wib][0] = part;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int w = 0; w < WPB; ++w) s += sm_y[w][0];
+      if (s != 0.0) atomicAdd(&a.acc[0].nrm, s);
+    }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) a.d[k] = A[k + k * lda];
   if (!grid_barrier(a.sync, a.spin)) return;
@@ -201,7 +213,10 @@ __global__ void __launch_bounds__(TRD_THREADS) trd_panel_kernel(TrdArgs a) {
     const long long RB = (n - rbase + 63) / 64, NC = (R + CW - 1) / CW;
 
     // ---- phase A: y0 = A22 v by 64-row x CW-column tiles; every load of a
-    // tile is issued before the first use ----
+    // tile is issued before the first use.  v^T y0 is summed per warp, then
+    // per CTA, and added with one atomic per CTA (same-address atomics from
+    // every tile would serialise in one L2 slice). ----
+    double vty_part = 0.0;
     for (long long tile = gw; tile < RB * NC; tile += GW) {
       const long long rb = tile % RB, ch = tile / RB;
       const long long r = rbase + rb * 64 + 2 * lane;
@@ -230,8 +245,15 @@ __global__ void __launch_bounds__(TRD_THREADS) trd_panel_kernel(TrdArgs a) {
       }
       if (r >= j + 1 && r < n) a.ypart[ch * a.ldy + r] = acc0;
       if (r + 1 >= j + 1 && r + 1 < n) a.ypart[ch * a.ldy + r + 1] = acc1;
-      double s = warp_sum(v0 * acc0 + v1 * acc1);
-      if (lane == 0) atomicAdd(&cur->vty0, s);
+      vty_part += v0 * acc0 + v1 * acc1;
+    }
+    vty_part = warp_sum(vty_part);
+    if (lane == 0) sm_u[wib][0] = vty_part;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int w = 0; w < WPB; ++w) s += sm_u[w][0];
+      if (s != 0.0) atomicAdd(&cur->vty0, s);
     }
     if (!grid_barrier(a.sync, a.spin)) return;
 
@@ -818,29 +840,33 @@ __global__ void dc_assemble_kernel(const Node* nodes, DcWork wk, const double* O
 // 3. Back-transformation: T factor of a block of reflectors (dlarft)
 // ---------------------------------------------------------------------------
 // T(i,i) = tau_i, T(0:i, i) = -tau_i T(0:i, 0:i) G(0:i, i), G = V^T V.
+// T (upper triangle) and G (strict upper triangle, stored transposed in the
+// lower triangle) share one shared-memory tile, so the recurrence reads no
+// global memory.
 __global__ void __launch_bounds__(NBB) larft_kernel(const double* G, long long ldg,
                                                     const double* tau, int jb, double* T,
                                                     long long ldt) {
   extern __shared__ double smem_t[];
-  double(*Ts)[NBB + 1] = reinterpret_cast<double(*)[NBB + 1]>(smem_t);
-  __shared__ double col[NBB];
+  double(*S)[NBB + 1] = reinterpret_cast<double(*)[NBB + 1]>(smem_t);
   const int r = threadIdx.x;
-  for (int c = 0; c < jb; ++c) Ts[r][c] = 0.0;
+  // S[c][r] = G(r, c) for r < c (lower triangle); the upper triangle holds T
+  for (int c = 0; c < jb; ++c) {
+    if (r <= c) S[r][c] = 0.0;                          // T part: upper triangle
+    else S[r][c] = G[c + (long long)r * ldg];           // G(c, r), c < r: lower triangle
+  }
   __syncthreads();
   for (int i = 0; i < jb; ++i) {
     const double ti = tau[i];
-    if (r < i) col[r] = G[r + (long long)i * ldg];
+    double s = 0.0;
+    if (r < i)
+      for (int c = r; c < i; ++c) s += S[r][c] * S[i][c];
     __syncthreads();
-    if (r < i) {
-      double s = 0.0;
-      for (int c = r; c < i; ++c) s += Ts[r][c] * col[c];
-      Ts[r][i] = -ti * s;
-    }
-    if (r == i) Ts[i][i] = ti;
+    if (r < i) S[r][i] = -ti * s;
+    if (r == i) S[i][i] = ti;
     __syncthreads();
   }
   for (int c = 0; c < jb; ++c)
-    if (r < jb) T[r + (long long)c * ldt] = Ts[r][c];
+    if (r < jb) T[r + (long long)c * ldt] = (r <= c) ? S[r][c] : 0.0;
 }
 
 }  // namespace

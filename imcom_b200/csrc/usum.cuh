@@ -69,18 +69,18 @@ struct PixelSmem {
   size_t bytes;
 };
 
+// Staging columns pays only while it leaves >= 8 warps per CTA; otherwise
+// the columns stream from L2 and 16 warps per CTA hide the divide latency.
 inline PixelSmem plan_pixel_smem(int n, size_t limit = 200 * 1024) {
   PixelSmem p;
   size_t col = (size_t)n * sizeof(double);
-  for (int w = 8; w >= 2; --w) {
-    if (col * (w + 1) <= limit) {
-      p.warps = w;
-      p.lam_smem = p.col_smem = true;
-      p.bytes = col * (w + 1);
-      return p;
-    }
+  if (col * 9 <= limit) {
+    p.warps = 8;
+    p.lam_smem = p.col_smem = true;
+    p.bytes = col * 9;
+    return p;
   }
-  p.warps = 8;
+  p.warps = 16;
   p.col_smem = false;
   p.lam_smem = col <= limit;
   p.bytes = p.lam_smem ? col : 0;

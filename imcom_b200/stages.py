@@ -1,0 +1,48 @@
+"""Run one solve of a synthetic workload stage by stage and print the GPU time
+of every stage (CUDA events inside the library).  Each stage sits in an NVTX
+range named after it (SPECTRA, A, EIG, B, P, BISECT, T, EPI), so a profiler
+can select one stage's kernels, e.g.
+
+    ncu --nvtx --nvtx-include "P/" -k regex:dgemm_kernel -c 1 \\
+        python -m imcom_b200.stages n4096
+
+Usage: python -m imcom_b200.stages [workload] [--library-eigensolver]
+"""
+from __future__ import annotations
+
+import sys
+
+
+def main(argv):
+    import torch
+
+    from . import EIGH_DC, EIGH_LIBRARY, EPS, Solver, synth
+
+    wl = argv[0] if argv and not argv[0].startswith("-") else "n4096"
+    nv = torch.cuda.nvtx
+    prob = synth.make(wl, 0)
+    with Solver(0) as s:
+        s.set_eigensolver(EIGH_LIBRARY if "--library-eigensolver" in argv else EIGH_DC)
+        s.set_problem(prob)
+
+        def stage(name, fn):
+            nv.range_push(name)
+            r = fn()
+            s.synchronize()
+            nv.range_pop()
+            return r
+
+        C = stage("SPECTRA", lambda: s.psf_spectra())
+        stage("A", lambda: s.build_A(out=False))
+        stage("EIG", lambda: s.eigen_A(out=False))
+        stage("B", lambda: s.build_B(out=False))
+        stage("P", lambda: s.build_P(out=False))
+        stage("BISECT", lambda: s.bisect_kappa(True, 1e-2, C * EPS, C / EPS, 1e-5, 53, C,
+                                               out=False))
+        stage("T", lambda: s.build_T(out=False))
+        stage("EPI", lambda: (s.build_S(out=False), s.build_image(out=False)))
+        print({k: round(v, 3) for k, v in s.stage_times().items()})
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:])
