@@ -208,47 +208,94 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    def device_step():
+    learned = args.kappa == "learned"
+    nev_acc = {"plain": [], "learned": []}
+
+    def device_step(use_learned):
         C = s.psf_spectra()
         kmin, kmax = C * 1.1102230246251565e-16, C / 1.1102230246251565e-16
         s.build_A(out=False)
         s.eigen_A(out=False)
         s.build_B(out=False)
         s.build_P(out=False)
-        s.bisect_kappa(UNOTS, US_MAX, kmin, kmax, US_TOL, MAXNITS, C, out=False)
+        if use_learned:
+            s.bisect_kappa_learned(UNOTS, US_MAX, kmin, kmax, US_TOL, MAXNITS, C, out=False)
+        else:
+            s.bisect_kappa(UNOTS, US_MAX, kmin, kmax, US_TOL, MAXNITS, C, out=False)
         s.build_T(out=False)
         s.build_S(out=False)
         s.build_image(out=False)
 
+    # ---- learned-kappa model (trained outside the timed region) -------------
+    model_src = None
+    if learned:
+        from imcom_b200 import kappa_model as KM
+        if os.path.exists(KM.DEFAULT_WEIGHTS):
+            model = KM.KappaModel.load(KM.DEFAULT_WEIGHTS)
+            model_src = "committed weights " + os.path.basename(KM.DEFAULT_WEIGHTS)
+        else:
+            rng = np.random.default_rng(12345)
+            probs = [synth.make(WORKLOAD, seed=1000 + q) for q in range(8)]
+            targets = list(10.0 ** rng.uniform(np.log10(3e-3), np.log10(3e-2), len(probs)))
+            feat, y = KM.collect(s, probs, targets)
+            model, _ = KM.train(s, feat, y, epochs=40)
+            model_src = f"trained at start-up on {y.size} pixels of 8 fresh seeds"
+        model.install(s)
+
     # ---- value: inputs resident in HBM ------------------------------------
     s.set_problem(prob)
-    for _ in range(args.warmup):
-        device_step()
-    s.synchronize()
-    torch.cuda.synchronize()
-    barrier()
-    torch.cuda.synchronize()
+
+    def timed_steps(use_learned, nsteps):
+        for _ in range(args.warmup):
+            device_step(use_learned)
+        s.synchronize()
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        l0 = s.launch_count()
+        st, sm = [], []
+        for _ in range(nsteps):
+            flush.fill_(1.0)  # evict L2 between timed steps
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            device_step(use_learned)
+            e1.record(stream)
+            s.synchronize()
+            sm.append(e0.elapsed_time(e1))
+            st.append(s.stage_times())
+        return sm, st, (s.launch_count() - l0) // max(1, nsteps)
+
+    plain_ms, plain_st, _ = timed_steps(False, args.steps) if learned else (None, None, None)
     clocks = Clocks(local)
     clocks.start()
-    l0 = s.launch_count()
-    stage_ms = []
-    step_ms = []
-    for _ in range(args.steps):
-        flush.fill_(1.0)  # evict L2 between timed steps
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        device_step()
-        e1.record(stream)
-        s.synchronize()
-        step_ms.append(e0.elapsed_time(e1))
-        stage_ms.append(s.stage_times())
-    launches = (s.launch_count() - l0) // max(1, args.steps)
+    step_ms, stage_ms, launches = timed_steps(learned, args.steps)
     torch.cuda.synchronize()
     ck = clocks.stop()
     barrier()
     t_step = max_over_ranks(statistics.mean(step_ms))
     value = world * prob.m / (t_step * 1e-3)
+    # evaluation counts of the two kappa solvers on this workload (untimed)
+    C = s.psf_spectra()
+    _, _, nev_plain = s.bisect_kappa(UNOTS, US_MAX, C * 1.1102230246251565e-16,
+                                     C / 1.1102230246251565e-16, US_TOL, MAXNITS, C)
+    kappa_info = {"solver": "learned bracket + bisection replay" if learned else "bisection",
+                  "mean_evaluations_plain": float(np.mean(nev_plain))}
+    if learned:
+        K0 = s.bisect_kappa(UNOTS, US_MAX, C * 1.1102230246251565e-16, C / 1.1102230246251565e-16,
+                            US_TOL, MAXNITS, C)[0]
+        K1, _, nev_l, fb = s.bisect_kappa_learned(UNOTS, US_MAX, C * 1.1102230246251565e-16,
+                                                  C / 1.1102230246251565e-16, US_TOL, MAXNITS, C)
+        t_plain = max_over_ranks(statistics.mean(plain_ms))
+        kappa_info.update({
+            "mean_evaluations_learned": float(np.mean(nev_l)),
+            "no_bound_fraction": float(np.mean(fb)),
+            "kappa_bit_identical_to_plain": bool(np.array_equal(K0, K1)),
+            "model": model_src,
+            "plain_fp64_value": world * prob.m / (t_plain * 1e-3),
+            "bisect_ms_plain": statistics.mean(d["bisect"] for d in plain_st),
+            "bisect_ms_learned": statistics.mean(d["bisect"] for d in stage_ms),
+        })
 
     # ---- e2e: through the C-ABI with pinned host buffers -------------------
     keep = []
@@ -276,8 +323,12 @@ def run_ours(args):
         s.eigen_A(out=False)
         s.build_B(out=False)
         s.build_P(out=False)
-        s._call("imcom_gpu_bisect_kappa", 1, US_MAX, kmin, kmax, US_TOL, MAXNITS, C,
-                outs["K"].ctypes.data, outs["U"].ctypes.data, None)
+        if learned:
+            s._call("imcom_gpu_bisect_kappa_learned", 1, US_MAX, kmin, kmax, US_TOL, MAXNITS, C,
+                    outs["K"].ctypes.data, outs["U"].ctypes.data, None, None)
+        else:
+            s._call("imcom_gpu_bisect_kappa", 1, US_MAX, kmin, kmax, US_TOL, MAXNITS, C,
+                    outs["K"].ctypes.data, outs["U"].ctypes.data, None)
         s._call("imcom_gpu_build_T", outs["T"].ctypes.data)
         s._call("imcom_gpu_build_S", outs["S"].ctypes.data)
         s._call("imcom_gpu_build_image", outs["H"].ctypes.data)
@@ -350,10 +401,12 @@ def run_ours(args):
                                    "lambda/D=0.5 px PSF, 64x64 output at 0.5 px (m=4096), "
                                    "U mode U<1e-2 tol 1e-5, maxnits 53",
                        "n": n, "m": m, "nps": prob.nps, "lookup_side": 3 * prob.nps,
-                       "eigensolver": args.eigensolver, "kappa": "bisection",
+                       "eigensolver": args.eigensolver, "kappa": args.kappa,
+                       "P_T_precision": "fp64 (DMMA)",
                        "parallelism": f"replicas x{world}",
                        "l2": "flushed between timed steps (252 MB write)"},
             "stages_ms": avg,
+            "kappa": kappa_info,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": t_e2e},
             "gpu_launches": launches,
@@ -375,6 +428,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--eigensolver", choices=["dc", "library"], default="dc")
+    ap.add_argument("--kappa", choices=["learned", "bisection"], default="learned")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     args = ap.parse_args()
     if args.impl == "reference":

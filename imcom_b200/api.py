@@ -233,10 +233,30 @@ class Solver:
 
     def kappa_features(self, UnotS, US_max, C_a=None):
         C_a = self.C_a if C_a is None else C_a
-        F = np.zeros((12, self.m), dtype=np.float32, order="F")
+        F = np.zeros((12, self.m), dtype=np.float32)  # feature-major: F[k, a] at k * m + a
         self._call("imcom_gpu_kappa_features", 1 if UnotS else 0, float(US_max), float(C_a),
                    _ptr(F))
         return F
+
+    def mlp_train(self, feat, target, params, epochs=30, batch=512, lr=2e-3, seed=1):
+        """Train on the GPU (Adam); feat (12, N) and target (N) normalised."""
+        feat = np.ascontiguousarray(feat, dtype=np.float32)  # feature-major
+        target = np.ascontiguousarray(target, dtype=np.float32)
+        p = np.ascontiguousarray(params, dtype=np.float32).copy()
+        loss = np.zeros(epochs, dtype=np.float32)
+        self._call("imcom_gpu_mlp_train", int(target.size), _ptr(feat), _ptr(target), int(epochs),
+                   int(batch), C.c_float(lr), C.c_uint(seed), _ptr(p), _ptr(loss))
+        return p, loss
+
+    def mlp_gradient(self, feat, target, params):
+        feat = np.ascontiguousarray(feat, dtype=np.float32)  # feature-major
+        target = np.ascontiguousarray(target, dtype=np.float32)
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        g = np.zeros_like(p)
+        loss = np.zeros(1, dtype=np.float32)
+        self._call("imcom_gpu_mlp_gradient", int(target.size), _ptr(feat), _ptr(target), _ptr(p),
+                   _ptr(g), _ptr(loss))
+        return g, float(loss[0])
 
     def mlp_set_weights(self, W1, b1, W2, b2, W3, b3, mean, std):
         arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (W1, b1, W2, b2, W3, b3, mean, std)]

@@ -82,6 +82,10 @@ struct imcom_ctx {
   cufftHandle plan_r2c = 0;
   int plan_r2c_n = 0, plan_r2c_batch = 0;
 
+  int* fb = nullptr;        // per-pixel fallback flags of the learned bisection
+  size_t fb_bytes = 0;
+  void* train_buf = nullptr;  // MLP training data and state
+  size_t train_bytes = 0;
   void* gemm_ws = nullptr;  // split-K partial sums
   size_t gemm_ws_bytes = 0;
 

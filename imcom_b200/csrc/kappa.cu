@@ -1,24 +1,652 @@
-// kappa.cu -- learned-kappa bracket (features, MLP, bracketed bisection).
+// kappa.cu -- learned-kappa bracket for the per-pixel bisection.
+//
+// The reference finds kappa per output pixel by log-space bisection
+// (imcom_bisect_by_U / _by_S, imcom_bisect.f90:174-267).  Here a small MLP
+// predicts log10(kappa) and a bracket half-width from 12 cheap per-pixel
+// features.  Because U(kappa) rises and S(kappa) falls monotonically in
+// kappa, f = U - U_max (or S - S_max) evaluated at the two bracket ends
+// gives one-sided bounds: an end with f < -max(tol, C eps) makes every
+// bisection midpoint on its accept side a known accept that cannot trigger an
+// exit test; an end with f >= C eps makes every midpoint on its reject side a
+// known reject.  The kernel replays the reference's bisection sequence and
+// evaluates U/S only at midpoints between the bounds, so K_a and U_a/S_a are
+// bit-identical to the plain bisection (same evaluator, same operations).
+// A bracket that yields neither bound costs two extra evaluations.
+//
+// Features (feature-major, 12 x m, float):
+//   0  inputs within a 2 x 2 px box around (X_a, Y_a)
+//   1  distinct exposures among them
+//   2-9  log10(sum_{p in band b} P2_p / (4 C lambda_b) + 1e-30), bands of
+//        lambda / lambda_max by two decades (band 7: below 1e-14 or <= 0)
+//   10 log10(US_max)
+//   11 log10(lambda_max / C)
+// MLP: 12 -> 64 (ReLU) -> 64 (ReLU) -> 2; weights and activations rounded to
+// bf16, products accumulated in fp32.  Output 0 is log10(kappa), output 1 is
+// log of the bracket half-width in decades (the host folds the target
+// normalisation into the last layer).
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <vector>
+
 #include "common.cuh"
+#include "solve.cuh"
+#include "usum.cuh"
+
+namespace imcom {
+namespace {
+
+constexpr int NF = 12, NH = 64, NO = 2;
+// packed parameters (floats): W1 | b1 | W2 | b2 | W3 | b3
+constexpr int OFF_W1 = 0, OFF_B1 = OFF_W1 + NH * NF, OFF_W2 = OFF_B1 + NH,
+              OFF_B2 = OFF_W2 + NH * NH, OFF_W3 = OFF_B2 + NH, OFF_B3 = OFF_W3 + NO * NH,
+              NPARAM = OFF_B3 + NO;
+// device weight block: params (bf16-rounded weights) | feature mean | std
+constexpr int OFF_MEAN = NPARAM, OFF_STD = NPARAM + NF, NWEIGHT = NPARAM + 2 * NF;
+
+__device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+
+__device__ __forceinline__ double wsum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Features of one pixel, every lane gets all 12.
+__device__ void pixel_features(const double* __restrict__ x, const double* __restrict__ y,
+                               const int* __restrict__ expi, int n, double Xa, double Ya,
+                               const double* lam, const double* col, double C, double US_max,
+                               int lane, float* f) {
+  double cnt = 0.0;
+  unsigned mask = 0u;
+  for (int i = lane; i < n; i += 32) {
+    double dx = x[i] - Xa, dy = y[i] - Ya;
+    if (fabs(dx) < 1.0 && fabs(dy) < 1.0) {
+      cnt += 1.0;
+      mask |= 1u << ((expi[i] - 1) & 31);
+    }
+  }
+  cnt = wsum(cnt);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mask |= __shfl_xor_sync(0xffffffffu, mask, o);
+  const double lmax = lam[0];  // eigenvalues are in descending order
+  double band[8];
+#pragma unroll
+  for (int b = 0; b < 8; ++b) band[b] = 0.0;
+  for (int p = lane; p < n; p += 32) {
+    const double l = lam[p], pp = col[p];
+    const double r = (l > 0.0 && lmax > 0.0) ? l / lmax : 0.0;
+    int b = (r > 0.0) ? (int)floor(-log10(r) * 0.5) : 7;
+    b = b < 0 ? 0 : (b > 7 ? 7 : b);
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      if (q == b) band[q] += pp * pp;
+  }
+#pragma unroll
+  for (int b = 0; b < 8; ++b) {
+    const double s = wsum(band[b]);
+    const double lc = lmax * pow(10.0, -(2.0 * b + 1.0));
+    f[2 + b] = (float)log10(s / (4.0 * C * (lc > 0.0 ? lc : 1e-300)) + 1e-30);
+  }
+  f[0] = (float)cnt;
+  f[1] = (float)__popc(mask);
+  f[10] = (float)log10(fabs(US_max) + 1e-300);
+  f[11] = (float)log10(fabs(lmax / C) + 1e-300);
+}
+
+// MLP forward on one warp: lane owns hidden units lane and lane + 32.
+__device__ void mlp_forward_warp(const float* __restrict__ W, const float* f, int lane,
+                                 float* out) {
+  float fn[NF];
+#pragma unroll
+  for (int k = 0; k < NF; ++k) fn[k] = bf16r((f[k] - W[OFF_MEAN + k]) / W[OFF_STD + k]);
+  float h1[2], h2[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int u = lane + 32 * h;
+    float s = W[OFF_B1 + u];
+#pragma unroll
+    for (int k = 0; k < NF; ++k) s = fmaf(W[OFF_W1 + u * NF + k], fn[k], s);
+    h1[h] = bf16r(fmaxf(s, 0.0f));
+  }
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int u = lane + 32 * h;
+    float s = W[OFF_B2 + u];
+    for (int v = 0; v < NH; ++v) {
+      const float hv = __shfl_sync(0xffffffffu, h1[v >> 5], v & 31);
+      s = fmaf(W[OFF_W2 + u * NH + v], hv, s);
+    }
+    h2[h] = bf16r(fmaxf(s, 0.0f));
+  }
+#pragma unroll
+  for (int o = 0; o < NO; ++o) {
+    float s = W[OFF_W3 + o * NH + lane] * h2[0] + W[OFF_W3 + o * NH + lane + 32] * h2[1];
+#pragma unroll
+    for (int q = 16; q > 0; q >>= 1) s += __shfl_xor_sync(0xffffffffu, s, q);
+    out[o] = s + W[OFF_B3 + o];
+  }
+}
+
+__global__ void features_kernel(BisectArgs a, const double* __restrict__ x,
+                                const double* __restrict__ y, const int* __restrict__ expi,
+                                const double* __restrict__ X, const double* __restrict__ Y,
+                                float* __restrict__ feat) {
+  const int lane = threadIdx.x & 31;
+  const int pix = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (pix >= a.m) return;
+  float f[NF];
+  pixel_features(x, y, expi, a.n, X[pix], Y[pix], a.L, a.P + (size_t)pix * a.ldp, a.C, a.US_max,
+                 lane, f);
+  if (lane < NF) {
+#pragma unroll
+    for (int k = 0; k < NF; ++k)
+      if (k == lane) feat[(size_t)k * a.m + pix] = f[k];
+  }
+}
+
+struct LearnedExtra {
+  const double *x, *y, *X, *Y;
+  const int* expi;
+  const float* W;
+  int* fallback;
+  double half_scale;  // bracket half-width = half_scale * exp(output 1), decades
+  double min_half;    // smallest half-width, decades
+  double margin;      // safety margin of the verification tests (units of U or S)
+};
+
+__global__ void learned_bisect_kernel(BisectArgs a, PixelSmem plan, LearnedExtra ex) {
+  extern __shared__ __align__(16) double smem[];
+  __shared__ float sW[NWEIGHT];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int q = threadIdx.x; q < NWEIGHT; q += blockDim.x) sW[q] = ex.W[q];
+  const double* lam = a.L;
+  if (plan.lam_smem) {
+    for (int p = threadIdx.x; p < a.n; p += blockDim.x) smem[p] = a.L[p];
+    lam = smem;
+  }
+  __syncthreads();
+  double* mycol = plan.col_smem ? smem + (size_t)a.n * (1 + warp) : nullptr;
+  const bool U = a.UnotS != 0;
+  for (int pix = blockIdx.x * plan.warps + warp; pix < a.m; pix += gridDim.x * plan.warps) {
+    const double* col = a.P + (size_t)pix * a.ldp;
+    if (mycol) {
+      for (int p = lane; p < a.n; p += 32) mycol[p] = col[p];
+      __syncwarp();
+      col = mycol;
+    }
+    float f[NF], o[NO];
+    pixel_features(ex.x, ex.y, ex.expi, a.n, ex.X[pix], ex.Y[pix], lam, col, a.C, a.US_max, lane,
+                   f);
+    mlp_forward_warp(sW, f, lane, o);
+    double hw = ex.half_scale * exp((double)fminf(fmaxf(o[1], -20.0f), 5.0f));
+    hw = fmin(fmax(hw, ex.min_half), 4.0);
+    double bl = (double)o[0] - hw, bh = (double)o[0] + hw;
+    // (lg_min, lg_max) is the reference's search range
+    const double rlo = a.lg_min, rhi = a.lg_max;
+    bl = fmax(bl, rlo);
+    bh = fmin(bh, rhi);
+    int nev = 0;
+    double k_root = 0.0, us = 0.0;
+    const double ceps = __dmul_rn(a.C, a.eps);
+    const double thr = fmax(a.tol, ceps) + ex.margin;
+    // One-sided bounds from the evaluated bracket ends.  U rises with kappa:
+    // an end with f < -thr makes every midpoint at or below it a known
+    // accept; an end with f >= C eps (+ margin) makes every midpoint at or
+    // above it a known reject.  S falls with kappa, so the directions flip.
+    double accb = U ? -INFINITY : INFINITY;  // known accept beyond this point
+    double rejb = U ? INFINITY : -INFINITY;  // known reject beyond this point
+    const double ends[2] = {bl, bh};
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const double pt = ends[e];
+      if (!(pt > rlo && pt < rhi) || (e == 1 && bh <= bl)) continue;
+      const double fp =
+          __dsub_rn(warp_us(U, lam, col, a.Nd, a.n, pow(10.0, pt), a.C, lane), a.US_max);
+      ++nev;
+      if (fp < -thr) accb = U ? fmax(accb, pt) : fmin(accb, pt);
+      else if (fp >= ceps + ex.margin) rejb = U ? fmin(rejb, pt) : fmax(rejb, pt);
+    }
+    const bool have_acc = U ? (accb > rlo) : (accb < rhi);
+    const bool have_rej = U ? (rejb < rhi) : (rejb > rlo);
+    if (lane == 0 && ex.fallback) ex.fallback[pix] = (have_acc || have_rej) ? 0 : 1;
+    {
+      // The reference first evaluates f0 at the start of the range (kappa_min
+      // for U, kappa_max for S) and returns there if f0 >= 0.  A known accept
+      // point inside the range implies f0 < 0 by monotonicity, so f0 is then
+      // only needed if no later step is accepted.
+      double f0 = 0.0;
+      bool have_f0 = false;
+      if (!have_acc) {
+        const double k0 = U ? a.k_min : a.k_max;
+        us = warp_us(U, lam, col, a.Nd, a.n, k0, a.C, lane);
+        ++nev;
+        f0 = __dsub_rn(us, a.US_max);
+        have_f0 = true;
+      }
+      if (have_f0 && !(f0 < 0.0)) {
+        k_root = U ? a.k_min : a.k_max;
+      } else {
+        const double lo = U ? a.lg_min : a.lg_max, hi = U ? a.lg_max : a.lg_min;
+        double root = lo, dx = __dsub_rn(hi, lo);
+        bool last_known = false, any_acc = false;
+        for (int i = 1; i <= a.maxnits; ++i) {
+          dx = __dmul_rn(0.5, dx);
+          const double mid = __dadd_rn(root, dx);
+          const bool known_acc = U ? (mid <= accb) : (mid >= accb);
+          const bool known_rej = U ? (mid >= rejb) : (mid <= rejb);
+          if (known_acc) {
+            root = mid;
+            any_acc = true;
+            last_known = true;
+            continue;
+          }
+          if (known_rej) continue;
+          const double fmid =
+              __dsub_rn(warp_us(U, lam, col, a.Nd, a.n, pow(10.0, mid), a.C, lane), a.US_max);
+          ++nev;
+          if (fmid < 0.0) {
+            root = mid;
+            any_acc = true;
+            last_known = false;
+            us = __dadd_rn(fmid, a.US_max);
+            if (fabs(fmid) < a.tol) break;
+          }
+          if (fabs(fmid) < ceps) break;
+        }
+        if (!any_acc) {
+          if (!have_f0) {
+            const double k0 = U ? a.k_min : a.k_max;
+            us = warp_us(U, lam, col, a.Nd, a.n, k0, a.C, lane);
+            ++nev;
+          }
+        } else if (last_known) {
+          // value the reference holds at the last accepted midpoint
+          const double fl =
+              __dsub_rn(warp_us(U, lam, col, a.Nd, a.n, pow(10.0, root), a.C, lane), a.US_max);
+          ++nev;
+          us = __dadd_rn(fl, a.US_max);
+        }
+        k_root = pow(10.0, root);
+      }
+    }
+    write_pixel(a, lam, col, pix, lane, nev, k_root, us);
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Training: forward + backward for tiles of 32 samples per CTA, bf16
+// activations, fp32 accumulation; per-CTA gradient partials are added to a
+// global fp32 gradient with one atomic per parameter per CTA.
+// Loss per sample: (o0 - t)^2 + 0.25 (o1 - log(|o0 - t| + 0.01))^2, the second
+// term with the target held fixed (it fits the log of the first head's error).
+// ---------------------------------------------------------------------------
+constexpr int TB = 32;  // samples per CTA tile
+
+__global__ void __launch_bounds__(256) mlp_grad_kernel(const float* __restrict__ params,
+                                                       const float* __restrict__ feat, int nall,
+                                                       const float* __restrict__ target,
+                                                       const int* __restrict__ idx, int nb,
+                                                       float* __restrict__ grad,
+                                                       float* __restrict__ loss) {
+  __shared__ float sW1[NH * NF], sW2[NH * NH], sW3[NO * NH], sb1[NH], sb2[NH], sb3[NO];
+  __shared__ float X0[TB][NF + 1];
+  // H1 and H2 hold the activations, then (in place) their gradients
+  __shared__ float H1[TB][NH + 1], H2[TB][NH + 1];
+  __shared__ float DO[TB][NO];
+  __shared__ float sloss[256];
+  const int tid = threadIdx.x;
+  for (int q = tid; q < NH * NF; q += 256) sW1[q] = bf16r(params[OFF_W1 + q]);
+  for (int q = tid; q < NH * NH; q += 256) sW2[q] = bf16r(params[OFF_W2 + q]);
+  for (int q = tid; q < NO * NH; q += 256) sW3[q] = bf16r(params[OFF_W3 + q]);
+  for (int q = tid; q < NH; q += 256) {
+    sb1[q] = params[OFF_B1 + q];
+    sb2[q] = params[OFF_B2 + q];
+  }
+  if (tid < NO) sb3[tid] = params[OFF_B3 + tid];
+  const int s0 = blockIdx.x * TB;
+  for (int q = tid; q < TB * NF; q += 256) {
+    int r = q / NF, k = q % NF, s = s0 + r;
+    float v = 0.0f;
+    if (s < nb) {
+      int g = idx ? idx[s] : s;
+      v = bf16r(feat[(size_t)k * nall + g]);
+    }
+    X0[r][k] = v;
+  }
+  __syncthreads();
+  // layer 1
+  for (int q = tid; q < TB * NH; q += 256) {
+    int r = q / NH, u = q % NH;
+    float s = sb1[u];
+#pragma unroll
+    for (int k = 0; k < NF; ++k) s = fmaf(sW1[u * NF + k], X0[r][k], s);
+    H1[r][u] = bf16r(fmaxf(s, 0.0f));
+  }
+  __syncthreads();
+  // layer 2
+  for (int q = tid; q < TB * NH; q += 256) {
+    int r = q / NH, u = q % NH;
+    float s = sb2[u];
+    for (int v = 0; v < NH; ++v) s = fmaf(sW2[u * NH + v], H1[r][v], s);
+    H2[r][u] = bf16r(fmaxf(s, 0.0f));
+  }
+  __syncthreads();
+  // output, loss and d loss / d output
+  float lsum = 0.0f;
+  if (tid < TB) {
+    int r = tid, s = s0 + r;
+    float o[NO];
+#pragma unroll
+    for (int j = 0; j < NO; ++j) {
+      float acc = sb3[j];
+      for (int v = 0; v < NH; ++v) acc = fmaf(sW3[j * NH + v], H2[r][v], acc);
+      o[j] = acc;
+    }
+    float d0 = 0.0f, d1 = 0.0f;
+    if (s < nb) {
+      int g = idx ? idx[s] : s;
+      float e = o[0] - target[g];
+      float lt = logf(fabsf(e) + 0.01f);
+      float e1 = o[1] - lt;
+      lsum = e * e + 0.25f * e1 * e1;
+      d0 = 2.0f * e;
+      d1 = 0.5f * e1;
+    }
+    DO[r][0] = d0;
+    DO[r][1] = d1;
+  }
+  sloss[tid] = lsum;
+  __syncthreads();
+  // dW3, db3 (need H2 before it is overwritten)
+  for (int q = tid; q < NO * NH; q += 256) {
+    int j = q / NH, v = q % NH;
+    float g = 0.0f;
+    for (int r = 0; r < TB; ++r) g = fmaf(DO[r][j], H2[r][v], g);
+    atomicAdd(&grad[OFF_W3 + q], g);
+  }
+  if (tid < NO) {
+    float g = 0.0f;
+    for (int r = 0; r < TB; ++r) g += DO[r][tid];
+    atomicAdd(&grad[OFF_B3 + tid], g);
+  }
+  __syncthreads();
+  // H2 <- d(pre-activation 2) = (W3^T dO) masked by ReLU, in place
+  for (int q = tid; q < TB * NH; q += 256) {
+    int r = q / NH, u = q % NH;
+    float g = DO[r][0] * sW3[u] + DO[r][1] * sW3[NH + u];
+    H2[r][u] = H2[r][u] > 0.0f ? g : 0.0f;
+  }
+  __syncthreads();
+  // dW2 = dH2^T H1, db2 (need H1 before it is overwritten)
+  for (int q = tid; q < NH * NH; q += 256) {
+    int u = q / NH, v = q % NH;
+    float g = 0.0f;
+    for (int r = 0; r < TB; ++r) g = fmaf(H2[r][u], H1[r][v], g);
+    atomicAdd(&grad[OFF_W2 + q], g);
+  }
+  for (int q = tid; q < NH; q += 256) {
+    float g = 0.0f;
+    for (int r = 0; r < TB; ++r) g += H2[r][q];
+    atomicAdd(&grad[OFF_B2 + q], g);
+  }
+  __syncthreads();
+  // H1 <- d(pre-activation 1) = (W2^T dH2) masked by ReLU, in place
+  for (int q = tid; q < TB * NH; q += 256) {
+    int r = q / NH, v = q % NH;
+    float g = 0.0f;
+    for (int u = 0; u < NH; ++u) g = fmaf(sW2[u * NH + v], H2[r][u], g);
+    H1[r][v] = H1[r][v] > 0.0f ? g : 0.0f;
+  }
+  __syncthreads();
+  // dW1 = dH1^T X0, db1
+  for (int q = tid; q < NH * NF; q += 256) {
+    int u = q / NF, k = q % NF;
+    float g = 0.0f;
+    for (int r = 0; r < TB; ++r) g = fmaf(H1[r][u], X0[r][k], g);
+    atomicAdd(&grad[OFF_W1 + q], g);
+  }
+  for (int q = tid; q < NH; q += 256) {
+    float g = 0.0f;
+    for (int r = 0; r < TB; ++r) g += H1[r][q];
+    atomicAdd(&grad[OFF_B1 + q], g);
+  }
+  for (int w = 128; w > 0; w >>= 1) {
+    __syncthreads();
+    if (tid < w) sloss[tid] += sloss[tid + w];
+  }
+  if (tid == 0) atomicAdd(loss, sloss[0]);
+}
+
+// Adam step on fp32 master parameters with the batch-mean gradient.
+__global__ void adam_kernel(float* __restrict__ params, const float* __restrict__ grad,
+                            float* __restrict__ m1, float* __restrict__ m2, float lr, float b1,
+                            float b2, float c1, float c2, float inv_batch) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= NPARAM) return;
+  float g = grad[q] * inv_batch;
+  float a = b1 * m1[q] + (1.0f - b1) * g;
+  float b = b2 * m2[q] + (1.0f - b2) * g * g;
+  m1[q] = a;
+  m2[q] = b;
+  params[q] -= lr * (a / c1) / (sqrtf(b / c2) + 1e-8f);
+}
+
+}  // namespace
+
+int fill_learned(imcom_ctx* ctx, LearnedExtra& ex) {
+  if (!ctx->mlp.set) return set_err(ctx, IMCOM_ERR_STATE, "imcom_gpu_mlp_set_weights has not run");
+  ex.x = ctx->x;
+  ex.y = ctx->y;
+  ex.X = ctx->X;
+  ex.Y = ctx->Y;
+  ex.expi = ctx->exp_i;
+  ex.W = ctx->mlp.w;
+  ex.fallback = nullptr;
+  ex.half_scale = 3.0;
+  ex.min_half = 0.02;
+  ex.margin = 1e-10;
+  return 0;
+}
+
+}  // namespace imcom
 
 using namespace imcom;
 
 extern "C" int imcom_gpu_kappa_features(imcom_ctx* ctx, int UnotS, double US_max, double C_a,
                                         float* feat_out) {
-  (void)UnotS; (void)US_max; (void)C_a; (void)feat_out;
   if (!ctx) return -1;
-  return set_err(ctx, IMCOM_ERR_STATE, "learned-kappa features not built");
+  if (!feat_out) return -5;
+  BisectArgs a;
+  IMC_TRY(fill_bisect_args(ctx, a, UnotS, US_max, 1.0, 1.0, 0.0, 0, C_a));
+  cudaSetDevice(ctx->device);
+  IMC_TRY(ensure_vec(ctx, &ctx->feat, (size_t)NF * ctx->m));
+  int blocks = (ctx->m + 7) / 8;
+  features_kernel<<<blocks, 256, 0, ctx->stream>>>(a, ctx->x, ctx->y, ctx->exp_i, ctx->X, ctx->Y,
+                                                   ctx->feat);
+  IMC_LAUNCH();
+  IMC_CUDA(cudaMemcpyAsync(feat_out, ctx->feat, (size_t)NF * ctx->m * sizeof(float),
+                           cudaMemcpyDeviceToHost, ctx->stream));
+  IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  return 0;
 }
 
-extern "C" int imcom_gpu_mlp_set_weights(imcom_ctx* ctx, const float*, const float*, const float*,
-                                         const float*, const float*, const float*, const float*,
-                                         const float*) {
+extern "C" int imcom_gpu_mlp_set_weights(imcom_ctx* ctx, const float* W1, const float* b1,
+                                         const float* W2, const float* b2, const float* W3,
+                                         const float* b3, const float* mean, const float* stdv) {
   if (!ctx) return -1;
-  return set_err(ctx, IMCOM_ERR_STATE, "learned-kappa MLP not built");
+  const float* parts[8] = {W1, b1, W2, b2, W3, b3, mean, stdv};
+  for (int q = 0; q < 8; ++q)
+    if (!parts[q]) return -(q + 2);
+  std::vector<float> h(NWEIGHT);
+  auto put = [&](int off, const float* src, int cnt, bool round) {
+    for (int q = 0; q < cnt; ++q) {
+      float v = src[q];
+      if (round) v = __bfloat162float(__float2bfloat16_rn(v));
+      h[off + q] = v;
+    }
+  };
+  put(OFF_W1, W1, NH * NF, true);
+  put(OFF_B1, b1, NH, false);
+  put(OFF_W2, W2, NH * NH, true);
+  put(OFF_B2, b2, NH, false);
+  put(OFF_W3, W3, NO * NH, true);
+  put(OFF_B3, b3, NO, false);
+  put(OFF_MEAN, mean, NF, false);
+  put(OFF_STD, stdv, NF, false);
+  for (int q = 0; q < NF; ++q)
+    if (!(h[OFF_STD + q] > 0.0f)) return set_err(ctx, -9, "feature std must be positive");
+  cudaSetDevice(ctx->device);
+  if (!ctx->mlp.w) IMC_TRY(ensure_vec(ctx, &ctx->mlp.w, NWEIGHT));
+  IMC_CUDA(cudaMemcpyAsync(ctx->mlp.w, h.data(), NWEIGHT * sizeof(float), cudaMemcpyHostToDevice,
+                           ctx->stream));
+  IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->mlp.set = true;
+  return 0;
 }
 
-extern "C" int imcom_gpu_bisect_kappa_learned(imcom_ctx* ctx, int, double, double, double, double,
-                                              int, double, double*, double*, int*, int*) {
+extern "C" int imcom_gpu_bisect_kappa_learned(imcom_ctx* ctx, int UnotS, double US_max,
+                                              double k_min, double k_max, double tol,
+                                              int maxnits, double C_a, double* K_out,
+                                              double* US_out, int* nevals_out,
+                                              int* fallback_out) {
   if (!ctx) return -1;
-  return set_err(ctx, IMCOM_ERR_STATE, "learned-kappa bisection not built");
+  BisectArgs a;
+  IMC_TRY(fill_bisect_args(ctx, a, UnotS, US_max, k_min, k_max, tol, maxnits, C_a));
+  LearnedExtra ex;
+  IMC_TRY(fill_learned(ctx, ex));
+  cudaSetDevice(ctx->device);
+  stage_begin(ctx, ST_BISECT);
+  IMC_TRY(ensure_mat(ctx, ctx->Pt, ctx->n, ctx->m));
+  a.Pt = ctx->Pt.p;
+  a.ldt = ctx->Pt.ld;
+  IMC_TRY(ensure_buf(ctx, (void**)&ctx->fb, ctx->fb_bytes, (size_t)ctx->m * sizeof(int)));
+  ex.fallback = ctx->fb;
+  PixelSmem plan = plan_pixel_smem(ctx->n, 190 * 1024);
+  IMC_CUDA(cudaFuncSetAttribute(learned_bisect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)plan.bytes));
+  learned_bisect_kernel<<<pixel_grid(ctx, plan, ctx->m), plan.warps * 32, plan.bytes,
+                          ctx->stream>>>(a, plan, ex);
+  IMC_LAUNCH();
+  stage_end(ctx, ST_BISECT);
+  ctx->have_K = true;
+  ctx->have_Pt = true;
+  ctx->have_T = false;
+  if (fallback_out)
+    IMC_CUDA(cudaMemcpyAsync(fallback_out, ctx->fb, ctx->m * sizeof(int), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+  return copy_pixel_outputs(ctx, K_out, US_out, nevals_out);
+}
+
+// Gradient of the summed loss over `nsamples` samples at the given parameters
+// (the training kernel on one batch; used by the tests' gradient check).
+extern "C" int imcom_gpu_mlp_gradient(imcom_ctx* ctx, int nsamples, const float* feat,
+                                      const float* target, const float* params, float* grad_out,
+                                      float* loss_out) {
+  if (!ctx) return -1;
+  if (nsamples <= 0) return -2;
+  if (!feat) return -3;
+  if (!target) return -4;
+  if (!params) return -5;
+  if (!grad_out) return -6;
+  cudaSetDevice(ctx->device);
+  float *d = nullptr;
+  size_t need = ((size_t)NF * nsamples + nsamples + 2 * NPARAM + 64) * sizeof(float);
+  IMC_TRY(ensure_buf(ctx, (void**)&ctx->train_buf, ctx->train_bytes, need));
+  d = (float*)ctx->train_buf;
+  float* dfeat = d;
+  float* dtarget = dfeat + (size_t)NF * nsamples;
+  float* dparams = dtarget + nsamples;
+  float* dgrad = dparams + NPARAM;
+  float* dloss = dgrad + NPARAM;
+  IMC_CUDA(cudaMemcpyAsync(dfeat, feat, (size_t)NF * nsamples * sizeof(float),
+                           cudaMemcpyHostToDevice, ctx->stream));
+  IMC_CUDA(cudaMemcpyAsync(dtarget, target, nsamples * sizeof(float), cudaMemcpyHostToDevice,
+                           ctx->stream));
+  IMC_CUDA(cudaMemcpyAsync(dparams, params, NPARAM * sizeof(float), cudaMemcpyHostToDevice,
+                           ctx->stream));
+  IMC_CUDA(cudaMemsetAsync(dgrad, 0, (NPARAM + 1) * sizeof(float), ctx->stream));
+  mlp_grad_kernel<<<(nsamples + TB - 1) / TB, 256, 0, ctx->stream>>>(
+      dparams, dfeat, nsamples, dtarget, nullptr, nsamples, dgrad, dloss);
+  IMC_LAUNCH();
+  IMC_CUDA(cudaMemcpyAsync(grad_out, dgrad, NPARAM * sizeof(float), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+  float l = 0.0f;
+  IMC_CUDA(cudaMemcpyAsync(&l, dloss, sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (loss_out) *loss_out = l;
+  return 0;
+}
+
+// Adam training on normalised features/targets; params in/out (packed).
+extern "C" int imcom_gpu_mlp_train(imcom_ctx* ctx, int nsamples, const float* feat,
+                                   const float* target, int epochs, int batch, float lr,
+                                   unsigned seed, float* params, float* loss_out) {
+  if (!ctx) return -1;
+  if (nsamples <= 0) return -2;
+  if (!feat) return -3;
+  if (!target) return -4;
+  if (epochs <= 0) return -5;
+  if (batch <= 0) return -6;
+  if (!(lr > 0.0f)) return -7;
+  if (!params) return -9;
+  cudaSetDevice(ctx->device);
+  size_t need = ((size_t)NF * nsamples + nsamples + 4 * NPARAM + 64) * sizeof(float) +
+                (size_t)nsamples * sizeof(int);
+  IMC_TRY(ensure_buf(ctx, (void**)&ctx->train_buf, ctx->train_bytes, need));
+  float* dfeat = (float*)ctx->train_buf;
+  float* dtarget = dfeat + (size_t)NF * nsamples;
+  float* dparams = dtarget + nsamples;
+  float* dgrad = dparams + NPARAM;
+  float* dm1 = dgrad + NPARAM + 1;
+  float* dm2 = dm1 + NPARAM;
+  int* didx = (int*)(dm2 + NPARAM + 16);
+  IMC_CUDA(cudaMemcpyAsync(dfeat, feat, (size_t)NF * nsamples * sizeof(float),
+                           cudaMemcpyHostToDevice, ctx->stream));
+  IMC_CUDA(cudaMemcpyAsync(dtarget, target, nsamples * sizeof(float), cudaMemcpyHostToDevice,
+                           ctx->stream));
+  IMC_CUDA(cudaMemcpyAsync(dparams, params, NPARAM * sizeof(float), cudaMemcpyHostToDevice,
+                           ctx->stream));
+  IMC_CUDA(cudaMemsetAsync(dm1, 0, 2 * (NPARAM + 8) * sizeof(float), ctx->stream));
+  // shuffled order per epoch (host xorshift, reproducible from the seed)
+  std::vector<int> order(nsamples);
+  unsigned s = seed ? seed : 1u;
+  auto rnd = [&]() {
+    s ^= s << 13;
+    s ^= s >> 17;
+    s ^= s << 5;
+    return s;
+  };
+  const float b1 = 0.9f, b2 = 0.999f;
+  int step = 0;
+  std::vector<float> eloss(epochs, 0.0f);
+  float* dloss = dgrad + NPARAM;
+  for (int ep = 0; ep < epochs; ++ep) {
+    for (int q = 0; q < nsamples; ++q) order[q] = q;
+    for (int q = nsamples - 1; q > 0; --q) std::swap(order[q], order[rnd() % (q + 1)]);
+    IMC_CUDA(cudaMemcpyAsync(didx, order.data(), nsamples * sizeof(int), cudaMemcpyHostToDevice,
+                             ctx->stream));
+    IMC_CUDA(cudaMemsetAsync(dloss, 0, sizeof(float), ctx->stream));
+    for (int b0 = 0; b0 < nsamples; b0 += batch) {
+      const int nb = std::min(batch, nsamples - b0);
+      IMC_CUDA(cudaMemsetAsync(dgrad, 0, NPARAM * sizeof(float), ctx->stream));
+      mlp_grad_kernel<<<(nb + TB - 1) / TB, 256, 0, ctx->stream>>>(
+          dparams, dfeat, nsamples, dtarget, didx + b0, nb, dgrad, dloss);
+      IMC_LAUNCH();
+      ++step;
+      const float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
+      adam_kernel<<<(NPARAM + 255) / 256, 256, 0, ctx->stream>>>(dparams, dgrad, dm1, dm2, lr, b1,
+                                                                b2, c1, c2, 1.0f / nb);
+      IMC_LAUNCH();
+    }
+    IMC_CUDA(cudaMemcpyAsync(&eloss[ep], dloss, sizeof(float), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+  }
+  IMC_CUDA(cudaMemcpyAsync(params, dparams, NPARAM * sizeof(float), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+  IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (loss_out)
+    for (int ep = 0; ep < epochs; ++ep) loss_out[ep] = eloss[ep] / nsamples;
+  return 0;
 }

@@ -179,6 +179,22 @@ int imcom_gpu_mlp_set_weights(imcom_ctx* ctx, const float* W1,
                               const float* b3, const float* feat_mean,
                               const float* feat_std);
 
+/* Train the MLP on the GPU (Adam, bf16 activations, fp32 accumulation) on
+ * normalised features (12 x nsamples, feature-major) and targets (log10
+ * kappa, normalised).  params (5122 floats: W1 64x12 | b1 64 | W2 64x64 |
+ * b2 64 | W3 2x64 | b3 2, row-major [out][in]) holds the initial values on
+ * entry and the trained values on return; loss_out (epochs) may be NULL.
+ * No reference counterpart. */
+int imcom_gpu_mlp_train(imcom_ctx* ctx, int nsamples, const float* feat,
+                        const float* target, int epochs, int batch, float lr,
+                        unsigned seed, float* params, float* loss_out);
+/* Summed training loss and its gradient (5122 floats) over nsamples samples
+ * at the given parameters: the training kernel on one batch (for gradient
+ * checks).  No reference counterpart. */
+int imcom_gpu_mlp_gradient(imcom_ctx* ctx, int nsamples, const float* feat,
+                           const float* target, const float* params,
+                           float* grad_out, float* loss_out);
+
 /* ---- allocation-free projection ---------------------------------------- */
 
 /* P = Q^T B (the product imcom_gpu_build_P forms) without allocating any

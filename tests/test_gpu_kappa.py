@@ -1,0 +1,104 @@
+"""Learned-kappa bracket on the GPU: the training kernels against the CPU
+oracle, training convergence, the features, and the bracketed bisection's
+contract -- K and U/S bit-identical to the plain bisection with fewer U/S
+evaluations on seeds the model has not seen."""
+import numpy as np
+import pytest
+
+from imcom_b200 import EIGH_DC, EPS, kappa_model as KM, synth
+from oracle import mlp_oracle as M
+
+pytestmark = pytest.mark.gpu
+
+
+def test_mlp_gradient_matches_cpu_oracle(solver):
+    rng = np.random.default_rng(0)
+    p = KM.init_params(5)
+    f = rng.standard_normal((12, 300)).astype(np.float32)
+    t = rng.standard_normal(300).astype(np.float32)
+    g_gpu, l_gpu = solver.mlp_gradient(f, t, p)
+    l_ref, g_ref = M.loss_and_grad(p, f, t)
+    assert abs(l_gpu - l_ref) < 1e-5 * abs(l_ref)
+    assert np.max(np.abs(g_gpu - g_ref)) < 1e-4 * np.max(np.abs(g_ref))
+
+
+def _system(solver, prob, us):
+    solver.set_eigensolver(EIGH_DC)
+    solver.set_problem(prob)
+    C = solver.psf_spectra()
+    solver.build_A(out=False)
+    solver.eigen_A(out=False)
+    solver.build_B(out=False)
+    solver.build_P(out=False)
+    return C
+
+
+def test_features_match_numpy(solver):
+    prob = synth.make("small", 2)
+    us = 1e-6
+    C = _system(solver, prob, us)
+    F = solver.kappa_features(True, us, C)
+    P = solver.build_P()
+    _, L, _ = solver.eigen_A()
+    for a in [0, 37, 255]:
+        dx = np.abs(prob.x_i - prob.X_a[a]) < 1.0
+        dy = np.abs(prob.y_i - prob.Y_a[a]) < 1.0
+        box = dx & dy
+        assert F[0, a] == box.sum()
+        assert F[1, a] == len(set(prob.exp_i[box]))
+        r = np.where(L > 0, L / L[0], 0.0)
+        with np.errstate(divide="ignore"):
+            b = np.where(r > 0, np.floor(-np.log10(r) * 0.5), 7).clip(0, 7).astype(int)
+        for k in range(8):
+            s = np.sum(P[b == k, a] ** 2)
+            lc = L[0] * 10.0 ** (-(2 * k + 1))
+            ref = np.log10(s / (4 * C * lc) + 1e-30)
+            assert abs(F[2 + k, a] - ref) < 1e-4 * max(1.0, abs(ref))
+    assert np.allclose(F[10], np.log10(us))
+
+
+@pytest.fixture(scope="module")
+def small_model(solver):
+    rng = np.random.default_rng(7)
+    probs = [synth.make("small", 100 + s) for s in range(32)]
+    targets = list(10.0 ** rng.uniform(np.log10(4e-7), np.log10(4e-6), len(probs)))
+    solver.set_eigensolver(EIGH_DC)
+    feat, y = KM.collect(solver, probs, targets)
+    model, loss = KM.train(solver, feat, y, epochs=60, batch=256, lr=3e-3)
+    return model, loss
+
+
+def test_training_reduces_loss(small_model):
+    _, loss = small_model
+    assert loss[-1] < 0.5 * loss[0]
+
+
+@pytest.mark.parametrize("seed,us", [(0, 1e-6), (3, 2e-6)])
+def test_learned_bisection_identical_and_cheaper(solver, small_model, seed, us):
+    model, _ = small_model
+    prob = synth.make("small", seed)  # seeds not used in training
+    C = _system(solver, prob, us)
+    kmin, kmax = C * EPS, C / EPS
+    tol = us * 1e-3
+    K0, U0, n0 = solver.bisect_kappa(True, us, kmin, kmax, tol, 40, C)
+    model.install(solver)
+    K1, U1, n1, fb = solver.bisect_kappa_learned(True, us, kmin, kmax, tol, 40, C)
+    assert np.array_equal(K0, K1)
+    assert np.array_equal(U0, U1)
+    assert n1.mean() < 0.85 * n0.mean(), (n0.mean(), n1.mean(), fb.mean())
+    # T from the learned kappa equals T from the plain kappa
+    T1 = solver.build_T()
+    solver.bisect_kappa(True, us, kmin, kmax, tol, 40, C)
+    assert np.array_equal(T1, solver.build_T())
+
+
+def test_learned_bisection_S_mode_identical(solver, small_model):
+    model, _ = small_model
+    prob = synth.make("small", 5)
+    C = _system(solver, prob, 0.12)
+    kmin, kmax = C * EPS, C / EPS
+    K0, S0, n0 = solver.bisect_kappa(False, 0.12, kmin, kmax, 1e-4, 53, C)
+    model.install(solver)
+    K1, S1, n1, fb = solver.bisect_kappa_learned(False, 0.12, kmin, kmax, 1e-4, 53, C)
+    assert np.array_equal(K0, K1)
+    assert np.array_equal(S0, S1)
