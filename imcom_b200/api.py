@@ -21,6 +21,11 @@ from ._lib import ImcomError
 
 EIGH_DC, EIGH_JACOBI, EIGH_LIBRARY = 0, 1, 2
 OPT_EIGENSOLVER, OPT_EIGEN_MAXITER = 1, 2
+OPT_PRECISION, OPT_SPLIT_SLICES_P, OPT_SPLIT_SLICES_T = 3, 4, 5
+OPT_SPLIT_TOL_US, OPT_SPLIT_TOL_T = 6, 7
+PREC_FP64, PREC_SPLIT = 0, 1
+SPLIT_INFO = ("slices_P", "slices_T", "fp64_pixels_P", "fp64_columns_T", "max_bound_US",
+              "max_bound_T_from_P", "max_bound_T_product", "P_split")
 STAGES = ("spectra", "build_A", "eigen_A", "build_B", "build_P", "bisect", "build_T", "epilogue",
           "eig_tridiag", "eig_dc", "eig_backtransform")
 EPS = 1.1102230246251565e-16  # DLAMCH('Epsilon')
@@ -80,6 +85,27 @@ class Solver:
 
     def set_eigensolver(self, mode: int):
         self.set_option(OPT_EIGENSOLVER, mode)
+
+    def set_precision(self, split: bool, slices_P: int = 7, slices_T: int = 6,
+                      tol_us_exp: int = 7, tol_t_exp: int = 9):
+        """FP64 (split=False) or the audited int8 split product for P and T."""
+        self.set_option(OPT_PRECISION, PREC_SPLIT if split else PREC_FP64)
+        self.set_option(OPT_SPLIT_SLICES_P, slices_P)
+        self.set_option(OPT_SPLIT_SLICES_T, slices_T)
+        self.set_option(OPT_SPLIT_TOL_US, tol_us_exp)
+        self.set_option(OPT_SPLIT_TOL_T, tol_t_exp)
+
+    def split_pixels(self):
+        """(fp64_P, fp64_T): per-pixel flags of the audit's FP64 recomputations."""
+        fp = np.zeros(self.m, dtype=np.int32)
+        ft = np.zeros(self.m, dtype=np.int32)
+        self._call("imcom_gpu_split_pixels", _ptr(fp), _ptr(ft))
+        return fp.astype(bool), ft.astype(bool)
+
+    def split_info(self) -> dict:
+        v = np.zeros(8)
+        self._call("imcom_gpu_split_info", _ptr(v))
+        return dict(zip(SPLIT_INFO, v.tolist()))
 
     def stage_times(self) -> dict:
         ms = np.zeros(len(STAGES))

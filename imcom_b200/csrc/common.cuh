@@ -35,6 +35,18 @@ struct MlpWeights {
 
 struct EigWork;  // eigen.cu
 
+// One operand of the split-precision product (ozaki.cu): S int8 digit
+// slices of an FP64 matrix in tensor-core tile order, plus the power-of-two
+// scale of every operand row.
+struct SplitOp {
+  int8_t* dig = nullptr;
+  double* scale = nullptr;
+  int* exps = nullptr;
+  size_t dig_bytes = 0, scale_bytes = 0, exps_bytes = 0;
+  long long rows = 0, K = 0, rb = 0, kb = 0;
+  int S = 0, R = 0;
+};
+
 }  // namespace imcom
 
 struct imcom_ctx {
@@ -88,6 +100,23 @@ struct imcom_ctx {
   size_t train_bytes = 0;
   void* gemm_ws = nullptr;  // split-K partial sums
   size_t gemm_ws_bytes = 0;
+
+  // split-precision products (IMCOM_PREC_SPLIT)
+  int prec = IMCOM_PREC_FP64;
+  int split_SP = 7, split_ST = 6;        // digit slices of the P and T products
+  double split_tol_us = 1e-7, split_tol_t = 1e-9;
+  imcom::SplitOp sq_P, sq_T, sb_P, spt_T;  // Q columns, Q rows, B, P~
+  bool sq_P_valid = false, sq_T_valid = false;
+  double sq_T_norm = 0.0;  // 2-norm of the row scales of Q
+  bool p_split = false;    // the resident P came from the split product
+  bool p_audited = false, t_audited = false;  // sp_flag holds the audit's verdicts
+  double* sp_margin = nullptr;  // per pixel: smallest distance of f to a decision threshold
+  double* sp_est = nullptr;     // per pixel: U/S bound, T-from-P bound, T-product bound
+  int* sp_flag = nullptr;
+  int* sp_list = nullptr;
+  size_t sp_margin_bytes = 0, sp_est_bytes = 0, sp_flag_bytes = 0, sp_list_bytes = 0;
+  imcom::DMat fbX, fbY;  // gathered columns for the FP64 recomputation
+  double split_info[8] = {};
 
   imcom::EigWork* eig = nullptr;
   imcom::MlpWeights mlp;
@@ -161,6 +190,24 @@ int dgemm(imcom_ctx* ctx, char transA, char transB, long long M, long long N,
           long long ldc);
 
 int eigen_dc(imcom_ctx* ctx, const DMat& A, DMat& W, double* w);
+
+// Split-precision products (ozaki.cu).  split_operand slices the operand
+// rows of X (cols: row r = column r of X; else row r of X) into S digits
+// for row blocks of R (128: A operand, 64: B operand); split_gemm forms
+// C = alpha * A B^T (C column-major, M = A rows, N = B rows).
+int split_operand(imcom_ctx* ctx, const double* X, long long ld, long long rows, long long K,
+                  bool cols, int S, int R, SplitOp& op);
+int split_gemm(imcom_ctx* ctx, const SplitOp& a, const SplitOp& b, double alpha, double* C,
+               long long ldc);
+long long split_max_k(int S);
+// The GEMM's bounded waits OR an error code into a device word; it is
+// zeroed before a split stage and checked after the stage's last sync.
+int split_reset_error(imcom_ctx* ctx);
+int split_check_error(imcom_ctx* ctx);
+void split_free(SplitOp& op);
+void split_release(imcom_ctx* ctx);  // split.cu
+int build_P_split(imcom_ctx* ctx);
+int build_T_split(imcom_ctx* ctx);
 int eigen_jacobi(imcom_ctx* ctx, const DMat& A, DMat& Q, double* L);
 int eigen_library(imcom_ctx* ctx, const DMat& A, DMat& Q, double* L);
 void eig_free(imcom_ctx* ctx);

@@ -166,6 +166,7 @@ int imcom_gpu_destroy(imcom_ctx* ctx) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   eig_free(ctx);
+  split_release(ctx);
   void* ptrs[] = {ctx->x, ctx->y, ctx->X, ctx->Y, ctx->I, ctx->Nd, ctx->exp_i, ctx->G,
                   ctx->Gamma, ctx->Gt, ctx->Gammat, ctx->A.p, ctx->Q.p, ctx->B.p, ctx->P.p,
                   ctx->T.p, ctx->Pt.p, ctx->L, ctx->K, ctx->US, ctx->H, ctx->S, ctx->U,
@@ -207,6 +208,21 @@ int imcom_gpu_set_option(imcom_ctx* ctx, int option, long long value) {
     case IMCOM_OPT_EIGEN_MAXITER:
       if (value < 0) return -3;
       ctx->eig_maxiter = value;
+      return 0;
+    case IMCOM_OPT_PRECISION:
+      if (value != IMCOM_PREC_FP64 && value != IMCOM_PREC_SPLIT) return -3;
+      ctx->prec = (int)value;
+      return 0;
+    case IMCOM_OPT_SPLIT_SLICES_P:
+    case IMCOM_OPT_SPLIT_SLICES_T:
+      if (value < 2 || value > 8) return -3;
+      (option == IMCOM_OPT_SPLIT_SLICES_P ? ctx->split_SP : ctx->split_ST) = (int)value;
+      return 0;
+    case IMCOM_OPT_SPLIT_TOL_US:
+    case IMCOM_OPT_SPLIT_TOL_T:
+      if (value < 0 || value > 300) return -3;
+      (option == IMCOM_OPT_SPLIT_TOL_US ? ctx->split_tol_us : ctx->split_tol_t) =
+          std::pow(10.0, -(double)value);
       return 0;
     default:
       return -2;
@@ -335,6 +351,7 @@ int imcom_gpu_load_QL(imcom_ctx* ctx, const double* Q, const double* L) {
                            ctx->stream));
   IMC_CUDA(cudaStreamSynchronize(ctx->stream));
   ctx->have_QL = true;
+  ctx->sq_P_valid = ctx->sq_T_valid = false;
   return 0;
 }
 
@@ -357,6 +374,7 @@ int imcom_gpu_load_P(imcom_ctx* ctx, const double* P) {
   IMC_TRY(upload_mat(ctx, ctx->P, P, ctx->n, ctx->m));
   IMC_CUDA(cudaStreamSynchronize(ctx->stream));
   ctx->have_P = true;
+  ctx->p_split = false;
   return 0;
 }
 
@@ -408,6 +426,7 @@ int imcom_gpu_device_buffer(imcom_ctx* ctx, char which, void** dptr, long long* 
     case 'B': p = ctx->B.p; l = ctx->B.ld; break;
     case 'P': p = ctx->P.p; l = ctx->P.ld; break;
     case 'T': p = ctx->T.p; l = ctx->T.ld; break;
+    case 'W': p = ctx->Pt.p; l = ctx->Pt.ld; break;
     case 'L': p = ctx->L; l = ctx->n; break;
     case 'K': p = ctx->K; l = ctx->m; break;
     case 'H': p = ctx->H; l = ctx->m; break;

@@ -134,6 +134,7 @@ extern "C" int imcom_gpu_eigen_A(imcom_ctx* ctx, double* Q_out, double* L_out, d
   IMC_LAUNCH();
   stage_end(ctx, ST_EIG);
   ctx->have_QL = true;
+  ctx->sq_P_valid = ctx->sq_T_valid = false;
   ctx->have_P = ctx->have_K = ctx->have_T = ctx->have_Pt = false;
   std::vector<double> hL(n);
   IMC_CUDA(cudaMemcpyAsync(hL.data(), ctx->L, n * sizeof(double), cudaMemcpyDeviceToHost,

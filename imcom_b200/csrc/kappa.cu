@@ -190,6 +190,7 @@ __global__ void learned_bisect_kernel(BisectArgs a, PixelSmem plan, LearnedExtra
     double k_root = 0.0, us = 0.0;
     const double ceps = __dmul_rn(a.C, a.eps);
     const double thr = fmax(a.tol, ceps) + ex.margin;
+    double mg = INFINITY;  // smallest decision margin over the evaluations
     // One-sided bounds from the evaluated bracket ends.  U rises with kappa:
     // an end with f < -thr makes every midpoint at or below it a known
     // accept; an end with f >= C eps (+ margin) makes every midpoint at or
@@ -204,6 +205,7 @@ __global__ void learned_bisect_kernel(BisectArgs a, PixelSmem plan, LearnedExtra
       const double fp =
           __dsub_rn(warp_us(U, lam, col, a.Nd, a.n, pow(10.0, pt), a.C, lane), a.US_max);
       ++nev;
+      mg = fmin(mg, fmin(fabs(fp + thr), fabs(fp - (ceps + ex.margin))));
       if (fp < -thr) accb = U ? fmax(accb, pt) : fmin(accb, pt);
       else if (fp >= ceps + ex.margin) rejb = U ? fmin(rejb, pt) : fmax(rejb, pt);
     }
@@ -223,6 +225,7 @@ __global__ void learned_bisect_kernel(BisectArgs a, PixelSmem plan, LearnedExtra
         ++nev;
         f0 = __dsub_rn(us, a.US_max);
         have_f0 = true;
+        mg = fmin(mg, fabs(f0));
       }
       if (have_f0 && !(f0 < 0.0)) {
         k_root = U ? a.k_min : a.k_max;
@@ -245,6 +248,7 @@ __global__ void learned_bisect_kernel(BisectArgs a, PixelSmem plan, LearnedExtra
           const double fmid =
               __dsub_rn(warp_us(U, lam, col, a.Nd, a.n, pow(10.0, mid), a.C, lane), a.US_max);
           ++nev;
+          mg = fmin(mg, decision_margin(fmid, a.tol, ceps));
           if (fmid < 0.0) {
             root = mid;
             any_acc = true;
@@ -259,6 +263,7 @@ __global__ void learned_bisect_kernel(BisectArgs a, PixelSmem plan, LearnedExtra
             const double k0 = U ? a.k_min : a.k_max;
             us = warp_us(U, lam, col, a.Nd, a.n, k0, a.C, lane);
             ++nev;
+            mg = fmin(mg, fabs(__dsub_rn(us, a.US_max)));
           }
         } else if (last_known) {
           // value the reference holds at the last accepted midpoint
@@ -270,7 +275,7 @@ __global__ void learned_bisect_kernel(BisectArgs a, PixelSmem plan, LearnedExtra
         k_root = pow(10.0, root);
       }
     }
-    write_pixel(a, lam, col, pix, lane, nev, k_root, us);
+    write_pixel(a, lam, col, pix, lane, nev, k_root, us, mg);
     __syncwarp();
   }
 }
@@ -523,12 +528,14 @@ extern "C" int imcom_gpu_bisect_kappa_learned(imcom_ctx* ctx, int UnotS, double 
   a.ldt = ctx->Pt.ld;
   IMC_TRY(ensure_buf(ctx, (void**)&ctx->fb, ctx->fb_bytes, (size_t)ctx->m * sizeof(int)));
   ex.fallback = ctx->fb;
+  if (ctx->p_split) IMC_TRY(split_margin_buffer(ctx, a));
   PixelSmem plan = plan_pixel_smem(ctx->n, 190 * 1024);
   IMC_CUDA(cudaFuncSetAttribute(learned_bisect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)plan.bytes));
   learned_bisect_kernel<<<pixel_grid(ctx, plan, ctx->m), plan.warps * 32, plan.bytes,
                           ctx->stream>>>(a, plan, ex);
   IMC_LAUNCH();
+  if (ctx->p_split) IMC_TRY(split_audit(ctx, a));
   stage_end(ctx, ST_BISECT);
   ctx->have_K = true;
   ctx->have_Pt = true;

@@ -34,7 +34,9 @@ __global__ void bisect_kernel(BisectArgs a, PixelSmem plan) {
     lam = smem;
   }
   double* mycol = plan.col_smem ? smem + (size_t)a.n * (1 + warp) : nullptr;
-  for (int pix = blockIdx.x * plan.warps + warp; pix < a.m; pix += gridDim.x * plan.warps) {
+  const int total = a.list ? a.count : a.m;
+  for (int t = blockIdx.x * plan.warps + warp; t < total; t += gridDim.x * plan.warps) {
+    const int pix = a.list ? a.list[t] : t;
     const double* col = a.P + (size_t)pix * a.ldp;
     if (mycol) {
       for (int p = lane; p < a.n; p += 32) mycol[p] = col[p];
@@ -42,9 +44,9 @@ __global__ void bisect_kernel(BisectArgs a, PixelSmem plan) {
       col = mycol;
     }
     int nev;
-    double k, us;
-    bisect_pixel(a, lam, col, lane, &nev, &k, &us);
-    write_pixel(a, lam, col, pix, lane, nev, k, us);
+    double k, us, mg;
+    bisect_pixel(a, lam, col, lane, &nev, &k, &us, &mg);
+    write_pixel(a, lam, col, pix, lane, nev, k, us, mg);
     __syncwarp();
   }
 }
@@ -113,6 +115,9 @@ int fill_bisect_args(imcom_ctx* ctx, BisectArgs& a, int UnotS, double US_max, do
   a.K = ctx->K;
   a.US = ctx->US;
   a.nev = ctx->nev;
+  a.margin = nullptr;
+  a.list = nullptr;
+  a.count = 0;
   a.n = ctx->n;
   a.m = ctx->m;
   a.UnotS = UnotS ? 1 : 0;
@@ -131,6 +136,18 @@ int fill_bisect_args(imcom_ctx* ctx, BisectArgs& a, int UnotS, double US_max, do
 int pixel_grid(imcom_ctx* ctx, const PixelSmem& plan, int m) {
   int blocks = (m + plan.warps - 1) / plan.warps;
   return blocks;
+}
+
+int launch_bisect(imcom_ctx* ctx, const BisectArgs& a) {
+  PixelSmem plan = plan_pixel_smem(ctx->n);
+  IMC_CUDA(cudaFuncSetAttribute(bisect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)plan.bytes));
+  const int total = a.list ? a.count : a.m;
+  if (total <= 0) return 0;
+  bisect_kernel<<<pixel_grid(ctx, plan, total), plan.warps * 32, plan.bytes, ctx->stream>>>(a,
+                                                                                          plan);
+  IMC_LAUNCH();
+  return 0;
 }
 
 int copy_pixel_outputs(imcom_ctx* ctx, double* K_out, double* US_out, int* nev_out) {
@@ -158,15 +175,22 @@ extern "C" int imcom_gpu_build_P(imcom_ctx* ctx, double* P_out) {
   cudaSetDevice(ctx->device);
   stage_begin(ctx, ST_P);
   IMC_TRY(ensure_mat(ctx, ctx->P, ctx->n, ctx->m));
-  // P = Q^T B (DGEMM 'T', 'N', n, m, n)
-  IMC_TRY(dgemm(ctx, 'T', 'N', ctx->n, ctx->m, ctx->n, 1.0, ctx->Q.p, ctx->Q.ld, ctx->B.p,
-                ctx->B.ld, 0.0, ctx->P.p, ctx->P.ld));
+  if (ctx->prec == IMCOM_PREC_SPLIT) {
+    IMC_TRY(build_P_split(ctx));
+  } else {
+    // P = Q^T B (DGEMM 'T', 'N', n, m, n)
+    IMC_TRY(dgemm(ctx, 'T', 'N', ctx->n, ctx->m, ctx->n, 1.0, ctx->Q.p, ctx->Q.ld, ctx->B.p,
+                  ctx->B.ld, 0.0, ctx->P.p, ctx->P.ld));
+    ctx->p_split = false;
+    ctx->p_audited = ctx->t_audited = false;
+  }
   stage_end(ctx, ST_P);
   ctx->have_P = true;
   ctx->have_K = ctx->have_T = ctx->have_Pt = false;
   if (P_out) {
     IMC_TRY(download_mat(ctx, ctx->P, P_out));
     IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (ctx->p_split) IMC_TRY(split_check_error(ctx));
   }
   return 0;
 }
@@ -182,11 +206,9 @@ extern "C" int imcom_gpu_bisect_kappa(imcom_ctx* ctx, int UnotS, double US_max, 
   IMC_TRY(ensure_mat(ctx, ctx->Pt, ctx->n, ctx->m));
   a.Pt = ctx->Pt.p;
   a.ldt = ctx->Pt.ld;
-  PixelSmem plan = plan_pixel_smem(ctx->n);
-  IMC_CUDA(cudaFuncSetAttribute(bisect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)plan.bytes));
-  bisect_kernel<<<pixel_grid(ctx, plan, ctx->m), plan.warps * 32, plan.bytes, ctx->stream>>>(a, plan);
-  IMC_LAUNCH();
+  if (ctx->p_split) IMC_TRY(split_margin_buffer(ctx, a));
+  IMC_TRY(launch_bisect(ctx, a));
+  if (ctx->p_split) IMC_TRY(split_audit(ctx, a));
   stage_end(ctx, ST_BISECT);
   ctx->have_K = true;
   ctx->have_Pt = true;
@@ -206,9 +228,16 @@ extern "C" int imcom_gpu_build_T(imcom_ctx* ctx, double* T_out) {
     ctx->have_Pt = true;
   }
   IMC_TRY(ensure_mat(ctx, ctx->T, ctx->n, ctx->m));
-  // T = -1/2 Q P~ with P~(:, a) = P(:, a) / (L + K_a) written by the bisection.
-  IMC_TRY(dgemm(ctx, 'N', 'N', ctx->n, ctx->m, ctx->n, -0.5, ctx->Q.p, ctx->Q.ld, ctx->Pt.p,
-                ctx->Pt.ld, 0.0, ctx->T.p, ctx->T.ld));
+  if (ctx->prec == IMCOM_PREC_SPLIT) {
+    IMC_TRY(build_T_split(ctx));
+  } else {
+    // T = -1/2 Q P~ with P~(:, a) = P(:, a) / (L + K_a) written by the bisection.
+    IMC_TRY(dgemm(ctx, 'N', 'N', ctx->n, ctx->m, ctx->n, -0.5, ctx->Q.p, ctx->Q.ld, ctx->Pt.p,
+                  ctx->Pt.ld, 0.0, ctx->T.p, ctx->T.ld));
+    ctx->split_info[3] = 0.0;
+    ctx->split_info[6] = 0.0;
+    ctx->t_audited = false;
+  }
   stage_end(ctx, ST_T);
   ctx->have_T = true;
   if (T_out) {

@@ -17,6 +17,9 @@ struct BisectArgs {
   double* K;
   double* US;
   int* nev;
+  double* margin;   // per pixel: smallest |f - threshold| over the evaluations, may be null
+  const int* list;  // pixels to solve (count of them), or null for all m
+  int count;
   int n, m;
   int UnotS;
   double US_max, k_min, k_max, tol, C, eps;
@@ -24,18 +27,29 @@ struct BisectArgs {
   int maxnits;
 };
 
+// Distance of f = U - U_max (or S - S_max) to the thresholds the bisection
+// compares it with (0, tol, C eps): a perturbation of f smaller than this
+// cannot change any decision taken on it.
+__device__ __forceinline__ double decision_margin(double f, double tol, double ceps) {
+  const double af = fabs(f);
+  return fmin(af, fmin(fabs(af - tol), fabs(af - ceps)));
+}
+
 // The reference's bisection for one pixel (imcom_bisect_by_U / _by_S).
+// *mg_out receives the smallest decision margin over the evaluations.
 __device__ __forceinline__ void bisect_pixel(const BisectArgs& a, const double* lam,
                                              const double* col, int lane, int* nev_out,
-                                             double* k_out, double* us_out) {
+                                             double* k_out, double* us_out, double* mg_out) {
   const bool U = a.UnotS != 0;
   int nev = 0;
   double k_root, us;
+  const double ceps = __dmul_rn(a.C, a.eps);
   // imcom_bisect_by_U: U(k_min) first; imcom_bisect_by_S: S(k_max) first.
   double k0 = U ? a.k_min : a.k_max;
   us = warp_us(U, lam, col, a.Nd, a.n, k0, a.C, lane);
   nev = 1;
   double f = __dsub_rn(us, a.US_max);
+  double mg = fabs(f);
   if (!(f < 0.0)) {
     k_root = k0;
   } else {
@@ -47,26 +61,29 @@ __device__ __forceinline__ void bisect_pixel(const BisectArgs& a, const double* 
       double mid = __dadd_rn(root, dx);
       double fmid = __dsub_rn(warp_us(U, lam, col, a.Nd, a.n, pow(10.0, mid), a.C, lane), a.US_max);
       ++nev;
+      mg = fmin(mg, decision_margin(fmid, a.tol, ceps));
       if (fmid < 0.0) {
         root = mid;
         us = __dadd_rn(fmid, a.US_max);
         if (fabs(fmid) < a.tol) break;
       }
-      if (fabs(fmid) < __dmul_rn(a.C, a.eps)) break;
+      if (fabs(fmid) < ceps) break;
     }
     k_root = pow(10.0, root);
   }
   *nev_out = nev;
   *k_out = k_root;
   *us_out = us;
+  *mg_out = mg;
 }
 
 __device__ __forceinline__ void write_pixel(const BisectArgs& a, const double* lam, const double* col, int pix,
-                            int lane, int nev, double k, double us) {
+                            int lane, int nev, double k, double us, double mg) {
   if (lane == 0) {
     a.K[pix] = k;
     a.US[pix] = us;
     if (a.nev) a.nev[pix] = nev;
+    if (a.margin) a.margin[pix] = mg;
   }
   if (a.Pt) {
     double* dst = a.Pt + (size_t)pix * a.ldt;
@@ -79,5 +96,12 @@ int fill_bisect_args(imcom_ctx* ctx, BisectArgs& a, int UnotS, double US_max, do
 int pixel_grid(imcom_ctx* ctx, const PixelSmem& plan, int m);
 int copy_pixel_outputs(imcom_ctx* ctx, double* K_out, double* US_out, int* nev_out);
 int make_Pt(imcom_ctx* ctx);
+// Plain bisection over a.list (or all pixels).
+int launch_bisect(imcom_ctx* ctx, const BisectArgs& a);
+// Split-precision P: per-pixel margin buffer before the bisection, and the
+// error audit with FP64 recomputation of the failing pixels after it
+// (split.cu).
+int split_margin_buffer(imcom_ctx* ctx, BisectArgs& a);
+int split_audit(imcom_ctx* ctx, const BisectArgs& a);
 
 }  // namespace imcom

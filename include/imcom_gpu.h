@@ -44,6 +44,7 @@ typedef struct imcom_ctx imcom_ctx;
 #define IMCOM_ERR_ALLOC 6       /* device allocation failed                   */
 #define IMCOM_ERR_NOT_FINITE 7  /* non-finite input                           */
 #define IMCOM_ERR_NOALLOC_SIZE 8 /* problem too large for imcom_gpu_build_P_noalloc */
+#define IMCOM_ERR_SPLIT 9       /* split-precision product unavailable (K too large, pipeline wait ran out) */
 
 /* Eigensolver selection for imcom_gpu_set_option(IMCOM_OPT_EIGENSOLVER). */
 #define IMCOM_EIGH_DC 0         /* own tridiagonalisation + divide & conquer  */
@@ -53,6 +54,19 @@ typedef struct imcom_ctx imcom_ctx;
 /* Options for imcom_gpu_set_option. */
 #define IMCOM_OPT_EIGENSOLVER 1
 #define IMCOM_OPT_EIGEN_MAXITER 2 /* iteration cap of the iterative solvers  */
+/* Arithmetic of P = Q^T B and T = -1/2 Q P~ (the reference's DGEMM,
+ * imcom_matrix.f90:699, and DGEMVs, imcom_matrix.f90:734). */
+#define IMCOM_OPT_PRECISION 3
+#define IMCOM_PREC_FP64 0       /* FP64 tensor cores (default)                 */
+#define IMCOM_PREC_SPLIT 1      /* int8 digit slices on the tensor cores, exact
+                                   int32 sums, per-pixel error audit and FP64
+                                   recomputation of the pixels that fail it   */
+#define IMCOM_OPT_SPLIT_SLICES_P 4 /* digit slices of the P product, 2..8 (7) */
+#define IMCOM_OPT_SPLIT_SLICES_T 5 /* digit slices of the T product, 2..8 (6) */
+#define IMCOM_OPT_SPLIT_TOL_US 6   /* audit bound on the relative U/S error of a
+                                      kept pixel: 10^-value (7)                */
+#define IMCOM_OPT_SPLIT_TOL_T 7    /* audit bound on the relative error of a
+                                      kept T column: 10^-value (9)             */
 
 /* ---- context ---------------------------------------------------------- */
 
@@ -119,7 +133,10 @@ int imcom_gpu_build_B(imcom_ctx* ctx, int npoly, int npad, double* B_out);
 int imcom_gpu_load_B(imcom_ctx* ctx, const double* B);
 
 /* P = Q^T B in FP64 (imcom_build_P, :682-712; build branch of imcom_get_P,
- * :113-151).  P2 = P*P is formed where it is used, bit-identical. */
+ * :113-151).  P2 = P*P is formed where it is used, bit-identical.  With
+ * IMCOM_PREC_SPLIT the product runs on the int8 digit slices; the next
+ * bisection audits every pixel and recomputes in FP64 the P columns of the
+ * pixels whose kappa or U/S accuracy the split product cannot guarantee. */
 int imcom_gpu_build_P(imcom_ctx* ctx, double* P_out);
 int imcom_gpu_load_P(imcom_ctx* ctx, const double* P);
 
@@ -150,7 +167,9 @@ int imcom_gpu_bisect_kappa_learned(imcom_ctx* ctx, int UnotS, double US_max,
 
 /* T(:,a) = -1/2 Q (P(:,a) / (L + K_a)) (imcom_build_T,
  * imcom_matrix.f90:716-750).  Needs the bisection to have run (or
- * imcom_gpu_load_K).  T_out (n, m) may be NULL. */
+ * imcom_gpu_load_K).  T_out (n, m) may be NULL.  With IMCOM_PREC_SPLIT the
+ * product runs on the int8 digit slices and the columns whose error bound
+ * exceeds the T tolerance are recomputed in FP64. */
 int imcom_gpu_build_T(imcom_ctx* ctx, double* T_out);
 /* T-reuse path (imcom_bisect.f90:47-62): T read from FITS by the caller. */
 int imcom_gpu_load_T(imcom_ctx* ctx, const double* T);
@@ -195,6 +214,26 @@ int imcom_gpu_mlp_gradient(imcom_ctx* ctx, int nsamples, const float* feat,
                            const float* target, const float* params,
                            float* grad_out, float* loss_out);
 
+/* ---- split-precision products (no reference counterpart) --------------- */
+
+/* Report of the split-precision path (IMCOM_OPT_PRECISION = IMCOM_PREC_SPLIT)
+ * for the resident solve: info[0] digit slices of P, info[1] digit slices of
+ * T, info[2] pixels whose P column was recomputed in FP64 by the audit of the
+ * last bisection, info[3] pixels whose T column was recomputed in FP64 by
+ * the last imcom_gpu_build_T, info[4] largest bound on the relative U (or S)
+ * error among the pixels kept, info[5] largest bound on the relative T
+ * column error caused by the split P among the pixels kept, info[6] the same
+ * for the split T product, info[7] 1 if the resident P came from the split
+ * product.  Bounds are six standard deviations of the error model: digit
+ * rounding of each product term with standard deviation at most
+ * 0.5 * 2^(1-8S) * sqrt(K) * scale_row * scale_col. */
+int imcom_gpu_split_info(imcom_ctx* ctx, double* info8);
+/* Per pixel (m each, may be NULL): 1 where the audit of the last bisection
+ * recomputed the P column in FP64 (fp64_P), 1 where the last
+ * imcom_gpu_build_T recomputed the T column in FP64 (fp64_T); zeros when no
+ * split product was audited. */
+int imcom_gpu_split_pixels(imcom_ctx* ctx, int* fp64_P, int* fp64_T);
+
 /* ---- allocation-free projection ---------------------------------------- */
 
 /* P = Q^T B (the product imcom_gpu_build_P forms) without allocating any
@@ -225,7 +264,8 @@ int imcom_gpu_build_P_noalloc(const double* dQ, long long ldq, const double* dB,
 /* ---- device views (for callers that keep data on the GPU) -------------- */
 
 /* Device pointer and leading dimension of an internal buffer:
- * which = 'A','Q','L','B','P','T','K','H','S','U' (column-major, ld rows). */
+ * which = 'A','Q','L','B','P','T','K','H','S','U', or 'W' for the T operand
+ * P~ = P(:,a) / (L + K_a) (column-major, ld rows). */
 int imcom_gpu_device_buffer(imcom_ctx* ctx, char which, void** dptr,
                             long long* ld);
 /* Number of this library's own kernel launches since the process started

@@ -1,0 +1,189 @@
+"""Split-precision P and T (int8 digit slices on the tcgen05 tensor cores)
+through the C-ABI.
+
+* The tensor-core product equals the CPU model of the split product
+  (oracle/split_oracle.py) bit for bit, including row/column/K tails.
+* A whole split solve gives the same kappa and evaluation counts as the FP64
+  path, U/S within 1e-6 relative (and within the reported bound), T columns
+  within 1e-8 relative, H within 1e-8 relative (normwise).
+* Too few slices make the audit send pixels back to FP64 and the bars still
+  hold; an audit tolerance no pixel can meet recomputes everything in FP64
+  and reproduces the FP64 path bit for bit.
+"""
+import numpy as np
+import pytest
+
+from imcom_b200 import EPS, synth
+from oracle import oracle as O
+from oracle import split_oracle as SO
+
+from devcopy import download
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture()
+def sp(solver):
+    solver.set_precision(True)
+    yield solver
+    solver.set_precision(False)
+
+
+def system(s, prob):
+    s.set_problem(prob)
+    C = s.psf_spectra()
+    s.build_A(out=False)
+    Q, L, _ = s.eigen_A()
+    B = s.build_B()
+    return C, Q, L, B
+
+
+def stage2(s, C, UnotS, US, tol, learned=False):
+    """P -> kappa -> T -> maps on the resident system (the cached-system path)."""
+    r = {"P": s.build_P()}
+    if learned:
+        r["K"], r["US"], r["nevals"], _ = s.bisect_kappa_learned(UnotS, US, C * EPS, C / EPS,
+                                                                 tol, 53, C)
+    else:
+        r["K"], r["US"], r["nevals"] = s.bisect_kappa(UnotS, US, C * EPS, C / EPS, tol, 53, C)
+    r["T"] = s.build_T()
+    r["S"] = s.build_S() if UnotS else r["US"]
+    r["U"] = r["US"] if UnotS else s.build_U(C)
+    r["H"] = s.build_image()
+    return r
+
+
+def colrel(a, b):
+    return np.linalg.norm(a - b, axis=0) / np.maximum(np.linalg.norm(b, axis=0), 1e-300)
+
+
+def relmax(a, b):
+    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)))
+
+
+@pytest.mark.parametrize("wl,S", [("tiny", 7), ("small", 7), ("small", 3), ("small_rot", 8)])
+def test_split_P_bit_exact(sp, wl, S):
+    prob = synth.make(wl, 1)
+    sp.set_precision(True, slices_P=S)
+    _, Q, _, B = system(sp, prob)
+    P = sp.build_P()
+    assert sp.split_info()["P_split"] == 1.0
+    assert np.array_equal(P, SO.split_product(Q.T, B.T, S))
+
+
+def test_split_T_bit_exact(sp):
+    prob = synth.make("small", 2)
+    C, Q, L, _ = system(sp, prob)
+    sp.build_P(out=False)
+    K, _, _ = sp.bisect_kappa(True, 1e-6, C * EPS, C / EPS, 1e-8, 40, C)
+    T = sp.build_T()
+    info = sp.split_info()
+    n, m = prob.n, prob.m
+    P = download(sp, "P", n, m)
+    Pt = download(sp, "W", n, m)
+    assert np.array_equal(Pt, P / (L[:, None] + K[None, :]))
+    ref = SO.split_product(Q, Pt.T, int(info["slices_T"]), alpha=-0.5)
+    same = np.all(T == ref, axis=0)
+    assert same.sum() >= m - info["fp64_columns_T"]
+    assert np.max(colrel(T, ref)) < 1e-8
+
+
+CASES = [("small_rot", True, 1e-6, 1e-8), ("small_rot", True, 1e-2, 1e-5),
+         ("small", False, 0.12, 1e-4)]
+
+
+@pytest.mark.parametrize("wl,UnotS,US,tol", CASES)
+def test_split_solve_matches_fp64(solver, wl, UnotS, US, tol):
+    prob = synth.make(wl, 3)
+    C, _, _, _ = system(solver, prob)
+    solver.set_precision(False)
+    r64 = stage2(solver, C, UnotS, US, tol)
+    solver.set_precision(True)
+    try:
+        rs = stage2(solver, C, UnotS, US, tol)
+        info = solver.split_info()
+        fp, _ = solver.split_pixels()
+    finally:
+        solver.set_precision(False)
+    assert np.array_equal(rs["K"], r64["K"])
+    assert np.array_equal(rs["nevals"], r64["nevals"])
+    assert fp.sum() == info["fp64_pixels_P"]
+    assert relmax(rs["US"], r64["US"]) <= 1e-6
+    if (~fp).any():  # kept pixels: within the audit's bound
+        assert relmax(rs["US"][~fp], r64["US"][~fp]) <= max(info["max_bound_US"], 1e-13)
+    assert np.max(colrel(rs["T"], r64["T"])) < 1e-8
+    assert np.linalg.norm(rs["H"] - r64["H"]) <= 1e-8 * np.linalg.norm(r64["H"])
+    assert relmax(rs["S"], r64["S"]) < 1e-6
+    assert relmax(rs["U"], r64["U"]) < 1e-6
+
+
+def test_split_solve_vs_oracle(solver):
+    prob = synth.make("small_rot", 5)
+    r = O.solve(prob, UnotS=True, US_max=1e-6, US_tol=1e-8, maxnits=53)
+    solver.set_precision(True)
+    try:
+        g = solver.solve(prob, True, 1e-6, 1e-8, 53)
+    finally:
+        solver.set_precision(False)
+    assert np.max(np.abs(g.K / r.K - 1)) < 1e-6
+    assert relmax(g.US, r.US) < 1e-6
+    assert np.linalg.norm(g.T - r.T) <= 1e-8 * np.linalg.norm(r.T)
+    assert np.linalg.norm(g.H - r.H) <= 1e-8 * np.linalg.norm(r.H)
+
+
+def test_split_audit_falls_back(solver):
+    """Three slices (~23 bits) cannot meet the bars: the audit must send pixels
+    to FP64 and the results must still meet them."""
+    prob = synth.make("small_rot", 6)
+    C, _, _, _ = system(solver, prob)
+    solver.set_precision(False)
+    r64 = stage2(solver, C, True, 1e-6, 1e-8)
+    solver.set_precision(True, slices_P=3, slices_T=3)
+    try:
+        rs = stage2(solver, C, True, 1e-6, 1e-8)
+        info = solver.split_info()
+        fp, ft = solver.split_pixels()
+    finally:
+        solver.set_precision(False)
+    assert info["fp64_pixels_P"] > 0 and fp.sum() == info["fp64_pixels_P"]
+    assert info["fp64_columns_T"] > 0 and ft.sum() == info["fp64_columns_T"]
+    assert np.array_equal(rs["K"], r64["K"])
+    assert relmax(rs["US"], r64["US"]) <= 1e-6
+    assert np.max(colrel(rs["T"], r64["T"])) < 1e-8
+
+
+def test_split_all_fp64_is_bit_identical(solver):
+    """An audit tolerance no pixel meets recomputes every P and T column in
+    FP64: the result equals the FP64 path bit for bit."""
+    prob = synth.make("small", 7)
+    C, _, _, _ = system(solver, prob)
+    solver.set_precision(False)
+    r64 = stage2(solver, C, True, 1e-6, 1e-8)
+    solver.set_precision(True, tol_us_exp=300, tol_t_exp=300)
+    try:
+        rs = stage2(solver, C, True, 1e-6, 1e-8)
+        info = solver.split_info()
+    finally:
+        solver.set_precision(False)
+    assert info["fp64_pixels_P"] == prob.m
+    assert info["fp64_columns_T"] == prob.m
+    for f in ("K", "US", "nevals", "T", "H", "S"):
+        assert np.array_equal(rs[f], r64[f]), f
+
+
+def test_split_learned_matches_plain_fp64(solver):
+    from imcom_b200 import kappa_model
+    model = kappa_model.KappaModel.load(kappa_model.DEFAULT_WEIGHTS)
+    prob = synth.make("small_rot", 8)
+    C, _, _, _ = system(solver, prob)
+    solver.set_precision(False)
+    r64 = stage2(solver, C, True, 1e-2, 1e-5)
+    model.install(solver)
+    solver.set_precision(True)
+    try:
+        rs = stage2(solver, C, True, 1e-2, 1e-5, learned=True)
+    finally:
+        solver.set_precision(False)
+    assert np.array_equal(rs["K"], r64["K"])
+    assert relmax(rs["US"], r64["US"]) <= 1e-6
+    assert np.max(colrel(rs["T"], r64["T"])) < 1e-8
