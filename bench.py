@@ -8,8 +8,17 @@ lookup side 1728): PSF spectra -> A tables + assembly -> eigendecomposition
 -> B tables + assembly -> P -> per-pixel kappa bisection (U < 1e-2, tolerance
 1e-5) -> T -> S and H.  Synthetic seeded inputs (synth.make("n4096")).
 
-  value  pixels/s with the inputs resident in HBM (no host copies timed),
-         CUDA events on the library's stream, L2 flushed between steps.
+Two forms of the path are timed on the same workload and tolerance:
+  plain  FP64 P and T (DMMA) and the plain bisection;
+  fast   learned-kappa bracket and split-precision P and T (int8 digit slices
+         on the tcgen05 tensor cores, audited, FP64 recomputation of the
+         pixels that fail the audit) -- the headline `value`.
+Each is timed as the full solve and as the cached-system stage (P -> kappa ->
+T -> S, H with Q, L and B resident, the reference's cached path).
+
+  value  fast full-solve pixels/s with the inputs resident in HBM (no host
+         copies timed), CUDA events on the library's stream, L2 flushed
+         between steps.
   e2e    the same metric through the C-ABI with pinned host buffers: inputs
          copied in and H, K, U, S and T copied out inside every step.
 
@@ -103,20 +112,20 @@ def measured_peaks():
         return {}
 
 
-def fp64_gemm_peak(torch, dev):
-    """cuBLAS DGEMM throughput (TFLOP/s) measured here: the FP64 roofline
-    denominator (MEASURED_PEAKS.json carries HBM and bf16 only)."""
+def int8_gemm_peak(torch, dev):
+    """cuBLAS int8 GEMM throughput (TOP/s, torch._int_mm, 8192^3) measured
+    here: the denominator of the split product's tensor roofline."""
     n = 8192
-    a = torch.randn(n, n, dtype=torch.float64, device=dev)
-    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    a = torch.randint(-128, 127, (n, n), dtype=torch.int8, device=dev)
+    b = torch.randint(-128, 127, (n, n), dtype=torch.int8, device=dev)
     for _ in range(2):
-        torch.matmul(a, b)
+        torch._int_mm(a, b)
     torch.cuda.synchronize()
     best = 0.0
     for _ in range(3):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        torch.matmul(a, b)
+        torch._int_mm(a, b)
         e1.record()
         torch.cuda.synchronize()
         best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
@@ -209,22 +218,35 @@ def run_ours(args):
         return float(t.item())
 
     learned = args.kappa == "learned"
-    nev_acc = {"plain": [], "learned": []}
+    split = args.precision == "split"
+    EPS = 1.1102230246251565e-16
 
-    def device_step(use_learned):
+    def system():
         C = s.psf_spectra()
-        kmin, kmax = C * 1.1102230246251565e-16, C / 1.1102230246251565e-16
         s.build_A(out=False)
         s.eigen_A(out=False)
         s.build_B(out=False)
-        s.build_P(out=False)
-        if use_learned:
-            s.bisect_kappa_learned(UNOTS, US_MAX, kmin, kmax, US_TOL, MAXNITS, C, out=False)
+        return C
+
+    def stage2(fast, C, out=False):
+        """P -> kappa -> T -> S, H on the resident system."""
+        s.set_precision(fast and split)
+        kmin, kmax = C * EPS, C / EPS
+        r = {"P": s.build_P(out=out)}
+        if fast and learned:
+            r["K"], r["US"], r["nev"], _ = s.bisect_kappa_learned(UNOTS, US_MAX, kmin, kmax,
+                                                                  US_TOL, MAXNITS, C, out=out)
         else:
-            s.bisect_kappa(UNOTS, US_MAX, kmin, kmax, US_TOL, MAXNITS, C, out=False)
-        s.build_T(out=False)
-        s.build_S(out=False)
-        s.build_image(out=False)
+            r["K"], r["US"], r["nev"] = s.bisect_kappa(UNOTS, US_MAX, kmin, kmax, US_TOL,
+                                                       MAXNITS, C, out=out)
+        r["T"] = s.build_T(out=out)
+        r["S"] = s.build_S(out=out)
+        r["H"] = s.build_image(out=out)
+        return r
+
+    def device_step(fast):
+        C = system()
+        stage2(fast, C)
 
     # ---- learned-kappa model (trained outside the timed region) -------------
     model_src = None
@@ -245,9 +267,9 @@ def run_ours(args):
     # ---- value: inputs resident in HBM ------------------------------------
     s.set_problem(prob)
 
-    def timed_steps(use_learned, nsteps):
+    def timed(fn, nsteps):
         for _ in range(args.warmup):
-            device_step(use_learned)
+            fn()
         s.synchronize()
         torch.cuda.synchronize()
         barrier()
@@ -259,43 +281,70 @@ def run_ours(args):
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            device_step(use_learned)
+            fn()
             e1.record(stream)
             s.synchronize()
             sm.append(e0.elapsed_time(e1))
             st.append(s.stage_times())
         return sm, st, (s.launch_count() - l0) // max(1, nsteps)
 
-    plain_ms, plain_st, _ = timed_steps(False, args.steps) if learned else (None, None, None)
+    plain_ms, plain_st, _ = timed(lambda: device_step(False), args.steps)
     clocks = Clocks(local)
     clocks.start()
-    step_ms, stage_ms, launches = timed_steps(learned, args.steps)
+    step_ms, stage_ms, launches = timed(lambda: device_step(True), args.steps)
     torch.cuda.synchronize()
     ck = clocks.stop()
     barrier()
     t_step = max_over_ranks(statistics.mean(step_ms))
+    t_plain = max_over_ranks(statistics.mean(plain_ms))
     value = world * prob.m / (t_step * 1e-3)
-    # evaluation counts of the two kappa solvers on this workload (untimed)
-    C = s.psf_spectra()
-    _, _, nev_plain = s.bisect_kappa(UNOTS, US_MAX, C * 1.1102230246251565e-16,
-                                     C / 1.1102230246251565e-16, US_TOL, MAXNITS, C)
+    plain_value = world * prob.m / (t_plain * 1e-3)
+
+    # ---- cached-system stage: P -> kappa -> T -> S, H on resident Q, L, B ---
+    C = system()
+    c_plain, c_plain_st, _ = timed(lambda: stage2(False, C), args.steps)
+    c_fast, c_fast_st, _ = timed(lambda: stage2(True, C), args.steps)
+    tc_plain = max_over_ranks(statistics.mean(c_plain))
+    tc_fast = max_over_ranks(statistics.mean(c_fast))
+    cached = {"plain_fp64_value": world * prob.m / (tc_plain * 1e-3),
+              "value": world * prob.m / (tc_fast * 1e-3),
+              "ms_plain": tc_plain, "ms": tc_fast, "speedup_vs_plain_fp64": tc_plain / tc_fast,
+              "stages_ms_plain": {k: statistics.mean(d[k] for d in c_plain_st)
+                                  for k in ("build_P", "bisect", "build_T", "epilogue")},
+              "stages_ms": {k: statistics.mean(d[k] for d in c_fast_st)
+                            for k in ("build_P", "bisect", "build_T", "epilogue")}}
+
+    # ---- accuracy of the fast path against the plain FP64 path (same system)
+    rp = stage2(False, C, out=True)
+    rf = stage2(True, C, out=True)
+    info = s.split_info() if split else {}
+    s.set_precision(False)
+
+    def relmax(a, b):
+        return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)))
+
+    colT = np.linalg.norm(rf["T"] - rp["T"], axis=0) / np.linalg.norm(rp["T"], axis=0)
+    accuracy = {
+        "kappa_identical": bool(np.array_equal(rf["K"], rp["K"])),
+        "U_max_rel": relmax(rf["US"], rp["US"]),
+        "S_max_rel": relmax(rf["S"], rp["S"]),
+        "T_column_max_rel": float(colT.max()),
+        "H_rel_normwise": float(np.linalg.norm(rf["H"] - rp["H"]) / np.linalg.norm(rp["H"])),
+        "P_rel_normwise": float(np.linalg.norm(rf["P"] - rp["P"]) / np.linalg.norm(rp["P"])),
+        "bars": "kappa identical, U/S <= 1e-6 rel, T columns <= 1e-8 rel",
+        "split_audit": info,
+    }
     kappa_info = {"solver": "learned bracket + bisection replay" if learned else "bisection",
-                  "mean_evaluations_plain": float(np.mean(nev_plain))}
+                  "mean_evaluations_plain": float(np.mean(rp["nev"])),
+                  "mean_evaluations_fast": float(np.mean(rf["nev"])),
+                  "model": model_src}
     if learned:
-        K0 = s.bisect_kappa(UNOTS, US_MAX, C * 1.1102230246251565e-16, C / 1.1102230246251565e-16,
-                            US_TOL, MAXNITS, C)[0]
-        K1, _, nev_l, fb = s.bisect_kappa_learned(UNOTS, US_MAX, C * 1.1102230246251565e-16,
-                                                  C / 1.1102230246251565e-16, US_TOL, MAXNITS, C)
-        t_plain = max_over_ranks(statistics.mean(plain_ms))
-        kappa_info.update({
-            "mean_evaluations_learned": float(np.mean(nev_l)),
-            "no_bound_fraction": float(np.mean(fb)),
-            "kappa_bit_identical_to_plain": bool(np.array_equal(K0, K1)),
-            "model": model_src,
-            "plain_fp64_value": world * prob.m / (t_plain * 1e-3),
-            "bisect_ms_plain": statistics.mean(d["bisect"] for d in plain_st),
-            "bisect_ms_learned": statistics.mean(d["bisect"] for d in stage_ms),
-        })
+        K1, _, nev_l, fb = s.bisect_kappa_learned(UNOTS, US_MAX, C * EPS, C / EPS, US_TOL,
+                                                  MAXNITS, C)
+        kappa_info.update({"mean_evaluations_learned_fp64P": float(np.mean(nev_l)),
+                           "no_bound_fraction": float(np.mean(fb)),
+                           "bisect_ms_plain": cached["stages_ms_plain"]["bisect"],
+                           "bisect_ms_fast": cached["stages_ms"]["bisect"]})
 
     # ---- e2e: through the C-ABI with pinned host buffers -------------------
     keep = []
@@ -317,8 +366,9 @@ def run_ours(args):
         s.set_inputs(host["x_i"], host["y_i"], host["exp_i"], host["X_a"], host["Y_a"],
                      host["I_i"], host["Nd"], prob.psfxscale, prob.psfyscale)
         s.set_psfs(host["G_unrot"], host["rotangdeg"], host["Gamma"], prob.psfconst)
+        s.set_precision(split)
         C = s.psf_spectra()
-        kmin, kmax = C * 1.1102230246251565e-16, C / 1.1102230246251565e-16
+        kmin, kmax = C * EPS, C / EPS
         s.build_A(out=False)
         s.eigen_A(out=False)
         s.build_B(out=False)
@@ -349,12 +399,12 @@ def run_ours(args):
     t_e2e = max_over_ranks(statistics.mean(e2e_ms))
     e2e_value = world * prob.m / (t_e2e * 1e-3)
 
+    s.set_precision(False)
+
     # ---- roofline of the dominant own kernel -------------------------------
     avg = {k: statistics.mean(d[k] for d in stage_ms) for k in stage_ms[0]}
     n, m = prob.n, prob.m
     peaks = measured_peaks()
-    dgemm_peak = fp64_gemm_peak(torch, dev) if rank == 0 else None
-    # per-stage algorithmic work: FP64 GEMM flops 2 n^2 m (P and T)
     own = {k: v for k, v in avg.items()
            if not k.startswith("eig_") and not (k == "eigen_A" and args.eigensolver == "library")}
     dom = max(own, key=own.get)
@@ -369,21 +419,32 @@ def run_ours(args):
                 "achieved": ach, "peak": pk, "unit": "GB/s", "frac": ach / pk,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
                 "algorithmic_bytes": byts, "traffic": None}
-    elif dom in ("build_P", "build_T"):
-        ach = 2.0 * n * n * m / (avg[dom] * 1e-3) / 1e12
-        roof = {"kernel": dom, "bound": "tensor", "achieved": ach, "peak": dgemm_peak,
-                "unit": "TFLOP/s", "frac": ach / dgemm_peak if dgemm_peak else None,
-                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 DMMA path)",
-                "traffic": None}
     else:
-        # interpolation / others: HBM bytes written (A n^2 or B n m doubles) as the
-        # algorithmic traffic; the kernel is bound by L1/L2 gathers of the tables
         byts = {"build_A": 8.0 * n * n, "build_B": 8.0 * n * m}.get(dom, 8.0 * n * m)
         ach = byts / (avg[dom] * 1e-3) / 1e9
         pk = peaks.get("hbm_gbs", 6650.0)
         roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": pk, "unit": "GB/s",
                 "frac": ach / pk, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
                 "traffic": None}
+    # the split product (tensor-bound): P takes 7 slices (28 int8 products),
+    # T 6 slices (21); algorithmic int8 ops = products x 2 n^2 m per stage
+    # time of the stage (slicing, product, audit included)
+    split_roof = None
+    if split and rank == 0:
+        i8 = int8_gemm_peak(torch, dev)
+        sP, sT = int(info.get("slices_P", 7)), int(info.get("slices_T", 6))
+        opsP = sP * (sP + 1) / 2 * 2.0 * n * n * m
+        opsT = sT * (sT + 1) / 2 * 2.0 * n * n * m
+        tP, tT = cached["stages_ms"]["build_P"], cached["stages_ms"]["build_T"]
+        split_roof = {"bound": "tensor", "unit": "TOP/s (int8)", "peak": i8,
+                      "peak_source": "cuBLAS int8 GEMM 8192^3 (torch._int_mm) in this run",
+                      "build_P": {"achieved": opsP / (tP * 1e-3) / 1e12,
+                                  "frac": opsP / (tP * 1e-3) / 1e12 / i8},
+                      "build_T": {"achieved": opsT / (tT * 1e-3) / 1e12,
+                                  "frac": opsT / (tT * 1e-3) / 1e12 / i8},
+                      "fp64_equivalent_TFLOPs": {
+                          "build_P": 2.0 * n * n * m / (tP * 1e-3) / 1e12,
+                          "build_T": 2.0 * n * n * m / (tT * 1e-3) / 1e12}}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -402,15 +463,22 @@ def run_ours(args):
                                    "U mode U<1e-2 tol 1e-5, maxnits 53",
                        "n": n, "m": m, "nps": prob.nps, "lookup_side": 3 * prob.nps,
                        "eigensolver": args.eigensolver, "kappa": args.kappa,
-                       "P_T_precision": "fp64 (DMMA)",
+                       "P_T_precision": ("split int8 digits on tcgen05 (7/6 slices), audited, "
+                                         "FP64 fallback") if split else "fp64 (DMMA)",
                        "parallelism": f"replicas x{world}",
                        "l2": "flushed between timed steps (252 MB write)"},
+            "plain_fp64_value": plain_value,
+            "speedup_vs_plain_fp64": value / plain_value,
+            "cached_stage": cached,
             "stages_ms": avg,
+            "stages_ms_plain": {k: statistics.mean(d[k] for d in plain_st) for k in plain_st[0]},
+            "accuracy_vs_plain_fp64": accuracy,
             "kappa": kappa_info,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": t_e2e},
             "gpu_launches": launches,
             "roofline": roof,
+            "split_roofline": split_roof,
             "cpu_baseline": cpu,
             "clocks": ck,
         }
@@ -429,6 +497,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--eigensolver", choices=["dc", "library"], default="dc")
     ap.add_argument("--kappa", choices=["learned", "bisection"], default="learned")
+    ap.add_argument("--precision", choices=["split", "fp64"], default="split",
+                    help="P and T arithmetic of the fast path")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     args = ap.parse_args()
     if args.impl == "reference":

@@ -87,7 +87,7 @@ class Solver:
         self.set_option(OPT_EIGENSOLVER, mode)
 
     def set_precision(self, split: bool, slices_P: int = 7, slices_T: int = 6,
-                      tol_us_exp: int = 7, tol_t_exp: int = 9):
+                      tol_us_exp: int = 7, tol_t_exp: int = 8):
         """FP64 (split=False) or the audited int8 split product for P and T."""
         self.set_option(OPT_PRECISION, PREC_SPLIT if split else PREC_FP64)
         self.set_option(OPT_SPLIT_SLICES_P, slices_P)

@@ -104,7 +104,7 @@ struct imcom_ctx {
   // split-precision products (IMCOM_PREC_SPLIT)
   int prec = IMCOM_PREC_FP64;
   int split_SP = 7, split_ST = 6;        // digit slices of the P and T products
-  double split_tol_us = 1e-7, split_tol_t = 1e-9;
+  double split_tol_us = 1e-7, split_tol_t = 1e-8;
   imcom::SplitOp sq_P, sq_T, sb_P, spt_T;  // Q columns, Q rows, B, P~
   bool sq_P_valid = false, sq_T_valid = false;
   double sq_T_norm = 0.0;  // 2-norm of the row scales of Q

@@ -155,7 +155,7 @@ struct LearnedExtra {
   double margin;      // safety margin of the verification tests (units of U or S)
 };
 
-__global__ void learned_bisect_kernel(BisectArgs a, PixelSmem plan, LearnedExtra ex) {
+__global__ void __launch_bounds__(128, 7) learned_bisect_kernel(BisectArgs a, PixelSmem plan, LearnedExtra ex) {
   extern __shared__ __align__(16) double smem[];
   __shared__ float sW[NWEIGHT];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -529,7 +529,7 @@ extern "C" int imcom_gpu_bisect_kappa_learned(imcom_ctx* ctx, int UnotS, double 
   IMC_TRY(ensure_buf(ctx, (void**)&ctx->fb, ctx->fb_bytes, (size_t)ctx->m * sizeof(int)));
   ex.fallback = ctx->fb;
   if (ctx->p_split) IMC_TRY(split_margin_buffer(ctx, a));
-  PixelSmem plan = plan_pixel_smem(ctx->n, 190 * 1024);
+  PixelSmem plan = plan_pixel_smem(ctx->n);
   IMC_CUDA(cudaFuncSetAttribute(learned_bisect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)plan.bytes));
   learned_bisect_kernel<<<pixel_grid(ctx, plan, ctx->m), plan.warps * 32, plan.bytes,

@@ -24,7 +24,7 @@ namespace imcom {
 
 namespace {
 
-__global__ void bisect_kernel(BisectArgs a, PixelSmem plan) {
+__global__ void __launch_bounds__(128, 7) bisect_kernel(BisectArgs a, PixelSmem plan) {
   extern __shared__ __align__(16) double smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const double* lam = a.L;

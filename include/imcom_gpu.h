@@ -66,7 +66,7 @@ typedef struct imcom_ctx imcom_ctx;
 #define IMCOM_OPT_SPLIT_TOL_US 6   /* audit bound on the relative U/S error of a
                                       kept pixel: 10^-value (7)                */
 #define IMCOM_OPT_SPLIT_TOL_T 7    /* audit bound on the relative error of a
-                                      kept T column: 10^-value (9)             */
+                                      kept T column: 10^-value (8)             */
 
 /* ---- context ---------------------------------------------------------- */
 
