@@ -94,6 +94,8 @@ struct imcom_ctx {
   cufftHandle plan_r2c = 0;
   int plan_r2c_n = 0, plan_r2c_batch = 0;
 
+  int8_t* band = nullptr;   // eigenmode band indices of the learned-kappa features
+  size_t band_bytes = 0;
   int* fb = nullptr;        // per-pixel fallback flags of the learned bisection
   size_t fb_bytes = 0;
   void* train_buf = nullptr;  // MLP training data and state
@@ -103,6 +105,7 @@ struct imcom_ctx {
 
   // split-precision products (IMCOM_PREC_SPLIT)
   int prec = IMCOM_PREC_FP64;
+  int bisect_kernel = IMCOM_BISECT_AUTO;
   int split_SP = 7, split_ST = 6;        // digit slices of the P and T products
   double split_tol_us = 1e-7, split_tol_t = 1e-8;
   imcom::SplitOp sq_P, sq_T, sb_P, spt_T;  // Q columns, Q rows, B, P~

@@ -171,7 +171,7 @@ int imcom_gpu_destroy(imcom_ctx* ctx) {
                   ctx->Gamma, ctx->Gt, ctx->Gammat, ctx->A.p, ctx->Q.p, ctx->B.p, ctx->P.p,
                   ctx->T.p, ctx->Pt.p, ctx->L, ctx->K, ctx->US, ctx->H, ctx->S, ctx->U,
                   ctx->nev, ctx->flags, ctx->tables, ctx->fftbuf, ctx->mlp.w, ctx->feat,
-                  ctx->gemm_ws, ctx->fb, ctx->train_buf};
+                  ctx->gemm_ws, ctx->fb, ctx->train_buf, ctx->band};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete[] ctx->rot;
@@ -208,6 +208,10 @@ int imcom_gpu_set_option(imcom_ctx* ctx, int option, long long value) {
     case IMCOM_OPT_EIGEN_MAXITER:
       if (value < 0) return -3;
       ctx->eig_maxiter = value;
+      return 0;
+    case IMCOM_OPT_BISECT_KERNEL:
+      if (value < IMCOM_BISECT_AUTO || value > IMCOM_BISECT_RESIDENT) return -3;
+      ctx->bisect_kernel = (int)value;
       return 0;
     case IMCOM_OPT_PRECISION:
       if (value != IMCOM_PREC_FP64 && value != IMCOM_PREC_SPLIT) return -3;

@@ -26,6 +26,7 @@
 // normalisation into the last layer).
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -52,11 +53,24 @@ __device__ __forceinline__ double wsum(double v) {
   return v;
 }
 
+// Band of every eigenmode: floor(-log10(L_p / L_max) / 2) clipped to 0..7
+// (7 also for L_p <= 0); computed once per call instead of per pixel.
+__global__ void band_index_kernel(const double* __restrict__ lam, int n,
+                                  int8_t* __restrict__ band) {
+  const double lmax = lam[0];  // eigenvalues are in descending order
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const double l = lam[p];
+    const double r = (l > 0.0 && lmax > 0.0) ? l / lmax : 0.0;
+    int b = (r > 0.0) ? (int)floor(-log10(r) * 0.5) : 7;
+    band[p] = (int8_t)(b < 0 ? 0 : (b > 7 ? 7 : b));
+  }
+}
+
 // Features of one pixel, every lane gets all 12.
 __device__ void pixel_features(const double* __restrict__ x, const double* __restrict__ y,
                                const int* __restrict__ expi, int n, double Xa, double Ya,
-                               const double* lam, const double* col, double C, double US_max,
-                               int lane, float* f) {
+                               const double* lam, const int8_t* __restrict__ bidx,
+                               const double* col, double C, double US_max, int lane, float* f) {
   double cnt = 0.0;
   unsigned mask = 0u;
   for (int i = lane; i < n; i += 32) {
@@ -74,10 +88,8 @@ __device__ void pixel_features(const double* __restrict__ x, const double* __res
 #pragma unroll
   for (int b = 0; b < 8; ++b) band[b] = 0.0;
   for (int p = lane; p < n; p += 32) {
-    const double l = lam[p], pp = col[p];
-    const double r = (l > 0.0 && lmax > 0.0) ? l / lmax : 0.0;
-    int b = (r > 0.0) ? (int)floor(-log10(r) * 0.5) : 7;
-    b = b < 0 ? 0 : (b > 7 ? 7 : b);
+    const double pp = col[p];
+    const int b = bidx[p];
 #pragma unroll
     for (int q = 0; q < 8; ++q)
       if (q == b) band[q] += pp * pp;
@@ -95,6 +107,26 @@ __device__ void pixel_features(const double* __restrict__ x, const double* __res
 }
 
 // MLP forward on one warp: lane owns hidden units lane and lane + 32.
+// Shared-memory copy of the weight block for the warp forward: W1 and W2
+// transposed ([in][out]) so that the 32 lanes (consecutive hidden units) read
+// consecutive words; the other parts keep their offsets.
+__device__ __forceinline__ void load_weights_smem(const float* __restrict__ W, float* sW) {
+  for (int q = threadIdx.x; q < NWEIGHT; q += blockDim.x) {
+    float v = W[q];
+    int d = q;
+    if (q >= OFF_W1 && q < OFF_B1) {
+      const int u = (q - OFF_W1) / NF, k = (q - OFF_W1) % NF;
+      d = OFF_W1 + k * NH + u;
+    } else if (q >= OFF_W2 && q < OFF_B2) {
+      const int u = (q - OFF_W2) / NH, v2 = (q - OFF_W2) % NH;
+      d = OFF_W2 + v2 * NH + u;
+    }
+    sW[d] = v;
+  }
+}
+
+// Forward pass of one pixel on one warp (lane = hidden units lane, lane+32),
+// weights from load_weights_smem.
 __device__ void mlp_forward_warp(const float* __restrict__ W, const float* f, int lane,
                                  float* out) {
   float fn[NF];
@@ -106,7 +138,7 @@ __device__ void mlp_forward_warp(const float* __restrict__ W, const float* f, in
     const int u = lane + 32 * h;
     float s = W[OFF_B1 + u];
 #pragma unroll
-    for (int k = 0; k < NF; ++k) s = fmaf(W[OFF_W1 + u * NF + k], fn[k], s);
+    for (int k = 0; k < NF; ++k) s = fmaf(W[OFF_W1 + k * NH + u], fn[k], s);
     h1[h] = bf16r(fmaxf(s, 0.0f));
   }
 #pragma unroll
@@ -115,7 +147,7 @@ __device__ void mlp_forward_warp(const float* __restrict__ W, const float* f, in
     float s = W[OFF_B2 + u];
     for (int v = 0; v < NH; ++v) {
       const float hv = __shfl_sync(0xffffffffu, h1[v >> 5], v & 31);
-      s = fmaf(W[OFF_W2 + u * NH + v], hv, s);
+      s = fmaf(W[OFF_W2 + v * NH + u], hv, s);
     }
     h2[h] = bf16r(fmaxf(s, 0.0f));
   }
@@ -131,13 +163,13 @@ __device__ void mlp_forward_warp(const float* __restrict__ W, const float* f, in
 __global__ void features_kernel(BisectArgs a, const double* __restrict__ x,
                                 const double* __restrict__ y, const int* __restrict__ expi,
                                 const double* __restrict__ X, const double* __restrict__ Y,
-                                float* __restrict__ feat) {
+                                const int8_t* __restrict__ bidx, float* __restrict__ feat) {
   const int lane = threadIdx.x & 31;
   const int pix = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (pix >= a.m) return;
   float f[NF];
-  pixel_features(x, y, expi, a.n, X[pix], Y[pix], a.L, a.P + (size_t)pix * a.ldp, a.C, a.US_max,
-                 lane, f);
+  pixel_features(x, y, expi, a.n, X[pix], Y[pix], a.L, bidx, a.P + (size_t)pix * a.ldp, a.C,
+                 a.US_max, lane, f);
   if (lane < NF) {
 #pragma unroll
     for (int k = 0; k < NF; ++k)
@@ -148,6 +180,7 @@ __global__ void features_kernel(BisectArgs a, const double* __restrict__ x,
 struct LearnedExtra {
   const double *x, *y, *X, *Y;
   const int* expi;
+  const int8_t* bidx;  // band of every eigenmode (band_index_kernel)
   const float* W;
   int* fallback;
   double half_scale;  // bracket half-width = half_scale * exp(output 1), decades
@@ -155,11 +188,124 @@ struct LearnedExtra {
   double margin;      // safety margin of the verification tests (units of U or S)
 };
 
-__global__ void __launch_bounds__(128, 7) learned_bisect_kernel(BisectArgs a, PixelSmem plan, LearnedExtra ex) {
+// One pixel of the learned-bracket bisection: features from lam and the P
+// column `col`, MLP bracket, verification of the bracket ends and the replay
+// of the reference's bisection; ev(k, lane) evaluates U or S.
+template <class Eval>
+__device__ __forceinline__ void learned_pixel(const BisectArgs& a, const LearnedExtra& ex,
+                                              const float* sW, const double* lam,
+                                              const double* col, const Eval& ev, int pix,
+                                              int lane) {
+  const bool U = a.UnotS != 0;
+  float f[NF], o[NO];
+  pixel_features(ex.x, ex.y, ex.expi, a.n, ex.X[pix], ex.Y[pix], lam, ex.bidx, col, a.C,
+                 a.US_max, lane, f);
+  mlp_forward_warp(sW, f, lane, o);
+  double hw = ex.half_scale * exp((double)fminf(fmaxf(o[1], -20.0f), 5.0f));
+  hw = fmin(fmax(hw, ex.min_half), 4.0);
+  double bl = (double)o[0] - hw, bh = (double)o[0] + hw;
+  // (lg_min, lg_max) is the reference's search range
+  const double rlo = a.lg_min, rhi = a.lg_max;
+  bl = fmax(bl, rlo);
+  bh = fmin(bh, rhi);
+  int nev = 0;
+  double k_root = 0.0, us = 0.0;
+  const double ceps = __dmul_rn(a.C, a.eps);
+  const double thr = fmax(a.tol, ceps) + ex.margin;
+  double mg = INFINITY;  // smallest decision margin over the evaluations
+  // One-sided bounds from the evaluated bracket ends.  U rises with kappa:
+  // an end with f < -thr makes every midpoint at or below it a known
+  // accept; an end with f >= C eps (+ margin) makes every midpoint at or
+  // above it a known reject.  S falls with kappa, so the directions flip.
+  double accb = U ? -INFINITY : INFINITY;  // known accept beyond this point
+  double rejb = U ? INFINITY : -INFINITY;  // known reject beyond this point
+  const double ends[2] = {bl, bh};
+#pragma unroll
+  for (int e = 0; e < 2; ++e) {
+    const double pt = ends[e];
+    if (!(pt > rlo && pt < rhi) || (e == 1 && bh <= bl)) continue;
+    const double fp =
+        __dsub_rn(ev(pow(10.0, pt), lane), a.US_max);
+    ++nev;
+    mg = fmin(mg, fmin(fabs(fp + thr), fabs(fp - (ceps + ex.margin))));
+    if (fp < -thr) accb = U ? fmax(accb, pt) : fmin(accb, pt);
+    else if (fp >= ceps + ex.margin) rejb = U ? fmin(rejb, pt) : fmax(rejb, pt);
+  }
+  const bool have_acc = U ? (accb > rlo) : (accb < rhi);
+  const bool have_rej = U ? (rejb < rhi) : (rejb > rlo);
+  if (lane == 0 && ex.fallback) ex.fallback[pix] = (have_acc || have_rej) ? 0 : 1;
+  {
+    // The reference first evaluates f0 at the start of the range (kappa_min
+    // for U, kappa_max for S) and returns there if f0 >= 0.  A known accept
+    // point inside the range implies f0 < 0 by monotonicity, so f0 is then
+    // only needed if no later step is accepted.
+    double f0 = 0.0;
+    bool have_f0 = false;
+    if (!have_acc) {
+      const double k0 = U ? a.k_min : a.k_max;
+      us = ev(k0, lane);
+      ++nev;
+      f0 = __dsub_rn(us, a.US_max);
+      have_f0 = true;
+      mg = fmin(mg, fabs(f0));
+    }
+    if (have_f0 && !(f0 < 0.0)) {
+      k_root = U ? a.k_min : a.k_max;
+    } else {
+      const double lo = U ? a.lg_min : a.lg_max, hi = U ? a.lg_max : a.lg_min;
+      double root = lo, dx = __dsub_rn(hi, lo);
+      bool last_known = false, any_acc = false;
+      for (int i = 1; i <= a.maxnits; ++i) {
+        dx = __dmul_rn(0.5, dx);
+        const double mid = __dadd_rn(root, dx);
+        const bool known_acc = U ? (mid <= accb) : (mid >= accb);
+        const bool known_rej = U ? (mid >= rejb) : (mid <= rejb);
+        if (known_acc) {
+          root = mid;
+          any_acc = true;
+          last_known = true;
+          continue;
+        }
+        if (known_rej) continue;
+        const double fmid =
+            __dsub_rn(ev(pow(10.0, mid), lane), a.US_max);
+        ++nev;
+        mg = fmin(mg, decision_margin(fmid, a.tol, ceps));
+        if (fmid < 0.0) {
+          root = mid;
+          any_acc = true;
+          last_known = false;
+          us = __dadd_rn(fmid, a.US_max);
+          if (fabs(fmid) < a.tol) break;
+        }
+        if (fabs(fmid) < ceps) break;
+      }
+      if (!any_acc) {
+        if (!have_f0) {
+          const double k0 = U ? a.k_min : a.k_max;
+          us = ev(k0, lane);
+          ++nev;
+          mg = fmin(mg, fabs(__dsub_rn(us, a.US_max)));
+        }
+      } else if (last_known) {
+        // value the reference holds at the last accepted midpoint
+        const double fl =
+            __dsub_rn(ev(pow(10.0, root), lane), a.US_max);
+        ++nev;
+        us = __dadd_rn(fl, a.US_max);
+      }
+      k_root = pow(10.0, root);
+    }
+  }
+  write_pixel(a, lam, col, pix, lane, nev, k_root, us, mg);
+}
+
+__global__ void __launch_bounds__(128, 7) learned_bisect_kernel(BisectArgs a, PixelSmem plan,
+                                                                LearnedExtra ex) {
   extern __shared__ __align__(16) double smem[];
   __shared__ float sW[NWEIGHT];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int q = threadIdx.x; q < NWEIGHT; q += blockDim.x) sW[q] = ex.W[q];
+  load_weights_smem(ex.W, sW);
   const double* lam = a.L;
   if (plan.lam_smem) {
     for (int p = threadIdx.x; p < a.n; p += blockDim.x) smem[p] = a.L[p];
@@ -167,115 +313,47 @@ __global__ void __launch_bounds__(128, 7) learned_bisect_kernel(BisectArgs a, Pi
   }
   __syncthreads();
   double* mycol = plan.col_smem ? smem + (size_t)a.n * (1 + warp) : nullptr;
-  const bool U = a.UnotS != 0;
   for (int pix = blockIdx.x * plan.warps + warp; pix < a.m; pix += gridDim.x * plan.warps) {
-    const double* col = a.P + (size_t)pix * a.ldp;
+    const double* gcol = a.P + (size_t)pix * a.ldp;
+    const double* col = gcol;
     if (mycol) {
-      for (int p = lane; p < a.n; p += 32) mycol[p] = col[p];
+      for (int p = lane; p < a.n; p += 32) mycol[p] = gcol[p];
       __syncwarp();
       col = mycol;
     }
-    float f[NF], o[NO];
-    pixel_features(ex.x, ex.y, ex.expi, a.n, ex.X[pix], ex.Y[pix], lam, col, a.C, a.US_max, lane,
-                   f);
-    mlp_forward_warp(sW, f, lane, o);
-    double hw = ex.half_scale * exp((double)fminf(fmaxf(o[1], -20.0f), 5.0f));
-    hw = fmin(fmax(hw, ex.min_half), 4.0);
-    double bl = (double)o[0] - hw, bh = (double)o[0] + hw;
-    // (lg_min, lg_max) is the reference's search range
-    const double rlo = a.lg_min, rhi = a.lg_max;
-    bl = fmax(bl, rlo);
-    bh = fmin(bh, rhi);
-    int nev = 0;
-    double k_root = 0.0, us = 0.0;
-    const double ceps = __dmul_rn(a.C, a.eps);
-    const double thr = fmax(a.tol, ceps) + ex.margin;
-    double mg = INFINITY;  // smallest decision margin over the evaluations
-    // One-sided bounds from the evaluated bracket ends.  U rises with kappa:
-    // an end with f < -thr makes every midpoint at or below it a known
-    // accept; an end with f >= C eps (+ margin) makes every midpoint at or
-    // above it a known reject.  S falls with kappa, so the directions flip.
-    double accb = U ? -INFINITY : INFINITY;  // known accept beyond this point
-    double rejb = U ? INFINITY : -INFINITY;  // known reject beyond this point
-    const double ends[2] = {bl, bh};
-#pragma unroll
-    for (int e = 0; e < 2; ++e) {
-      const double pt = ends[e];
-      if (!(pt > rlo && pt < rhi) || (e == 1 && bh <= bl)) continue;
-      const double fp =
-          __dsub_rn(warp_us(U, lam, col, a.Nd, a.n, pow(10.0, pt), a.C, lane), a.US_max);
-      ++nev;
-      mg = fmin(mg, fmin(fabs(fp + thr), fabs(fp - (ceps + ex.margin))));
-      if (fp < -thr) accb = U ? fmax(accb, pt) : fmin(accb, pt);
-      else if (fp >= ceps + ex.margin) rejb = U ? fmin(rejb, pt) : fmax(rejb, pt);
-    }
-    const bool have_acc = U ? (accb > rlo) : (accb < rhi);
-    const bool have_rej = U ? (rejb < rhi) : (rejb > rlo);
-    if (lane == 0 && ex.fallback) ex.fallback[pix] = (have_acc || have_rej) ? 0 : 1;
-    {
-      // The reference first evaluates f0 at the start of the range (kappa_min
-      // for U, kappa_max for S) and returns there if f0 >= 0.  A known accept
-      // point inside the range implies f0 < 0 by monotonicity, so f0 is then
-      // only needed if no later step is accepted.
-      double f0 = 0.0;
-      bool have_f0 = false;
-      if (!have_acc) {
-        const double k0 = U ? a.k_min : a.k_max;
-        us = warp_us(U, lam, col, a.Nd, a.n, k0, a.C, lane);
-        ++nev;
-        f0 = __dsub_rn(us, a.US_max);
-        have_f0 = true;
-        mg = fmin(mg, fabs(f0));
-      }
-      if (have_f0 && !(f0 < 0.0)) {
-        k_root = U ? a.k_min : a.k_max;
-      } else {
-        const double lo = U ? a.lg_min : a.lg_max, hi = U ? a.lg_max : a.lg_min;
-        double root = lo, dx = __dsub_rn(hi, lo);
-        bool last_known = false, any_acc = false;
-        for (int i = 1; i <= a.maxnits; ++i) {
-          dx = __dmul_rn(0.5, dx);
-          const double mid = __dadd_rn(root, dx);
-          const bool known_acc = U ? (mid <= accb) : (mid >= accb);
-          const bool known_rej = U ? (mid >= rejb) : (mid <= rejb);
-          if (known_acc) {
-            root = mid;
-            any_acc = true;
-            last_known = true;
-            continue;
-          }
-          if (known_rej) continue;
-          const double fmid =
-              __dsub_rn(warp_us(U, lam, col, a.Nd, a.n, pow(10.0, mid), a.C, lane), a.US_max);
-          ++nev;
-          mg = fmin(mg, decision_margin(fmid, a.tol, ceps));
-          if (fmid < 0.0) {
-            root = mid;
-            any_acc = true;
-            last_known = false;
-            us = __dadd_rn(fmid, a.US_max);
-            if (fabs(fmid) < a.tol) break;
-          }
-          if (fabs(fmid) < ceps) break;
-        }
-        if (!any_acc) {
-          if (!have_f0) {
-            const double k0 = U ? a.k_min : a.k_max;
-            us = warp_us(U, lam, col, a.Nd, a.n, k0, a.C, lane);
-            ++nev;
-            mg = fmin(mg, fabs(__dsub_rn(us, a.US_max)));
-          }
-        } else if (last_known) {
-          // value the reference holds at the last accepted midpoint
-          const double fl =
-              __dsub_rn(warp_us(U, lam, col, a.Nd, a.n, pow(10.0, root), a.C, lane), a.US_max);
-          ++nev;
-          us = __dadd_rn(fl, a.US_max);
-        }
-        k_root = pow(10.0, root);
-      }
-    }
-    write_pixel(a, lam, col, pix, lane, nev, k_root, us, mg);
+    const StreamCol ev{lam, col, a.Nd, a.n, a.UnotS != 0, a.C};
+    learned_pixel(a, ex, sW, lam, col, ev, pix, lane);
+    __syncwarp();
+  }
+}
+
+// Learned-bracket bisection with the pixel's column resident in its warp
+// (n <= RES_MAX_N): one CTA per SM, pixels handed out by an atomic counter.
+__global__ void __launch_bounds__(RES_WARPS_LEARNED * 32, 1) learned_res_kernel(BisectArgs a,
+                                                                               LearnedExtra ex,
+                                                                               int* counter) {
+  extern __shared__ __align__(16) double smem[];
+  __shared__ float sW[NWEIGHT];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  load_weights_smem(ex.W, sW);
+  for (int p = threadIdx.x; p < a.n; p += blockDim.x) smem[p] = a.L[p];
+  __syncthreads();
+  double* smw = smem + RES_MAX_N + (size_t)warp * RES_S * 32;
+  ResCol rc;
+  rc.lam = smem;
+  rc.n = a.n;
+  rc.jn = (a.n + 31) / 32;
+  rc.U = a.UnotS != 0;
+  rc.C = a.C;
+  for (;;) {
+    int t = 0;
+    if (lane == 0) t = atomicAdd(counter, 1);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= a.m) break;
+    const double* col = a.P + (size_t)t * a.ldp;
+    rc.load(col, a.Nd, lane, smw);
+    __syncwarp();
+    learned_pixel(a, ex, sW, smem, col, rc, t, lane);
     __syncwarp();
   }
 }
@@ -449,6 +527,11 @@ int fill_learned(imcom_ctx* ctx, LearnedExtra& ex) {
   ex.expi = ctx->exp_i;
   ex.W = ctx->mlp.w;
   ex.fallback = nullptr;
+  // band of every eigenmode for the P2 band features
+  IMC_TRY(ensure_buf(ctx, (void**)&ctx->band, ctx->band_bytes, (size_t)ctx->n));
+  band_index_kernel<<<(ctx->n + 255) / 256, 256, 0, ctx->stream>>>(ctx->L, ctx->n, ctx->band);
+  IMC_LAUNCH();
+  ex.bidx = ctx->band;
   ex.half_scale = 3.0;
   ex.min_half = 0.02;
   ex.margin = 1e-10;
@@ -467,9 +550,12 @@ extern "C" int imcom_gpu_kappa_features(imcom_ctx* ctx, int UnotS, double US_max
   IMC_TRY(fill_bisect_args(ctx, a, UnotS, US_max, 1.0, 1.0, 0.0, 0, C_a));
   cudaSetDevice(ctx->device);
   IMC_TRY(ensure_vec(ctx, &ctx->feat, (size_t)NF * ctx->m));
+  IMC_TRY(ensure_buf(ctx, (void**)&ctx->band, ctx->band_bytes, (size_t)ctx->n));
+  band_index_kernel<<<(ctx->n + 255) / 256, 256, 0, ctx->stream>>>(ctx->L, ctx->n, ctx->band);
+  IMC_LAUNCH();
   int blocks = (ctx->m + 7) / 8;
   features_kernel<<<blocks, 256, 0, ctx->stream>>>(a, ctx->x, ctx->y, ctx->exp_i, ctx->X, ctx->Y,
-                                                   ctx->feat);
+                                                   ctx->band, ctx->feat);
   IMC_LAUNCH();
   IMC_CUDA(cudaMemcpyAsync(feat_out, ctx->feat, (size_t)NF * ctx->m * sizeof(float),
                            cudaMemcpyDeviceToHost, ctx->stream));
@@ -529,12 +615,24 @@ extern "C" int imcom_gpu_bisect_kappa_learned(imcom_ctx* ctx, int UnotS, double 
   IMC_TRY(ensure_buf(ctx, (void**)&ctx->fb, ctx->fb_bytes, (size_t)ctx->m * sizeof(int)));
   ex.fallback = ctx->fb;
   if (ctx->p_split) IMC_TRY(split_margin_buffer(ctx, a));
-  PixelSmem plan = plan_pixel_smem(ctx->n);
-  IMC_CUDA(cudaFuncSetAttribute(learned_bisect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)plan.bytes));
-  learned_bisect_kernel<<<pixel_grid(ctx, plan, ctx->m), plan.warps * 32, plan.bytes,
-                          ctx->stream>>>(a, plan, ex);
-  IMC_LAUNCH();
+  if (use_resident(ctx->bisect_kernel, ctx->n)) {
+    int* counter = ctx->flags + 24;
+    IMC_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), ctx->stream));
+    const size_t bytes = res_smem_bytes(RES_WARPS_LEARNED);
+    IMC_CUDA(cudaFuncSetAttribute(learned_res_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)bytes));
+    const int grid =
+        std::min(sm_count(ctx), (ctx->m + RES_WARPS_LEARNED - 1) / RES_WARPS_LEARNED);
+    learned_res_kernel<<<grid, RES_WARPS_LEARNED * 32, bytes, ctx->stream>>>(a, ex, counter);
+    IMC_LAUNCH();
+  } else {
+    PixelSmem plan = plan_pixel_smem(ctx->n);
+    IMC_CUDA(cudaFuncSetAttribute(learned_bisect_kernel,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.bytes));
+    learned_bisect_kernel<<<pixel_grid(ctx, plan, ctx->m), plan.warps * 32, plan.bytes,
+                            ctx->stream>>>(a, plan, ex);
+    IMC_LAUNCH();
+  }
   if (ctx->p_split) IMC_TRY(split_audit(ctx, a));
   stage_end(ctx, ST_BISECT);
   ctx->have_K = true;

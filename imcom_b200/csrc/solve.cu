@@ -14,6 +14,7 @@
 // warp-wide sum (usum.cuh).  Its epilogue also writes the T operand
 // P~(:, a) = P(:, a) / (L + K_a) (the DGEMV argument of imcom_matrix.f90:734),
 // so T = -1/2 Q P~ is a single FP64 GEMM.
+#include <algorithm>
 #include <cmath>
 
 #include "common.cuh"
@@ -45,8 +46,42 @@ __global__ void __launch_bounds__(128, 7) bisect_kernel(BisectArgs a, PixelSmem 
     }
     int nev;
     double k, us, mg;
-    bisect_pixel(a, lam, col, lane, &nev, &k, &us, &mg);
-    write_pixel(a, lam, col, pix, lane, nev, k, us, mg);
+    const StreamCol ev{lam, col, a.Nd, a.n, a.UnotS != 0, a.C};
+    bisect_pixel(a, ev, lane, &nev, &k, &us, &mg);
+    write_pixel(a, lam, a.P + (size_t)pix * a.ldp, pix, lane, nev, k, us, mg);
+    __syncwarp();
+  }
+}
+
+// Bisection with the pixel's column resident in its warp (n <= RES_MAX_N):
+// one CTA per SM, pixels handed out by an atomic counter.
+__global__ void __launch_bounds__(RES_WARPS_PLAIN * 32, 1) bisect_res_kernel(BisectArgs a,
+                                                                            int* counter) {
+  extern __shared__ __align__(16) double smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int p = threadIdx.x; p < a.n; p += blockDim.x) smem[p] = a.L[p];
+  __syncthreads();
+  double* smw = smem + RES_MAX_N + (size_t)warp * RES_S * 32;
+  ResCol rc;
+  rc.lam = smem;
+  rc.n = a.n;
+  rc.jn = (a.n + 31) / 32;
+  rc.U = a.UnotS != 0;
+  rc.C = a.C;
+  const int total = a.list ? a.count : a.m;
+  for (;;) {
+    int t = 0;
+    if (lane == 0) t = atomicAdd(counter, 1);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= total) break;
+    const int pix = a.list ? a.list[t] : t;
+    const double* col = a.P + (size_t)pix * a.ldp;
+    rc.load(col, a.Nd, lane, smw);
+    __syncwarp();
+    int nev;
+    double k, us, mg;
+    bisect_pixel(a, rc, lane, &nev, &k, &us, &mg);
+    write_pixel(a, smem, col, pix, lane, nev, k, us, mg);
     __syncwarp();
   }
 }
@@ -139,11 +174,22 @@ int pixel_grid(imcom_ctx* ctx, const PixelSmem& plan, int m) {
 }
 
 int launch_bisect(imcom_ctx* ctx, const BisectArgs& a) {
+  const int total = a.list ? a.count : a.m;
+  if (total <= 0) return 0;
+  if (use_resident(ctx->bisect_kernel, ctx->n)) {
+    int* counter = ctx->flags + 24;
+    IMC_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), ctx->stream));
+    const size_t bytes = res_smem_bytes(RES_WARPS_PLAIN);
+    IMC_CUDA(cudaFuncSetAttribute(bisect_res_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)bytes));
+    const int grid = std::min(sm_count(ctx), (total + RES_WARPS_PLAIN - 1) / RES_WARPS_PLAIN);
+    bisect_res_kernel<<<grid, RES_WARPS_PLAIN * 32, bytes, ctx->stream>>>(a, counter);
+    IMC_LAUNCH();
+    return 0;
+  }
   PixelSmem plan = plan_pixel_smem(ctx->n);
   IMC_CUDA(cudaFuncSetAttribute(bisect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)plan.bytes));
-  const int total = a.list ? a.count : a.m;
-  if (total <= 0) return 0;
   bisect_kernel<<<pixel_grid(ctx, plan, total), plan.warps * 32, plan.bytes, ctx->stream>>>(a,
                                                                                           plan);
   IMC_LAUNCH();

@@ -35,18 +35,20 @@ __device__ __forceinline__ double decision_margin(double f, double tol, double c
   return fmin(af, fmin(fabs(af - tol), fabs(af - ceps)));
 }
 
-// The reference's bisection for one pixel (imcom_bisect_by_U / _by_S).
-// *mg_out receives the smallest decision margin over the evaluations.
-__device__ __forceinline__ void bisect_pixel(const BisectArgs& a, const double* lam,
-                                             const double* col, int lane, int* nev_out,
-                                             double* k_out, double* us_out, double* mg_out) {
+// The reference's bisection for one pixel (imcom_bisect_by_U / _by_S);
+// ev(k, lane) is U or S at kappa k (StreamCol or ResCol).  *mg_out receives
+// the smallest decision margin over the evaluations.
+template <class Eval>
+__device__ __forceinline__ void bisect_pixel(const BisectArgs& a, const Eval& ev, int lane,
+                                             int* nev_out, double* k_out, double* us_out,
+                                             double* mg_out) {
   const bool U = a.UnotS != 0;
   int nev = 0;
   double k_root, us;
   const double ceps = __dmul_rn(a.C, a.eps);
   // imcom_bisect_by_U: U(k_min) first; imcom_bisect_by_S: S(k_max) first.
   double k0 = U ? a.k_min : a.k_max;
-  us = warp_us(U, lam, col, a.Nd, a.n, k0, a.C, lane);
+  us = ev(k0, lane);
   nev = 1;
   double f = __dsub_rn(us, a.US_max);
   double mg = fabs(f);
@@ -59,7 +61,7 @@ __device__ __forceinline__ void bisect_pixel(const BisectArgs& a, const double* 
     for (int i = 1; i <= a.maxnits; ++i) {
       dx = __dmul_rn(0.5, dx);
       double mid = __dadd_rn(root, dx);
-      double fmid = __dsub_rn(warp_us(U, lam, col, a.Nd, a.n, pow(10.0, mid), a.C, lane), a.US_max);
+      double fmid = __dsub_rn(ev(pow(10.0, mid), lane), a.US_max);
       ++nev;
       mg = fmin(mg, decision_margin(fmid, a.tol, ceps));
       if (fmid < 0.0) {

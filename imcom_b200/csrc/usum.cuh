@@ -4,10 +4,15 @@
 //   U = (C - 1/4 sum_p (L_p + 2k) P2_pa / ((L_p + k)(L_p + k))) / C
 // imcom_S_from_kappa (imcom_matrix.f90:955-970):
 //   S = 1/4 sum_p Ndiag_p P2_pa / ((L_p + k)(L_p + k))
-// Each term is formed with the reference's operations in the reference's
-// order (explicit _rn intrinsics: no FMA contraction); the sum over p is a
-// per-lane sequential sum followed by an xor-butterfly, which leaves the
-// bit-identical total in every lane so control flow stays warp-uniform.
+// Each term's numerator and (L_p + k)^2 are formed with the reference's
+// operations (explicit _rn intrinsics: no FMA contraction); the quotient is
+// the numerator times a Newton-refined reciprocal of (L_p + k)^2, which
+// shortens the per-term dependency chain of a correctly rounded division
+// (the term may differ from num / den by one rounding).  The sum over p is a
+// per-lane sum (four partial sums) followed by an xor-butterfly, which leaves
+// the bit-identical total in every lane so control flow stays warp-uniform.
+// Every U/S evaluator of the library uses these terms and this order, so the
+// plain, learned and split-precision bisections take identical decisions.
 #pragma once
 
 namespace imcom {
@@ -17,16 +22,30 @@ namespace imcom {
 // Each lane keeps four independent partial sums (modes p = lane + 32 j with
 // j mod 4 selecting the sum) so that four divisions are in flight per lane;
 // the partials are added as (s0 + s1) + (s2 + s3) before the butterfly.
+// 1/a by two Newton-Raphson steps r <- r + r (1 - a r) from the PTX
+// rcp.approx.ftz.f64 seed (measured relative error 2^-19.9 on B200; after
+// two steps 4.2M random arguments over |a| in [1e-30, 1e30] gave the correctly
+// rounded reciprocal).  Arguments here are (L_p + k)^2 >= (C eps)^2, never
+// subnormal.
+__device__ __forceinline__ double rcp_nr(double a) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(a));
+  double e = fma(-a, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-a, r, 1.0);
+  return fma(r, e, r);
+}
+
 __device__ __forceinline__ double uterm(double l, double pp, double k, double k2) {
   const double p2 = __dmul_rn(pp, pp);
   const double t = __dadd_rn(l, k);
-  return __ddiv_rn(__dmul_rn(__dadd_rn(l, k2), p2), __dmul_rn(t, t));
+  return __dmul_rn(__dmul_rn(__dadd_rn(l, k2), p2), rcp_nr(__dmul_rn(t, t)));
 }
 
 __device__ __forceinline__ double sterm(double l, double pp, double nd, double k) {
   const double p2 = __dmul_rn(pp, pp);
   const double t = __dadd_rn(l, k);
-  return __ddiv_rn(__dmul_rn(nd, p2), __dmul_rn(t, t));
+  return __dmul_rn(__dmul_rn(nd, p2), rcp_nr(__dmul_rn(t, t)));
 }
 
 __device__ __forceinline__ double warp_reduce_sum(double s) {
@@ -35,18 +54,38 @@ __device__ __forceinline__ double warp_reduce_sum(double s) {
   return s;
 }
 
+// Modes p = lane + 32 j go to partial sum j mod 4, in increasing j; blocks
+// of eight modes per lane keep eight column loads in flight.
 __device__ __forceinline__ double warp_usum(const double* lam, const double* col, int n,
                                             double k, int lane) {
   const double k2 = __dmul_rn(2.0, k);
   double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
   int p = lane;
+  for (; p + 224 < n; p += 256) {
+    double c[8], l[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      c[q] = col[p + 32 * q];
+      l[q] = lam[p + 32 * q];
+    }
+    s0 = __dadd_rn(s0, uterm(l[0], c[0], k, k2));
+    s1 = __dadd_rn(s1, uterm(l[1], c[1], k, k2));
+    s2 = __dadd_rn(s2, uterm(l[2], c[2], k, k2));
+    s3 = __dadd_rn(s3, uterm(l[3], c[3], k, k2));
+    s0 = __dadd_rn(s0, uterm(l[4], c[4], k, k2));
+    s1 = __dadd_rn(s1, uterm(l[5], c[5], k, k2));
+    s2 = __dadd_rn(s2, uterm(l[6], c[6], k, k2));
+    s3 = __dadd_rn(s3, uterm(l[7], c[7], k, k2));
+  }
   for (; p + 96 < n; p += 128) {
     s0 = __dadd_rn(s0, uterm(lam[p], col[p], k, k2));
     s1 = __dadd_rn(s1, uterm(lam[p + 32], col[p + 32], k, k2));
     s2 = __dadd_rn(s2, uterm(lam[p + 64], col[p + 64], k, k2));
     s3 = __dadd_rn(s3, uterm(lam[p + 96], col[p + 96], k, k2));
   }
-  for (; p < n; p += 32) s0 = __dadd_rn(s0, uterm(lam[p], col[p], k, k2));
+  if (p < n) s0 = __dadd_rn(s0, uterm(lam[p], col[p], k, k2));
+  if (p + 32 < n) s1 = __dadd_rn(s1, uterm(lam[p + 32], col[p + 32], k, k2));
+  if (p + 64 < n) s2 = __dadd_rn(s2, uterm(lam[p + 64], col[p + 64], k, k2));
   return warp_reduce_sum(__dadd_rn(__dadd_rn(s0, s1), __dadd_rn(s2, s3)));
 }
 
@@ -54,13 +93,32 @@ __device__ __forceinline__ double warp_ssum(const double* lam, const double* col
                                             const double* nd, int n, double k, int lane) {
   double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
   int p = lane;
+  for (; p + 224 < n; p += 256) {
+    double c[8], l[8], w[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      c[q] = col[p + 32 * q];
+      l[q] = lam[p + 32 * q];
+      w[q] = nd[p + 32 * q];
+    }
+    s0 = __dadd_rn(s0, sterm(l[0], c[0], w[0], k));
+    s1 = __dadd_rn(s1, sterm(l[1], c[1], w[1], k));
+    s2 = __dadd_rn(s2, sterm(l[2], c[2], w[2], k));
+    s3 = __dadd_rn(s3, sterm(l[3], c[3], w[3], k));
+    s0 = __dadd_rn(s0, sterm(l[4], c[4], w[4], k));
+    s1 = __dadd_rn(s1, sterm(l[5], c[5], w[5], k));
+    s2 = __dadd_rn(s2, sterm(l[6], c[6], w[6], k));
+    s3 = __dadd_rn(s3, sterm(l[7], c[7], w[7], k));
+  }
   for (; p + 96 < n; p += 128) {
     s0 = __dadd_rn(s0, sterm(lam[p], col[p], nd[p], k));
     s1 = __dadd_rn(s1, sterm(lam[p + 32], col[p + 32], nd[p + 32], k));
     s2 = __dadd_rn(s2, sterm(lam[p + 64], col[p + 64], nd[p + 64], k));
     s3 = __dadd_rn(s3, sterm(lam[p + 96], col[p + 96], nd[p + 96], k));
   }
-  for (; p < n; p += 32) s0 = __dadd_rn(s0, sterm(lam[p], col[p], nd[p], k));
+  if (p < n) s0 = __dadd_rn(s0, sterm(lam[p], col[p], nd[p], k));
+  if (p + 32 < n) s1 = __dadd_rn(s1, sterm(lam[p + 32], col[p + 32], nd[p + 32], k));
+  if (p + 64 < n) s2 = __dadd_rn(s2, sterm(lam[p + 64], col[p + 64], nd[p + 64], k));
   return warp_reduce_sum(__dadd_rn(__dadd_rn(s0, s1), __dadd_rn(s2, s3)));
 }
 
@@ -73,6 +131,112 @@ __device__ __forceinline__ double warp_us(bool UnotS, const double* lam, const d
     return __ddiv_rn(__dsub_rn(C, __ddiv_rn(usum, 4.0)), C);
   }
   return __ddiv_rn(warp_ssum(lam, col, nd, n, k, lane), 4.0);
+}
+
+// U/S evaluator that streams the pixel's P column (any n).
+struct StreamCol {
+  const double* lam;
+  const double* col;
+  const double* nd;
+  int n;
+  bool U;
+  double C;
+  __device__ __forceinline__ double operator()(double k, int lane) const {
+    return warp_us(U, lam, col, nd, n, k, C, lane);
+  }
+};
+
+// U/S evaluator with the pixel's column resident in its warp: the weights
+// w_p = P_p^2 (U mode) or Ndiag_p P_p^2 (S mode, the reference's product
+// formed once) for modes p = lane + 32 j, j < RES_R in registers and
+// RES_R <= j < RES_R + RES_S in shared memory.  Terms are added to partial
+// sum j mod 4 in increasing j, exactly as warp_usum / warp_ssum do, so both
+// evaluators give bit-identical U and S.
+constexpr int RES_R = 64;
+constexpr int RES_S = 64;
+constexpr int RES_MAX_N = 32 * (RES_R + RES_S);  // 4096
+
+struct ResCol {
+  double r[RES_R];
+  const double* sm;   // this warp's slice: sm[(j - RES_R) * 32 + lane]
+  const double* lam;  // eigenvalues
+  int n, jn;
+  bool U;
+  double C;
+
+  __device__ __forceinline__ void load(const double* col, const double* nd, int lane,
+                                       double* smw) {
+#pragma unroll
+    for (int j = 0; j < RES_R; ++j) {
+      const int p = lane + 32 * j;
+      double v = 0.0;
+      if (p < n) {
+        const double pp = col[p];
+        v = __dmul_rn(pp, pp);
+        if (!U) v = __dmul_rn(nd[p], v);
+      }
+      r[j] = v;
+    }
+    for (int j = RES_R; j < jn; ++j) {
+      const int p = lane + 32 * j;
+      double v = 0.0;
+      if (p < n) {
+        const double pp = col[p];
+        v = __dmul_rn(pp, pp);
+        if (!U) v = __dmul_rn(nd[p], v);
+      }
+      smw[(j - RES_R) * 32 + lane] = v;
+    }
+    sm = smw;
+  }
+
+  __device__ __forceinline__ double term(double l, double w, double k, double k2) const {
+    const double t = __dadd_rn(l, k);
+    const double num = U ? __dmul_rn(__dadd_rn(l, k2), w) : w;
+    return __dmul_rn(num, rcp_nr(__dmul_rn(t, t)));
+  }
+
+  __device__ __forceinline__ double operator()(double k, int lane) const {
+    const double k2 = __dmul_rn(2.0, k);
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int j = 0; j < RES_R; ++j) {
+      const int p = lane + 32 * j;
+      if (p < n) s[j & 3] = __dadd_rn(s[j & 3], term(lam[p], r[j], k, k2));
+    }
+    for (int j = RES_R; j < jn; j += 4) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int p = lane + 32 * (j + q);
+        if (j + q < jn && p < n)
+          s[q] = __dadd_rn(s[q], term(lam[p], sm[(j + q - RES_R) * 32 + lane], k, k2));
+      }
+    }
+    const double sum = warp_reduce_sum(__dadd_rn(__dadd_rn(s[0], s[1]), __dadd_rn(s[2], s[3])));
+    if (U) return __ddiv_rn(__dsub_rn(C, __ddiv_rn(sum, 4.0)), C);
+    return __ddiv_rn(sum, 4.0);
+  }
+};
+
+// Launch shape of the resident kernels: one CTA per SM holding the
+// eigenvalues (RES_MAX_N doubles) and RES_S * 32 doubles per warp.  8 warps
+// (2 per SM sub-partition) leave 255 registers per thread for the 64
+// register-resident weights; with 3 warps on a sub-partition the limit drops
+// to 168 and the column spills.
+constexpr int RES_WARPS_PLAIN = 8;    // 32 KB + 8 x 16 KB = 160 KB
+constexpr int RES_WARPS_LEARNED = 8;  // + 20 KB of MLP weights
+// Resident kernel for this problem?  mode: IMCOM_BISECT_* option value.
+// Automatic choice: streaming.  With the Newton reciprocal the per-term
+// chain is short and the streaming kernel's ~28 warps per SM hide L2
+// latency; the resident kernel's 8 warps do not hide the FP64 latency
+// (n = m = 4096: 0.47 vs 1.03 ms).
+inline bool use_resident(int mode, int n) {
+  if (n > RES_MAX_N) return false;
+  return mode == 2;
+}
+
+inline size_t res_smem_bytes(int warps) {
+  return (size_t)RES_MAX_N * sizeof(double) + (size_t)warps * RES_S * 32 * sizeof(double);
 }
 
 // Shared-memory plan of the per-pixel kernels: the eigenvalues (n) plus one

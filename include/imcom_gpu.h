@@ -67,6 +67,13 @@ typedef struct imcom_ctx imcom_ctx;
                                       kept pixel: 10^-value (7)                */
 #define IMCOM_OPT_SPLIT_TOL_T 7    /* audit bound on the relative error of a
                                       kept T column: 10^-value (8)             */
+/* Bisection kernel: 0 automatic (the autotuned choice for the problem
+ * size), 1 columns streamed from L2 (any n), 2 columns resident in
+ * registers and shared memory (n <= 4096).  Same results either way. */
+#define IMCOM_OPT_BISECT_KERNEL 8
+#define IMCOM_BISECT_AUTO 0
+#define IMCOM_BISECT_STREAM 1
+#define IMCOM_BISECT_RESIDENT 2
 
 /* ---- context ---------------------------------------------------------- */
 
