@@ -15,7 +15,8 @@
 //               v^T y = v^T y0 - 2 (V^T v).(W^T v), the update of the next
 //               column, its norm and its dot products with the panel's
 //               W and V (the rows already hold them in registers).
-//    The trailing update A22 -= V W^T + W V^T runs on the DMMA GEMM.
+//    The trailing update A22 -= V W^T + W V^T runs on the DMMA GEMM as one
+//    product with K = 2 NB ([V W] [W V]^T: one pass over A22).
 //    Grid barriers spin with a bound and report a timeout instead of hanging.
 // 2. Divide and conquer (LAPACK dstedc / dlaed0-4 structure).  Leaves of at
 //    most 32 rows are diagonalised by a cyclic Jacobi sweep in one CTA each.
@@ -843,12 +844,19 @@ __global__ void dc_assemble_kernel(const Node* nodes, DcWork wk, const double* O
 // T (upper triangle) and G (strict upper triangle, stored transposed in the
 // lower triangle) share one shared-memory tile, so the recurrence reads no
 // global memory.
-__global__ void __launch_bounds__(NBB) larft_kernel(const double* G, long long ldg,
-                                                    const double* tau, int jb, double* T,
-                                                    long long ldt) {
+// One CTA per block of NBB reflectors: block b holds reflectors
+// b NBB .. b NBB + jb - 1 (jb = min(NBB, nref - b NBB)), its Gram matrix at
+// G + b NBB ldg and its T factor at T + b NBB ldt.
+__global__ void __launch_bounds__(NBB) larft_kernel(const double* Gall, long long ldg,
+                                                    const double* tau_all, int nref,
+                                                    double* Tall, long long ldt) {
   extern __shared__ double smem_t[];
   double(*S)[NBB + 1] = reinterpret_cast<double(*)[NBB + 1]>(smem_t);
   const int r = threadIdx.x;
+  const int j0 = blockIdx.x * NBB, jb = min(NBB, nref - j0);
+  const double* G = Gall + (size_t)blockIdx.x * NBB * ldg;
+  const double* tau = tau_all + j0;
+  double* T = Tall + (size_t)blockIdx.x * NBB * ldt;
   // S[c][r] = G(r, c) for r < c (lower triangle); the upper triangle holds T
   for (int c = 0; c < jb; ++c) {
     if (r <= c) S[r][c] = 0.0;                          // T part: upper triangle
@@ -879,9 +887,25 @@ struct DcBuffers {
   size_t bytes = 0;
 };
 
+// X = [V(:, k:k+b) | W(:, 0:b)] and Y = [W | V], rows t0..n-1 (ld ldx): the
+// operands of the fused trailing update A22 -= X Y^T = V W^T + W V^T.
+__global__ void pack_update_kernel(const double* __restrict__ V, long long ldv,
+                                   const double* __restrict__ W, long long ldw, int t0, int n,
+                                   int b, double* __restrict__ X, double* __restrict__ Y,
+                                   long long ldx) {
+  const int c = blockIdx.y;  // 0 .. b-1
+  for (int r = t0 + blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const double v = V[r + (long long)c * ldv], w = W[r + (long long)c * ldw];
+    X[r + (long long)c * ldx] = v;
+    X[r + (long long)(b + c) * ldx] = w;
+    Y[r + (long long)c * ldx] = w;
+    Y[r + (long long)(b + c) * ldx] = v;
+  }
+}
+
 static int sytrd_gpu(imcom_ctx* ctx, DMat& Aw, DMat& Vall, double* d, double* e, double* tau,
                      double* W, long long ldw, double* ypart, long long ldy, void* accbuf,
-                     long long spin) {
+                     long long spin, double* XY) {
   const int n = (int)Aw.rows;
   int dev = ctx->device, coop = 0;
   cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
@@ -906,11 +930,15 @@ static int sytrd_gpu(imcom_ctx* ctx, DMat& Aw, DMat& Vall, double* d, double* e,
     IMC_LAUNCH();
     const int t0 = k + b, rem = n - t0;
     if (rem > 0) {
-      // A22 -= V W^T + W V^T
-      const double* Vp = Vall.p + t0 + (long long)k * Vall.ld;
-      IMC_TRY(dgemm(ctx, 'N', 'T', rem, rem, b, -1.0, Vp, Vall.ld, W + t0, ldw, 1.0,
-                    Aw.p + t0 + (long long)t0 * Aw.ld, Aw.ld));
-      IMC_TRY(dgemm(ctx, 'N', 'T', rem, rem, b, -1.0, W + t0, ldw, Vp, Vall.ld, 1.0,
+      // A22 -= V W^T + W V^T as one K = 2b product (one pass over A22)
+      const long long ldx = ldw;
+      double* X = XY;
+      double* Y = XY + (size_t)ldx * 2 * NB;
+      dim3 grd((rem + 255) / 256, b);
+      pack_update_kernel<<<grd, 256, 0, ctx->stream>>>(Vall.p + (long long)k * Vall.ld, Vall.ld,
+                                                       W, ldw, t0, n, b, X, Y, ldx);
+      IMC_LAUNCH();
+      IMC_TRY(dgemm(ctx, 'N', 'T', rem, rem, 2 * b, -1.0, X + t0, ldx, Y + t0, ldx, 1.0,
                     Aw.p + t0 + (long long)t0 * Aw.ld, Aw.ld));
     }
     // a timed-out barrier ends the factorisation with an error
@@ -955,11 +983,13 @@ int eigen_dc(imcom_ctx* ctx, const DMat& A, DMat& Wout, double* wout) {
   };
   size_t o_d = take(n * 8), o_e = take(n * 8), o_tau = take(n * 8), o_dt = take(n * 8);
   size_t o_W = take((size_t)ldw * NB * 8), o_y = take((size_t)ldy * nch * 8);
+  size_t o_XY = take((size_t)ldw * 4 * NB * 8);
   size_t o_acc = take(4096);
   size_t o_split = take((size_t)n * 4), o_nodes = take((size_t)n * sizeof(Node));
   size_t o_wk = take(((size_t)n * 8 + 16) * 9 + ((size_t)n * 4 + 16) * 8 + ((size_t)n * 24 + 32) +
                      4096);
-  size_t o_T = take((size_t)NBB * NBB * 8), o_G = take((size_t)NBB * NBB * 8);
+  const size_t nblk_bt = (size_t)(n - 1 + NBB - 1) / NBB + 1;
+  size_t o_T = take(nblk_bt * NBB * NBB * 8), o_G = take(nblk_bt * NBB * NBB * 8);
   size_t o_X = take((size_t)NBB * ld * 8 * 2);
   size_t o_err = take(64);
   IMC_TRY(eig_buf(ctx, off + 256));
@@ -983,7 +1013,8 @@ int eigen_dc(imcom_ctx* ctx, const DMat& A, DMat& Wout, double* wout) {
   IMC_TRY(copy_mat(ctx, A.p, A.ld, Aw.p, Aw.ld, n, n));
   IMC_CUDA(cudaMemsetAsync(Vall.p, 0, Vall.bytes(), ctx->stream));
   IMC_CUDA(cudaMemsetAsync(Wp, 0, (size_t)ldw * NB * 8, ctx->stream));
-  IMC_TRY(sytrd_gpu(ctx, Aw, Vall, d, e, tau, Wp, ldw, yp, ldy, base + o_acc, spin));
+  IMC_TRY(sytrd_gpu(ctx, Aw, Vall, d, e, tau, Wp, ldw, yp, ldy, base + o_acc, spin,
+                    (double*)(base + o_XY)));
   stage_end(ctx, ST_EIG_TRD);
   stage_begin(ctx, ST_EIG_DC);
 
@@ -1113,17 +1144,26 @@ int eigen_dc(imcom_ctx* ctx, const DMat& A, DMat& Wout, double* wout) {
                                 (int)LARFT_SMEM));
   double* X = Xb;
   double* X2 = Xb + (size_t)NBB * ld;
+  // Gram matrices of every block, then every T factor in one launch (one CTA
+  // per block: the T recurrences run concurrently)
+  for (int bi = 0; bi < nblk; ++bi) {
+    const int j0 = bi * NBB, jb = std::min(NBB, nref - j0);
+    const int r0 = j0, K = n - r0;
+    const double* Vb = Vall.p + r0 + (size_t)j0 * Vall.ld;
+    IMC_TRY(dgemm(ctx, 'T', 'N', jb, jb, K, 1.0, Vb, Vall.ld, Vb, Vall.ld, 0.0,
+                  Gb + (size_t)bi * NBB * NBB, NBB));
+  }
+  larft_kernel<<<nblk, NBB, LARFT_SMEM, ctx->stream>>>(Gb, NBB, tau, nref, Tb, NBB);
+  IMC_LAUNCH();
   for (int bi = nblk - 1; bi >= 0; --bi) {
     const int j0 = bi * NBB, jb = std::min(NBB, nref - j0);
     // rows from j0: row j0 of the block's reflectors is zero, and an even
     // first row keeps the GEMM operands 16-byte aligned
     const int r0 = j0, K = n - r0;
     const double* Vb = Vall.p + r0 + (size_t)j0 * Vall.ld;
-    IMC_TRY(dgemm(ctx, 'T', 'N', jb, jb, K, 1.0, Vb, Vall.ld, Vb, Vall.ld, 0.0, Gb, NBB));
-    larft_kernel<<<1, NBB, LARFT_SMEM, ctx->stream>>>(Gb, NBB, tau + j0, jb, Tb, NBB);
-    IMC_LAUNCH();
+    const double* Tblk = Tb + (size_t)bi * NBB * NBB;
     IMC_TRY(dgemm(ctx, 'T', 'N', jb, n, K, 1.0, Vb, Vall.ld, Zcur + r0, ld, 0.0, X, NBB));
-    IMC_TRY(dgemm(ctx, 'N', 'N', jb, n, jb, 1.0, Tb, NBB, X, NBB, 0.0, X2, NBB));
+    IMC_TRY(dgemm(ctx, 'N', 'N', jb, n, jb, 1.0, Tblk, NBB, X, NBB, 0.0, X2, NBB));
     IMC_TRY(dgemm(ctx, 'N', 'N', K, n, jb, -1.0, Vb, Vall.ld, X2, NBB, 1.0, Zcur + r0, ld));
   }
   if (Zcur != Wout.p) IMC_TRY(copy_mat(ctx, Zcur, ld, Wout.p, Wout.ld, n, n));
