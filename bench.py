@@ -475,7 +475,8 @@ def run_ours(args):
             "accuracy_vs_plain_fp64": accuracy,
             "kappa": kappa_info,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "ms_per_step": t_e2e},
+                    "d2h_bytes_per_step": d2h, "ms_per_step": t_e2e,
+                    "ms_steps": [round(x, 3) for x in e2e_ms]},
             "gpu_launches": launches,
             "roofline": roof,
             "split_roofline": split_roof,

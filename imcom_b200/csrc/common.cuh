@@ -8,6 +8,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <unordered_map>
 
 #include "../../include/imcom_gpu.h"
 
@@ -125,6 +126,10 @@ struct imcom_ctx {
   imcom::MlpWeights mlp;
   float* feat = nullptr;
 
+  // capacity in bytes of every buffer grown by ensure_vec, keyed by the
+  // address of the context field that holds its pointer
+  std::unordered_map<void**, size_t> vec_cap;
+
   cudaEvent_t ev0[imcom::ST_N] = {}, ev1[imcom::ST_N] = {};
   bool ev_used[imcom::ST_N] = {};
 };
@@ -167,7 +172,8 @@ extern unsigned long long g_launches;
   } while (0)
 
 // (Re)allocate a device matrix of the given shape; keeps the buffer when it
-// is already large enough.
+// is already large enough.  ensure_vec likewise keeps a vector whose buffer
+// already holds `count` elements (the contents are not preserved on growth).
 int ensure_mat(imcom_ctx* ctx, DMat& M, long long rows, long long cols);
 int ensure_buf(imcom_ctx* ctx, void** p, size_t& have, size_t need);
 template <class T>

@@ -1,5 +1,6 @@
 // ctx.cu -- context, module state upload/download and the cache-read branches
 // of the reference's imcom_get_* routines.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -64,15 +65,20 @@ int ensure_mat(imcom_ctx* ctx, DMat& M, long long rows, long long cols) {
 
 template <class T>
 int ensure_vec(imcom_ctx* ctx, T** p, size_t count) {
+  const size_t need = count * sizeof(T) + 256;
+  size_t& cap = ctx->vec_cap[reinterpret_cast<void**>(p)];
+  if (*p && cap >= need) return 0;
   if (*p) cudaFree(*p);
   *p = nullptr;
-  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T) + 256);
+  cap = 0;
+  cudaError_t e = cudaMalloc((void**)p, need);
   if (e != cudaSuccess) {
     *p = nullptr;
     cudaGetLastError();
     return set_err(ctx, IMCOM_ERR_ALLOC, "cudaMalloc(%zu): %s", count * sizeof(T),
                    cudaGetErrorString(e));
   }
+  cap = need;
   return 0;
 }
 template int ensure_vec<double>(imcom_ctx*, double**, size_t);
@@ -128,6 +134,32 @@ static int check_finite(imcom_ctx* ctx, const double* p, long long count, const 
   for (long long k = 0; k < count; ++k)
     if (!std::isfinite(p[k]))
       return set_err(ctx, IMCOM_ERR_NOT_FINITE, "non-finite value in %s at index %lld", what, k);
+  return 0;
+}
+
+// First index of a non-finite value in a device array (atomicMin into *first,
+// which starts at LLONG_MAX).
+__global__ void first_nonfinite_kernel(const double* __restrict__ p, long long count,
+                                       unsigned long long* first) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < count;
+       k += (long long)gridDim.x * blockDim.x)
+    if (!isfinite(p[k])) atomicMin(first, (unsigned long long)k);
+}
+
+// Finiteness check of arrays already on the device (large PSF arrays: one
+// pass on the GPU instead of a host pass over host memory).
+static int check_finite_dev(imcom_ctx* ctx, const double* d, long long count, const char* what) {
+  unsigned long long* first = reinterpret_cast<unsigned long long*>(ctx->flags + 28);
+  IMC_CUDA(cudaMemsetAsync(first, 0xff, sizeof(unsigned long long), ctx->stream));
+  const int blocks = (int)std::min<long long>((count + 255) / 256, 4 * 148);
+  first_nonfinite_kernel<<<blocks, 256, 0, ctx->stream>>>(d, count, first);
+  IMC_LAUNCH();
+  unsigned long long h = 0;
+  IMC_CUDA(cudaMemcpyAsync(&h, first, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+  IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (h != ~0ULL)
+    return set_err(ctx, IMCOM_ERR_NOT_FINITE, "non-finite value in %s at index %lld", what,
+                   (long long)h);
   return 0;
 }
 
@@ -309,8 +341,6 @@ int imcom_gpu_set_psfs(imcom_ctx* ctx, int nps, int nexppsf, int psfconst,
   if (!rotangdeg) return -6;
   if (!Gamma) return -7;
   size_t ps2 = (size_t)nps * nps;
-  IMC_TRY(check_finite(ctx, G_unrot, (long long)(ps2 * nexppsf), "G_unrot"));
-  IMC_TRY(check_finite(ctx, Gamma, (long long)ps2, "Gamma"));
   IMC_TRY(check_finite(ctx, rotangdeg, nexppsf, "rotangdeg"));
   cudaSetDevice(ctx->device);
   ctx->nps = nps;
@@ -327,7 +357,9 @@ int imcom_gpu_set_psfs(imcom_ctx* ctx, int nps, int nexppsf, int psfconst,
                            cudaMemcpyHostToDevice, ctx->stream));
   IMC_CUDA(cudaMemcpyAsync(ctx->Gamma, Gamma, ps2 * sizeof(double), cudaMemcpyHostToDevice,
                            ctx->stream));
-  IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->have_psf = false;
+  IMC_TRY(check_finite_dev(ctx, ctx->G, (long long)(ps2 * nexppsf), "G_unrot"));
+  IMC_TRY(check_finite_dev(ctx, ctx->Gamma, (long long)ps2, "Gamma"));
   ctx->have_psf = true;
   ctx->have_spectra = false;
   return 0;

@@ -66,6 +66,27 @@ def test_state_and_argument_errors(solver):
         solver.set_inputs(prob.x_i, prob.y_i, prob.exp_i[::-1], prob.X_a, prob.Y_a)
 
 
+def test_nonfinite_psf_is_rejected(solver):
+    """A NaN or inf in the PSF arrays is reported with its index (checked on
+    the device after the upload) and leaves no usable PSF state behind."""
+    prob = synth.make("tiny", 0)
+    solver.set_problem(prob)
+    G = np.array(prob.G_unrot, order="F")
+    G.ravel(order="F")[1234] = np.nan
+    with pytest.raises(ImcomError) as ex:
+        solver.set_psfs(G, prob.rotangdeg, prob.Gamma, prob.psfconst)
+    assert ex.value.status == 7 and "G_unrot" in str(ex.value) and "1234" in str(ex.value)
+    with pytest.raises(ImcomError):
+        solver.psf_spectra()
+    Gam = np.array(prob.Gamma, order="F")
+    Gam[3, 5] = np.inf
+    with pytest.raises(ImcomError) as ex:
+        solver.set_psfs(prob.G_unrot, prob.rotangdeg, Gam, prob.psfconst)
+    assert ex.value.status == 7 and "Gamma" in str(ex.value)
+    solver.set_problem(prob)  # a clean upload works again
+    assert solver.psf_spectra() > 0
+
+
 def test_cached_system_path_reuses_T(gs):
     """T-reuse path (imcom_bisect.f90:47-62): H from a loaded T equals H of the solve."""
     prob = synth.make("tiny", 0)
