@@ -245,6 +245,10 @@ int imcom_gpu_set_option(imcom_ctx* ctx, int option, long long value) {
       if (value < IMCOM_BISECT_AUTO || value > IMCOM_BISECT_RESIDENT) return -3;
       ctx->bisect_kernel = (int)value;
       return 0;
+    case IMCOM_OPT_BISECT_CTAS_PER_SM:
+      if (value < 0 || value > 64) return -3;
+      ctx->bisect_ctas = (int)value;
+      return 0;
     case IMCOM_OPT_PRECISION:
       if (value != IMCOM_PREC_FP64 && value != IMCOM_PREC_SPLIT) return -3;
       ctx->prec = (int)value;

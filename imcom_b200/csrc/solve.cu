@@ -170,6 +170,7 @@ int fill_bisect_args(imcom_ctx* ctx, BisectArgs& a, int UnotS, double US_max, do
 
 int pixel_grid(imcom_ctx* ctx, const PixelSmem& plan, int m) {
   int blocks = (m + plan.warps - 1) / plan.warps;
+  if (ctx->bisect_ctas > 0) blocks = std::min(blocks, ctx->bisect_ctas * sm_count(ctx));
   return blocks;
 }
 

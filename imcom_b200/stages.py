@@ -6,7 +6,12 @@ can select one stage's kernels, e.g.
     ncu --nvtx --nvtx-include "P/" -k regex:dgemm_kernel -c 1 \\
         python -m imcom_b200.stages n4096
 
-Usage: python -m imcom_b200.stages [workload] [--library-eigensolver]
+Usage: python -m imcom_b200.stages [workload] [--library-eigensolver] [--split]
+                                    [--learned]
+
+--split    P and T on the split-precision int8 product (IMCOM_PREC_SPLIT)
+--learned  learned-kappa bracket (committed weights) instead of the plain
+           bisection
 """
 from __future__ import annotations
 
@@ -23,6 +28,11 @@ def main(argv):
     prob = synth.make(wl, 0)
     with Solver(0) as s:
         s.set_eigensolver(EIGH_LIBRARY if "--library-eigensolver" in argv else EIGH_DC)
+        s.set_precision("--split" in argv)
+        learned = "--learned" in argv
+        if learned:
+            from .kappa_model import DEFAULT_WEIGHTS, KappaModel
+            KappaModel.load(DEFAULT_WEIGHTS).install(s)
         s.set_problem(prob)
 
         def stage(name, fn):
@@ -37,8 +47,12 @@ def main(argv):
         stage("EIG", lambda: s.eigen_A(out=False))
         stage("B", lambda: s.build_B(out=False))
         stage("P", lambda: s.build_P(out=False))
-        stage("BISECT", lambda: s.bisect_kappa(True, 1e-2, C * EPS, C / EPS, 1e-5, 53, C,
-                                               out=False))
+        if learned:
+            stage("BISECT", lambda: s.bisect_kappa_learned(True, 1e-2, C * EPS, C / EPS, 1e-5,
+                                                           53, C, out=False))
+        else:
+            stage("BISECT", lambda: s.bisect_kappa(True, 1e-2, C * EPS, C / EPS, 1e-5, 53, C,
+                                                   out=False))
         stage("T", lambda: s.build_T(out=False))
         stage("EPI", lambda: (s.build_S(out=False), s.build_image(out=False)))
         print({k: round(v, 3) for k, v in s.stage_times().items()})

@@ -74,6 +74,10 @@ typedef struct imcom_ctx imcom_ctx;
 #define IMCOM_BISECT_AUTO 0
 #define IMCOM_BISECT_STREAM 1
 #define IMCOM_BISECT_RESIDENT 2
+/* CTAs (of 4 pixel warps) per SM of the streaming bisection kernels; 0 puts
+ * every pixel in flight at once.  Fewer pixels in flight keep their P columns
+ * in L2 across their U/S evaluations. */
+#define IMCOM_OPT_BISECT_CTAS_PER_SM 9
 
 /* ---- context ---------------------------------------------------------- */
 
