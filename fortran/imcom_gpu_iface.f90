@@ -173,6 +173,37 @@ INTERFACE
     REAL(C_DOUBLE), DIMENSION(*) :: U_out
   END FUNCTION
 
+  ! Options (no reference counterpart), e.g. option 3 = IMCOM_OPT_PRECISION,
+  ! value 1 = IMCOM_PREC_SPLIT for the split-precision P and T
+  INTEGER(C_INT) FUNCTION imcom_gpu_set_option(ctx, option, value) &
+                                               BIND(C, NAME="imcom_gpu_set_option")
+    IMPORT :: C_INT, C_PTR, C_LONG_LONG
+    TYPE(C_PTR), VALUE :: ctx
+    INTEGER(C_INT), VALUE :: option
+    INTEGER(C_LONG_LONG), VALUE :: value
+  END FUNCTION
+
+  ! imcom_bisect_kappa with the learned-kappa bracket (same K; weights set
+  ! with imcom_gpu_mlp_set_weights)
+  INTEGER(C_INT) FUNCTION imcom_gpu_bisect_kappa_learned(ctx, UnotS, US_max, k_min, k_max, &
+                                                         tol, maxnits, C_a, K_out, US_out, &
+                                                         nevals_out, fallback_out) &
+                                                         BIND(C, NAME="imcom_gpu_bisect_kappa_learned")
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: ctx
+    INTEGER(C_INT), VALUE :: UnotS, maxnits
+    REAL(C_DOUBLE), VALUE :: US_max, k_min, k_max, tol, C_a
+    REAL(C_DOUBLE), DIMENSION(*) :: K_out, US_out
+    TYPE(C_PTR), VALUE :: nevals_out, fallback_out
+  END FUNCTION
+
+  ! Report of the split-precision audit (8 values)
+  INTEGER(C_INT) FUNCTION imcom_gpu_split_info(ctx, info8) BIND(C, NAME="imcom_gpu_split_info")
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: ctx
+    REAL(C_DOUBLE), DIMENSION(8) :: info8
+  END FUNCTION
+
 END INTERFACE
 
 TYPE(C_PTR), SAVE :: imcom_gpu_ctx = C_NULL_PTR
