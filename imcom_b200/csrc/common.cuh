@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <string>
 #include <unordered_map>
+#include <vector>
 
 #include "../../include/imcom_gpu.h"
 
@@ -19,6 +20,7 @@ namespace imcom {
 struct DMat {
   double* p = nullptr;
   long long rows = 0, cols = 0, ld = 0;
+  size_t cap = 0;  // bytes allocated (kept when a smaller matrix reuses it)
   size_t bytes() const { return (size_t)ld * (size_t)cols * sizeof(double); }
 };
 
@@ -90,10 +92,22 @@ struct imcom_ctx {
   size_t tables_bytes = 0;
   double2* fftbuf = nullptr;
   size_t fftbuf_bytes = 0;
-  cufftHandle plan_big[2] = {0, 0};  // [0] A tables, [1] B tables
-  int plan_big_L[2] = {0, 0}, plan_big_batch[2] = {0, 0};
-  cufftHandle plan_r2c = 0;
-  int plan_r2c_n = 0, plan_r2c_batch = 0;
+  // cuFFT plans by (type, side, batch), least recently used evicted.  The PSF
+  // stamp side follows each patch's input footprint, so a run over many
+  // patches revisits a handful of sizes; planning one (Bluestein sizes
+  // included) costs tens to hundreds of milliseconds of host time.  All plans
+  // of a context share one work area: their executions are serialised on
+  // the context's stream.
+  struct FftPlan {
+    int type, side, batch;
+    cufftHandle h;
+    size_t work;
+    unsigned long long used;
+  };
+  std::vector<FftPlan> fft_plans;
+  unsigned long long fft_clock = 0;
+  void* fft_work = nullptr;
+  size_t fft_work_bytes = 0;
 
   int8_t* band = nullptr;   // eigenmode band indices of the learned-kappa features
   size_t band_bytes = 0;
@@ -108,6 +122,7 @@ struct imcom_ctx {
   int prec = IMCOM_PREC_FP64;
   int bisect_kernel = IMCOM_BISECT_AUTO;
   int bisect_ctas = 0;  // CTAs per SM of the streaming pixel kernels (0: all pixels at once)
+  int sm_share = 0;     // SMs for persistent / cooperative grids (0: the whole device)
   int split_SP = 7, split_ST = 6;        // digit slices of the P and T products
   double split_tol_us = 1e-7, split_tol_t = 1e-8;
   imcom::SplitOp sq_P, sq_T, sb_P, spt_T;  // Q columns, Q rows, B, P~
@@ -177,6 +192,11 @@ extern unsigned long long g_launches;
 // already holds `count` elements (the contents are not preserved on growth).
 int ensure_mat(imcom_ctx* ctx, DMat& M, long long rows, long long cols);
 int ensure_buf(imcom_ctx* ctx, void** p, size_t& have, size_t need);
+// Cached 2-D cuFFT plan of `batch` contiguous side x side transforms (type
+// CUFFT_Z2Z in place, or CUFFT_D2Z from side^2 reals to side*(side/2+1)
+// complex values), bound to the context's stream and shared work area.
+int fft_plan(imcom_ctx* ctx, cufftType type, int side, int batch, cufftHandle* out);
+void fft_free(imcom_ctx* ctx);
 template <class T>
 int ensure_vec(imcom_ctx* ctx, T** p, size_t count);
 

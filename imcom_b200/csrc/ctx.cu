@@ -38,11 +38,59 @@ int ensure_buf(imcom_ctx* ctx, void** p, size_t& have, size_t need) {
   return 0;
 }
 
+int fft_plan(imcom_ctx* ctx, cufftType type, int side, int batch, cufftHandle* out) {
+  constexpr size_t kMaxPlans = 64;  // about twenty sides of the three plan kinds
+  auto& plans = ctx->fft_plans;
+  size_t hit = plans.size();
+  for (size_t i = 0; i < plans.size(); ++i)
+    if (plans[i].type == (int)type && plans[i].side == side && plans[i].batch == batch) hit = i;
+  if (hit == plans.size()) {
+    if (plans.size() >= kMaxPlans) {
+      size_t lru = 0;
+      for (size_t i = 1; i < plans.size(); ++i)
+        if (plans[i].used < plans[lru].used) lru = i;
+      cufftDestroy(plans[lru].h);
+      plans.erase(plans.begin() + lru);
+    }
+    imcom_ctx::FftPlan f{(int)type, side, batch, 0, 0, 0};
+    IMC_CUFFT(cufftCreate(&f.h));
+    cufftResult r = cufftSetAutoAllocation(f.h, 0);
+    int dims[2] = {side, side};
+    long long dist_in = (long long)side * side;
+    long long dist_out = type == CUFFT_D2Z ? (long long)side * (side / 2 + 1) : dist_in;
+    if (r == CUFFT_SUCCESS)
+      r = cufftMakePlanMany(f.h, 2, dims, nullptr, 1, (int)dist_in, nullptr, 1, (int)dist_out,
+                            type, batch, &f.work);
+    if (r != CUFFT_SUCCESS) {
+      cufftDestroy(f.h);
+      return set_err(ctx, IMCOM_ERR_CUDA, "cuFFT plan %dx%d x%d (type %d): error %d", side, side,
+                     batch, (int)type, (int)r);
+    }
+    plans.push_back(f);
+    hit = plans.size() - 1;
+  }
+  imcom_ctx::FftPlan& f = plans[hit];
+  f.used = ++ctx->fft_clock;
+  IMC_TRY(ensure_buf(ctx, &ctx->fft_work, ctx->fft_work_bytes, f.work));
+  if (f.work) IMC_CUFFT(cufftSetWorkArea(f.h, ctx->fft_work));
+  IMC_CUFFT(cufftSetStream(f.h, ctx->stream));
+  *out = f.h;
+  return 0;
+}
+
+void fft_free(imcom_ctx* ctx) {
+  for (auto& f : ctx->fft_plans) cufftDestroy(f.h);
+  ctx->fft_plans.clear();
+  if (ctx->fft_work) cudaFree(ctx->fft_work);
+  ctx->fft_work = nullptr;
+  ctx->fft_work_bytes = 0;
+}
+
 int ensure_mat(imcom_ctx* ctx, DMat& M, long long rows, long long cols) {
   long long ld = pad_ld(rows);
   size_t need = (size_t)ld * (size_t)cols * sizeof(double);
   if (M.p && M.ld == ld && M.cols == cols && M.rows == rows) return 0;
-  if (M.p && M.bytes() >= need) {
+  if (M.p && M.cap >= need) {
     M.rows = rows;
     M.cols = cols;
     M.ld = ld;
@@ -50,6 +98,7 @@ int ensure_mat(imcom_ctx* ctx, DMat& M, long long rows, long long cols) {
   }
   if (M.p) cudaFree(M.p);
   M.p = nullptr;
+  M.cap = 0;
   cudaError_t e = cudaMalloc(&M.p, need);
   if (e != cudaSuccess) {
     M.p = nullptr;
@@ -57,6 +106,7 @@ int ensure_mat(imcom_ctx* ctx, DMat& M, long long rows, long long cols) {
     return set_err(ctx, IMCOM_ERR_ALLOC, "cudaMalloc(%zu bytes) for %lldx%lld matrix: %s",
                    need, rows, cols, cudaGetErrorString(e));
   }
+  M.cap = need;
   M.rows = rows;
   M.cols = cols;
   M.ld = ld;
@@ -115,14 +165,21 @@ void stage_end(imcom_ctx* ctx, Stage s) {
   ctx->ev_used[s] = true;
 }
 
-int sm_count(imcom_ctx* ctx) {
+int device_sm_count(int d) {
   static int cached[64] = {0};
-  int d = ctx->device;
   if (d >= 0 && d < 64 && cached[d]) return cached[d];
   int v = 148;
   cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, d);
   if (d >= 0 && d < 64) cached[d] = v;
   return v;
+}
+
+// SMs this context sizes its persistent and cooperative grids for: the whole
+// device, or the share set with IMCOM_OPT_SM_SHARE (contexts that solve
+// independent patches side by side each take a share).
+int sm_count(imcom_ctx* ctx) {
+  const int v = device_sm_count(ctx->device);
+  return (ctx->sm_share > 0 && ctx->sm_share < v) ? ctx->sm_share : v;
 }
 
 }  // namespace imcom
@@ -207,9 +264,7 @@ int imcom_gpu_destroy(imcom_ctx* ctx) {
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete[] ctx->rot;
-  for (int q = 0; q < 2; ++q)
-    if (ctx->plan_big[q]) cufftDestroy(ctx->plan_big[q]);
-  if (ctx->plan_r2c) cufftDestroy(ctx->plan_r2c);
+  fft_free(ctx);
   for (int s = 0; s < ST_N; ++s) {
     if (ctx->ev0[s]) cudaEventDestroy(ctx->ev0[s]);
     if (ctx->ev1[s]) cudaEventDestroy(ctx->ev1[s]);
@@ -244,6 +299,10 @@ int imcom_gpu_set_option(imcom_ctx* ctx, int option, long long value) {
     case IMCOM_OPT_BISECT_KERNEL:
       if (value < IMCOM_BISECT_AUTO || value > IMCOM_BISECT_RESIDENT) return -3;
       ctx->bisect_kernel = (int)value;
+      return 0;
+    case IMCOM_OPT_SM_SHARE:
+      if (value < 0 || value > 1024) return -3;
+      ctx->sm_share = (int)value;
       return 0;
     case IMCOM_OPT_BISECT_CTAS_PER_SM:
       if (value < 0 || value > 64) return -3;

@@ -262,18 +262,8 @@ int build_tables(imcom_ctx* ctx, int npad, int isB) {
                                          big2 * ntab * sizeof(double2));
   IMC_CUDA(cudaMemcpyAsync(dpairs, pairs.data(), ntab * sizeof(int2), cudaMemcpyHostToDevice,
                            ctx->stream));
-  // one cached plan per table kind (the A and B passes have different batches)
-  cufftHandle& plan = ctx->plan_big[isB ? 1 : 0];
-  if (!plan || ctx->plan_big_L[isB] != nbig || ctx->plan_big_batch[isB] != ntab) {
-    if (plan) cufftDestroy(plan);
-    plan = 0;
-    int dims[2] = {nbig, nbig};
-    IMC_CUFFT(cufftPlanMany(&plan, 2, dims, nullptr, 1, (int)big2, nullptr, 1, (int)big2,
-                            CUFFT_Z2Z, ntab));
-    ctx->plan_big_L[isB] = nbig;
-    ctx->plan_big_batch[isB] = ntab;
-  }
-  IMC_CUFFT(cufftSetStream(plan, ctx->stream));
+  cufftHandle plan = 0;
+  IMC_TRY(fft_plan(ctx, CUFFT_Z2Z, nbig, ntab, &plan));
   dim3 blk(128), grd((nbig + 127) / 128, nbig, ntab);
   embed_kernel<<<grd, blk, 0, ctx->stream>>>(ctx->Gt, ctx->Gammat, dpairs, ctx->fftbuf, nps, nbig);
   IMC_LAUNCH();
@@ -336,17 +326,9 @@ extern "C" int imcom_gpu_psf_spectra(imcom_ctx* ctx, int npoly_in, double* C_out
   }
   IMC_CUDA(cudaMemcpyAsync(rin + (size_t)E * ps2, ctx->Gamma, ps2 * sizeof(double),
                            cudaMemcpyDeviceToDevice, ctx->stream));
-  if (!ctx->plan_r2c || ctx->plan_r2c_n != nps || ctx->plan_r2c_batch != E + 1) {
-    if (ctx->plan_r2c) cufftDestroy(ctx->plan_r2c);
-    ctx->plan_r2c = 0;
-    int dims[2] = {nps, nps};
-    IMC_CUFFT(cufftPlanMany(&ctx->plan_r2c, 2, dims, nullptr, 1, (int)ps2, nullptr, 1,
-                            nh * nps, CUFFT_D2Z, E + 1));
-    ctx->plan_r2c_n = nps;
-    ctx->plan_r2c_batch = E + 1;
-  }
-  IMC_CUFFT(cufftSetStream(ctx->plan_r2c, ctx->stream));
-  IMC_CUFFT(cufftExecD2Z(ctx->plan_r2c, rin, (cufftDoubleComplex*)half));
+  cufftHandle plan = 0;
+  IMC_TRY(fft_plan(ctx, CUFFT_D2Z, nps, E + 1, &plan));
+  IMC_CUFFT(cufftExecD2Z(plan, rin, (cufftDoubleComplex*)half));
   {
     dim3 blk(128), grd((nps + 127) / 128, nps, E);
     hermitian_fill_kernel<<<grd, blk, 0, ctx->stream>>>(half, ctx->Gt, nps, nps);

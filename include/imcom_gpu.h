@@ -78,6 +78,12 @@ typedef struct imcom_ctx imcom_ctx;
  * every pixel in flight at once.  Fewer pixels in flight keep their P columns
  * in L2 across their U/S evaluations. */
 #define IMCOM_OPT_BISECT_CTAS_PER_SM 9
+/* Number of SMs this context sizes its persistent and cooperative grids for
+ * (the tridiagonalisation panel kernel, the resident bisection, split-K
+ * GEMMs); 0 = the whole device.  Contexts that solve independent patches at
+ * the same time on one GPU each take a share.  Results agree to rounding
+ * (the reduction order of the eigensolver follows the grid). */
+#define IMCOM_OPT_SM_SHARE 10
 
 /* ---- context ---------------------------------------------------------- */
 
