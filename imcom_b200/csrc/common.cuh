@@ -214,6 +214,11 @@ int sm_count(imcom_ctx* ctx);
 // FP64 GEMM: C (M x N) = alpha * op(A) * op(B) + beta * C, column-major.
 // transA: 'N' (A is M x K, ld lda) or 'T' (A is K x M).  transB: 'N' (B is
 // K x N) or 'T' (B is N x K).
+// C (M x M, lower triangle and the tiles crossing the diagonal) = alpha A B^T
+// + beta C with A, B M x K column-major (the symmetric rank-2k update).
+int dgemm_lower_nt(imcom_ctx* ctx, long long M, long long K, double alpha, const double* A,
+                   long long lda, const double* B, long long ldb, double beta, double* C,
+                   long long ldc);
 int dgemm(imcom_ctx* ctx, char transA, char transB, long long M, long long N,
           long long K, double alpha, const double* A, long long lda,
           const double* B, long long ldb, double beta, double* C,

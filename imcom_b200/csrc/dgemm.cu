@@ -68,7 +68,10 @@ __device__ __forceinline__ void load_tile(double* S, const double* __restrict__ 
   }
 }
 
-template <bool AK, bool BKC, int VEC>
+// LOWER: only output tiles with a row on or below the diagonal (row >= col)
+// are computed; tiles strictly above it are left as they are (the symmetric
+// rank-2k update of a matrix kept in its lower triangle, LAPACK dsyr2k 'L').
+template <bool AK, bool BKC, int VEC, bool LOWER = false>
 __global__ void __launch_bounds__(THREADS, 1)
 dgemm_kernel(long long M, long long N, long long K, double alpha, const double* __restrict__ A,
              long long lda, const double* __restrict__ B, long long ldb, double beta,
@@ -78,6 +81,7 @@ dgemm_kernel(long long M, long long N, long long K, double alpha, const double* 
   const int wm = warp & 1, wn = warp >> 1;  // 2 x 4 warps
   const int g = lane >> 2, t = lane & 3;
   const long long m0 = (long long)blockIdx.x * BM, n0 = (long long)blockIdx.y * BN;
+  if (LOWER && m0 + BM <= n0) return;
   // split-K: this CTA covers k in [kb, ke); partial sums go to slice z of C
   const long long kb = (long long)blockIdx.z * kchunk;
   const long long ke = min(K, kb + kchunk);
@@ -221,6 +225,26 @@ int launch(imcom_ctx* ctx, long long M, long long N, long long K, double alpha, 
                                                       ldc);
     IMC_LAUNCH();
   }
+  return 0;
+}
+
+int dgemm_lower_nt(imcom_ctx* ctx, long long M, long long K, double alpha, const double* A,
+                   long long lda, const double* B, long long ldb, double beta, double* C,
+                   long long ldc) {
+  if (M <= 0 || K <= 0) return 0;
+  const long long g = (M + BM - 1) / BM;
+  dim3 grd((unsigned)g, (unsigned)g, 1);
+  auto al16 = [](const void* p) { return ((uintptr_t)p & 15) == 0; };
+  if (al16(A) && al16(B) && lda % 2 == 0 && ldb % 2 == 0) {
+    auto k = dgemm_kernel<false, false, 2, true>;
+    IMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES));
+    k<<<grd, THREADS, SMEM_BYTES, ctx->stream>>>(M, M, K, alpha, A, lda, B, ldb, beta, C, ldc, K);
+  } else {
+    auto k = dgemm_kernel<false, false, 1, true>;
+    IMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES));
+    k<<<grd, THREADS, SMEM_BYTES, ctx->stream>>>(M, M, K, alpha, A, lda, B, ldb, beta, C, ldc, K);
+  }
+  IMC_LAUNCH();
   return 0;
 }
 

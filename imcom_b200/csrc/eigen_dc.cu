@@ -5,18 +5,23 @@
 // reversed by the caller (imcom_matrix.f90:656-662).
 //
 // 1. Tridiagonalisation (LAPACK dsytrd/dlatrd, lower).  Panels of NB = 32
-//    columns.  Inside a panel every column needs the trailing symmetric
+//    columns; only the lower triangle of the trailing matrix is read or
+//    updated.  Inside a panel every column needs the trailing symmetric
 //    matrix-vector product y0 = A22 v and the panel corrections
 //    y = y0 - V (W^T v) - W (V^T v).  One persistent cooperative kernel per
 //    panel runs the whole panel with two grid-wide barriers per column:
-//      phase A: y0 tiles over the trailing matrix (all SMs) and v^T y0
-//               (summed per CTA, one atomic per CTA);
-//      phase B: w = tau (y - 1/2 tau (y^T v) v) row by row, using
-//               v^T y = v^T y0 - 2 (V^T v).(W^T v), the update of the next
-//               column, its norm and its dot products with the panel's
-//               W and V (the rows already hold them in registers).
+//      phase A: A22 x for the raw column x = A(j+1:n, j) (so the tiles need
+//               not wait for the reflector), from 64 x 16 lower-triangle
+//               tiles staged through shared memory by cp.async: row sums
+//               and column sums per tile, and x^T A22 x (one atomic per CTA);
+//      phase B: y0 = scl A22 x + delta A22(:, j+1) for v = scl x +
+//               delta e_{j+1}, then w = tau (y - 1/2 tau (y^T v) v) row by
+//               row, using v^T y = v^T y0 - 2 (V^T v).(W^T v), the update of
+//               the next column, its norm and its dot products with the
+//               panel's W and V (the rows already hold them in registers).
 //    The trailing update A22 -= V W^T + W V^T runs on the DMMA GEMM as one
-//    product with K = 2 NB ([V W] [W V]^T: one pass over A22).
+//    product with K = 2 NB ([V W] [W V]^T), over the tiles on or below the
+//    diagonal (LAPACK dsyr2k 'L').
 //    Grid barriers spin with a bound and report a timeout instead of hanging.
 // 2. Divide and conquer (LAPACK dstedc / dlaed0-4 structure).  Leaves of at
 //    most 32 rows are diagonalised by a cyclic Jacobi sweep in one CTA each.
@@ -41,8 +46,14 @@ namespace imcom {
 namespace {
 
 constexpr int NB = 32;            // tridiagonalisation panel width
-constexpr int TRD_THREADS = 512;  // threads per CTA of the panel kernel
+constexpr int TRD_THREADS = 384;  // threads per CTA of the panel kernel
 constexpr int CW = 16;            // columns per symv tile
+constexpr int TR = 64;            // rows per symv tile (two per lane)
+constexpr int CPB = TR / CW;      // column chunks per row block along the diagonal
+// one staging slot: a CW x TR tile, then the TR rows and CW columns of the
+// reflector column it multiplies
+constexpr int TRD_SLOT = CW * TR + TR + CW;
+constexpr size_t TRD_SMEM = (size_t)(TRD_THREADS / 32) * 2 * TRD_SLOT * sizeof(double);
 constexpr int LEAF = 32;          // largest leaf of the divide-and-conquer tree
 constexpr int NBB = 128;          // reflectors per back-transformation block
 constexpr double EPS = 1.1102230246251565e-16;
@@ -53,6 +64,21 @@ __device__ __forceinline__ double warp_sum(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
+
+// 16-byte global -> shared copy; bytes < 16 zero-fill the rest (0: all zero)
+__device__ __forceinline__ void cp_async16(double* dst, const double* src, int bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, int bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_wait_0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 __device__ __forceinline__ double ld_cg(const double* p) {
   double v;
@@ -111,7 +137,7 @@ __device__ __forceinline__ bool grid_barrier(GridSync* s, long long limit) {
 struct TrdAcc {
   double SW[NB];  // sum_{r >= j+2} A(r, j) W(r, p) for the column j this parity serves
   double SV[NB];  // sum_{r >= j+2} A(r, j) V(r, p)
-  double vty0;    // v^T y0
+  double vty0;    // x^T A22 x of the raw column x = A(j+1:n, j)
   double nrm;     // squared norm of the column below its subdiagonal
 };
 
@@ -123,7 +149,8 @@ struct TrdArgs {
   double* W;  // n x NB panel
   long long ldw;
   double *d, *e, *tau;
-  double* ypart;  // [chunk][ldy]
+  double* ypart;  // [chunk][ldy]: row sums of the tiles of one column chunk
+  double* ycol;   // [row block][ldy]: column sums of the tiles of one row block
   long long ldy;
   TrdAcc* acc;  // [2] by column parity
   GridSync* sync;
@@ -134,6 +161,7 @@ struct TrdArgs {
 __global__ void __launch_bounds__(TRD_THREADS) trd_panel_kernel(TrdArgs a) {
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   constexpr int WPB = TRD_THREADS / 32;
+  constexpr int HP = (NB + WPB - 1) / WPB;  // panel columns per warp in phase B
   const long long gw = (long long)blockIdx.x * WPB + wib;
   const long long GW = (long long)gridDim.x * WPB;
   const int n = a.n, k = a.k;
@@ -141,7 +169,10 @@ __global__ void __launch_bounds__(TRD_THREADS) trd_panel_kernel(TrdArgs a) {
   const long long lda = a.lda, ldv = a.ldv, ldw = a.ldw;
   __shared__ double s_pq[2 * NB];            // p = W^T v, q = V^T v of the current column
   __shared__ double s_rowV[NB], s_rowW[NB];  // row j+1 of V and W
+  __shared__ double s_alpha2;                  // -1/2 tau^2 v^T y of the current column
   __shared__ double sm_y[WPB][32], sm_c[WPB][32], sm_u[WPB][32];
+  extern __shared__ __align__(16) double trd_tiles[];  // [warp][slot][TRD_SLOT]
+  double* wbuf = trd_tiles + (size_t)wib * 2 * TRD_SLOT;
   if (*(volatile int*)&a.sync->err) return;  // an earlier panel failed
 
   // Column k: d(k) and the norm of A(k+2:n, k) (one atomic per CTA).
@@ -169,9 +200,151 @@ __global__ void __launch_bounds__(TRD_THREADS) trd_panel_kernel(TrdArgs a) {
     const int par = i & 1;
     TrdAcc* cur = a.acc + par;
     TrdAcc* nxt = a.acc + (par ^ 1);
+    // rows handled in pairs from an even base row so the loads are 16-byte
+    const long long rbase = (j + 1) & ~1LL;
+    const long long R = n - (j + 1);
+    const long long RB = (n - rbase + TR - 1) / TR, NC = (R + CW - 1) / CW;
+    // Tiles on or below the diagonal: row block rb (TR rows from rbase +
+    // TR rb) with column chunks ch < min(NC, CPB (rb + 1)), counted row block
+    // by row block; rb < rbc has CPB (rb + 1) chunks, the rest NC.
+    const long long rbc = min(RB, max(0LL, (NC - 1) / CPB));
+    const long long tri = (long long)CPB * rbc * (rbc + 1) / 2;
+    const long long ntiles = tri + (RB - rbc) * NC;
+
+    // tiles are staged through a two-slot shared-memory buffer per warp by
+    // cp.async (zero-filled outside the triangle and below row n), together
+    // with the segments of column j they multiply, so the next tile is in
+    // flight while this one is summed
+    const double* colj = A + (long long)j * lda;
+    auto decode = [&](long long tile, long long& rb, long long& ch) {
+      if (tile < tri) {
+        // largest rb with CPB rb (rb + 1) / 2 <= tile
+        long long q = (long long)((sqrt(1.0 + 8.0 * (double)tile / CPB) - 1.0) * 0.5);
+        while ((long long)CPB * (q + 1) * (q + 2) / 2 <= tile) ++q;
+        while (q > 0 && (long long)CPB * q * (q + 1) / 2 > tile) --q;
+        rb = q;
+        ch = tile - (long long)CPB * q * (q + 1) / 2;
+      } else {
+        rb = rbc + (tile - tri) / NC;
+        ch = (tile - tri) % NC;
+      }
+    };
+    auto issue = [&](long long tile, int slot) {
+      long long rb, ch;
+      decode(tile, rb, ch);
+      const long long r = rbase + rb * TR + 2 * lane;
+      const long long c0 = j + 1 + ch * CW, c1 = min((long long)n, c0 + CW);
+      double* dst = wbuf + slot * TRD_SLOT + 2 * lane;
+#pragma unroll
+      for (int u = 0; u < CW; ++u) {
+        const long long c = c0 + u;
+        // a row of the pair on or below the diagonal; the second row only
+        // if it exists
+        const bool ok = c < c1 && r + 1 >= c && r < n;
+        cp_async16(dst + u * TR, ok ? A + r + c * lda : A, ok ? (r + 1 < n ? 16 : 8) : 0);
+      }
+      const bool okr = r < n;
+      cp_async16(dst + CW * TR, okr ? colj + r : A, okr ? (r + 1 < n ? 16 : 8) : 0);
+      if (lane < CW) {
+        const bool okc = c0 + lane < c1;
+        cp_async8(wbuf + slot * TRD_SLOT + CW * TR + TR + lane, okc ? colj + c0 + lane : A,
+                  okc ? 8 : 0);
+      }
+    };
+    // Phase A forms A22 x for the raw column x = A(j+1:n, j); the reflector
+    // v = scl x + delta e_{j+1} (delta = 1 - scl x(j+1)) only enters in
+    // phase B, y0 = A22 v = scl (A22 x) + delta A22(:, j+1), so the tiles do
+    // not wait for the reflector.  Its loads are issued now, used after the
+    // tile loop.
+    if (gw < ntiles) issue(gw, 0);
+    cp_commit();
+    const double alpha = ld_cg(A + (j + 1) + (long long)j * lda);
+    const double xn2 = ld_cg(&cur->nrm);
+    // A(j+1, j+1) before this column's phase B rewrites column j+1
+    const double a11 = (wib == 0) ? ld_cg(A + (j + 1) + (long long)(j + 1) * lda) : 0.0;
+    if (blockIdx.x == 0 && threadIdx.x < 2 * NB + 2) {
+      // clear the other parity's accumulators (last read one phase ago)
+      if (threadIdx.x < NB) nxt->SW[threadIdx.x] = 0.0;
+      else if (threadIdx.x < 2 * NB) nxt->SV[threadIdx.x - NB] = 0.0;
+      else if (threadIdx.x == 2 * NB) nxt->vty0 = 0.0;
+      else nxt->nrm = 0.0;
+    }
+    // Row j+1 of V and W, and p = W^T v = W(j+1, :) + scl * SW, q = V^T v
+    // likewise (sums from the previous column's phase B); loaded now, kept
+    // in shared memory for phase B after the tile loop
+    double wr1 = 0.0, vr1 = 0.0, sw1 = 0.0, sv1 = 0.0;
+    if (wib == 0 && lane < i) {
+      wr1 = ld_cg(a.W + (j + 1) + lane * ldw);
+      vr1 = ld_cg(a.V + (j + 1) + (k + lane) * ldv);
+      sw1 = ld_cg(&cur->SW[lane]);
+      sv1 = ld_cg(&cur->SV[lane]);
+    }
+    // x(r) = A(r, j) for j < r < n, else 0
+    auto xsel = [&](long long r, double raw) -> double { return (r <= j || r >= n) ? 0.0 : raw; };
+    // ---- phase A: A22 x from the lower triangle (LAPACK dsymv 'L').
+    // Tile (rb, ch) reads A(r, c) for r >= c once and gives the row sums
+    // sum_c A(r, c) x(c) (to ypart[ch]) and the column sums
+    // sum_{r > c} A(r, c) x(r) (to ycol[rb]); (A22 x)(r) is the sum of both
+    // kinds.  x^T A22 x is summed per warp, then per CTA, and added with one
+    // atomic per CTA. ----
+    double vty_part = 0.0;
+    int slot = 0;
+    for (long long tile = gw; tile < ntiles; tile += GW, slot ^= 1) {
+      if (tile + GW < ntiles) issue(tile + GW, slot ^ 1);
+      cp_commit();
+      cp_wait_1();
+      long long rb, ch;
+      decode(tile, rb, ch);
+      const long long r = rbase + rb * TR + 2 * lane;
+      const long long c0 = j + 1 + ch * CW, c1 = min((long long)n, c0 + CW);
+      const double* sl = wbuf + slot * TRD_SLOT;
+      const double2 vraw = reinterpret_cast<const double2*>(sl + CW * TR)[lane];
+      const double* vcol = sl + CW * TR + TR;  // raw column-j values at c0 ..
+      const double v0 = xsel(r, vraw.x), v1 = xsel(r + 1, vraw.y);
+      const double2* av = reinterpret_cast<const double2*>(sl) + lane;
+      double acc0 = 0.0, acc1 = 0.0, vtz = 0.0;
+      // two halves of CW / 2 columns: row sums, then the column sums of the
+      // half transpose-reduced over the warp (lane L ends with the sum for
+      // column c0 + H + (L >> 2)), so only CW / 2 partials are live at once
+#pragma unroll
+      for (int H = 0; H < CW; H += CW / 2) {
+        double z[CW / 2];
+#pragma unroll
+        for (int u = 0; u < CW / 2; ++u) {
+          const long long c = c0 + H + u;
+          const double2 e2 = av[(H + u) * (TR / 2)];
+          const double ax = (r >= c) ? e2.x : 0.0;  // drop the element above the diagonal
+          const double vc = xsel(c, vcol[H + u]);  // zero past column n
+          acc0 = fma(ax, vc, acc0);
+          acc1 = fma(e2.y, vc, acc1);
+          // strictly below the diagonal for the column sums
+          z[u] = fma((r + 1 > c) ? e2.y : 0.0, v1, (r > c) ? ax * v0 : 0.0);
+        }
+#pragma unroll
+        for (int h = CW / 4, m = 16; h >= 1; h >>= 1, m >>= 1) {
+          const bool hi = (lane & m) != 0;
+#pragma unroll
+          for (int q = 0; q < h; ++q) {
+            const double send = hi ? z[q] : z[q + h];
+            const double keep = hi ? z[q + h] : z[q];
+            z[q] = keep + __shfl_xor_sync(0xffffffffu, send, m);
+          }
+        }
+        double zc = z[0] + __shfl_xor_sync(0xffffffffu, z[0], 2);
+        zc += __shfl_xor_sync(0xffffffffu, zc, 1);
+        const long long cz = c0 + H + (lane >> 2);
+        const double vz = xsel(cz, vcol[H + (lane >> 2)]);
+        if (!(lane & 3) && cz < c1) {
+          a.ycol[rb * a.ldy + cz] = zc;
+          vtz += vz * zc;
+        }
+      }
+      if (r >= j + 1 && r < n) a.ypart[ch * a.ldy + r] = acc0;
+      if (r + 1 >= j + 1 && r + 1 < n) a.ypart[ch * a.ldy + r + 1] = acc1;
+      vty_part += v0 * acc0 + v1 * acc1 + vtz;
+    }
+    cp_wait_0();
     // Householder reflector of x = A(j+1:n, j) (LAPACK dlarfg)
-    const double alpha = __ldcg(A + (j + 1) + (long long)j * lda);
-    const double xn2 = __ldcg(&cur->nrm);
     double beta, t, scl;
     if (xn2 == 0.0) {
       t = 0.0;
@@ -182,71 +355,16 @@ __global__ void __launch_bounds__(TRD_THREADS) trd_panel_kernel(TrdArgs a) {
       t = (beta - alpha) / beta;
       scl = 1.0 / (alpha - beta);
     }
+    const double delta = 1.0 - scl * alpha;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       a.e[j] = beta;
       a.tau[j] = t;
     }
-    if (blockIdx.x == 0 && threadIdx.x < 2 * NB + 2) {
-      // clear the other parity's accumulators (last read one phase ago)
-      if (threadIdx.x < NB) nxt->SW[threadIdx.x] = 0.0;
-      else if (threadIdx.x < 2 * NB) nxt->SV[threadIdx.x - NB] = 0.0;
-      else if (threadIdx.x == 2 * NB) nxt->vty0 = 0.0;
-      else nxt->nrm = 0.0;
-    }
-    // Row j+1 of V and W, and p = W^T v = W(j+1, :) + scl * SW, q = V^T v
-    // likewise (sums from the previous column's phase B).
     if (wib == 0 && lane < i) {
-      const double wr1 = __ldcg(a.W + (j + 1) + lane * ldw);
-      const double vr1 = __ldcg(a.V + (j + 1) + (k + lane) * ldv);
       s_rowW[lane] = wr1;
       s_rowV[lane] = vr1;
-      s_pq[lane] = wr1 + scl * __ldcg(&cur->SW[lane]);
-      s_pq[NB + lane] = vr1 + scl * __ldcg(&cur->SV[lane]);
-    }
-    const double* colj = A + (long long)j * lda;
-    // v(r): 0 above row j+1, 1 at j+1, A(r, j) * scl below
-    auto vrow = [&](long long r) -> double {
-      return (r <= j || r >= n) ? 0.0 : (r == j + 1 ? 1.0 : __ldcg(colj + r) * scl);
-    };
-    // rows handled in pairs from an even base row so the loads are 16-byte
-    const long long rbase = (j + 1) & ~1LL;
-    const long long R = n - (j + 1);
-    const long long RB = (n - rbase + 63) / 64, NC = (R + CW - 1) / CW;
-
-    // ---- phase A: y0 = A22 v by 64-row x CW-column tiles; every load of a
-    // tile is issued before the first use.  v^T y0 is summed per warp, then
-    // per CTA, and added with one atomic per CTA (same-address atomics from
-    // every tile would serialise in one L2 slice). ----
-    double vty_part = 0.0;
-    for (long long tile = gw; tile < RB * NC; tile += GW) {
-      const long long rb = tile % RB, ch = tile / RB;
-      const long long r = rbase + rb * 64 + 2 * lane;
-      const long long c0 = j + 1 + ch * CW, c1 = min((long long)n, c0 + CW);
-      const long long cl = c0 + lane;
-      const double vreg = (cl < c1) ? vrow(cl) : 0.0;
-      const double v0 = vrow(r), v1 = vrow(r + 1);
-      const bool pair = (r + 1 < n), single = (r < n);
-      const double* Ar = A + r;
-      double2 av[CW];
-#pragma unroll
-      for (int u = 0; u < CW; ++u) {
-        const long long c = c0 + u;
-        av[u] = make_double2(0.0, 0.0);
-        if (c < c1) {
-          if (pair) av[u] = *reinterpret_cast<const double2*>(Ar + c * lda);
-          else if (single) av[u].x = Ar[c * lda];
-        }
-      }
-      double acc0 = 0.0, acc1 = 0.0;
-#pragma unroll
-      for (int u = 0; u < CW; ++u) {
-        const double vc = __shfl_sync(0xffffffffu, vreg, u);
-        acc0 = fma(av[u].x, vc, acc0);
-        acc1 = fma(av[u].y, vc, acc1);
-      }
-      if (r >= j + 1 && r < n) a.ypart[ch * a.ldy + r] = acc0;
-      if (r + 1 >= j + 1 && r + 1 < n) a.ypart[ch * a.ldy + r + 1] = acc1;
-      vty_part += v0 * acc0 + v1 * acc1;
+      s_pq[lane] = wr1 + scl * sw1;
+      s_pq[NB + lane] = vr1 + scl * sv1;
     }
     vty_part = warp_sum(vty_part);
     if (lane == 0) sm_u[wib][0] = vty_part;
@@ -260,53 +378,66 @@ __global__ void __launch_bounds__(TRD_THREADS) trd_panel_kernel(TrdArgs a) {
 
     // ---- phase B: w, the next column, its norm and dot products ----
     const bool next = (i + 1 < a.b);
-    double alpha2 = 0.0;
     bool have_w1 = false;
     // one 32-row block per CTA at a time; the warps split the chunk partials
     // and the panel columns, then reduce through shared memory
+    // warp 0: this lane's share of y0(j+1), loaded alongside the first row
+    // block's partial sums
+    double y1 = 0.0;
+    if (wib == 0) {
+      if (lane < min(NC, (long long)CPB)) y1 = __ldcg(a.ypart + lane * a.ldy + (j + 1));
+      for (long long q = lane; q < RB; q += 32) y1 += __ldcg(a.ycol + q * a.ldy + (j + 1));
+    }
     for (long long rb = blockIdx.x; j + 1 + rb * 32 < n; rb += gridDim.x) {
       const long long r = j + 1 + rb * 32 + lane;
       const bool valid = r < n;
       // issue every load of the row block first
-      double ys = 0.0, vp[2] = {0.0, 0.0}, wp[2] = {0.0, 0.0};
+      double ys = 0.0, vp[HP] = {}, wp[HP] = {};
       double vr = 0.0, aold = 0.0;
       const double vty0 = __ldcg(&cur->vty0);
       if (valid) {
-#pragma unroll 8
-        for (long long ch = wib; ch < NC; ch += WPB) ys += __ldcg(a.ypart + ch * a.ldy + r);
+        // row sums of the chunks its row block covers, column sums of the
+        // row blocks below its chunk
+        const long long ncr = min(NC, (long long)CPB * ((r - rbase) / TR + 1));
+        const long long rb0 = (r - (j + 1)) / CW / CPB;
+#pragma unroll 4
+        for (long long ch = wib; ch < ncr; ch += WPB) ys += __ldcg(a.ypart + ch * a.ldy + r);
+#pragma unroll 4
+        for (long long q = rb0 + wib; q < RB; q += WPB) ys += __ldcg(a.ycol + q * a.ldy + r);
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < HP; ++h) {
           const int p = wib + WPB * h;
           if (p < i) {
             vp[h] = __ldcg(a.V + r + (k + p) * ldv);
             wp[h] = __ldcg(a.W + r + p * ldw);
           }
         }
-        vr = vrow(r);
-        if (next) aold = __ldcg(A + r + (long long)(j + 1) * lda);
+        vr = (r == j + 1) ? 1.0 : __ldcg(colj + r) * scl;
+        aold = __ldcg(A + r + (long long)(j + 1) * lda);
       }
-      if (!have_w1) {
+      if (!have_w1 && wib == 0) {
+        // v^T y0 = scl^2 x^T A22 x + 2 scl delta (A22 x)(j+1) + delta^2 A(j+1, j+1),
+        // alpha2 = -1/2 tau^2 v^T y with v^T y = v^T y0 - 2 (V^T v).(W^T v), and
+        // w(j+1) (the new entry of row j+1 of W)
+        const double s1 = warp_sum(y1);
         double qp = 0.0;
         for (int p = 0; p < i; ++p) qp += s_pq[NB + p] * s_pq[p];
-        alpha2 = -0.5 * t * t * (vty0 - 2.0 * qp);
-        if (next && wib == 0) {
-          // w(j+1) (the new entry of row j+1 of W)
-          double y = 0.0;
-#pragma unroll 8
-          for (long long ch = lane; ch < NC; ch += 32) y += __ldcg(a.ypart + ch * a.ldy + (j + 1));
-          y = warp_sum(y);
-          double corr = (lane < i) ? s_rowV[lane] * s_pq[lane] + s_rowW[lane] * s_pq[NB + lane] : 0.0;
-          corr = warp_sum(corr);
-          if (lane == 0) {
-            s_rowW[i] = t * (y - corr) + alpha2;
+        const double vty = scl * scl * vty0 + 2.0 * scl * delta * s1 + delta * delta * a11;
+        const double al2 = -0.5 * t * t * (vty - 2.0 * qp);
+        double corr = (lane < i) ? s_rowV[lane] * s_pq[lane] + s_rowW[lane] * s_pq[NB + lane] : 0.0;
+        corr = warp_sum(corr);
+        if (lane == 0) {
+          s_alpha2 = al2;
+          if (next) {
+            s_rowW[i] = t * ((scl * s1 + delta * a11) - corr) + al2;
             s_rowV[i] = 1.0;
           }
         }
-        have_w1 = true;
       }
+      have_w1 = true;
       double cs = 0.0, us = 0.0;
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
+      for (int h = 0; h < HP; ++h) {
         const int p = wib + WPB * h;
         if (p < i) {
           cs += vp[h] * s_pq[p] + wp[h] * s_pq[NB + p];
@@ -324,7 +455,8 @@ __global__ void __launch_bounds__(TRD_THREADS) trd_panel_kernel(TrdArgs a) {
         corr += sm_c[w][lane];
         upd += sm_u[w][lane];
       }
-      const double wr = t * (y0 - corr) + alpha2 * vr;
+      y0 = scl * y0 + delta * aold;  // A22 v from A22 x
+      const double wr = t * (y0 - corr) + s_alpha2 * vr;
       if (valid && wib == 0) {
         a.V[r + (long long)j * ldv] = vr;
         a.W[r + i * ldw] = wr;
@@ -342,7 +474,7 @@ __global__ void __launch_bounds__(TRD_THREADS) trd_panel_kernel(TrdArgs a) {
         // column j+1's dot products with W, V over rows >= j+3 and its norm
         const double am = (valid && r >= j + 3) ? anew : 0.0;
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < HP; ++h) {
           const int p = wib + WPB * h;
           if (p <= i) {
             const double wv = (p == i) ? wr : wp[h];
@@ -904,14 +1036,18 @@ __global__ void pack_update_kernel(const double* __restrict__ V, long long ldv,
 }
 
 static int sytrd_gpu(imcom_ctx* ctx, DMat& Aw, DMat& Vall, double* d, double* e, double* tau,
-                     double* W, long long ldw, double* ypart, long long ldy, void* accbuf,
+                     double* W, long long ldw, double* ypart, double* ycol, long long ldy,
+                     void* accbuf,
                      long long spin, double* XY) {
   const int n = (int)Aw.rows;
   int dev = ctx->device, coop = 0;
   cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
   if (!coop) return set_err(ctx, IMCOM_ERR_CUDA, "device lacks cooperative launch");
   int per_sm = 0;
-  IMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trd_panel_kernel, TRD_THREADS, 0));
+  IMC_CUDA(cudaFuncSetAttribute(trd_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)TRD_SMEM));
+  IMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trd_panel_kernel, TRD_THREADS,
+                                                         TRD_SMEM));
   if (per_sm < 1) return set_err(ctx, IMCOM_ERR_CUDA, "panel kernel does not fit on an SM");
   int grid = sm_count(ctx);  // one CTA per SM: the cheapest grid barrier
   TrdAcc* acc = (TrdAcc*)accbuf;
@@ -922,15 +1058,16 @@ static int sytrd_gpu(imcom_ctx* ctx, DMat& Aw, DMat& Vall, double* d, double* e,
     const int b = std::min(NB, n - 1 - k);
     IMC_CUDA(cudaMemsetAsync(accbuf, 0, 2 * sizeof(TrdAcc), ctx->stream));
     static_assert(2 * sizeof(TrdAcc) + 64 + sizeof(GridSync) <= 4096, "panel scratch");
-    TrdArgs a{Aw.p, Aw.ld, Vall.p, Vall.ld, W, ldw, d, e, tau, ypart, ldy, acc, sync, n, k, b,
-              spin};
+    TrdArgs a{Aw.p, Aw.ld, Vall.p, Vall.ld, W, ldw, d, e, tau, ypart, ycol, ldy, acc, sync, n,
+              k, b, spin};
     void* args[] = {&a};
-    IMC_CUDA(cudaLaunchCooperativeKernel((void*)trd_panel_kernel, grid, TRD_THREADS, args, 0,
-                                         ctx->stream));
+    IMC_CUDA(cudaLaunchCooperativeKernel((void*)trd_panel_kernel, grid, TRD_THREADS, args,
+                                         TRD_SMEM, ctx->stream));
     IMC_LAUNCH();
     const int t0 = k + b, rem = n - t0;
     if (rem > 0) {
-      // A22 -= V W^T + W V^T as one K = 2b product (one pass over A22)
+      // A22 -= V W^T + W V^T as one K = 2b product over the lower triangle
+      // (the only part the panel kernel reads)
       const long long ldx = ldw;
       double* X = XY;
       double* Y = XY + (size_t)ldx * 2 * NB;
@@ -938,8 +1075,8 @@ static int sytrd_gpu(imcom_ctx* ctx, DMat& Aw, DMat& Vall, double* d, double* e,
       pack_update_kernel<<<grd, 256, 0, ctx->stream>>>(Vall.p + (long long)k * Vall.ld, Vall.ld,
                                                        W, ldw, t0, n, b, X, Y, ldx);
       IMC_LAUNCH();
-      IMC_TRY(dgemm(ctx, 'N', 'T', rem, rem, 2 * b, -1.0, X + t0, ldx, Y + t0, ldx, 1.0,
-                    Aw.p + t0 + (long long)t0 * Aw.ld, Aw.ld));
+      IMC_TRY(dgemm_lower_nt(ctx, rem, 2 * b, -1.0, X + t0, ldx, Y + t0, ldx, 1.0,
+                             Aw.p + t0 + (long long)t0 * Aw.ld, Aw.ld));
     }
     // a timed-out barrier ends the factorisation with an error
     if ((k / NB) % 16 == 15 || k + NB >= n - 1) {
@@ -974,7 +1111,7 @@ int eigen_dc(imcom_ctx* ctx, const DMat& A, DMat& Wout, double* wout) {
   const size_t nn = (size_t)ld * n;
   // scratch vectors and small matrices in one allocation
   const long long ldw = pad_ld(n), ldy = pad_ld(n);
-  const long long nch = (n + CW - 1) / CW + 1;
+  const long long nch = (n + CW - 1) / CW + 1, nrb = (n + TR - 1) / TR + 1;
   size_t off = 0;
   auto take = [&](size_t bytes) {
     size_t o = off;
@@ -982,7 +1119,7 @@ int eigen_dc(imcom_ctx* ctx, const DMat& A, DMat& Wout, double* wout) {
     return o;
   };
   size_t o_d = take(n * 8), o_e = take(n * 8), o_tau = take(n * 8), o_dt = take(n * 8);
-  size_t o_W = take((size_t)ldw * NB * 8), o_y = take((size_t)ldy * nch * 8);
+  size_t o_W = take((size_t)ldw * NB * 8), o_y = take((size_t)ldy * (nch + nrb) * 8);
   size_t o_XY = take((size_t)ldw * 4 * NB * 8);
   size_t o_acc = take(4096);
   size_t o_split = take((size_t)n * 4), o_nodes = take((size_t)n * sizeof(Node));
@@ -1013,8 +1150,8 @@ int eigen_dc(imcom_ctx* ctx, const DMat& A, DMat& Wout, double* wout) {
   IMC_TRY(copy_mat(ctx, A.p, A.ld, Aw.p, Aw.ld, n, n));
   IMC_CUDA(cudaMemsetAsync(Vall.p, 0, Vall.bytes(), ctx->stream));
   IMC_CUDA(cudaMemsetAsync(Wp, 0, (size_t)ldw * NB * 8, ctx->stream));
-  IMC_TRY(sytrd_gpu(ctx, Aw, Vall, d, e, tau, Wp, ldw, yp, ldy, base + o_acc, spin,
-                    (double*)(base + o_XY)));
+  IMC_TRY(sytrd_gpu(ctx, Aw, Vall, d, e, tau, Wp, ldw, yp, yp + (size_t)ldy * nch, ldy,
+                    base + o_acc, spin, (double*)(base + o_XY)));
   stage_end(ctx, ST_EIG_TRD);
   stage_begin(ctx, ST_EIG_DC);
 
