@@ -36,6 +36,7 @@
 //    reflectors, T built from V^T V (dlarft), three GEMMs per block.
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -216,24 +217,26 @@ __global__ void __launch_bounds__(TRD_THREADS) trd_panel_kernel(TrdArgs a) {
     // with the segments of column j they multiply, so the next tile is in
     // flight while this one is summed
     const double* colj = A + (long long)j * lda;
-    auto decode = [&](long long tile, long long& rb, long long& ch) {
-      if (tile < tri) {
+    // tile counts stay far below 2^31 (n^2 / 2048), so 32-bit arithmetic; the
+    // float square root is only a first guess that the loops correct
+    auto decode = [&](int tile, int& rb, int& ch) {
+      if (tile < (int)tri) {
         // largest rb with CPB rb (rb + 1) / 2 <= tile
-        long long q = (long long)((sqrt(1.0 + 8.0 * (double)tile / CPB) - 1.0) * 0.5);
-        while ((long long)CPB * (q + 1) * (q + 2) / 2 <= tile) ++q;
-        while (q > 0 && (long long)CPB * q * (q + 1) / 2 > tile) --q;
+        int q = (int)((sqrtf(1.0f + 8.0f * (float)tile / CPB) - 1.0f) * 0.5f);
+        while (CPB * (q + 1) * (q + 2) / 2 <= tile) ++q;
+        while (q > 0 && CPB * q * (q + 1) / 2 > tile) --q;
         rb = q;
-        ch = tile - (long long)CPB * q * (q + 1) / 2;
+        ch = tile - CPB * q * (q + 1) / 2;
       } else {
-        rb = rbc + (tile - tri) / NC;
-        ch = (tile - tri) % NC;
+        const unsigned t2 = (unsigned)(tile - (int)tri), nc = (unsigned)NC;
+        const unsigned qq = t2 / nc;
+        rb = (int)rbc + (int)qq;
+        ch = (int)(t2 - qq * nc);
       }
     };
-    auto issue = [&](long long tile, int slot) {
-      long long rb, ch;
-      decode(tile, rb, ch);
-      const long long r = rbase + rb * TR + 2 * lane;
-      const long long c0 = j + 1 + ch * CW, c1 = min((long long)n, c0 + CW);
+    auto issue = [&](int rb, int ch, int slot) {
+      const long long r = rbase + (long long)rb * TR + 2 * lane;
+      const long long c0 = j + 1 + (long long)ch * CW, c1 = min((long long)n, c0 + CW);
       double* dst = wbuf + slot * TRD_SLOT + 2 * lane;
 #pragma unroll
       for (int u = 0; u < CW; ++u) {
@@ -256,7 +259,11 @@ __global__ void __launch_bounds__(TRD_THREADS) trd_panel_kernel(TrdArgs a) {
     // phase B, y0 = A22 v = scl (A22 x) + delta A22(:, j+1), so the tiles do
     // not wait for the reflector.  Its loads are issued now, used after the
     // tile loop.
-    if (gw < ntiles) issue(gw, 0);
+    int rb_n = 0, ch_n = 0;  // decoded indices of this warp's next tile
+    if (gw < ntiles) {
+      decode((int)gw, rb_n, ch_n);
+      issue(rb_n, ch_n, 0);
+    }
     cp_commit();
     const double alpha = ld_cg(A + (j + 1) + (long long)j * lda);
     const double xn2 = ld_cg(&cur->nrm);
@@ -279,8 +286,6 @@ __global__ void __launch_bounds__(TRD_THREADS) trd_panel_kernel(TrdArgs a) {
       sw1 = ld_cg(&cur->SW[lane]);
       sv1 = ld_cg(&cur->SV[lane]);
     }
-    // x(r) = A(r, j) for j < r < n, else 0
-    auto xsel = [&](long long r, double raw) -> double { return (r <= j || r >= n) ? 0.0 : raw; };
     // ---- phase A: A22 x from the lower triangle (LAPACK dsymv 'L').
     // Tile (rb, ch) reads A(r, c) for r >= c once and gives the row sums
     // sum_c A(r, c) x(c) (to ypart[ch]) and the column sums
@@ -290,57 +295,71 @@ __global__ void __launch_bounds__(TRD_THREADS) trd_panel_kernel(TrdArgs a) {
     double vty_part = 0.0;
     int slot = 0;
     for (long long tile = gw; tile < ntiles; tile += GW, slot ^= 1) {
-      if (tile + GW < ntiles) issue(tile + GW, slot ^ 1);
+      const int rb = rb_n, ch = ch_n;
+      if (tile + GW < ntiles) {
+        decode((int)(tile + GW), rb_n, ch_n);
+        issue(rb_n, ch_n, slot ^ 1);
+      }
       cp_commit();
       cp_wait_1();
-      long long rb, ch;
-      decode(tile, rb, ch);
-      const long long r = rbase + rb * TR + 2 * lane;
-      const long long c0 = j + 1 + ch * CW, c1 = min((long long)n, c0 + CW);
+      const long long r = rbase + (long long)rb * TR + 2 * lane;
+      const long long c0 = j + 1 + (long long)ch * CW, c1 = min((long long)n, c0 + CW);
       const double* sl = wbuf + slot * TRD_SLOT;
       const double2 vraw = reinterpret_cast<const double2*>(sl + CW * TR)[lane];
-      const double* vcol = sl + CW * TR + TR;  // raw column-j values at c0 ..
-      const double v0 = xsel(r, vraw.x), v1 = xsel(r + 1, vraw.y);
+      // raw column-j values at rows r, r + 1 and at columns c0 .. c0 + CW - 1
+      // (zero-filled past row n); only row j (when rbase = j) lies above x
+      const double* vcol = sl + CW * TR + TR;
+      const double v0 = (r <= j) ? 0.0 : vraw.x, v1 = vraw.y;
       const double2* av = reinterpret_cast<const double2*>(sl) + lane;
+      const int dr = (int)(r - c0);  // this lane's first row relative to column c0
       double acc0 = 0.0, acc1 = 0.0, vtz = 0.0;
       // two halves of CW / 2 columns: row sums, then the column sums of the
       // half transpose-reduced over the warp (lane L ends with the sum for
-      // column c0 + H + (L >> 2)), so only CW / 2 partials are live at once
+      // column c0 + H + (L >> 2)), so only CW / 2 partials are live at once.
+      // Tiles crossing the diagonal mask A(r, c) with r < c from the row sums
+      // and r <= c from the column sums; the others need no mask.
+      auto tile_sums = [&](auto masked) {
 #pragma unroll
-      for (int H = 0; H < CW; H += CW / 2) {
-        double z[CW / 2];
+        for (int H = 0; H < CW; H += CW / 2) {
+          double z[CW / 2];
 #pragma unroll
-        for (int u = 0; u < CW / 2; ++u) {
-          const long long c = c0 + H + u;
-          const double2 e2 = av[(H + u) * (TR / 2)];
-          const double ax = (r >= c) ? e2.x : 0.0;  // drop the element above the diagonal
-          const double vc = xsel(c, vcol[H + u]);  // zero past column n
-          acc0 = fma(ax, vc, acc0);
-          acc1 = fma(e2.y, vc, acc1);
-          // strictly below the diagonal for the column sums
-          z[u] = fma((r + 1 > c) ? e2.y : 0.0, v1, (r > c) ? ax * v0 : 0.0);
-        }
+          for (int u = 0; u < CW / 2; ++u) {
+            const int cu = H + u;
+            const double2 e2 = av[cu * (TR / 2)];
+            const double vc = vcol[cu];
+            double ax = e2.x, zx = e2.x, zy = e2.y;
+            if (decltype(masked)::value) {
+              ax = (dr >= cu) ? e2.x : 0.0;
+              zx = (dr > cu) ? e2.x : 0.0;
+              zy = (dr + 1 > cu) ? e2.y : 0.0;
+            }
+            acc0 = fma(ax, vc, acc0);
+            acc1 = fma(e2.y, vc, acc1);
+            z[u] = fma(zy, v1, zx * v0);
+          }
 #pragma unroll
-        for (int h = CW / 4, m = 16; h >= 1; h >>= 1, m >>= 1) {
-          const bool hi = (lane & m) != 0;
+          for (int h = CW / 4, m = 16; h >= 1; h >>= 1, m >>= 1) {
+            const bool hi = (lane & m) != 0;
 #pragma unroll
-          for (int q = 0; q < h; ++q) {
-            const double send = hi ? z[q] : z[q + h];
-            const double keep = hi ? z[q + h] : z[q];
-            z[q] = keep + __shfl_xor_sync(0xffffffffu, send, m);
+            for (int q = 0; q < h; ++q) {
+              const double send = hi ? z[q] : z[q + h];
+              const double keep = hi ? z[q + h] : z[q];
+              z[q] = keep + __shfl_xor_sync(0xffffffffu, send, m);
+            }
+          }
+          double zc = z[0] + __shfl_xor_sync(0xffffffffu, z[0], 2);
+          zc += __shfl_xor_sync(0xffffffffu, zc, 1);
+          const long long cz = c0 + H + (lane >> 2);
+          if (!(lane & 3) && cz < c1) {
+            a.ycol[(long long)rb * a.ldy + cz] = zc;
+            vtz += vcol[H + (lane >> 2)] * zc;
           }
         }
-        double zc = z[0] + __shfl_xor_sync(0xffffffffu, z[0], 2);
-        zc += __shfl_xor_sync(0xffffffffu, zc, 1);
-        const long long cz = c0 + H + (lane >> 2);
-        const double vz = xsel(cz, vcol[H + (lane >> 2)]);
-        if (!(lane & 3) && cz < c1) {
-          a.ycol[rb * a.ldy + cz] = zc;
-          vtz += vz * zc;
-        }
-      }
-      if (r >= j + 1 && r < n) a.ypart[ch * a.ldy + r] = acc0;
-      if (r + 1 >= j + 1 && r + 1 < n) a.ypart[ch * a.ldy + r + 1] = acc1;
+      };
+      if (rbase + (long long)rb * TR <= c0 + CW - 1) tile_sums(std::true_type{});
+      else tile_sums(std::false_type{});
+      if (r >= j + 1 && r < n) a.ypart[(long long)ch * a.ldy + r] = acc0;
+      if (r + 1 >= j + 1 && r + 1 < n) a.ypart[(long long)ch * a.ldy + r + 1] = acc1;
       vty_part += v0 * acc0 + v1 * acc1 + vtz;
     }
     cp_wait_0();
@@ -495,6 +514,7 @@ __global__ void __launch_bounds__(TRD_THREADS) trd_panel_kernel(TrdArgs a) {
     }
     if (!grid_barrier(a.sync, a.spin)) return;
   }
+
 }
 
 __global__ void set_last_diag_kernel(const double* A, long long lda, int n, double* d) {
