@@ -22,6 +22,11 @@ T -> S, H with Q, L and B resident, the reference's cached path).
   e2e    the same metric through the C-ABI with pinned host buffers: inputs
          copied in and H, K, U, S and T copied out inside every step.
 
+``batch`` (N=1 only): the batched-patch workload -- 256 independent patches
+of uneven n (990-2270, masked pixels) solved by a pool of contexts, each on a
+share of the SMs, concurrency chosen by the autotuner; patches/s and output
+pixels/s, wall clock.
+
 ``--impl reference`` times the CPU oracle (the reference's algorithm restated
 in C++ with OpenMP + LAPACK/BLAS) on the same workload, all host cores.
 Multi-GPU (``torchrun``): replicas only -- every rank solves its own
@@ -157,6 +162,34 @@ def cpu_baseline(prob, steps=1):
                 keep_tables=False)
         t.append(time.perf_counter() - t0)
     return t, O.get_threads()
+
+
+BATCH_KW = dict(UnotS=True, US_max=1e-6, US_tol=1e-8, maxnits=40)
+
+
+def batched_patches(npatch=256, sample=16):
+    """The batched-patch workload: `npatch` patches of 4 exposures of side
+    U{16..24} with 2% of input pixels masked (n ~ 990-2270), per-exposure
+    Gaussian PSF sigma ~ U[0.5, 0.8] px, 24x24 outputs; U < 1e-6, tolerance
+    1e-8, 40 iterations.  The concurrency (contexts side by side, each on a
+    share of the SMs) is chosen by the autotuner on the first `sample`
+    patches; the whole batch is then solved once to plan every FFT size and
+    once timed (wall clock around the pool, results copied to the host)."""
+    from imcom_b200 import batch
+    problems = batch.make_batch(npatch, seed0=1000)
+    k = batch.autotune(problems[:sample], candidates=(1, 2, 3, 4, 6), **BATCH_KW)
+    rates = dict(batch.LAST_RATES)
+    with batch.BatchSolver(k) as b:
+        b.solve(problems, **BATCH_KW)
+        r = b.solve(problems, **BATCH_KW)
+    ns = [p.n for p in problems]
+    return {"workload": f"{npatch} patches, 4 exposures of side U{{16..24}}, 2% masked, "
+                        "24x24 outputs, U<1e-6 tol 1e-8",
+            "n_range": [min(ns), max(ns)], "psf_sides": len({p.nps for p in problems}),
+            "patches_per_s": r.patches_per_s, "pixels_per_s": r.pixels_per_s,
+            "seconds": r.seconds, "concurrency": k, "sm_share": r.sm_share,
+            "autotune_patches_per_s": {str(q): v for q, v in rates.items()},
+            "timing": "wall clock around the thread pool after one warm pass"}
 
 
 def run_reference(args):
@@ -446,6 +479,11 @@ def run_ours(args):
                           "build_P": 2.0 * n * n * m / (tP * 1e-3) / 1e12,
                           "build_T": 2.0 * n * n * m / (tT * 1e-3) / 1e12}}
 
+    s.close()
+    batch_line = None
+    if rank == 0 and world == 1 and not args.no_batch:
+        batch_line = batched_patches()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         t_cpu, cores = cpu_baseline(prob, steps=1)
@@ -481,10 +519,10 @@ def run_ours(args):
             "roofline": roof,
             "split_roofline": split_roof,
             "cpu_baseline": cpu,
+            "batch": batch_line,
             "clocks": ck,
         }
         print(json.dumps(line), flush=True)
-    s.close()
     if dist is not None:
         dist.destroy_process_group()
     return 0
@@ -501,6 +539,7 @@ def main():
     ap.add_argument("--precision", choices=["split", "fp64"], default="split",
                     help="P and T arithmetic of the fast path")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-patch measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

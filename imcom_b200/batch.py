@@ -27,6 +27,7 @@ from . import _lib
 from .api import OPT_SM_SHARE, Solver
 
 _TUNED: dict = {}
+LAST_RATES: dict = {}
 
 
 @dataclass
@@ -145,11 +146,13 @@ def autotune(problems, candidates=(1, 2, 4, 6, 8), device: int = 0, setup=None,
     """Concurrency with the highest patch throughput on `problems` (a sample of
     the batch).  Each candidate pool is warmed up on the sample once (plans,
     buffers, lazy module loading) and then timed on it; the result is cached
-    per (GPU, size class)."""
+    per (GPU, size class).  The measured rates of the last tuning run are in
+    `LAST_RATES` (patches/s by concurrency)."""
     import torch
     key = (torch.cuda.get_device_name(device), size_class(problems))
     if key in _TUNED:
         return _TUNED[key]
+    LAST_RATES.clear()
     best, best_rate = 1, -1.0
     for k in candidates:
         if k > len(problems):
@@ -157,6 +160,7 @@ def autotune(problems, candidates=(1, 2, 4, 6, 8), device: int = 0, setup=None,
         with BatchSolver(k, device, setup) as b:
             b.solve(problems, **solve_kw)
             r = b.solve(problems, **solve_kw)
+        LAST_RATES[k] = r.patches_per_s
         if r.patches_per_s > best_rate:
             best, best_rate = k, r.patches_per_s
     _TUNED[key] = best

@@ -92,20 +92,7 @@ struct imcom_ctx {
   size_t tables_bytes = 0;
   double2* fftbuf = nullptr;
   size_t fftbuf_bytes = 0;
-  // cuFFT plans by (type, side, batch), least recently used evicted.  The PSF
-  // stamp side follows each patch's input footprint, so a run over many
-  // patches revisits a handful of sizes; planning one (Bluestein sizes
-  // included) costs tens to hundreds of milliseconds of host time.  All plans
-  // of a context share one work area: their executions are serialised on
-  // the context's stream.
-  struct FftPlan {
-    int type, side, batch;
-    cufftHandle h;
-    size_t work;
-    unsigned long long used;
-  };
-  std::vector<FftPlan> fft_plans;
-  unsigned long long fft_clock = 0;
+  // work area bound to the shared cuFFT plans when this context runs them
   void* fft_work = nullptr;
   size_t fft_work_bytes = 0;
 
@@ -192,10 +179,13 @@ extern unsigned long long g_launches;
 // already holds `count` elements (the contents are not preserved on growth).
 int ensure_mat(imcom_ctx* ctx, DMat& M, long long rows, long long cols);
 int ensure_buf(imcom_ctx* ctx, void** p, size_t& have, size_t need);
-// Cached 2-D cuFFT plan of `batch` contiguous side x side transforms (type
-// CUFFT_Z2Z in place, or CUFFT_D2Z from side^2 reals to side*(side/2+1)
-// complex values), bound to the context's stream and shared work area.
-int fft_plan(imcom_ctx* ctx, cufftType type, int side, int batch, cufftHandle* out);
+// `batch` contiguous 2-D side x side transforms on the context's stream
+// through the process-wide plan cache: in place complex-to-complex
+// (dir = CUFFT_FORWARD / CUFFT_INVERSE), or real side^2 -> side*(side/2+1)
+// complex.  fft_attach/fft_free count the contexts sharing the plans.
+int fft_z2z(imcom_ctx* ctx, int side, int batch, double2* data, int dir);
+int fft_d2z(imcom_ctx* ctx, int side, int batch, const double* in, double2* out);
+void fft_attach();
 void fft_free(imcom_ctx* ctx);
 template <class T>
 int ensure_vec(imcom_ctx* ctx, T** p, size_t count);

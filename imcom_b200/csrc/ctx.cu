@@ -5,6 +5,8 @@
 #include <cstring>
 #include <vector>
 
+#include <mutex>
+
 #include "common.cuh"
 
 namespace imcom {
@@ -38,21 +40,48 @@ int ensure_buf(imcom_ctx* ctx, void** p, size_t& have, size_t need) {
   return 0;
 }
 
-int fft_plan(imcom_ctx* ctx, cufftType type, int side, int batch, cufftHandle* out) {
-  constexpr size_t kMaxPlans = 64;  // about twenty sides of the three plan kinds
-  auto& plans = ctx->fft_plans;
-  size_t hit = plans.size();
-  for (size_t i = 0; i < plans.size(); ++i)
-    if (plans[i].type == (int)type && plans[i].side == side && plans[i].batch == batch) hit = i;
-  if (hit == plans.size()) {
-    if (plans.size() >= kMaxPlans) {
+// cuFFT plans shared by every context of the process, keyed by (device,
+// type, side, batch).  Planning a size costs tens to hundreds of
+// milliseconds of host time (Bluestein sizes included) and the PSF side
+// follows each patch's input footprint, so contexts solving a run of patches
+// side by side plan each size once between them.  Plans have no work area of
+// their own: each execution binds the calling context's work area and stream
+// and enqueues under one lock, so two contexts never race on a plan's state.
+// Plans live until the last context is destroyed; past kMaxPlans the device
+// is synchronised before the least recently used plan is dropped (a plan is
+// never destroyed while its kernels may be in flight).
+namespace {
+struct SharedPlan {
+  int dev, type, side, batch;
+  cufftHandle h;
+  size_t work;
+  unsigned long long used;
+};
+std::mutex g_fft_mu;
+std::vector<SharedPlan> g_fft_plans;
+unsigned long long g_fft_clock = 0;
+int g_fft_contexts = 0;
+constexpr size_t kMaxPlans = 512;
+
+int fft_exec(imcom_ctx* ctx, cufftType type, int side, int batch, void* in, void* out, int dir) {
+  std::lock_guard<std::mutex> lk(g_fft_mu);
+  size_t hit = g_fft_plans.size();
+  for (size_t i = 0; i < g_fft_plans.size(); ++i) {
+    const SharedPlan& f = g_fft_plans[i];
+    if (f.dev == ctx->device && f.type == (int)type && f.side == side && f.batch == batch) hit = i;
+  }
+  if (hit == g_fft_plans.size()) {
+    if (g_fft_plans.size() >= kMaxPlans) {
       size_t lru = 0;
-      for (size_t i = 1; i < plans.size(); ++i)
-        if (plans[i].used < plans[lru].used) lru = i;
-      cufftDestroy(plans[lru].h);
-      plans.erase(plans.begin() + lru);
+      for (size_t i = 1; i < g_fft_plans.size(); ++i)
+        if (g_fft_plans[i].used < g_fft_plans[lru].used) lru = i;
+      cudaSetDevice(g_fft_plans[lru].dev);
+      cudaDeviceSynchronize();
+      cufftDestroy(g_fft_plans[lru].h);
+      g_fft_plans.erase(g_fft_plans.begin() + lru);
+      cudaSetDevice(ctx->device);
     }
-    imcom_ctx::FftPlan f{(int)type, side, batch, 0, 0, 0};
+    SharedPlan f{ctx->device, (int)type, side, batch, 0, 0, 0};
     IMC_CUFFT(cufftCreate(&f.h));
     cufftResult r = cufftSetAutoAllocation(f.h, 0);
     int dims[2] = {side, side};
@@ -66,21 +95,44 @@ int fft_plan(imcom_ctx* ctx, cufftType type, int side, int batch, cufftHandle* o
       return set_err(ctx, IMCOM_ERR_CUDA, "cuFFT plan %dx%d x%d (type %d): error %d", side, side,
                      batch, (int)type, (int)r);
     }
-    plans.push_back(f);
-    hit = plans.size() - 1;
+    g_fft_plans.push_back(f);
+    hit = g_fft_plans.size() - 1;
   }
-  imcom_ctx::FftPlan& f = plans[hit];
-  f.used = ++ctx->fft_clock;
+  SharedPlan& f = g_fft_plans[hit];
+  f.used = ++g_fft_clock;
   IMC_TRY(ensure_buf(ctx, &ctx->fft_work, ctx->fft_work_bytes, f.work));
   if (f.work) IMC_CUFFT(cufftSetWorkArea(f.h, ctx->fft_work));
   IMC_CUFFT(cufftSetStream(f.h, ctx->stream));
-  *out = f.h;
+  if (type == CUFFT_Z2Z)
+    IMC_CUFFT(cufftExecZ2Z(f.h, (cufftDoubleComplex*)in, (cufftDoubleComplex*)out, dir));
+  else
+    IMC_CUFFT(cufftExecD2Z(f.h, (cufftDoubleReal*)in, (cufftDoubleComplex*)out));
   return 0;
+}
+}  // namespace
+
+int fft_z2z(imcom_ctx* ctx, int side, int batch, double2* data, int dir) {
+  return fft_exec(ctx, CUFFT_Z2Z, side, batch, data, data, dir);
+}
+
+int fft_d2z(imcom_ctx* ctx, int side, int batch, const double* in, double2* out) {
+  return fft_exec(ctx, CUFFT_D2Z, side, batch, const_cast<double*>(in), out, 0);
+}
+
+void fft_attach() {
+  std::lock_guard<std::mutex> lk(g_fft_mu);
+  ++g_fft_contexts;
 }
 
 void fft_free(imcom_ctx* ctx) {
-  for (auto& f : ctx->fft_plans) cufftDestroy(f.h);
-  ctx->fft_plans.clear();
+  {
+    std::lock_guard<std::mutex> lk(g_fft_mu);
+    if (--g_fft_contexts == 0) {
+      // every context's stream has drained (destroy synchronises first)
+      for (auto& f : g_fft_plans) cufftDestroy(f.h);
+      g_fft_plans.clear();
+    }
+  }
   if (ctx->fft_work) cudaFree(ctx->fft_work);
   ctx->fft_work = nullptr;
   ctx->fft_work_bytes = 0;
@@ -246,6 +298,7 @@ int imcom_gpu_create(int device, imcom_ctx** out) {
     return IMCOM_ERR_ALLOC;
   }
   cudaMemset(ctx->flags, 0, 64 * sizeof(int));
+  fft_attach();
   *out = ctx;
   return 0;
 }

@@ -262,13 +262,10 @@ int build_tables(imcom_ctx* ctx, int npad, int isB) {
                                          big2 * ntab * sizeof(double2));
   IMC_CUDA(cudaMemcpyAsync(dpairs, pairs.data(), ntab * sizeof(int2), cudaMemcpyHostToDevice,
                            ctx->stream));
-  cufftHandle plan = 0;
-  IMC_TRY(fft_plan(ctx, CUFFT_Z2Z, nbig, ntab, &plan));
   dim3 blk(128), grd((nbig + 127) / 128, nbig, ntab);
   embed_kernel<<<grd, blk, 0, ctx->stream>>>(ctx->Gt, ctx->Gammat, dpairs, ctx->fftbuf, nps, nbig);
   IMC_LAUNCH();
-  IMC_CUFFT(cufftExecZ2Z(plan, (cufftDoubleComplex*)ctx->fftbuf,
-                         (cufftDoubleComplex*)ctx->fftbuf, CUFFT_INVERSE));
+  IMC_TRY(fft_z2z(ctx, nbig, ntab, ctx->fftbuf, CUFFT_INVERSE));
   shift_scale_kernel<<<grd, blk, 0, ctx->stream>>>(ctx->fftbuf, ctx->tables, nbig, nps, isB);
   IMC_LAUNCH();
   return 0;
@@ -326,9 +323,7 @@ extern "C" int imcom_gpu_psf_spectra(imcom_ctx* ctx, int npoly_in, double* C_out
   }
   IMC_CUDA(cudaMemcpyAsync(rin + (size_t)E * ps2, ctx->Gamma, ps2 * sizeof(double),
                            cudaMemcpyDeviceToDevice, ctx->stream));
-  cufftHandle plan = 0;
-  IMC_TRY(fft_plan(ctx, CUFFT_D2Z, nps, E + 1, &plan));
-  IMC_CUFFT(cufftExecD2Z(plan, rin, (cufftDoubleComplex*)half));
+  IMC_TRY(fft_d2z(ctx, nps, E + 1, rin, half));
   {
     dim3 blk(128), grd((nps + 127) / 128, nps, E);
     hermitian_fill_kernel<<<grd, blk, 0, ctx->stream>>>(half, ctx->Gt, nps, nps);

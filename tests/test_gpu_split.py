@@ -187,3 +187,31 @@ def test_split_learned_matches_plain_fp64(solver):
     assert np.array_equal(rs["K"], r64["K"])
     assert relmax(rs["US"], r64["US"]) <= 1e-6
     assert np.max(colrel(rs["T"], r64["T"])) < 1e-8
+
+
+def test_split_n16200_matches_fp64():
+    """Largest workload (8 x 45x45 exposures, n=16200, m=16384): learned kappa
+    on the split products against the plain FP64 path on the same resident
+    system.  At the 1e-6 leakage target most pixels sit near kappa_min,
+    where the audit sends their P columns back to FP64; the bars hold either
+    way."""
+    from imcom_b200 import Solver, kappa_model
+    prob = synth.make("n16200", 0)
+    with Solver(0) as s:
+        s.set_problem(prob)
+        C = s.psf_spectra()
+        s.build_A(out=False)
+        s.eigen_A(out=False)
+        s.build_B(out=False)
+        r64 = stage2(s, C, True, 1e-6, 1e-8)
+        kappa_model.KappaModel.load(kappa_model.DEFAULT_WEIGHTS).install(s)
+        s.set_precision(True)
+        rs = stage2(s, C, True, 1e-6, 1e-8, learned=True)
+        info = s.split_info()
+        fp, _ = s.split_pixels()
+    assert info["P_split"] == 1.0 and fp.sum() == info["fp64_pixels_P"]
+    assert np.array_equal(rs["K"], r64["K"])
+    assert relmax(rs["US"], r64["US"]) <= 1e-6
+    assert relmax(rs["S"], r64["S"]) <= 1e-6
+    assert np.max(colrel(rs["T"], r64["T"])) < 1e-8
+    assert np.linalg.norm(rs["H"] - r64["H"]) <= 1e-8 * np.linalg.norm(r64["H"])
