@@ -39,6 +39,8 @@
 #include <type_traits>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 #include "eigen.cuh"
 
@@ -515,6 +517,211 @@ __global__ void __launch_bounds__(TRD_THREADS) trd_panel_kernel(TrdArgs a) {
     if (!grid_barrier(a.sync, a.spin)) return;
   }
 
+}
+
+// ---------------------------------------------------------------------------
+// 1b. The last columns of the tridiagonalisation in one thread-block cluster.
+//
+// Once the trailing matrix is small, every column of the panel kernel is a
+// chain of dependent L2 round trips and two grid barriers (~9 us whatever
+// the size).  From trailing size S <= tail_max the rest of the matrix is
+// factorised by one cluster of up to 16 CTAs holding it in distributed
+// shared memory: full symmetric rows, CTA q owning rows [q rpc, (q+1) rpc).
+// Unblocked LAPACK dsytd2 'L', per column j:
+//   the owner of row j forms the reflector of x = A(j+1:S, j) (= its row j)
+//   and stores v and tau into every CTA's shared memory;  cluster barrier 1
+//   every CTA forms p = tau A22 v on its rows and stores p and its part of
+//   p^T v into every CTA;                                 cluster barrier 2
+//   every CTA forms w = p - 1/2 tau (p^T v) v and applies A22 -= v w^T +
+//   w v^T to its rows; the warp updating row j+1 also sums |x|^2 for the
+//   next reflector.
+// Values move by remote stores before a barrier, never by remote loads after
+// it, so no step waits on a distributed-shared-memory round trip.
+// The reflectors go to V (column j: 1 at row j+1, v below), d, e and tau to
+// global memory; the hardware cluster barrier needs no poll limit.
+// ---------------------------------------------------------------------------
+constexpr int TAIL_THREADS = 512;
+constexpr int TAIL_MAX_CTAS = 16;
+constexpr int TAIL_RPW = 4;  // rows per warp: rpc <= TAIL_RPW * (TAIL_THREADS / 32)
+
+struct TailArgs {
+  const double* A;  // lower triangle valid for rows and columns k0 .. n-1
+  long long lda;
+  double* V;
+  long long ldv;
+  double *d, *e, *tau;
+  int n, k0, rpc;  // rows per CTA
+};
+
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+  return t;
+}
+
+__global__ void __launch_bounds__(TAIL_THREADS, 1) trd_tail_kernel(TailArgs a) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const int q = (int)cl.block_rank(), nct = (int)cl.num_blocks();
+  const int S = a.n - a.k0, rpc = a.rpc, k0 = a.k0;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  constexpr int NW = TAIL_THREADS / 32;
+  extern __shared__ __align__(16) double tsm[];
+  // Buffers written by other CTAs alternate with the column's parity: the
+  // owner of column j+1 may push v while a CTA still updates with column j's.
+  double* Ar = tsm;                     // [rpc][S] this CTA's rows
+  double* vb = Ar + (size_t)rpc * S;    // [2][S] v of the column (pushed by its owner)
+  double* pb = vb + 2 * (size_t)S;      // [2][S] p of the column (pushed by each row's owner)
+  double* tb = pb + 2 * (size_t)S;      // [2] tau of the column
+  double* pvb = tb + 2;                 // [2][TAIL_MAX_CTAS] each CTA's part of p^T v
+  __shared__ double red[TAIL_THREADS / 32];
+  __shared__ double nx;  // |x|^2 below alpha of the next column, if this CTA owns its row
+  const int r0 = q * rpc;
+  const int nrow = max(0, min(rpc, S - r0));
+
+  // rows r0 .. r0+nrow-1: entries on and right of the diagonal from the
+  // lower triangle's columns (coalesced), then the entries left of it from
+  // the owners of those columns' rows
+  for (int idx = tid; idx < nrow * S; idx += TAIL_THREADS) {
+    const int i = idx / S, c = idx - i * S;
+    if (c >= r0 + i) Ar[idx] = a.A[(long long)(k0 + c) + (long long)(k0 + r0 + i) * a.lda];
+  }
+  cl.sync();
+  for (int idx = tid; idx < nrow * S; idx += TAIL_THREADS) {
+    const int i = idx / S, c = idx - i * S;
+    if (c < r0 + i) {
+      const int o = c / rpc;
+      const double* rem = cl.map_shared_rank(Ar, o);
+      Ar[idx] = rem[(size_t)(c - o * rpc) * S + (r0 + i)];
+    }
+  }
+  cl.sync();
+
+  for (int jl = 0; jl < S - 1; ++jl) {
+    const int j = k0 + jl, par = jl & 1;
+    double* v = vb + (size_t)par * S;
+    double* p = pb + (size_t)par * S;
+    const int o = jl / rpc;
+    if (q == o) {
+      // Householder reflector of x = A(j+1:n, j) (LAPACK dlarfg); |x|^2 below
+      // alpha was summed while row j was updated for the previous column
+      const double* row = Ar + (size_t)(jl - r0) * S;
+      double xn2;
+      if (jl == 0) {
+        double part = 0.0;
+        for (int c = 2 + tid; c < S; c += TAIL_THREADS) part += row[c] * row[c];
+        xn2 = block_sum(part, red);
+      } else {
+        xn2 = nx;
+      }
+      const double alpha = row[jl + 1];
+      double beta, t, scl;
+      if (xn2 == 0.0) {
+        t = 0.0;
+        beta = alpha;
+        scl = 0.0;
+      } else {
+        beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+        t = (beta - alpha) / beta;
+        scl = 1.0 / (alpha - beta);
+      }
+      // push v and tau into every CTA (stores complete before the barrier)
+      for (int c = jl + 1 + tid; c < S; c += TAIL_THREADS) {
+        const double vc = (c == jl + 1) ? 1.0 : row[c] * scl;
+        for (int r = 0; r < nct; ++r) cl.map_shared_rank(v, r)[c] = vc;
+        a.V[(long long)(k0 + c) + (long long)j * a.ldv] = vc;
+      }
+      if (tid < nct) cl.map_shared_rank(tb, tid)[par] = t;
+      if (tid == 0) {
+        a.d[j] = row[jl];
+        a.e[j] = beta;
+        a.tau[j] = t;
+      }
+    }
+    cl.sync();
+    const double t = tb[par];
+    // p = tau A22 v on this CTA's rows below row j, pushed into every CTA.
+    // A warp takes rows wid, wid + NW, ... together: one pass over the
+    // columns with one independent chain per row.
+    const double* rowp[TAIL_RPW];
+    bool act[TAIL_RPW];
+#pragma unroll
+    for (int h = 0; h < TAIL_RPW; ++h) {
+      const int i = wid + NW * h;
+      act[h] = i < nrow && r0 + i > jl;
+      rowp[h] = Ar + (size_t)min(i, rpc - 1) * S;
+    }
+    double pv = 0.0;
+    {
+      double acc[TAIL_RPW];
+#pragma unroll
+      for (int h = 0; h < TAIL_RPW; ++h) acc[h] = 0.0;
+      for (int c = jl + 1 + lane; c < S; c += 32) {
+        const double vc = v[c];
+#pragma unroll
+        for (int h = 0; h < TAIL_RPW; ++h)
+          if (act[h]) acc[h] = fma(rowp[h][c], vc, acc[h]);
+      }
+#pragma unroll
+      for (int h = 0; h < TAIL_RPW; ++h) {
+        if (!act[h]) continue;
+        const int rr = r0 + wid + NW * h;
+        const double ph = t * warp_sum(acc[h]);  // every lane holds the sum
+        if (lane < nct) cl.map_shared_rank(p, lane)[rr] = ph;
+        if (lane == 0) pv += ph * v[rr];
+      }
+    }
+    pv = block_sum(pv, red);
+    if (tid < nct) cl.map_shared_rank(pvb, tid)[par * TAIL_MAX_CTAS + q] = pv;
+    cl.sync();
+    double ptv = 0.0;
+    for (int r = 0; r < nct; ++r) ptv += pvb[par * TAIL_MAX_CTAS + r];
+    // w = p - 1/2 tau (p^T v) v;  A22 -= v w^T + w v^T on this CTA's rows;
+    // the warp that updates row j+1 also sums |x|^2 of the next column
+    const double a2 = -0.5 * t * ptv;
+    {
+      double vr[TAIL_RPW], wr[TAIL_RPW];
+      int nxt = -1;  // which of this warp's rows is row j+1
+#pragma unroll
+      for (int h = 0; h < TAIL_RPW; ++h) {
+        const int rr = r0 + wid + NW * h;
+        vr[h] = act[h] ? v[rr] : 0.0;
+        wr[h] = act[h] ? p[rr] + a2 * vr[h] : 0.0;
+        if (act[h] && rr == jl + 1) nxt = h;
+      }
+      double s2 = 0.0;
+      for (int c = jl + 1 + lane; c < S; c += 32) {
+        const double vc = v[c], wc = p[c] + a2 * vc;
+#pragma unroll
+        for (int h = 0; h < TAIL_RPW; ++h) {
+          if (!act[h]) continue;
+          double* row = const_cast<double*>(rowp[h]);
+          const double nv = row[c] - (vr[h] * wc + wr[h] * vc);
+          row[c] = nv;
+          if (h == nxt && c >= jl + 3) s2 += nv * nv;
+        }
+      }
+      if (nxt >= 0) {
+        s2 = warp_sum(s2);
+        if (lane == 0) nx = s2;
+      }
+    }
+    __syncthreads();
+  }
+  // the last diagonal entry
+  if (S >= 1 && q == (S - 1) / rpc && tid == 0)
+    a.d[k0 + S - 1] = Ar[(size_t)(S - 1 - r0) * S + (S - 1)];
+}
+
+// Shared memory of the cluster tail for trailing size S with `ctas` CTAs.
+inline size_t tail_smem(int S, int ctas) {
+  const int rpc = (S + ctas - 1) / ctas;
+  return ((size_t)rpc * S + 4 * (size_t)S + 2 + 2 * TAIL_MAX_CTAS) * sizeof(double);
 }
 
 __global__ void set_last_diag_kernel(const double* A, long long lda, int n, double* d) {
@@ -1074,7 +1281,66 @@ static int sytrd_gpu(imcom_ctx* ctx, DMat& Aw, DMat& Vall, double* d, double* e,
   GridSync* sync = (GridSync*)((char*)accbuf + 2 * sizeof(TrdAcc) + 64);
   int* flag = &sync->err;
   IMC_CUDA(cudaMemsetAsync(sync, 0, sizeof(GridSync), ctx->stream));
+  // the cluster tail: 16 CTAs (non-portable cluster size) if the device can
+  // co-schedule them, else 8; tail_max = the largest trailing size whose rows
+  // fit the cluster's shared memory
+  int tail_ctas = 0, tail_max = 0;
+  {
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const size_t limit = optin > 2048 ? (size_t)optin - 1024 : 0;  // room for static shared
+    cudaFuncSetAttribute(trd_tail_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    cudaFuncSetAttribute(trd_tail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)limit);
+    for (int c : {16, 8}) {
+      int smax = 1024;
+      while (smax > 32 && (tail_smem(smax, c) > limit ||
+                           (smax + c - 1) / c > TAIL_RPW * (TAIL_THREADS / 32)))
+        --smax;
+      cudaLaunchConfig_t cfg = {};
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = c;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.gridDim = dim3(c);
+      cfg.blockDim = dim3(TAIL_THREADS);
+      cfg.dynamicSmemBytes = tail_smem(smax, c);
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      int nc = 0;
+      if (cudaOccupancyMaxActiveClusters(&nc, (void*)trd_tail_kernel, &cfg) == cudaSuccess &&
+          nc >= 1) {
+        tail_ctas = c;
+        tail_max = smax;
+        break;
+      }
+    }
+    cudaGetLastError();  // an unsupported cluster size only disables the tail
+  }
+  bool tail_done = false, panels = false;
   for (int k = 0; k < n - 1; k += NB) {
+    if (tail_ctas && n - k <= tail_max) {
+      const int S = n - k;
+      TailArgs ta{Aw.p, Aw.ld, Vall.p, Vall.ld, d, e, tau, n, k, (S + tail_ctas - 1) / tail_ctas};
+      cudaLaunchConfig_t cfg = {};
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = tail_ctas;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.gridDim = dim3(tail_ctas);
+      cfg.blockDim = dim3(TAIL_THREADS);
+      cfg.dynamicSmemBytes = tail_smem(S, tail_ctas);
+      cfg.stream = ctx->stream;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      IMC_CUDA(cudaLaunchKernelEx(&cfg, trd_tail_kernel, ta));
+      IMC_LAUNCH();
+      tail_done = true;
+      break;
+    }
+    panels = true;
     const int b = std::min(NB, n - 1 - k);
     IMC_CUDA(cudaMemsetAsync(accbuf, 0, 2 * sizeof(TrdAcc), ctx->stream));
     static_assert(2 * sizeof(TrdAcc) + 64 + sizeof(GridSync) <= 4096, "panel scratch");
@@ -1099,15 +1365,23 @@ static int sytrd_gpu(imcom_ctx* ctx, DMat& Aw, DMat& Vall, double* d, double* e,
                              Aw.p + t0 + (long long)t0 * Aw.ld, Aw.ld));
     }
     // a timed-out barrier ends the factorisation with an error
-    if ((k / NB) % 16 == 15 || k + NB >= n - 1) {
+    if ((k / NB) % 16 == 15) {
       int h = 0;
       IMC_CUDA(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
       IMC_CUDA(cudaStreamSynchronize(ctx->stream));
       if (h) return set_err(ctx, IMCOM_ERR_EIGEN, "tridiagonalisation grid barrier timed out");
     }
   }
-  set_last_diag_kernel<<<1, 1, 0, ctx->stream>>>(Aw.p, Aw.ld, n, d);
-  IMC_LAUNCH();
+  if (panels) {
+    int h = 0;
+    IMC_CUDA(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (h) return set_err(ctx, IMCOM_ERR_EIGEN, "tridiagonalisation grid barrier timed out");
+  }
+  if (!tail_done) {  // the tail writes the last diagonal entry itself
+    set_last_diag_kernel<<<1, 1, 0, ctx->stream>>>(Aw.p, Aw.ld, n, d);
+    IMC_LAUNCH();
+  }
   return 0;
 }
 
