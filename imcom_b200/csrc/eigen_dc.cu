@@ -528,15 +528,16 @@ __global__ void __launch_bounds__(TRD_THREADS) trd_panel_kernel(TrdArgs a) {
 // factorised by one cluster of up to 16 CTAs holding it in distributed
 // shared memory: full symmetric rows, CTA q owning rows [q rpc, (q+1) rpc).
 // Unblocked LAPACK dsytd2 'L', per column j:
-//   the owner of row j forms the reflector of x = A(j+1:S, j) (= its row j)
-//   and stores v and tau into every CTA's shared memory;  cluster barrier 1
-//   every CTA forms p = tau A22 v on its rows and stores p and its part of
-//   p^T v into every CTA;                                 cluster barrier 2
-//   every CTA forms w = p - 1/2 tau (p^T v) v and applies A22 -= v w^T +
-//   w v^T to its rows; the warp updating row j+1 also sums |x|^2 for the
-//   next reflector.
+//   the owner of row j applies the previous column's update to row j, forms
+//   the reflector of x = A(j+1:S, j) (= its row j) and stores v and tau into
+//   every CTA's shared memory;                            cluster barrier 1
+//   every CTA applies the previous column's update to its other rows and,
+//   in the same pass, forms p = tau A22 v on them; it stores p and its part
+//   of p^T v into every CTA;                              cluster barrier 2
+//   w = p - 1/2 tau (p^T v) v is formed where the next pass needs it.
 // Values move by remote stores before a barrier, never by remote loads after
-// it, so no step waits on a distributed-shared-memory round trip.
+// it, so no step waits on a distributed-shared-memory round trip; one pass
+// over the rows per column both updates them and multiplies them by v.
 // The reflectors go to V (column j: 1 at row j+1, v below), d, e and tau to
 // global memory; the hardware cluster barrier needs no poll limit.
 // ---------------------------------------------------------------------------
@@ -580,7 +581,6 @@ __global__ void __launch_bounds__(TAIL_THREADS, 1) trd_tail_kernel(TailArgs a) {
   double* tb = pb + 2 * (size_t)S;      // [2] tau of the column
   double* pvb = tb + 2;                 // [2][TAIL_MAX_CTAS] each CTA's part of p^T v
   __shared__ double red[TAIL_THREADS / 32];
-  __shared__ double nx;  // |x|^2 below alpha of the next column, if this CTA owns its row
   const int r0 = q * rpc;
   const int nrow = max(0, min(rpc, S - r0));
 
@@ -602,23 +602,34 @@ __global__ void __launch_bounds__(TAIL_THREADS, 1) trd_tail_kernel(TailArgs a) {
   }
   cl.sync();
 
+  // Column j's update A22 -= v w^T + w v^T is applied lazily: the owner of
+  // row j+1 applies it to that row first (the next reflector needs it), the
+  // other rows receive it in the same pass that forms their part of the next
+  // column's p = tau A22 v.  w = p + a2 v comes from the parity buffers.
+  double a2 = 0.0;  // -1/2 tau (p^T v) of the pending (previous) column
   for (int jl = 0; jl < S - 1; ++jl) {
     const int j = k0 + jl, par = jl & 1;
     double* v = vb + (size_t)par * S;
-    double* p = pb + (size_t)par * S;
+    const double* vq = vb + (size_t)(par ^ 1) * S;  // pending column's v
+    const double* pq = pb + (size_t)(par ^ 1) * S;  // pending column's p
     const int o = jl / rpc;
     if (q == o) {
-      // Householder reflector of x = A(j+1:n, j) (LAPACK dlarfg); |x|^2 below
-      // alpha was summed while row j was updated for the previous column
-      const double* row = Ar + (size_t)(jl - r0) * S;
-      double xn2;
-      if (jl == 0) {
-        double part = 0.0;
-        for (int c = 2 + tid; c < S; c += TAIL_THREADS) part += row[c] * row[c];
-        xn2 = block_sum(part, red);
+      // row j: the pending update, then the Householder reflector of
+      // x = A(j+1:n, j) (LAPACK dlarfg)
+      double* row = Ar + (size_t)(jl - r0) * S;
+      double part = 0.0;
+      if (jl > 0) {
+        const double vr = vq[jl], wr = pq[jl] + a2 * vr;
+        for (int c = jl + tid; c < S; c += TAIL_THREADS) {
+          const double vc = vq[c];
+          const double nv = row[c] - (vr * (pq[c] + a2 * vc) + wr * vc);
+          row[c] = nv;
+          if (c >= jl + 2) part += nv * nv;
+        }
       } else {
-        xn2 = nx;
+        for (int c = 2 + tid; c < S; c += TAIL_THREADS) part += row[c] * row[c];
       }
+      const double xn2 = block_sum(part, red);  // also orders the row's new values
       const double alpha = row[jl + 1];
       double beta, t, scl;
       if (xn2 == 0.0) {
@@ -645,34 +656,43 @@ __global__ void __launch_bounds__(TAIL_THREADS, 1) trd_tail_kernel(TailArgs a) {
     }
     cl.sync();
     const double t = tb[par];
-    // p = tau A22 v on this CTA's rows below row j, pushed into every CTA.
-    // A warp takes rows wid, wid + NW, ... together: one pass over the
-    // columns with one independent chain per row.
-    const double* rowp[TAIL_RPW];
-    bool act[TAIL_RPW];
-#pragma unroll
-    for (int h = 0; h < TAIL_RPW; ++h) {
-      const int i = wid + NW * h;
-      act[h] = i < nrow && r0 + i > jl;
-      rowp[h] = Ar + (size_t)min(i, rpc - 1) * S;
-    }
+    // this CTA's rows below row j: the pending update (columns >= j) and
+    // p = tau A22 v (columns > j) in one pass; a warp takes rows wid,
+    // wid + NW, ... together with one independent chain per row
     double pv = 0.0;
     {
-      double acc[TAIL_RPW];
+      double* rowp[TAIL_RPW];
+      bool act[TAIL_RPW];
+      double acc[TAIL_RPW], vr[TAIL_RPW], wr[TAIL_RPW];
 #pragma unroll
-      for (int h = 0; h < TAIL_RPW; ++h) acc[h] = 0.0;
-      for (int c = jl + 1 + lane; c < S; c += 32) {
-        const double vc = v[c];
+      for (int h = 0; h < TAIL_RPW; ++h) {
+        const int i = wid + NW * h;
+        act[h] = i < nrow && r0 + i > jl;
+        rowp[h] = Ar + (size_t)min(i, rpc - 1) * S;
+        acc[h] = 0.0;
+        vr[h] = (act[h] && jl > 0) ? vq[r0 + i] : 0.0;
+        wr[h] = (act[h] && jl > 0) ? pq[r0 + i] + a2 * vr[h] : 0.0;
+      }
+      for (int c = jl + lane; c < S; c += 32) {
+        const double vc = vq[c], wc = pq[c] + a2 * vc;  // zero terms when jl = 0
+        const double vn = (c > jl) ? v[c] : 0.0;
 #pragma unroll
-        for (int h = 0; h < TAIL_RPW; ++h)
-          if (act[h]) acc[h] = fma(rowp[h][c], vc, acc[h]);
+        for (int h = 0; h < TAIL_RPW; ++h) {
+          if (!act[h]) continue;
+          double nv = rowp[h][c];
+          if (jl > 0) {
+            nv -= vr[h] * wc + wr[h] * vc;
+            rowp[h][c] = nv;
+          }
+          acc[h] = fma(nv, vn, acc[h]);
+        }
       }
 #pragma unroll
       for (int h = 0; h < TAIL_RPW; ++h) {
         if (!act[h]) continue;
         const int rr = r0 + wid + NW * h;
         const double ph = t * warp_sum(acc[h]);  // every lane holds the sum
-        if (lane < nct) cl.map_shared_rank(p, lane)[rr] = ph;
+        if (lane < nct) cl.map_shared_rank(pb + (size_t)par * S, lane)[rr] = ph;
         if (lane == 0) pv += ph * v[rr];
       }
     }
@@ -681,41 +701,18 @@ __global__ void __launch_bounds__(TAIL_THREADS, 1) trd_tail_kernel(TailArgs a) {
     cl.sync();
     double ptv = 0.0;
     for (int r = 0; r < nct; ++r) ptv += pvb[par * TAIL_MAX_CTAS + r];
-    // w = p - 1/2 tau (p^T v) v;  A22 -= v w^T + w v^T on this CTA's rows;
-    // the warp that updates row j+1 also sums |x|^2 of the next column
-    const double a2 = -0.5 * t * ptv;
-    {
-      double vr[TAIL_RPW], wr[TAIL_RPW];
-      int nxt = -1;  // which of this warp's rows is row j+1
-#pragma unroll
-      for (int h = 0; h < TAIL_RPW; ++h) {
-        const int rr = r0 + wid + NW * h;
-        vr[h] = act[h] ? v[rr] : 0.0;
-        wr[h] = act[h] ? p[rr] + a2 * vr[h] : 0.0;
-        if (act[h] && rr == jl + 1) nxt = h;
-      }
-      double s2 = 0.0;
-      for (int c = jl + 1 + lane; c < S; c += 32) {
-        const double vc = v[c], wc = p[c] + a2 * vc;
-#pragma unroll
-        for (int h = 0; h < TAIL_RPW; ++h) {
-          if (!act[h]) continue;
-          double* row = const_cast<double*>(rowp[h]);
-          const double nv = row[c] - (vr[h] * wc + wr[h] * vc);
-          row[c] = nv;
-          if (h == nxt && c >= jl + 3) s2 += nv * nv;
-        }
-      }
-      if (nxt >= 0) {
-        s2 = warp_sum(s2);
-        if (lane == 0) nx = s2;
-      }
-    }
-    __syncthreads();
+    a2 = -0.5 * t * ptv;
   }
-  // the last diagonal entry
-  if (S >= 1 && q == (S - 1) / rpc && tid == 0)
-    a.d[k0 + S - 1] = Ar[(size_t)(S - 1 - r0) * S + (S - 1)];
+  // the last diagonal entry receives the last column's update
+  if (S >= 2 && q == (S - 1) / rpc && tid == 0) {
+    const int par = (S - 2) & 1;
+    const double* vl = vb + (size_t)par * S;
+    const double* pl = pb + (size_t)par * S;
+    const double vr = vl[S - 1], wr = pl[S - 1] + a2 * vr;
+    a.d[k0 + S - 1] = Ar[(size_t)(S - 1 - r0) * S + (S - 1)] - (vr * wr + wr * vr);
+  } else if (S == 1 && q == 0 && tid == 0) {
+    a.d[k0] = Ar[0];
+  }
 }
 
 // Shared memory of the cluster tail for trailing size S with `ctas` CTAs.
@@ -921,11 +918,19 @@ __global__ void dc_prep_kernel(const Node* nodes, const double* w, const double*
 
 // Deflation (LAPACK dlaed2): one CTA per node; reductions in parallel, the
 // scan by thread 0.
+// The scan is sequential (LAPACK dlaed2): one thread walks the node's sorted
+// (d, z) pairs, carrying the previous non-deflated entry (possibly rotated)
+// in registers.  The other warps stage the input into shared memory one
+// chunk ahead, so the walk never waits on a global-memory round trip.
+constexpr int DEF_CH = 1024;
+
 __global__ void __launch_bounds__(256) dc_deflate_kernel(const Node* nodes, DcWork wk) {
   const Node nd = nodes[blockIdx.x];
   const int s = nd.s, nm = nd.nm;
   const double rho = wk.rho[blockIdx.x];
   __shared__ double sh_d[256], sh_z[256];
+  __shared__ double cd[2][DEF_CH], cz[2][DEF_CH];
+  __shared__ int cpm[2][DEF_CH];
   double md = 0.0, mz = 0.0;
   for (int q = threadIdx.x; q < nm; q += blockDim.x) {
     md = fmax(md, fabs(wk.ds[s + q]));
@@ -933,6 +938,11 @@ __global__ void __launch_bounds__(256) dc_deflate_kernel(const Node* nodes, DcWo
   }
   sh_d[threadIdx.x] = md;
   sh_z[threadIdx.x] = mz;
+  for (int q = threadIdx.x; q < min(nm, DEF_CH); q += blockDim.x) {
+    cd[0][q] = wk.ds[s + q];
+    cz[0][q] = wk.zs[s + q];
+    cpm[0][q] = wk.perm[s + q];
+  }
   __syncthreads();
   for (int o = 128; o > 0; o >>= 1) {
     if (threadIdx.x < o) {
@@ -941,53 +951,72 @@ __global__ void __launch_bounds__(256) dc_deflate_kernel(const Node* nodes, DcWo
     }
     __syncthreads();
   }
-  if (threadIdx.x != 0) return;
   const double tol = 8.0 * EPS * fmax(sh_d[0], rho * sh_z[0]);
-  double* d = wk.ds + s;
-  double* z = wk.zs + s;
-  const int* perm = wk.perm + s;
-  int k = 0, ndef = 0, nrot = 0, prev = -1;
-  for (int jj = 0; jj < nm; ++jj) {
-    if (rho * fabs(z[jj]) <= tol) {
-      wk.defd[s + ndef] = d[jj];
-      wk.defcol[s + ndef] = perm[jj];
-      ++ndef;
-      continue;
+  int k = 0, ndef = 0, nrot = 0;
+  bool have = false;      // a previous non-deflated entry exists
+  double dp = 0.0, zp = 0.0;
+  int pp = 0;
+  for (int c0 = 0, b = 0; c0 < nm; c0 += DEF_CH, b ^= 1) {
+    if (threadIdx.x >= 32) {
+      const int n0 = c0 + DEF_CH;
+      for (int q = threadIdx.x - 32; q < min(DEF_CH, nm - n0); q += blockDim.x - 32) {
+        cd[b ^ 1][q] = wk.ds[s + n0 + q];
+        cz[b ^ 1][q] = wk.zs[s + n0 + q];
+        cpm[b ^ 1][q] = wk.perm[s + n0 + q];
+      }
+    } else if (threadIdx.x == 0) {
+      const int cn = min(DEF_CH, nm - c0);
+      for (int jj = 0; jj < cn; ++jj) {
+        const double dj = cd[b][jj], zj = cz[b][jj];
+        const int pj = cpm[b][jj];
+        if (rho * fabs(zj) <= tol) {
+          wk.defd[s + ndef] = dj;
+          wk.defcol[s + ndef] = pj;
+          ++ndef;
+          continue;
+        }
+        if (!have) {
+          have = true;
+          dp = dj;
+          zp = zj;
+          pp = pj;
+          continue;
+        }
+        double sv = zp, cv = zj;
+        const double tau = hypot(cv, sv);
+        const double t = dj - dp;
+        cv /= tau;
+        sv = -sv / tau;
+        if (fabs(t * cv * sv) <= tol) {
+          wk.rcol[s + nrot] = make_int2(pp, pj);
+          wk.rcs[s + nrot] = make_double2(cv, sv);
+          ++nrot;
+          const double tt = dp * cv * cv + dj * sv * sv;
+          const double dn = dp * sv * sv + dj * cv * cv;
+          wk.defd[s + ndef] = tt;
+          wk.defcol[s + ndef] = pp;
+          ++ndef;
+          dp = dn;
+          zp = tau;
+          pp = pj;
+        } else {
+          wk.dl[s + k] = dp;
+          wk.zz[s + k] = zp;
+          wk.ndcol[s + k] = pp;
+          ++k;
+          dp = dj;
+          zp = zj;
+          pp = pj;
+        }
+      }
     }
-    if (prev < 0) {
-      prev = jj;
-      continue;
-    }
-    double sv = z[prev], cv = z[jj];
-    double tau = hypot(cv, sv);
-    double t = d[jj] - d[prev];
-    cv /= tau;
-    sv = -sv / tau;
-    if (fabs(t * cv * sv) <= tol) {
-      z[jj] = tau;
-      z[prev] = 0.0;
-      wk.rcol[s + nrot] = make_int2(perm[prev], perm[jj]);
-      wk.rcs[s + nrot] = make_double2(cv, sv);
-      ++nrot;
-      double tt = d[prev] * cv * cv + d[jj] * sv * sv;
-      d[jj] = d[prev] * sv * sv + d[jj] * cv * cv;
-      d[prev] = tt;
-      wk.defd[s + ndef] = d[prev];
-      wk.defcol[s + ndef] = perm[prev];
-      ++ndef;
-      prev = jj;
-    } else {
-      wk.dl[s + k] = d[prev];
-      wk.zz[s + k] = z[prev];
-      wk.ndcol[s + k] = perm[prev];
-      ++k;
-      prev = jj;
-    }
+    __syncthreads();
   }
-  if (prev >= 0) {
-    wk.dl[s + k] = d[prev];
-    wk.zz[s + k] = z[prev];
-    wk.ndcol[s + k] = perm[prev];
+  if (threadIdx.x != 0) return;
+  if (have) {
+    wk.dl[s + k] = dp;
+    wk.zz[s + k] = zp;
+    wk.ndcol[s + k] = pp;
     ++k;
   }
   wk.kcnt[blockIdx.x] = k;
