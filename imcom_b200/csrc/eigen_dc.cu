@@ -32,8 +32,9 @@
 //    linearised, so each step solves a quadratic), the
 //    Gu-Eisenstat z-hat (dlaed3) and the eigenvector columns (one warp each),
 //    then Q_node = Q_old(:, nondeflated) U as one DMMA GEMM per node.
-// 3. Back-transformation (dormtr): Z <- (I - V T V^T) Z over blocks of 128
-//    reflectors, T built from V^T V (dlarft), three GEMMs per block.
+// 3. Back-transformation (dormtr): Z <- (I - V T V^T) Z over blocks of 256
+//    reflectors, three GEMMs per block.  T is built from V^T V: dlarft on
+//    each 128-reflector half, joined by T12 = -T1 (V1^T V2) T2.
 #include <algorithm>
 #include <cmath>
 #include <type_traits>
@@ -1233,8 +1234,10 @@ __global__ void dc_assemble_kernel(const Node* nodes, DcWork wk, const double* O
 // lower triangle) share one shared-memory tile, so the recurrence reads no
 // global memory.
 // One CTA per block of NBB reflectors: block b holds reflectors
-// b NBB .. b NBB + jb - 1 (jb = min(NBB, nref - b NBB)), its Gram matrix at
-// G + b NBB ldg and its T factor at T + b NBB ldt.
+// b NBB .. b NBB + jb - 1 (jb = min(NBB, nref - b NBB)).
+// The Gram matrices and T factors are stored per pair of blocks (2 NBB x
+// 2 NBB, leading dimension ldg = ldt = 2 NBB): block b is the diagonal
+// sub-block b % 2 of pair b / 2.
 __global__ void __launch_bounds__(NBB) larft_kernel(const double* Gall, long long ldg,
                                                     const double* tau_all, int nref,
                                                     double* Tall, long long ldt) {
@@ -1242,9 +1245,11 @@ __global__ void __launch_bounds__(NBB) larft_kernel(const double* Gall, long lon
   double(*S)[NBB + 1] = reinterpret_cast<double(*)[NBB + 1]>(smem_t);
   const int r = threadIdx.x;
   const int j0 = blockIdx.x * NBB, jb = min(NBB, nref - j0);
-  const double* G = Gall + (size_t)blockIdx.x * NBB * ldg;
+  if (jb <= 0) return;
+  const int pr = blockIdx.x >> 1, h = blockIdx.x & 1;
+  const double* G = Gall + (size_t)pr * 2 * NBB * ldg + (size_t)h * NBB * (ldg + 1);
   const double* tau = tau_all + j0;
-  double* T = Tall + (size_t)blockIdx.x * NBB * ldt;
+  double* T = Tall + (size_t)pr * 2 * NBB * ldt + (size_t)h * NBB * (ldt + 1);
   // S[c][r] = G(r, c) for r < c (lower triangle); the upper triangle holds T
   for (int c = 0; c < jb; ++c) {
     if (r <= c) S[r][c] = 0.0;                          // T part: upper triangle
@@ -1449,8 +1454,9 @@ int eigen_dc(imcom_ctx* ctx, const DMat& A, DMat& Wout, double* wout) {
   size_t o_wk = take(((size_t)n * 8 + 16) * 9 + ((size_t)n * 4 + 16) * 8 + ((size_t)n * 24 + 32) +
                      4096);
   const size_t nblk_bt = (size_t)(n - 1 + NBB - 1) / NBB + 1;
-  size_t o_T = take(nblk_bt * NBB * NBB * 8), o_G = take(nblk_bt * NBB * NBB * 8);
-  size_t o_X = take((size_t)NBB * ld * 8 * 2);
+  const size_t npair_bt = (nblk_bt + 1) / 2;
+  size_t o_T = take(npair_bt * 4 * NBB * NBB * 8), o_G = take(npair_bt * 4 * NBB * NBB * 8);
+  size_t o_X = take((size_t)2 * NBB * ld * 8 * 2);
   size_t o_err = take(64);
   IMC_TRY(eig_buf(ctx, off + 256));
   char* base = (char*)ew->buf;
@@ -1600,31 +1606,48 @@ int eigen_dc(imcom_ctx* ctx, const DMat& A, DMat& Wout, double* wout) {
   stage_begin(ctx, ST_EIG_BT);
   const int nref = n - 1;
   const int nblk = (nref + NBB - 1) / NBB;
+  const int NB2 = 2 * NBB, npair = (nblk + 1) / 2;
   IMC_CUDA(cudaFuncSetAttribute(larft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)LARFT_SMEM));
   double* X = Xb;
-  double* X2 = Xb + (size_t)NBB * ld;
-  // Gram matrices of every block, then every T factor in one launch (one CTA
-  // per block: the T recurrences run concurrently)
-  for (int bi = 0; bi < nblk; ++bi) {
-    const int j0 = bi * NBB, jb = std::min(NBB, nref - j0);
+  double* X2 = Xb + (size_t)NB2 * ld;
+  // Blocks of 2 NBB reflectors: the Gram matrix of each pair, the T factors of
+  // its two halves in one launch (one CTA per half: the T recurrences run
+  // concurrently), then T12 = -T1 (V1^T V2) T2 joins them (H1 H2 = I - V T V^T
+  // with V = [V1 V2], T = [T1 T12; 0 T2]).  Pairs halve the passes over Z and
+  // double the inner dimension of the update product.
+  for (int pi = 0; pi < npair; ++pi) {
+    const int j0 = pi * NB2, jb = std::min(NB2, nref - j0);
     const int r0 = j0, K = n - r0;
     const double* Vb = Vall.p + r0 + (size_t)j0 * Vall.ld;
     IMC_TRY(dgemm(ctx, 'T', 'N', jb, jb, K, 1.0, Vb, Vall.ld, Vb, Vall.ld, 0.0,
-                  Gb + (size_t)bi * NBB * NBB, NBB));
+                  Gb + (size_t)pi * NB2 * NB2, NB2));
   }
-  larft_kernel<<<nblk, NBB, LARFT_SMEM, ctx->stream>>>(Gb, NBB, tau, nref, Tb, NBB);
+  IMC_CUDA(cudaMemsetAsync(Tb, 0, (size_t)npair * NB2 * NB2 * sizeof(double), ctx->stream));
+  larft_kernel<<<nblk, NBB, LARFT_SMEM, ctx->stream>>>(Gb, NB2, tau, nref, Tb, NB2);
   IMC_LAUNCH();
-  for (int bi = nblk - 1; bi >= 0; --bi) {
-    const int j0 = bi * NBB, jb = std::min(NBB, nref - j0);
+  for (int pi = 0; pi < npair; ++pi) {
+    const int j0 = pi * NB2, jb = std::min(NB2, nref - j0);
+    if (jb <= NBB) continue;  // a single block: no T12
+    const int jb2 = jb - NBB;
+    double* T = Tb + (size_t)pi * NB2 * NB2;
+    const double* G = Gb + (size_t)pi * NB2 * NB2;
+    // X = G12 T2 (NBB x jb2), then T12 = -T1 X
+    IMC_TRY(dgemm(ctx, 'N', 'N', NBB, jb2, jb2, 1.0, G + (size_t)NBB * NB2, NB2,
+                  T + NBB + (size_t)NBB * NB2, NB2, 0.0, X, NBB));
+    IMC_TRY(dgemm(ctx, 'N', 'N', NBB, jb2, NBB, -1.0, T, NB2, X, NBB, 0.0,
+                  T + (size_t)NBB * NB2, NB2));
+  }
+  for (int pi = npair - 1; pi >= 0; --pi) {
+    const int j0 = pi * NB2, jb = std::min(NB2, nref - j0);
     // rows from j0: row j0 of the block's reflectors is zero, and an even
     // first row keeps the GEMM operands 16-byte aligned
     const int r0 = j0, K = n - r0;
     const double* Vb = Vall.p + r0 + (size_t)j0 * Vall.ld;
-    const double* Tblk = Tb + (size_t)bi * NBB * NBB;
-    IMC_TRY(dgemm(ctx, 'T', 'N', jb, n, K, 1.0, Vb, Vall.ld, Zcur + r0, ld, 0.0, X, NBB));
-    IMC_TRY(dgemm(ctx, 'N', 'N', jb, n, jb, 1.0, Tblk, NBB, X, NBB, 0.0, X2, NBB));
-    IMC_TRY(dgemm(ctx, 'N', 'N', K, n, jb, -1.0, Vb, Vall.ld, X2, NBB, 1.0, Zcur + r0, ld));
+    const double* Tblk = Tb + (size_t)pi * NB2 * NB2;
+    IMC_TRY(dgemm(ctx, 'T', 'N', jb, n, K, 1.0, Vb, Vall.ld, Zcur + r0, ld, 0.0, X, NB2));
+    IMC_TRY(dgemm(ctx, 'N', 'N', jb, n, jb, 1.0, Tblk, NB2, X, NB2, 0.0, X2, NB2));
+    IMC_TRY(dgemm(ctx, 'N', 'N', K, n, jb, -1.0, Vb, Vall.ld, X2, NB2, 1.0, Zcur + r0, ld));
   }
   if (Zcur != Wout.p) IMC_TRY(copy_mat(ctx, Zcur, ld, Wout.p, Wout.ld, n, n));
   stage_end(ctx, ST_EIG_BT);
