@@ -173,13 +173,15 @@ def batched_patches(npatch=256, sample=16):
     Gaussian PSF sigma ~ U[0.5, 0.8] px, 24x24 outputs; U < 1e-6, tolerance
     1e-8, 40 iterations.  The concurrency (contexts side by side, each on a
     share of the SMs) is chosen by the autotuner on the first `sample`
-    patches; the whole batch is then solved once to plan every FFT size and
-    once timed (wall clock around the pool, results copied to the host)."""
+    patches, together with the cluster that finishes each tridiagonalisation;
+    the whole batch is then solved once to plan every FFT size and once timed
+    (wall clock around the pool, results copied to the host)."""
     from imcom_b200 import batch
     problems = batch.make_batch(npatch, seed0=1000)
-    k = batch.autotune(problems[:sample], candidates=(1, 2, 3, 4, 6), **BATCH_KW)
-    rates = dict(batch.LAST_RATES)
-    with batch.BatchSolver(k) as b:
+    tune = batch.autotune(problems[:sample], candidates=(1, 2, 3, 4, 6), tails=(0, 8, -1),
+                          **BATCH_KW)
+    k = tune.concurrency
+    with batch.BatchSolver(k, tail_ctas=tune.tail_ctas) as b:
         b.solve(problems, **BATCH_KW)
         r = b.solve(problems, **BATCH_KW)
     ns = [p.n for p in problems]
@@ -188,7 +190,9 @@ def batched_patches(npatch=256, sample=16):
             "n_range": [min(ns), max(ns)], "psf_sides": len({p.nps for p in problems}),
             "patches_per_s": r.patches_per_s, "pixels_per_s": r.pixels_per_s,
             "seconds": r.seconds, "concurrency": k, "sm_share": r.sm_share,
-            "autotune_patches_per_s": {str(q): v for q, v in rates.items()},
+            "tail_ctas": tune.tail_ctas,
+            "autotune_patches_per_s": {f"{q}x{'auto' if t == 0 else ('none' if t < 0 else t)}": v
+                                       for (q, t), v in tune.rates.items()},
             "timing": "wall clock around the thread pool after one warm pass"}
 
 

@@ -28,6 +28,7 @@ OPT_BISECT_KERNEL = 8
 BISECT_AUTO, BISECT_STREAM, BISECT_RESIDENT = 0, 1, 2
 OPT_BISECT_CTAS_PER_SM = 9
 OPT_SM_SHARE = 10
+OPT_TAIL_CTAS = 11
 SPLIT_INFO = ("slices_P", "slices_T", "fp64_pixels_P", "fp64_columns_T", "max_bound_US",
               "max_bound_T_from_P", "max_bound_T_product", "P_split")
 STAGES = ("spectra", "build_A", "eigen_A", "build_B", "build_P", "bisect", "build_T", "epilogue",

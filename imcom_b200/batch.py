@@ -10,8 +10,11 @@ sized for a share of the SMs (IMCOM_OPT_SM_SHARE), so K patches advance at
 once and their kernels fill the GPU together.  Patches are dealt from a
 queue, largest n first.
 
-`autotune` measures the patch throughput of candidate concurrencies on a
-sample of the batch and returns the fastest (cached per GPU and size class).
+`autotune` measures the patch throughput of candidate configurations --
+concurrency x the thread-block cluster that finishes each tridiagonalisation
+(IMCOM_OPT_TAIL_CTAS: 16 CTAs hold the longest tail but need 16 free SMs of
+one GPC, which contexts working side by side can make wait) -- on a sample of
+the batch and returns the fastest (cached per GPU and size class).
 
 Results per patch are those of `Solver.solve` (K, U/S maps, H, the
 evaluation counts); only the m-length maps are copied to the host.
@@ -24,10 +27,9 @@ import time
 from dataclasses import dataclass, field
 
 from . import _lib
-from .api import OPT_SM_SHARE, Solver
+from .api import OPT_SM_SHARE, OPT_TAIL_CTAS, Solver
 
 _TUNED: dict = {}
-LAST_RATES: dict = {}
 
 
 @dataclass
@@ -57,10 +59,11 @@ class BatchSolver:
     """A pool of `concurrency` contexts on one GPU, each with a share of the
     SMs; the contexts (plans, buffers) persist across `solve` calls."""
 
-    def __init__(self, concurrency: int = 4, device: int = 0, setup=None):
+    def __init__(self, concurrency: int = 4, device: int = 0, setup=None, tail_ctas: int = 0):
         _lib.load()
         self.k = max(1, int(concurrency))
         self.device = device
+        self.tail_ctas = int(tail_ctas)
         sms = device_sms(device)
         self.share = sms // self.k if self.k > 1 else 0
         self.solvers = []
@@ -68,6 +71,8 @@ class BatchSolver:
             s = Solver(device)
             if self.share:
                 s.set_option(OPT_SM_SHARE, self.share)
+            if self.tail_ctas:
+                s.set_option(OPT_TAIL_CTAS, self.tail_ctas)
             if setup is not None:
                 setup(s)
             self.solvers.append(s)
@@ -125,10 +130,10 @@ class BatchSolver:
 
 
 def solve_patches(problems, concurrency: int = 4, device: int = 0, setup=None,
-                  **solve_kw) -> BatchResult:
+                  tail_ctas: int = 0, **solve_kw) -> BatchResult:
     """Solve every problem of `problems` (imcom_b200.problem.Problem) with
     `concurrency` contexts side by side (a one-off pool)."""
-    with BatchSolver(min(max(1, concurrency), len(problems)), device, setup) as b:
+    with BatchSolver(min(max(1, concurrency), len(problems)), device, setup, tail_ctas) as b:
         return b.solve(problems, **solve_kw)
 
 
@@ -141,30 +146,36 @@ def size_class(problems) -> int:
     return c
 
 
-def autotune(problems, candidates=(1, 2, 4, 6, 8), device: int = 0, setup=None,
-             **solve_kw) -> int:
-    """Concurrency with the highest patch throughput on `problems` (a sample of
-    the batch).  Each candidate pool is warmed up on the sample once (plans,
-    buffers, lazy module loading) and then timed on it; the result is cached
-    per (GPU, size class).  The measured rates of the last tuning run are in
-    `LAST_RATES` (patches/s by concurrency)."""
+@dataclass
+class Tuning:
+    concurrency: int
+    tail_ctas: int                               # IMCOM_OPT_TAIL_CTAS value
+    rates: dict = field(default_factory=dict)    # patches/s by (concurrency, tail_ctas)
+
+
+def autotune(problems, candidates=(1, 2, 4, 6, 8), tails=(0, 8, -1), device: int = 0,
+             setup=None, **solve_kw) -> Tuning:
+    """The configuration (concurrency, tail cluster) with the highest patch
+    throughput on `problems` (a sample of the batch).  Each candidate pool is
+    warmed up on the sample once (plans, buffers, lazy module loading) and
+    then timed on it; the result is cached per (GPU, size class)."""
     import torch
     key = (torch.cuda.get_device_name(device), size_class(problems))
     if key in _TUNED:
         return _TUNED[key]
-    LAST_RATES.clear()
-    best, best_rate = 1, -1.0
+    best, best_rate, rates = None, -1.0, {}
     for k in candidates:
         if k > len(problems):
             break
-        with BatchSolver(k, device, setup) as b:
-            b.solve(problems, **solve_kw)
-            r = b.solve(problems, **solve_kw)
-        LAST_RATES[k] = r.patches_per_s
-        if r.patches_per_s > best_rate:
-            best, best_rate = k, r.patches_per_s
-    _TUNED[key] = best
-    return best
+        for t in tails:
+            with BatchSolver(k, device, setup, t) as b:
+                b.solve(problems, **solve_kw)
+                r = b.solve(problems, **solve_kw)
+            rates[(k, t)] = r.patches_per_s
+            if r.patches_per_s > best_rate:
+                best, best_rate = (k, t), r.patches_per_s
+    _TUNED[key] = Tuning(best[0], best[1], rates)
+    return _TUNED[key]
 
 
 def make_batch(npatch: int, seed0: int = 0, mask_frac: float = 0.02):
@@ -181,4 +192,4 @@ def make_batch(npatch: int, seed0: int = 0, mask_frac: float = 0.02):
 
 
 __all__ = ["BatchSolver", "solve_patches", "autotune", "make_batch", "BatchResult",
-           "size_class"]
+           "Tuning", "size_class"]

@@ -1316,8 +1316,8 @@ static int sytrd_gpu(imcom_ctx* ctx, DMat& Aw, DMat& Vall, double* d, double* e,
   int* flag = &sync->err;
   IMC_CUDA(cudaMemsetAsync(sync, 0, sizeof(GridSync), ctx->stream));
   // the cluster tail: 16 CTAs (non-portable cluster size) if the device can
-  // co-schedule them, else 8; tail_max = the largest trailing size whose rows
-  // fit the cluster's shared memory
+  // co-schedule them, else 8 (or as IMCOM_OPT_TAIL_CTAS asks); tail_max = the
+  // largest trailing size whose rows fit the cluster's shared memory
   int tail_ctas = 0, tail_max = 0;
   {
     int optin = 0;
@@ -1326,7 +1326,9 @@ static int sytrd_gpu(imcom_ctx* ctx, DMat& Aw, DMat& Vall, double* d, double* e,
     cudaFuncSetAttribute(trd_tail_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     cudaFuncSetAttribute(trd_tail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)limit);
+    const int want = ctx->tail_ctas;
     for (int c : {16, 8}) {
+      if (want < 0 || (want == 8 && c == 16)) continue;
       int smax = 1024;
       while (smax > 32 && (tail_smem(smax, c) > limit ||
                            (smax + c - 1) / c > TAIL_RPW * (TAIL_THREADS / 32)))

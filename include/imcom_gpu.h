@@ -84,6 +84,14 @@ typedef struct imcom_ctx imcom_ctx;
  * the same time on one GPU each take a share.  Results agree to rounding
  * (the reduction order of the eigensolver follows the grid). */
 #define IMCOM_OPT_SM_SHARE 10
+/* Thread-block cluster that finishes the tridiagonalisation once the
+ * trailing matrix fits its distributed shared memory: 0 = automatic (16 CTAs
+ * where the device can place them, else 8), 8 or 16 = that many CTAs (8 if 16
+ * cannot be placed), -1 = no cluster tail (panels to the end).  A 16-CTA
+ * cluster must find 16 free SMs in one GPC, which contexts working side by
+ * side can make wait; smaller clusters hold smaller tails.  Same results to
+ * rounding either way. */
+#define IMCOM_OPT_TAIL_CTAS 11
 
 /* ---- context ---------------------------------------------------------- */
 

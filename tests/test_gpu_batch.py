@@ -10,7 +10,10 @@ solving independent patches of uneven size (masked input pixels).
   patches).
 * One patch of a batch against the oracle.
 * Results come back in input order whatever order the queue deals them in.
-* The autotuner returns one of its candidates and caches the choice.
+* The autotuner returns the best of its candidate configurations (concurrency
+  x tail cluster) and caches the choice.
+* The tridiagonalisation tail in an 8-CTA cluster, and no cluster tail at
+  all, agree with the default.
 """
 import numpy as np
 import pytest
@@ -73,8 +76,19 @@ def test_masked_inputs_are_uneven(patches):
 def test_autotune_picks_a_candidate(patches):
     sample = patches[:2]
     batch._TUNED.clear()
-    k = batch.autotune(sample, candidates=(1, 2), **KW)
-    assert k in (1, 2)
-    assert batch._TUNED[(__import__("torch").cuda.get_device_name(0),
-                         batch.size_class(sample))] == k
-    assert batch.autotune(sample, candidates=(1, 2), **KW) == k
+    tune = batch.autotune(sample, candidates=(1, 2), tails=(0, -1), **KW)
+    assert tune.concurrency in (1, 2) and tune.tail_ctas in (0, -1)
+    assert set(tune.rates) == {(1, 0), (1, -1), (2, 0), (2, -1)}
+    assert tune.rates[(tune.concurrency, tune.tail_ctas)] == max(tune.rates.values())
+    assert batch.autotune(sample, candidates=(1, 2), tails=(0, -1), **KW) is tune
+
+
+def test_tail_cluster_settings_agree(solver, patches):
+    """The cluster tail (16 or 8 CTAs) and the panel kernel to the end give
+    the same solve to the oracle-level bars."""
+    p = patches[0]
+    r = solver.solve(p, keep=(), **KW)
+    for t in (8, -1):
+        with batch.BatchSolver(1, tail_ctas=t) as b:
+            g = b.solve([p], **KW).results[0]
+        check_close(g, r)
