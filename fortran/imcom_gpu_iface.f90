@@ -174,7 +174,10 @@ INTERFACE
   END FUNCTION
 
   ! Options (no reference counterpart), e.g. option 3 = IMCOM_OPT_PRECISION,
-  ! value 1 = IMCOM_PREC_SPLIT for the split-precision P and T
+  ! value 1 = IMCOM_PREC_SPLIT for the split-precision P and T; option 10 =
+  ! IMCOM_OPT_SM_SHARE (SMs for this context's persistent grids when several
+  ! contexts run side by side); option 11 = IMCOM_OPT_TAIL_CTAS (cluster that
+  ! finishes the tridiagonalisation: 0 auto, 16, 8, -1 none)
   INTEGER(C_INT) FUNCTION imcom_gpu_set_option(ctx, option, value) &
                                                BIND(C, NAME="imcom_gpu_set_option")
     IMPORT :: C_INT, C_PTR, C_LONG_LONG
