@@ -61,6 +61,7 @@ void eig_free(imcom_ctx* ctx) {
   if (w->U.p) cudaFree(w->U.p);
   if (w->buf) cudaFree(w->buf);
   if (w->solver) cusolverDnDestroy((cusolverDnHandle_t)w->solver);
+  if (w->trd_exec) cudaGraphExecDestroy((cudaGraphExec_t)w->trd_exec);
   delete w;
   ctx->eig = nullptr;
 }

@@ -15,6 +15,13 @@ struct EigWork {
   void* buf = nullptr;  // general scratch
   size_t buf_bytes = 0;
   void* solver = nullptr;  // cuSOLVER handle (comparison baseline only)
+  // the tridiagonalisation's launch sequence as a CUDA graph, for the size
+  // and buffers of trd_key
+  static constexpr int kTrdKey = 24;
+  long long trd_key[kTrdKey] = {};
+  void* trd_exec = nullptr;              // cudaGraphExec_t
+  unsigned long long trd_launches = 0;   // kernel launches one replay stands for
+  bool trd_graph_off = false;            // capture refused: launch directly
 };
 
 EigWork* eig_work(imcom_ctx* ctx);

@@ -1296,29 +1296,14 @@ __global__ void pack_update_kernel(const double* __restrict__ V, long long ldv,
   }
 }
 
-static int sytrd_gpu(imcom_ctx* ctx, DMat& Aw, DMat& Vall, double* d, double* e, double* tau,
-                     double* W, long long ldw, double* ypart, double* ycol, long long ldy,
-                     void* accbuf,
-                     long long spin, double* XY) {
-  const int n = (int)Aw.rows;
-  int dev = ctx->device, coop = 0;
-  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
-  if (!coop) return set_err(ctx, IMCOM_ERR_CUDA, "device lacks cooperative launch");
-  int per_sm = 0;
-  IMC_CUDA(cudaFuncSetAttribute(trd_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)TRD_SMEM));
-  IMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trd_panel_kernel, TRD_THREADS,
-                                                         TRD_SMEM));
-  if (per_sm < 1) return set_err(ctx, IMCOM_ERR_CUDA, "panel kernel does not fit on an SM");
-  int grid = sm_count(ctx);  // one CTA per SM: the cheapest grid barrier
-  TrdAcc* acc = (TrdAcc*)accbuf;
-  GridSync* sync = (GridSync*)((char*)accbuf + 2 * sizeof(TrdAcc) + 64);
-  int* flag = &sync->err;
-  IMC_CUDA(cudaMemsetAsync(sync, 0, sizeof(GridSync), ctx->stream));
-  // the cluster tail: 16 CTAs (non-portable cluster size) if the device can
-  // co-schedule them, else 8 (or as IMCOM_OPT_TAIL_CTAS asks); tail_max = the
-  // largest trailing size whose rows fit the cluster's shared memory
+// Where the cluster tail starts and with how many CTAs (host-side queries,
+// made before any stream capture).
+static void tail_config(imcom_ctx* ctx, int* tail_ctas_out, int* tail_max_out) {
+  const int dev = ctx->device;
   int tail_ctas = 0, tail_max = 0;
+  // 16 CTAs (non-portable cluster size) if the device can co-schedule them,
+  // else 8 (or as IMCOM_OPT_TAIL_CTAS asks); tail_max = the largest trailing
+  // size whose rows fit the cluster's shared memory
   {
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
@@ -1354,7 +1339,24 @@ static int sytrd_gpu(imcom_ctx* ctx, DMat& Aw, DMat& Vall, double* d, double* e,
     }
     cudaGetLastError();  // an unsupported cluster size only disables the tail
   }
-  bool tail_done = false, panels = false;
+  *tail_ctas_out = tail_ctas;
+  *tail_max_out = tail_max;
+}
+
+// The launch sequence of the tridiagonalisation: panels, their trailing
+// updates and the cluster tail.  `capturing`: recorded into a graph, so the
+// periodic host check of the barrier's error word is left to the caller.
+static int sytrd_launches(imcom_ctx* ctx, DMat& Aw, DMat& Vall, double* d, double* e,
+                          double* tau, double* W, long long ldw, double* ypart, double* ycol,
+                          long long ldy, void* accbuf, long long spin, double* XY, int tail_ctas,
+                          int tail_max, bool capturing) {
+  const int n = (int)Aw.rows;
+  int grid = sm_count(ctx);  // one CTA per SM: the cheapest grid barrier
+  TrdAcc* acc = (TrdAcc*)accbuf;
+  GridSync* sync = (GridSync*)((char*)accbuf + 2 * sizeof(TrdAcc) + 64);
+  int* flag = &sync->err;
+  IMC_CUDA(cudaMemsetAsync(sync, 0, sizeof(GridSync), ctx->stream));
+  bool tail_done = false;
   for (int k = 0; k < n - 1; k += NB) {
     if (tail_ctas && n - k <= tail_max) {
       const int S = n - k;
@@ -1376,7 +1378,6 @@ static int sytrd_gpu(imcom_ctx* ctx, DMat& Aw, DMat& Vall, double* d, double* e,
       tail_done = true;
       break;
     }
-    panels = true;
     const int b = std::min(NB, n - 1 - k);
     IMC_CUDA(cudaMemsetAsync(accbuf, 0, 2 * sizeof(TrdAcc), ctx->stream));
     static_assert(2 * sizeof(TrdAcc) + 64 + sizeof(GridSync) <= 4096, "panel scratch");
@@ -1401,23 +1402,94 @@ static int sytrd_gpu(imcom_ctx* ctx, DMat& Aw, DMat& Vall, double* d, double* e,
                              Aw.p + t0 + (long long)t0 * Aw.ld, Aw.ld));
     }
     // a timed-out barrier ends the factorisation with an error
-    if ((k / NB) % 16 == 15) {
+    if (!capturing && (k / NB) % 16 == 15) {
       int h = 0;
       IMC_CUDA(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
       IMC_CUDA(cudaStreamSynchronize(ctx->stream));
       if (h) return set_err(ctx, IMCOM_ERR_EIGEN, "tridiagonalisation grid barrier timed out");
     }
   }
-  if (panels) {
-    int h = 0;
-    IMC_CUDA(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    IMC_CUDA(cudaStreamSynchronize(ctx->stream));
-    if (h) return set_err(ctx, IMCOM_ERR_EIGEN, "tridiagonalisation grid barrier timed out");
-  }
   if (!tail_done) {  // the tail writes the last diagonal entry itself
     set_last_diag_kernel<<<1, 1, 0, ctx->stream>>>(Aw.p, Aw.ld, n, d);
     IMC_LAUNCH();
   }
+  return 0;
+}
+
+// Householder tridiagonalisation (lower) of Aw into d, e, tau and the
+// reflectors Vall.  The launch sequence (about four launches per panel) is
+// replayed as a CUDA graph once the same size and buffers come back: the
+// first call at a key runs it directly, the second captures and instantiates
+// it, later calls launch the graph.  A capture the driver refuses leaves the
+// direct path in place.
+static int sytrd_gpu(imcom_ctx* ctx, DMat& Aw, DMat& Vall, double* d, double* e, double* tau,
+                     double* W, long long ldw, double* ypart, double* ycol, long long ldy,
+                     void* accbuf, long long spin, double* XY) {
+  const int n = (int)Aw.rows;
+  int dev = ctx->device, coop = 0;
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+  if (!coop) return set_err(ctx, IMCOM_ERR_CUDA, "device lacks cooperative launch");
+  int per_sm = 0;
+  IMC_CUDA(cudaFuncSetAttribute(trd_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)TRD_SMEM));
+  IMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trd_panel_kernel, TRD_THREADS,
+                                                         TRD_SMEM));
+  if (per_sm < 1) return set_err(ctx, IMCOM_ERR_CUDA, "panel kernel does not fit on an SM");
+  int tail_ctas = 0, tail_max = 0;
+  tail_config(ctx, &tail_ctas, &tail_max);
+  GridSync* sync = (GridSync*)((char*)accbuf + 2 * sizeof(TrdAcc) + 64);
+  EigWork* ew = eig_work(ctx);
+  const long long key[] = {n, (long long)(uintptr_t)Aw.p, Aw.ld, (long long)(uintptr_t)Vall.p,
+                           Vall.ld, (long long)(uintptr_t)d, (long long)(uintptr_t)e,
+                           (long long)(uintptr_t)tau, (long long)(uintptr_t)W, ldw,
+                           (long long)(uintptr_t)ypart, (long long)(uintptr_t)ycol, ldy,
+                           (long long)(uintptr_t)accbuf, spin, (long long)(uintptr_t)XY,
+                           sm_count(ctx), tail_ctas, tail_max};
+  constexpr int NKEY = (int)(sizeof(key) / sizeof(key[0]));
+  static_assert(NKEY <= EigWork::kTrdKey, "graph key size");
+  const bool same = std::equal(key, key + NKEY, ew->trd_key);
+  if (!same) {
+    if (ew->trd_exec) cudaGraphExecDestroy((cudaGraphExec_t)ew->trd_exec);
+    ew->trd_exec = nullptr;
+    std::copy(key, key + NKEY, ew->trd_key);
+  }
+  if (ew->trd_exec) {
+    IMC_CUDA(cudaGraphLaunch((cudaGraphExec_t)ew->trd_exec, ctx->stream));
+    __atomic_fetch_add(&g_launches, ew->trd_launches, __ATOMIC_RELAXED);
+  } else if (same && !ew->trd_graph_off) {
+    // second call at this key: capture, instantiate, launch
+    cudaGraph_t graph = nullptr;
+    const unsigned long long l0 = __atomic_load_n(&g_launches, __ATOMIC_RELAXED);
+    bool ok = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed) == cudaSuccess;
+    int st = 0;
+    if (ok) {
+      st = sytrd_launches(ctx, Aw, Vall, d, e, tau, W, ldw, ypart, ycol, ldy, accbuf, spin, XY,
+                          tail_ctas, tail_max, true);
+      ok = cudaStreamEndCapture(ctx->stream, &graph) == cudaSuccess && st == 0 && graph;
+    }
+    cudaGraphExec_t exec = nullptr;
+    if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    if (ok) {
+      ew->trd_exec = exec;
+      ew->trd_launches = __atomic_load_n(&g_launches, __ATOMIC_RELAXED) - l0;
+      IMC_CUDA(cudaGraphLaunch(exec, ctx->stream));
+    } else {
+      ew->trd_graph_off = true;  // run directly from now on
+      ctx->err.clear();
+      IMC_TRY(sytrd_launches(ctx, Aw, Vall, d, e, tau, W, ldw, ypart, ycol, ldy, accbuf, spin,
+                             XY, tail_ctas, tail_max, false));
+    }
+  } else {
+    IMC_TRY(sytrd_launches(ctx, Aw, Vall, d, e, tau, W, ldw, ypart, ycol, ldy, accbuf, spin, XY,
+                           tail_ctas, tail_max, false));
+  }
+  // a timed-out grid barrier ends the factorisation with an error
+  int h = 0;
+  IMC_CUDA(cudaMemcpyAsync(&h, &sync->err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (h) return set_err(ctx, IMCOM_ERR_EIGEN, "tridiagonalisation grid barrier timed out");
   return 0;
 }
 

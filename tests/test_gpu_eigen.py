@@ -57,3 +57,30 @@ def test_eigen_dc_matches_library_n2048(solver):
     assert np.max(np.abs(L1 - L2)) < 1e-12 * L2.max()
     assert np.max(np.abs(A @ Q1 - Q1 * L1)) < 1e-12 * L2.max()
     assert np.max(np.abs(Q1.T @ Q1 - np.eye(2048))) < 1e-12
+
+
+@pytest.mark.parametrize("tail", [0, -1])
+def test_tridiagonalisation_graph_replay(solver, tail):
+    """The first eigensolve at a size runs the tridiagonalisation's launches
+    directly, the second captures them into a CUDA graph and the third
+    replays it (with and without the cluster tail): all three meet the parity
+    bars, and each adds the same number of launches to the library's
+    counter."""
+    from imcom_b200.api import OPT_TAIL_CTAS
+    A = spectrum_matrix(1500, "decay", seed=3)
+    solver.set_option(OPT_TAIL_CTAS, tail)
+    try:
+        out, counts = [], []
+        for _ in range(3):
+            c0 = solver.launch_count()
+            out.append(run_eigen(solver, A, EIGH_DC))
+            counts.append(solver.launch_count() - c0)
+    finally:
+        solver.set_option(OPT_TAIL_CTAS, 0)
+    ref = np.linalg.eigvalsh(A)[::-1]
+    scale = np.abs(ref).max()
+    for Q, L, _ in out:
+        assert np.max(np.abs(L - ref)) < 1e-12 * scale
+        assert np.max(np.abs(A @ Q - Q * L)) < 1e-12 * scale
+        assert np.max(np.abs(Q.T @ Q - np.eye(A.shape[0]))) < 1e-12
+    assert counts[0] == counts[1] == counts[2]
