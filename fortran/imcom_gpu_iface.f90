@@ -207,6 +207,18 @@ INTERFACE
     REAL(C_DOUBLE), DIMENSION(8) :: info8
   END FUNCTION
 
+  ! Eigendecomposition of `count` small symmetric positive semi-definite
+  ! matrices (n <= 112) in one launch, one-sided Jacobi; ascending per matrix
+  INTEGER(C_INT) FUNCTION imcom_gpu_eigh_jacobi_batched(ctx, n, count, A, Q, L, sweeps) &
+                                                        BIND(C, NAME="imcom_gpu_eigh_jacobi_batched")
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: ctx
+    INTEGER(C_INT), VALUE :: n, count
+    REAL(C_DOUBLE), DIMENSION(n, n, count) :: A, Q
+    REAL(C_DOUBLE), DIMENSION(n, count) :: L
+    INTEGER(C_INT), DIMENSION(count) :: sweeps
+  END FUNCTION
+
 END INTERFACE
 
 TYPE(C_PTR), SAVE :: imcom_gpu_ctx = C_NULL_PTR

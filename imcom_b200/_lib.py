@@ -50,6 +50,7 @@ SIGNATURES = {
     "imcom_gpu_split_info": (_i, [_p, _p]),
     "imcom_gpu_split_pixels": (_i, [_p, _p, _p]),
     "imcom_gpu_build_P_noalloc": (_i, [_p, _ll, _p, _ll, _p, _ll, _i, _i, _p]),
+    "imcom_gpu_eigh_jacobi_batched": (_i, [_p, _i, _i, _p, _p, _p, _p]),
     "imcom_gpu_device_buffer": (_i, [_p, C.c_char, C.POINTER(_p), C.POINTER(_ll)]),
     "imcom_gpu_get_stream": (_i, [_p, C.POINTER(_p)]),
     "imcom_gpu_launch_count": (_i, [_p, C.POINTER(_ll)]),

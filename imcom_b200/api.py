@@ -129,6 +129,23 @@ class Solver:
         self._call("imcom_gpu_launch_count", C.byref(v))
         return int(v.value)
 
+    def eigh_jacobi_batched(self, A):
+        """Eigendecomposition of a stack of small symmetric positive
+        semi-definite matrices A (count, n, n), n <= 112, one thread block each
+        (one-sided Jacobi).  Returns Q (count, n, n) with eigenvectors in
+        columns, L (count, n) and the sweeps used, ascending per matrix."""
+        A = np.asarray(A, dtype=np.float64)
+        if A.ndim == 2:
+            A = A[None]
+        count, n = A.shape[0], A.shape[1]
+        At = np.ascontiguousarray(np.transpose(A, (0, 2, 1)))  # column-major per matrix
+        Q = np.zeros_like(At)
+        L = np.zeros((count, n))
+        sw = np.zeros(count, dtype=np.int32)
+        self._call("imcom_gpu_eigh_jacobi_batched", int(n), int(count), _ptr(At), _ptr(Q), _ptr(L),
+                   _ptr(sw))
+        return np.transpose(Q, (0, 2, 1)), L, sw
+
     def device_buffer(self, which: str):
         p, ld = C.c_void_p(), C.c_longlong()
         self._call("imcom_gpu_device_buffer", which.encode(), C.byref(p), C.byref(ld))

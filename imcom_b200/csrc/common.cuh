@@ -111,6 +111,8 @@ struct imcom_ctx {
   int bisect_ctas = 0;  // CTAs per SM of the streaming pixel kernels (0: all pixels at once)
   int sm_share = 0;     // SMs for persistent / cooperative grids (0: the whole device)
   int tail_ctas = 0;    // cluster of the tridiagonalisation tail (0 auto, -1 none, 8, 16)
+  void* jac_buf = nullptr;  // batched Jacobi: matrices, vectors, values, status
+  size_t jac_bytes = 0;
   int split_SP = 7, split_ST = 6;        // digit slices of the P and T products
   double split_tol_us = 1e-7, split_tol_t = 1e-8;
   imcom::SplitOp sq_P, sq_T, sb_P, spt_T;  // Q columns, Q rows, B, P~

@@ -6,7 +6,8 @@
 // point (imcom_gpu_set_option(IMCOM_OPT_EIGENSOLVER)):
 //   IMCOM_EIGH_DC       own FP64 blocked Householder tridiagonalisation +
 //                       divide and conquer + back-transformation (eigen_dc.cu)
-//   IMCOM_EIGH_JACOBI   own FP64 cyclic Jacobi for small systems (eigen_jacobi.cu)
+//   IMCOM_EIGH_JACOBI   own FP64 one-sided Jacobi for small systems, n <= 112
+//                       (eigen_jacobi.cu)
 //   IMCOM_EIGH_LIBRARY  cuSOLVER syevd, kept only as a comparison baseline.
 // All of them return ascending eigenpairs in a work matrix; reverse_kernel
 // writes them to Q and L in the reference's descending order.

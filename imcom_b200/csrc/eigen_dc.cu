@@ -1728,9 +1728,4 @@ int eigen_dc(imcom_ctx* ctx, const DMat& A, DMat& Wout, double* wout) {
   return 0;
 }
 
-int eigen_jacobi(imcom_ctx* ctx, const DMat& A, DMat& W, double* w) {
-  (void)A; (void)W; (void)w;
-  return set_err(ctx, IMCOM_ERR_STATE, "Jacobi eigensolver not built");
-}
-
 }  // namespace imcom

@@ -48,7 +48,7 @@ typedef struct imcom_ctx imcom_ctx;
 
 /* Eigensolver selection for imcom_gpu_set_option(IMCOM_OPT_EIGENSOLVER). */
 #define IMCOM_EIGH_DC 0         /* own tridiagonalisation + divide & conquer  */
-#define IMCOM_EIGH_JACOBI 1     /* own one-sided Jacobi (small n)             */
+#define IMCOM_EIGH_JACOBI 1     /* own one-sided Jacobi (n <= 112)            */
 #define IMCOM_EIGH_LIBRARY 2    /* cuSOLVER syevd: comparison baseline only   */
 
 /* Options for imcom_gpu_set_option. */
@@ -285,6 +285,27 @@ int imcom_gpu_split_pixels(imcom_ctx* ctx, int* fp64_P, int* fp64_T);
 int imcom_gpu_build_P_noalloc(const double* dQ, long long ldq, const double* dB,
                               long long ldb, double* dP, long long ldp, int n, int m,
                               void* stream);
+
+/* ---- batched eigendecomposition of small systems ------------------------ */
+
+/* Largest n of the one-sided Jacobi eigensolver (IMCOM_EIGH_JACOBI and the
+ * batched call below): the matrix and its rotations fill one CTA's shared
+ * memory. */
+#define IMCOM_JACOBI_MAX_N 112
+
+/* Eigendecomposition of `count` symmetric positive semi-definite n x n
+ * matrices (n <= IMCOM_JACOBI_MAX_N), one thread block each, by one-sided
+ * (Hestenes) Jacobi: the method IMCOM_EIGH_JACOBI applies to A, for many
+ * small patches in one launch.  No reference counterpart: the reference
+ * decomposes one A per run with DSYEVR (imcom_matrix.f90:617-643).
+ * A: count matrices, column-major, contiguous (matrix b at A + b n^2);
+ * Q: the eigenvectors in the same layout; L: count x n eigenvalues; both in
+ * ascending order per matrix.  sweeps (may be NULL): Jacobi sweeps used per
+ * matrix.  Host arrays; the call returns when Q and L are written.
+ * Returns 0, -k for a bad argument k, IMCOM_ERR_EIGEN if a matrix does not
+ * converge in 60 sweeps, IMCOM_ERR_CUDA / IMCOM_ERR_ALLOC. */
+int imcom_gpu_eigh_jacobi_batched(imcom_ctx* ctx, int n, int count, const double* A,
+                                  double* Q, double* L, int* sweeps);
 
 /* ---- device views (for callers that keep data on the GPU) -------------- */
 

@@ -84,3 +84,42 @@ def test_tridiagonalisation_graph_replay(solver, tail):
         assert np.max(np.abs(A @ Q - Q * L)) < 1e-12 * scale
         assert np.max(np.abs(Q.T @ Q - np.eye(A.shape[0]))) < 1e-12
     assert counts[0] == counts[1] == counts[2]
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 31, 33, 72, 112])
+@pytest.mark.parametrize("kind", ["decay", "cluster", "multiple"])
+def test_eigen_jacobi(solver, n, kind):
+    """The one-sided Jacobi eigensolver (IMCOM_EIGH_JACOBI, n <= 112) on the
+    positive semi-definite spectra, to the same bars as the D&C solver."""
+    from imcom_b200 import EIGH_JACOBI
+    A = spectrum_matrix(n, kind, seed=n)
+    try:
+        Q, L, _ = run_eigen(solver, A, EIGH_JACOBI)
+    finally:
+        solver.set_eigensolver(EIGH_DC)
+    ref = np.linalg.eigvalsh(A)[::-1]
+    scale = max(np.abs(ref).max(), 1e-300)
+    assert np.all(np.diff(L) <= 0)
+    assert np.max(np.abs(L - ref)) < 1e-12 * scale
+    assert np.max(np.abs(Q.T @ Q - np.eye(n))) < 1e-12
+    assert np.max(np.abs(A @ Q - Q * L)) < 1e-12 * scale
+
+
+def test_eigh_jacobi_batched(solver):
+    """Many small systems in one launch (one thread block each): every
+    matrix of the stack meets the bars; n above the limit is rejected."""
+    from imcom_b200 import ImcomError
+    mats = [spectrum_matrix(64, kind, seed=s) for s in range(4)
+            for kind in ("decay", "cluster", "multiple")]
+    Q, L, sweeps = solver.eigh_jacobi_batched(np.stack(mats))
+    assert Q.shape == (12, 64, 64) and L.shape == (12, 64)
+    assert np.all(sweeps > 0)
+    for A, Qb, Lb in zip(mats, Q, L):
+        ref = np.linalg.eigvalsh(A)
+        scale = np.abs(ref).max()
+        assert np.all(np.diff(Lb) >= 0)
+        assert np.max(np.abs(Lb - ref)) < 1e-12 * scale
+        assert np.max(np.abs(Qb.T @ Qb - np.eye(64))) < 1e-12
+        assert np.max(np.abs(A @ Qb - Qb * Lb)) < 1e-12 * scale
+    with pytest.raises(ImcomError):
+        solver.eigh_jacobi_batched(np.eye(113))

@@ -152,3 +152,21 @@ def test_full_solve_small_vs_oracle(gs, UnotS, US, tol):
     assert np.allclose(r.U, r_o.U, rtol=1e-6)
     assert np.allclose(r.S, r_o.S, rtol=1e-6)
     assert rel(r.H, r_o.H) < 1e-8
+
+
+def test_tiny_solve_with_jacobi_vs_oracle(solver):
+    """The whole solve of the tiny workload (n = 72) with the one-sided Jacobi
+    eigensolver against the oracle (LAPACK DSYEVR inside)."""
+    from imcom_b200 import EIGH_DC, EIGH_JACOBI
+    from oracle import oracle as Orc
+    prob = synth.make("tiny", 4)
+    r = Orc.solve(prob, UnotS=True, US_max=1e-6, US_tol=1e-8, maxnits=53)
+    solver.set_eigensolver(EIGH_JACOBI)
+    try:
+        g = solver.solve(prob, True, 1e-6, 1e-8, 53)
+    finally:
+        solver.set_eigensolver(EIGH_DC)
+    assert np.max(np.abs(g.K / r.K - 1)) < 1e-6
+    assert np.max(np.abs(g.US / r.US - 1)) < 1e-6
+    assert np.linalg.norm(g.T - r.T) <= 1e-8 * np.linalg.norm(r.T)
+    assert np.linalg.norm(g.H - r.H) <= 1e-8 * np.linalg.norm(r.H)
