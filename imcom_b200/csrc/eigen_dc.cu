@@ -31,9 +31,7 @@
 //    tau = lambda - d_org the nearest pole is kept exact and the rest
 //    linearised, so each step solves a quadratic), the
 //    Gu-Eisenstat z-hat (dlaed3) and the eigenvector columns (one warp each),
-//    then Q_node = Q_old(:, nondeflated) U as two DMMA GEMMs per node: the
-//    columns are ordered by the child whose rows they occupy (dlaed2's
-//    types), so the zero blocks of the children's eigenvectors are skipped.
+//    then Q_node = Q_old(:, nondeflated) U as one DMMA GEMM per node.
 // 3. Back-transformation (dormtr): Z <- (I - V T V^T) Z over blocks of 256
 //    reflectors, three GEMMs per block.  T is built from V^T V: dlarft on
 //    each 128-reflector half, joined by T12 = -T1 (V1^T V2) T2.
@@ -880,10 +878,6 @@ struct DcWork {
   // per node
   int *kcnt, *ndef, *nrot;
   double* rho;
-  // non-deflated column q: which child's rows it occupies (0 left, 1 both
-  // after a deflation rotation across children, 2 right) and its slot in the
-  // merge product ordered left | both | right; per node (k_left, k_both)
-  int *ndtype, *pos, *klm;
 };
 
 // z, merge ranks of the two sorted child lists, scatter into sorted order.
@@ -959,11 +953,10 @@ __global__ void __launch_bounds__(256) dc_deflate_kernel(const Node* nodes, DcWo
     __syncthreads();
   }
   const double tol = 8.0 * EPS * fmax(sh_d[0], rho * sh_z[0]);
-  int k = 0, ndef = 0, nrot = 0, kl = 0, km = 0;
+  int k = 0, ndef = 0, nrot = 0;
   bool have = false;      // a previous non-deflated entry exists
   double dp = 0.0, zp = 0.0;
-  int pp = 0, tp = 0;     // tp: child type of the previous entry's column
-  const int n1 = nd.n1;
+  int pp = 0;
   for (int c0 = 0, b = 0; c0 < nm; c0 += DEF_CH, b ^= 1) {
     if (threadIdx.x >= 32) {
       const int n0 = c0 + DEF_CH;
@@ -977,7 +970,6 @@ __global__ void __launch_bounds__(256) dc_deflate_kernel(const Node* nodes, DcWo
       for (int jj = 0; jj < cn; ++jj) {
         const double dj = cd[b][jj], zj = cz[b][jj];
         const int pj = cpm[b][jj];
-        const int tj = (pj < n1) ? 0 : 2;
         if (rho * fabs(zj) <= tol) {
           wk.defd[s + ndef] = dj;
           wk.defcol[s + ndef] = pj;
@@ -989,7 +981,6 @@ __global__ void __launch_bounds__(256) dc_deflate_kernel(const Node* nodes, DcWo
           dp = dj;
           zp = zj;
           pp = pj;
-          tp = tj;
           continue;
         }
         double sv = zp, cv = zj;
@@ -1009,19 +1000,14 @@ __global__ void __launch_bounds__(256) dc_deflate_kernel(const Node* nodes, DcWo
           dp = dn;
           zp = tau;
           pp = pj;
-          tp = (tp == tj) ? tj : 1;  // the kept column now mixes both columns
         } else {
           wk.dl[s + k] = dp;
           wk.zz[s + k] = zp;
           wk.ndcol[s + k] = pp;
-          wk.ndtype[s + k] = tp;
-          kl += (tp == 0);
-          km += (tp == 1);
           ++k;
           dp = dj;
           zp = zj;
           pp = pj;
-          tp = tj;
         }
       }
     }
@@ -1032,14 +1018,9 @@ __global__ void __launch_bounds__(256) dc_deflate_kernel(const Node* nodes, DcWo
     wk.dl[s + k] = dp;
     wk.zz[s + k] = zp;
     wk.ndcol[s + k] = pp;
-    wk.ndtype[s + k] = tp;
-    kl += (tp == 0);
-    km += (tp == 1);
     ++k;
   }
   wk.kcnt[blockIdx.x] = k;
-  wk.klm[2 * blockIdx.x] = kl;
-  wk.klm[2 * blockIdx.x + 1] = km;
   wk.ndef[blockIdx.x] = ndef;
   wk.nrot[blockIdx.x] = nrot;
 }
@@ -1188,58 +1169,27 @@ __global__ void dc_vectors_kernel(const Node* nodes, DcWork wk, double* U, long 
   const double* dl = wk.dl + s;
   const double dorg = dl[wk.org[s + j]], tau = wk.tau[s + j];
   double* col = U + s + (long long)(s + j) * ldu;
-  // rows in the merge product's order (pos): left | both | right
-  const int* pos = wk.pos + s;
   double nrm = 0.0;
   for (int q = lane; q < k; q += 32) {
     double v = wk.zhat[s + q] / ((dl[q] - dorg) - tau);
-    col[pos[q]] = v;
+    col[q] = v;
     nrm += v * v;
   }
   nrm = sqrt(warp_sum(nrm));
   __syncwarp();
-  for (int q = lane; q < k; q += 32) col[pos[q]] = col[pos[q]] / nrm;
+  for (int q = lane; q < k; q += 32) col[q] = col[q] / nrm;
 }
 
-// G(:, pos(jj)) = Z(node rows, ndcol(jj)) for the non-deflated columns.
+// G(:, jj) = Z(node rows, ndcol(jj)) for the non-deflated columns.
 __global__ void dc_gather_kernel(const Node* nodes, const double* Z, long long ldz, DcWork wk,
                                  double* G, long long ldg) {
   const Node nd = nodes[blockIdx.z];
   const int jj = blockIdx.y;
   if (jj >= wk.kcnt[blockIdx.z]) return;
   const int s = nd.s;
-  const int col = wk.ndcol[s + jj], dst = wk.pos[s + jj];
+  const int col = wk.ndcol[s + jj];
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nd.nm; r += gridDim.x * blockDim.x)
-    G[(s + r) + (long long)(s + dst) * ldg] = Z[(s + r) + (long long)(s + col) * ldz];
-}
-
-// Slot of each non-deflated column in the merge product: left-child columns
-// first, then the columns mixed by a deflation rotation, then right-child
-// columns, each group in its original order (LAPACK dlaed2's column types),
-// so the product splits into the top rows x (left | both) and the bottom rows
-// x (both | right): the zero blocks of the children's eigenvectors are
-// skipped.  One CTA per node: per-thread segment counts, a scan, the slots.
-__global__ void __launch_bounds__(256) dc_order_kernel(const Node* nodes, DcWork wk) {
-  const int b = blockIdx.x, s = nodes[b].s, k = wk.kcnt[b];
-  const int kl = wk.klm[2 * b], km = wk.klm[2 * b + 1];
-  __shared__ int cnt[3][256];
-  const int per = (k + 255) / 256;
-  const int q0 = min(k, (int)threadIdx.x * per), q1 = min(k, q0 + per);
-  int c[3] = {0, 0, 0};
-  for (int q = q0; q < q1; ++q) ++c[wk.ndtype[s + q]];
-  for (int t = 0; t < 3; ++t) cnt[t][threadIdx.x] = c[t];
-  __syncthreads();
-  if (threadIdx.x < 3) {
-    int acc = 0;
-    for (int i = 0; i < 256; ++i) {
-      const int v = cnt[threadIdx.x][i];
-      cnt[threadIdx.x][i] = acc;
-      acc += v;
-    }
-  }
-  __syncthreads();
-  int base[3] = {cnt[0][threadIdx.x], kl + cnt[1][threadIdx.x], kl + km + cnt[2][threadIdx.x]};
-  for (int q = q0; q < q1; ++q) wk.pos[s + q] = base[wk.ndtype[s + q]]++;
+    G[(s + r) + (long long)(s + jj) * ldg] = Z[(s + r) + (long long)(s + col) * ldz];
 }
 
 // Rank of each new eigenvalue within its node (stable, O(nm) per element).
@@ -1575,7 +1525,7 @@ int eigen_dc(imcom_ctx* ctx, const DMat& A, DMat& Wout, double* wout) {
   size_t o_XY = take((size_t)ldw * 4 * NB * 8);
   size_t o_acc = take(4096);
   size_t o_split = take((size_t)n * 4), o_nodes = take((size_t)n * sizeof(Node));
-  size_t o_wk = take(((size_t)n * 8 + 16) * 9 + ((size_t)n * 4 + 16) * 12 + ((size_t)n * 24 + 32) +
+  size_t o_wk = take(((size_t)n * 8 + 16) * 9 + ((size_t)n * 4 + 16) * 8 + ((size_t)n * 24 + 32) +
                      4096);
   const size_t nblk_bt = (size_t)(n - 1 + NBB - 1) / NBB + 1;
   const size_t npair_bt = (nblk_bt + 1) / 2;
@@ -1655,8 +1605,6 @@ int eigen_dc(imcom_ctx* ctx, const DMat& A, DMat& Wout, double* wout) {
     wk.rcol = (int2*)p; adv((size_t)n * 8);
     wk.kcnt = iv(); wk.ndef = iv(); wk.nrot = iv();
     wk.rho = dv();
-    wk.ndtype = iv(); wk.pos = iv();
-    wk.klm = (int*)p; adv((size_t)n * 8);
   }
   double* w = wout;
   // leaves
@@ -1689,8 +1637,6 @@ int eigen_dc(imcom_ctx* ctx, const DMat& A, DMat& Wout, double* wout) {
     IMC_LAUNCH();
     dc_deflate_kernel<<<nn_, 256, 0, ctx->stream>>>(dnodes, wk);
     IMC_LAUNCH();
-    dc_order_kernel<<<nn_, 256, 0, ctx->stream>>>(dnodes, wk);
-    IMC_LAUNCH();
     dc_rotate_kernel<<<ge, 256, 0, ctx->stream>>>(dnodes, Zcur, ld, wk);
     IMC_LAUNCH();
     dim3 gw((maxnm + 7) / 8, nn_);
@@ -1703,26 +1649,16 @@ int eigen_dc(imcom_ctx* ctx, const DMat& A, DMat& Wout, double* wout) {
     dim3 gg((maxnm + 255) / 256, maxnm, nn_);
     dc_gather_kernel<<<gg, 256, 0, ctx->stream>>>(dnodes, Zcur, ld, wk, Gm, UO.ld);
     IMC_LAUNCH();
-    std::vector<int> kh(nn_), klm(2 * (size_t)nn_);
+    std::vector<int> kh(nn_);
     IMC_CUDA(cudaMemcpyAsync(kh.data(), wk.kcnt, nn_ * 4, cudaMemcpyDeviceToHost, ctx->stream));
-    IMC_CUDA(cudaMemcpyAsync(klm.data(), wk.klm, 2 * (size_t)nn_ * 4, cudaMemcpyDeviceToHost,
-                             ctx->stream));
     IMC_CUDA(cudaStreamSynchronize(ctx->stream));
-    // OUT(node) = G(node) U(node): the new non-deflated eigenvectors.  G's
-    // columns are ordered left | both | right (U's rows alike), so the top
-    // n1 rows need only the left and mixed columns and the bottom rows only
-    // the mixed and right ones (LAPACK dlaed3).
+    // OUT(node) = G(node) U(node): the new non-deflated eigenvectors
     for (int b = 0; b < nn_; ++b) {
       const Node& x = nodes[b];
-      const int k = kh[b];
-      if (k == 0) continue;
-      const int kl = klm[2 * b], km = klm[2 * b + 1], kr = k - kl - km;
-      const size_t base = (size_t)x.s + (size_t)x.s * UO.ld;
-      IMC_TRY(dgemm(ctx, 'N', 'N', x.n1, k, kl + km, 1.0, Gm + base, UO.ld, Ub + base, UO.ld, 0.0,
-                    OUT + base, UO.ld));
-      IMC_TRY(dgemm(ctx, 'N', 'N', x.nm - x.n1, k, km + kr, 1.0,
-                    Gm + base + x.n1 + (size_t)kl * UO.ld, UO.ld, Ub + base + kl, UO.ld, 0.0,
-                    OUT + base + x.n1, UO.ld));
+      if (kh[b] == 0) continue;
+      IMC_TRY(dgemm(ctx, 'N', 'N', x.nm, kh[b], kh[b], 1.0, Gm + x.s + (size_t)x.s * UO.ld,
+                    UO.ld, Ub + x.s + (size_t)x.s * UO.ld, UO.ld, 0.0,
+                    OUT + x.s + (size_t)x.s * UO.ld, UO.ld));
     }
     dc_rank_kernel<<<ge, 256, 0, ctx->stream>>>(dnodes, wk);
     IMC_LAUNCH();
