@@ -113,20 +113,48 @@ __global__ void oz_digit_kernel(const double* __restrict__ X, long long ld, long
     e = live ? ex + 2 : 0;
     if (kb == 0 && kh == 0) scale[r] = scalbn(1.0, e);
   }
+  // x 2^(7 + 8 (S-1) - e) in one exact multiply when the power of two is a
+  // normal double (always for these operands), else two exact scalings
+  const int sh = 7 + 8 * (S - 1) - e;
+  const bool one_mul = sh > -1000 && sh < 1000;
+  const double mul = one_mul ? scalbn(1.0, sh) : 0.0;
   int8_t d[S][16];
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
     const long long k = kbase + j;
     double x = 0.0;
     if (live && k < K) x = COLS ? X[k + r * ld] : X[r + k * ld];
-    long long N = __double2ll_rn(scalbn(scalbn(x, -e), 7 + 8 * (S - 1)));
+    const double y = one_mul ? x * mul : scalbn(scalbn(x, -e), 7 + 8 * (S - 1));
+    long long N = __double2ll_rn(y);
+    if (S >= 4 && S <= 7) {
+      // |N| < 2^54: N = 2^24 H + L with 0 <= L < 2^24 and |H| < 2^30, so the
+      // three lowest balanced digits come from L in 32-bit arithmetic and
+      // carry into H (the same digits as the 64-bit recursion below)
+      int c = (int)(N & 0xFFFFFF);
+      int hi = (int)(N >> 24);
 #pragma unroll
-    for (int s = S - 1; s >= 1; --s) {
-      const long long q = ((N + 128) & 255) - 128;
-      d[s][j] = (int8_t)q;
-      N = (N - q) >> 8;
+      for (int s = S - 1; s >= 1; --s) {
+        if (s >= S - 3) {
+          const int q = ((c + 128) & 255) - 128;
+          d[s][j] = (int8_t)q;
+          c = (c - q) >> 8;
+          if (s == S - 3) hi += c;  // the carry out of the low 24 bits
+        } else {
+          const int q = ((hi + 128) & 255) - 128;
+          d[s][j] = (int8_t)q;
+          hi = (hi - q) >> 8;
+        }
+      }
+      d[0][j] = (int8_t)hi;
+    } else {
+#pragma unroll
+      for (int s = S - 1; s >= 1; --s) {
+        const long long q = ((N + 128) & 255) - 128;
+        d[s][j] = (int8_t)q;
+        N = (N - q) >> 8;
+      }
+      d[0][j] = (int8_t)N;
     }
-    d[0][j] = (int8_t)N;
   }
   const size_t tile = (size_t)R * OZ_KB;
   int8_t* base = dig + ((size_t)(rb * KB + kb) * S) * tile + (rr >> 3) * 256 + kh * 128 +
