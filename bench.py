@@ -22,10 +22,11 @@ T -> S, H with Q, L and B resident, the reference's cached path).
   e2e    the same metric through the C-ABI with pinned host buffers: inputs
          copied in and H, K, U, S and T copied out inside every step.
 
-``batch`` (N=1 only): the batched-patch workload -- 256 independent patches
-of uneven n (990-2270, masked pixels) solved by a pool of contexts, each on a
-share of the SMs, concurrency chosen by the autotuner; patches/s and output
-pixels/s, wall clock.
+``batch``: the batched-patch workload -- 256 independent patches of uneven n
+(990-2270, masked pixels) solved by a pool of contexts per GPU, each on a
+share of the SMs, concurrency chosen by the autotuner; with N GPUs the
+patches are split across ranks by cost (no data-path collective); patches/s
+and output pixels/s over the slowest rank's wall-clock time.
 
 ``--impl reference`` times the CPU oracle (the reference's algorithm restated
 in C++ with OpenMP + LAPACK/BLAS) on the same workload, all host cores.
@@ -167,33 +168,43 @@ def cpu_baseline(prob, steps=1):
 BATCH_KW = dict(UnotS=True, US_max=1e-6, US_tol=1e-8, maxnits=40)
 
 
-def batched_patches(npatch=256, sample=16):
+def batched_patches(npatch=256, sample=16, rank=0, world=1, dist=None, device=None):
     """The batched-patch workload: `npatch` patches of 4 exposures of side
     U{16..24} with 2% of input pixels masked (n ~ 990-2270), per-exposure
     Gaussian PSF sigma ~ U[0.5, 0.8] px, 24x24 outputs; U < 1e-6, tolerance
-    1e-8, 40 iterations.  The concurrency (contexts side by side, each on a
-    share of the SMs) is chosen by the autotuner on the first `sample`
-    patches, together with the cluster that finishes each tridiagonalisation;
-    the whole batch is then solved once to plan every FFT size and once timed
-    (wall clock around the pool, results copied to the host)."""
-    from imcom_b200 import batch
+    1e-8, 40 iterations.  With several ranks every rank solves its share of the
+    same `npatch` patches (balanced by n^3, no data-path collective).  Each
+    rank's concurrency (contexts side by side, each on a share of the SMs) is
+    chosen by the autotuner on the first `sample` of its patches, together
+    with the cluster that finishes each tridiagonalisation; its patches are
+    then solved once to plan every FFT size and once timed (wall clock around
+    the pool, results copied to the host); the job's time is the slowest
+    rank's."""
+    from imcom_b200 import batch, replicas
     problems = batch.make_batch(npatch, seed0=1000)
-    tune = batch.autotune(problems[:sample], candidates=(1, 2, 3, 4, 6), tails=(0, 8, -1),
+    mine = replicas.shard_by_cost([replicas.patch_cost(p) for p in problems], rank, world)
+    local = [problems[i] for i in mine]
+    tune = batch.autotune(local[:sample], candidates=(1, 2, 3, 4, 6), tails=(0, 8, -1),
                           **BATCH_KW)
     k = tune.concurrency
     with batch.BatchSolver(k, tail_ctas=tune.tail_ctas) as b:
-        b.solve(problems, **BATCH_KW)
-        r = b.solve(problems, **BATCH_KW)
+        b.solve(local, **BATCH_KW)
+        if dist is not None:
+            dist.barrier()
+        r = b.solve(local, **BATCH_KW)
+    t = replicas.max_over_ranks(r.seconds, dist, device)
     ns = [p.n for p in problems]
     return {"workload": f"{npatch} patches, 4 exposures of side U{{16..24}}, 2% masked, "
                         "24x24 outputs, U<1e-6 tol 1e-8",
             "n_range": [min(ns), max(ns)], "psf_sides": len({p.nps for p in problems}),
-            "patches_per_s": r.patches_per_s, "pixels_per_s": r.pixels_per_s,
-            "seconds": r.seconds, "concurrency": k, "sm_share": r.sm_share,
-            "tail_ctas": tune.tail_ctas,
-            "autotune_patches_per_s": {f"{q}x{'auto' if t == 0 else ('none' if t < 0 else t)}": v
-                                       for (q, t), v in tune.rates.items()},
-            "timing": "wall clock around the thread pool after one warm pass"}
+            "patches_per_s": replicas.job_rate(npatch, t),
+            "pixels_per_s": replicas.job_rate(sum(p.m for p in problems), t),
+            "seconds": t, "ranks": world, "patches_rank0": len(local),
+            "concurrency": k, "sm_share": r.sm_share, "tail_ctas": tune.tail_ctas,
+            "autotune_patches_per_s": {f"{q}x{'auto' if tt == 0 else ('none' if tt < 0 else tt)}": v
+                                       for (q, tt), v in tune.rates.items()},
+            "timing": "wall clock around each rank's thread pool after one warm pass, max "
+                      "over ranks"}
 
 
 def run_reference(args):
@@ -485,8 +496,8 @@ def run_ours(args):
 
     s.close()
     batch_line = None
-    if rank == 0 and world == 1 and not args.no_batch:
-        batch_line = batched_patches()
+    if not args.no_batch:  # every rank takes part (its share of the patches)
+        batch_line = batched_patches(rank=rank, world=world, dist=dist, device=dev)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
