@@ -50,14 +50,15 @@ namespace imcom {
 namespace {
 
 constexpr int NB = 32;            // tridiagonalisation panel width
-constexpr int TRD_THREADS = 384;  // threads per CTA of the panel kernel
+constexpr int TRD_THREADS = 256;  // threads per CTA of the panel kernel
+constexpr int TRD_SLOTS = 3;      // tiles staged per warp (two in flight ahead)
 constexpr int CW = 16;            // columns per symv tile
 constexpr int TR = 64;            // rows per symv tile (two per lane)
 constexpr int CPB = TR / CW;      // column chunks per row block along the diagonal
 // one staging slot: a CW x TR tile, then the TR rows and CW columns of the
 // reflector column it multiplies
 constexpr int TRD_SLOT = CW * TR + TR + CW;
-constexpr size_t TRD_SMEM = (size_t)(TRD_THREADS / 32) * 2 * TRD_SLOT * sizeof(double);
+constexpr size_t TRD_SMEM = (size_t)(TRD_THREADS / 32) * TRD_SLOTS * TRD_SLOT * sizeof(double);
 constexpr int LEAF = 32;          // largest leaf of the divide-and-conquer tree
 constexpr int NBB = 128;          // reflectors per back-transformation block
 constexpr double EPS = 1.1102230246251565e-16;
@@ -82,6 +83,7 @@ __device__ __forceinline__ void cp_async8(double* dst, const double* src, int by
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_wait_2() { asm volatile("cp.async.wait_group 2;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_wait_0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 __device__ __forceinline__ double ld_cg(const double* p) {
@@ -162,7 +164,7 @@ struct TrdArgs {
   long long spin;
 };
 
-__global__ void __launch_bounds__(TRD_THREADS) trd_panel_kernel(TrdArgs a) {
+__global__ void __launch_bounds__(TRD_THREADS, 1) trd_panel_kernel(TrdArgs a) {
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   constexpr int WPB = TRD_THREADS / 32;
   constexpr int HP = (NB + WPB - 1) / WPB;  // panel columns per warp in phase B
@@ -176,7 +178,7 @@ __global__ void __launch_bounds__(TRD_THREADS) trd_panel_kernel(TrdArgs a) {
   __shared__ double s_alpha2;                  // -1/2 tau^2 v^T y of the current column
   __shared__ double sm_y[WPB][32], sm_c[WPB][32], sm_u[WPB][32];
   extern __shared__ __align__(16) double trd_tiles[];  // [warp][slot][TRD_SLOT]
-  double* wbuf = trd_tiles + (size_t)wib * 2 * TRD_SLOT;
+  double* wbuf = trd_tiles + (size_t)wib * TRD_SLOTS * TRD_SLOT;
   if (*(volatile int*)&a.sync->err) return;  // an earlier panel failed
 
   // Column k: d(k) and the norm of A(k+2:n, k) (one atomic per CTA).
@@ -262,10 +264,16 @@ __global__ void __launch_bounds__(TRD_THREADS) trd_panel_kernel(TrdArgs a) {
     // phase B, y0 = A22 v = scl (A22 x) + delta A22(:, j+1), so the tiles do
     // not wait for the reflector.  Its loads are issued now, used after the
     // tile loop.
-    int rb_n = 0, ch_n = 0;  // decoded indices of this warp's next tile
+    // decoded indices of this warp's next two tiles
+    int rb_n = 0, ch_n = 0, rb_m = 0, ch_m = 0;
     if (gw < ntiles) {
       decode((int)gw, rb_n, ch_n);
       issue(rb_n, ch_n, 0);
+    }
+    cp_commit();
+    if (gw + GW < ntiles) {
+      decode((int)(gw + GW), rb_m, ch_m);
+      issue(rb_m, ch_m, 1);
     }
     cp_commit();
     const double alpha = ld_cg(A + (j + 1) + (long long)j * lda);
@@ -297,14 +305,16 @@ __global__ void __launch_bounds__(TRD_THREADS) trd_panel_kernel(TrdArgs a) {
     // atomic per CTA. ----
     double vty_part = 0.0;
     int slot = 0;
-    for (long long tile = gw; tile < ntiles; tile += GW, slot ^= 1) {
+    for (long long tile = gw; tile < ntiles; tile += GW, slot = (slot + 1) % TRD_SLOTS) {
       const int rb = rb_n, ch = ch_n;
-      if (tile + GW < ntiles) {
-        decode((int)(tile + GW), rb_n, ch_n);
-        issue(rb_n, ch_n, slot ^ 1);
+      rb_n = rb_m;
+      ch_n = ch_m;
+      if (tile + 2 * GW < ntiles) {
+        decode((int)(tile + 2 * GW), rb_m, ch_m);
+        issue(rb_m, ch_m, (slot + 2) % TRD_SLOTS);
       }
       cp_commit();
-      cp_wait_1();
+      cp_wait_2();
       const long long r = rbase + (long long)rb * TR + 2 * lane;
       const long long c0 = j + 1 + (long long)ch * CW, c1 = min((long long)n, c0 + CW);
       const double* sl = wbuf + slot * TRD_SLOT;
