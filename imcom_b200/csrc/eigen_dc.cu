@@ -1285,11 +1285,6 @@ __global__ void __launch_bounds__(NBB) larft_kernel(const double* Gall, long lon
 // ---------------------------------------------------------------------------
 // Host driver
 // ---------------------------------------------------------------------------
-struct DcBuffers {
-  double* base = nullptr;
-  size_t bytes = 0;
-};
-
 // X = [V(:, k:k+b) | W(:, 0:b)] and Y = [W | V], rows t0..n-1 (ld ldx): the
 // operands of the fused trailing update A22 -= X Y^T = V W^T + W V^T.
 __global__ void pack_update_kernel(const double* __restrict__ V, long long ldv,
