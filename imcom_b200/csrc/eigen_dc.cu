@@ -217,10 +217,10 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) trd_panel_kernel(TrdArgs a) {
     const long long tri = (long long)CPB * rbc * (rbc + 1) / 2;
     const long long ntiles = tri + (RB - rbc) * NC;
 
-    // tiles are staged through a two-slot shared-memory buffer per warp by
-    // cp.async (zero-filled outside the triangle and below row n), together
-    // with the segments of column j they multiply, so the next tile is in
-    // flight while this one is summed
+    // tiles are staged through a TRD_SLOTS-slot shared-memory buffer per warp
+    // by cp.async (zero-filled outside the triangle and below row n), together
+    // with the segments of column j they multiply, so the next two tiles are
+    // in flight while this one is summed
     const double* colj = A + (long long)j * lda;
     // tile counts stay far below 2^31 (n^2 / 2048), so 32-bit arithmetic; the
     // float square root is only a first guess that the loops correct
