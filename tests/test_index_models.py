@@ -1,0 +1,253 @@
+"""CPU models of the index arithmetic and update orders the device kernels
+rely on.  Each test restates a formula of a kernel in numpy / Python and
+checks the property the kernel needs; the kernels themselves are checked on
+the GPU against the oracle (test_gpu_*.py).
+
+* oz_digit_kernel (imcom_b200/csrc/ozaki.cu): for 4 <= S <= 7 slices the
+  balanced base-256 digits are taken from N = 2^24 H + L in 32-bit pieces;
+  they must equal the 64-bit recursion of the CPU model (oracle/split_oracle.py).
+* trd_panel_kernel (imcom_b200/csrc/eigen_dc.cu), phase A/B: the closed-form
+  decode of the lower-triangle tiles visits every tile on or below the
+  diagonal exactly once, and the per-row ranges of row and column partial
+  sums in phase B add up to the trailing product A22 x.
+* jacobi_kernel (imcom_b200/csrc/eigen_jacobi.cu): the round-robin rounds
+  pair every two columns exactly once per sweep, each round with disjoint
+  pairs.
+* trd_tail_kernel (imcom_b200/csrc/eigen_dc.cu): the distributed row layout
+  and the lazy update order (column j's update applied to row j+1 before its
+  reflector and to the other rows in the next pass) give a tridiagonal form
+  Q^T A Q = T.
+"""
+import itertools
+import math
+
+import numpy as np
+import pytest
+
+# -- split digits ----------------------------------------------------------
+
+
+def digits_64(N, S):
+    d = [0] * S
+    for s in range(S - 1, 0, -1):
+        q = ((N + 128) & 255) - 128
+        d[s] = q
+        N = (N - q) >> 8
+    d[0] = N
+    return d
+
+
+def digits_32(N, S):
+    d = [0] * S
+    c, hi = N & 0xFFFFFF, N >> 24
+    for s in range(S - 1, 0, -1):
+        if s >= S - 3:
+            q = ((c + 128) & 255) - 128
+            d[s] = q
+            c = (c - q) >> 8
+            if s == S - 3:
+                hi += c
+        else:
+            q = ((hi + 128) & 255) - 128
+            d[s] = q
+            hi = (hi - q) >> 8
+    d[0] = hi
+    return d
+
+
+@pytest.mark.parametrize("S", [4, 5, 6, 7])
+def test_digit_split_matches_64bit_recursion(S):
+    rng = np.random.default_rng(S)
+    lim = 2 ** (7 + 8 * (S - 1) - 1)  # |N| < 2^(6 + 8(S-1)) for rows scaled below 1/2
+    Ns = [int(v) for v in rng.integers(-lim, lim, 20000)]
+    Ns += [lim - 1, -lim, 0, 1, -1, 2 ** 24, -(2 ** 24), 2 ** 24 - 1, 128, -128, 127, -129]
+    for N in Ns:
+        d = digits_32(N, S)
+        assert d == digits_64(N, S)
+        assert all(-128 <= x <= 127 for x in d[1:]) and abs(d[0]) <= 65
+
+
+def test_digit_recursion_is_the_oracle_digits():
+    from oracle import split_oracle as SO
+    rng = np.random.default_rng(1)
+    X = rng.standard_normal((6, 40)) * np.logspace(-3, 3, 40)
+    for S in (4, 7):
+        planes, scale = SO.digits(X, S)
+        _, e = SO.row_scales(X)
+        for r in range(X.shape[0]):
+            for k in range(X.shape[1]):
+                N = int(np.rint(np.ldexp(np.ldexp(X[r, k], -int(e[r])), 7 + 8 * (S - 1))))
+                assert digits_32(N, S) == [int(p[r, k]) for p in planes]
+
+
+# -- lower-triangle tiles of the panel kernel --------------------------------
+
+CW, TR = 16, 64
+CPB = TR // CW
+
+
+def tile_geometry(n, j):
+    rbase = (j + 1) & ~1
+    R = n - (j + 1)
+    RB = (n - rbase + TR - 1) // TR
+    NC = (R + CW - 1) // CW
+    rbc = min(RB, max(0, (NC - 1) // CPB))
+    tri = CPB * rbc * (rbc + 1) // 2
+    return rbase, RB, NC, rbc, tri, tri + (RB - rbc) * NC
+
+
+def decode(tile, tri, rbc, NC):
+    if tile < tri:
+        q = int((math.sqrt(np.float32(1.0) + np.float32(8.0) * np.float32(tile) / CPB) - 1.0) * 0.5)
+        while CPB * (q + 1) * (q + 2) // 2 <= tile:
+            q += 1
+        while q > 0 and CPB * q * (q + 1) // 2 > tile:
+            q -= 1
+        return q, tile - CPB * q * (q + 1) // 2
+    return rbc + (tile - tri) // NC, (tile - tri) % NC
+
+
+@pytest.mark.parametrize("n,j", [(40, 0), (41, 0), (100, 3), (130, 64), (257, 100), (300, 17),
+                                 (199, 196), (70, 66), (640, 0), (1000, 1)])
+def test_panel_tiles_cover_lower_triangle_and_sum_to_product(n, j):
+    rng = np.random.default_rng(n + j)
+    M = rng.standard_normal((n, n))
+    A = M + M.T
+    x = np.zeros(n)
+    x[j + 1:] = rng.standard_normal(n - j - 1)
+    rbase, RB, NC, rbc, tri, ntiles = tile_geometry(n, j)
+    seen = set()
+    ypart = np.full((NC, n), np.nan)
+    ycol = np.full((RB, n), np.nan)
+    for t in range(ntiles):
+        rb, ch = decode(t, tri, rbc, NC)
+        assert 0 <= rb < RB and 0 <= ch < NC and (rb, ch) not in seen
+        seen.add((rb, ch))
+        c0, c1 = j + 1 + ch * CW, min(n, j + 1 + ch * CW + CW)
+        r0, r1 = rbase + rb * TR, min(n, rbase + rb * TR + TR)
+        blk = A[r0:r1, c0:c1]
+        rows = np.arange(r0, r1)[:, None]
+        cols = np.arange(c0, c1)[None, :]
+        low = np.where(rows >= cols, blk, 0.0)      # row sums: on or below the diagonal
+        strict = np.where(rows > cols, blk, 0.0)    # column sums: strictly below
+        rs = low @ x[c0:c1]
+        keep = np.arange(r0, r1) >= j + 1
+        ypart[ch, r0:r1][keep] = rs[keep]
+        ycol[rb, c0:c1] = strict.T @ x[r0:r1]
+    for rb in range(RB):
+        for ch in range(NC):
+            lower = rbase + rb * TR + TR - 1 >= j + 1 + ch * CW
+            assert ((rb, ch) in seen) == lower
+    y = np.zeros(n)
+    for r in range(j + 1, n):
+        ncr = min(NC, CPB * ((r - rbase) // TR + 1))
+        rb0 = (r - (j + 1)) // CW // CPB
+        parts = np.concatenate([ypart[:ncr, r], ycol[rb0:RB, r]])
+        assert not np.isnan(parts).any()
+        y[r] = parts.sum()
+    ref = A[j + 1:, j + 1:] @ x[j + 1:]
+    assert np.max(np.abs(y[j + 1:] - ref)) <= 1e-12 * max(1.0, np.max(np.abs(ref)))
+
+
+# -- Jacobi round-robin ------------------------------------------------------
+
+
+def jacobi_rounds(n):
+    npl = n + (n & 1)
+    m = npl - 1
+    for s in range(m):
+        pairs = []
+        for k in range(npl // 2):
+            p, q = (s, m) if k == 0 else ((s + k) % m, (s - k + m) % m)
+            p, q = min(p, q), max(p, q)
+            if q < n:
+                pairs.append((p, q))
+        yield pairs
+
+
+@pytest.mark.parametrize("n", [2, 3, 7, 8, 31, 64, 112])
+def test_jacobi_rounds_pair_every_two_columns_once(n):
+    seen = []
+    for pairs in jacobi_rounds(n):
+        flat = [c for pq in pairs for c in pq]
+        assert len(flat) == len(set(flat))
+        seen += pairs
+    assert sorted(seen) == sorted(itertools.combinations(range(n), 2))
+
+
+# -- cluster tail ------------------------------------------------------------
+
+
+def tail_lazy(A, ctas):
+    n = A.shape[0]
+    S, rpc = n, (n + ctas - 1) // ctas
+    Lw = np.tril(A)  # only the lower triangle is valid in global memory
+    rows = [np.full((max(0, min(rpc, S - q * rpc)), S), np.nan) for q in range(ctas)]
+    for q in range(ctas):  # phase 1: row r right of the diagonal = column r of the lower part
+        for i in range(rows[q].shape[0]):
+            r = q * rpc + i
+            rows[q][i, r:] = Lw[r:, r]
+    for q in range(ctas):  # phase 2: left of the diagonal, from the owner of row c
+        for i in range(rows[q].shape[0]):
+            r = q * rpc + i
+            for c in range(r):
+                o = c // rpc
+                rows[q][i, c] = rows[o][c - o * rpc, r]
+    d, e, tau = np.zeros(n), np.zeros(n - 1), np.zeros(n - 1)
+    V = np.zeros((n, n))
+    vb, pb = [np.zeros(S), np.zeros(S)], [np.zeros(S), np.zeros(S)]
+    a2 = 0.0
+    for jl in range(S - 1):
+        par = jl & 1
+        vq, pq = vb[par ^ 1], pb[par ^ 1]
+        o = jl // rpc
+        row = rows[o][jl - o * rpc]
+        if jl > 0:
+            vr = vq[jl]
+            wr = pq[jl] + a2 * vr
+            row[jl:] -= vr * (pq[jl:] + a2 * vq[jl:]) + wr * vq[jl:]
+        xn2 = np.sum(row[jl + 2:] ** 2)
+        alpha = row[jl + 1]
+        if xn2 == 0:
+            t, beta, scl = 0.0, alpha, 0.0
+        else:
+            beta = -math.copysign(math.sqrt(alpha * alpha + xn2), alpha)
+            t, scl = (beta - alpha) / beta, 1.0 / (alpha - beta)
+        v = np.zeros(S)
+        v[jl + 1] = 1.0
+        v[jl + 2:] = row[jl + 2:] * scl
+        V[:, jl], d[jl], e[jl], tau[jl] = v, row[jl], beta, t
+        newp, ptv = np.zeros(S), 0.0
+        for q in range(ctas):
+            for i in range(rows[q].shape[0]):
+                rr = q * rpc + i
+                if rr <= jl:
+                    continue
+                R = rows[q][i]
+                if jl > 0:
+                    vr = vq[rr]
+                    wr = pq[rr] + a2 * vr
+                    R[jl:] -= vr * (pq[jl:] + a2 * vq[jl:]) + wr * vq[jl:]
+                newp[rr] = t * (R[jl + 1:] @ v[jl + 1:])
+                ptv += newp[rr] * v[rr]
+        vb[par], pb[par] = v, newp
+        a2 = -0.5 * t * ptv
+    par = (S - 2) & 1
+    vr = vb[par][S - 1]
+    wr = pb[par][S - 1] + a2 * vr
+    oq = (S - 1) // rpc
+    d[S - 1] = rows[oq][S - 1 - oq * rpc][S - 1] - 2.0 * vr * wr
+    return d, e, tau, V
+
+
+@pytest.mark.parametrize("n,ctas", [(2, 16), (3, 16), (37, 16), (64, 8), (70, 16)])
+def test_cluster_tail_order_tridiagonalises(n, ctas):
+    rng = np.random.default_rng(n)
+    M = rng.standard_normal((n, n))
+    A = M + M.T
+    d, e, tau, V = tail_lazy(A, ctas)
+    Q = np.eye(n)
+    for j in range(n - 1):
+        Q = Q @ (np.eye(n) - tau[j] * np.outer(V[:, j], V[:, j]))
+    T = np.diag(d) + np.diag(e, -1) + np.diag(e, 1)
+    assert np.linalg.norm(Q.T @ A @ Q - T) <= 1e-13 * np.linalg.norm(A)
