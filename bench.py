@@ -184,14 +184,18 @@ def batched_patches(npatch=256, sample=16, rank=0, world=1, dist=None, device=No
     problems = batch.make_batch(npatch, seed0=1000)
     mine = replicas.shard_by_cost([replicas.patch_cost(p) for p in problems], rank, world)
     local = [problems[i] for i in mine]
-    tune = batch.autotune(local[:sample], candidates=(1, 2, 3, 4, 6), tails=(0, 8, -1),
-                          **BATCH_KW)
+    if local:
+        tune = batch.autotune(local[:sample], candidates=(1, 2, 3, 4, 6), tails=(0, 8, -1),
+                              **BATCH_KW)
+    else:  # more ranks than patches: this rank only joins the barrier and the MAX
+        tune = batch.Tuning(1, 0, {})
     k = tune.concurrency
     with batch.BatchSolver(k, tail_ctas=tune.tail_ctas) as b:
-        b.solve(local, **BATCH_KW)
+        if local:
+            b.solve(local, **BATCH_KW)
         if dist is not None:
             dist.barrier()
-        r = b.solve(local, **BATCH_KW)
+        r = b.solve(local, **BATCH_KW) if local else batch.BatchResult(concurrency=k)
     t = replicas.max_over_ranks(r.seconds, dist, device)
     ns = [p.n for p in problems]
     return {"workload": f"{npatch} patches, 4 exposures of side U{{16..24}}, 2% masked, "
