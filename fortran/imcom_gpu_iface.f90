@@ -219,6 +219,48 @@ INTERFACE
     INTEGER(C_INT), DIMENSION(count) :: sweeps
   END FUNCTION
 
+  ! FITS images without CFITSIO (host only, no context).  Paths are passed
+  ! as trim(name)//C_NULL_CHAR.
+  ! imcom_sizefits (imcom_io.f90:338-356)
+  INTEGER(C_INT) FUNCTION imcom_fits_size(path, naxis1, naxis2, bitpix) &
+                                          BIND(C, NAME="imcom_fits_size")
+    IMPORT :: C_INT, C_CHAR
+    CHARACTER(KIND=C_CHAR), DIMENSION(*), INTENT(IN) :: path
+    INTEGER(C_INT) :: naxis1, naxis2, bitpix
+  END FUNCTION
+
+  ! imcom_readfits (imcom_io.f90:360-403): any BITPIX, BSCALE/BZERO applied,
+  ! undefined pixels -666
+  INTEGER(C_INT) FUNCTION imcom_fits_read(path, naxis1, naxis2, image) &
+                                          BIND(C, NAME="imcom_fits_read")
+    IMPORT :: C_INT, C_CHAR, C_DOUBLE
+    CHARACTER(KIND=C_CHAR), DIMENSION(*), INTENT(IN) :: path
+    INTEGER(C_INT), VALUE :: naxis1, naxis2
+    REAL(C_DOUBLE), DIMENSION(naxis1, naxis2), INTENT(OUT) :: image
+  END FUNCTION
+
+  ! imcom_writefits (imcom_io.f90:407-457): BITPIX -64, replaces the file
+  INTEGER(C_INT) FUNCTION imcom_fits_write(path, naxis1, naxis2, image) &
+                                           BIND(C, NAME="imcom_fits_write")
+    IMPORT :: C_INT, C_CHAR, C_DOUBLE
+    CHARACTER(KIND=C_CHAR), DIMENSION(*), INTENT(IN) :: path
+    INTEGER(C_INT), VALUE :: naxis1, naxis2
+    REAL(C_DOUBLE), DIMENSION(naxis1, naxis2), INTENT(IN) :: image
+  END FUNCTION
+
+  ! imcom_writefitscube (imcom_io.f90:460-494)
+  INTEGER(C_INT) FUNCTION imcom_fits_write_cube(path, naxis1, naxis2, naxis3, cube) &
+                                                BIND(C, NAME="imcom_fits_write_cube")
+    IMPORT :: C_INT, C_CHAR, C_DOUBLE
+    CHARACTER(KIND=C_CHAR), DIMENSION(*), INTENT(IN) :: path
+    INTEGER(C_INT), VALUE :: naxis1, naxis2, naxis3
+    REAL(C_DOUBLE), DIMENSION(naxis1, naxis2, naxis3), INTENT(IN) :: cube
+  END FUNCTION
+
+  TYPE(C_PTR) FUNCTION imcom_fits_last_error() BIND(C, NAME="imcom_fits_last_error")
+    IMPORT :: C_PTR
+  END FUNCTION
+
 END INTERFACE
 
 TYPE(C_PTR), SAVE :: imcom_gpu_ctx = C_NULL_PTR
@@ -230,6 +272,24 @@ SUBROUTINE imcom_gpu_check(status, what)
 implicit none
 integer(C_INT), intent(IN) :: status
 character(LEN=*), intent(IN) :: what
+if (status.eq.0) return
+call imcom_stop_with(status, what, imcom_gpu_last_error(imcom_gpu_ctx))
+END SUBROUTINE imcom_gpu_check
+
+SUBROUTINE imcom_fits_check(status, what)
+! The same for the FITS functions, whose reason is kept per host thread.
+implicit none
+integer(C_INT), intent(IN) :: status
+character(LEN=*), intent(IN) :: what
+if (status.eq.0) return
+call imcom_stop_with(status, what, imcom_fits_last_error())
+END SUBROUTINE imcom_fits_check
+
+SUBROUTINE imcom_stop_with(status, what, p)
+implicit none
+integer(C_INT), intent(IN) :: status
+character(LEN=*), intent(IN) :: what
+type(C_PTR), intent(IN) :: p
 character(KIND=C_CHAR), dimension(:), pointer :: msg
 integer :: i
 interface
@@ -238,9 +298,6 @@ interface
     type(C_PTR), value :: s
   end function
 end interface
-type(C_PTR) :: p
-if (status.eq.0) return
-p = imcom_gpu_last_error(imcom_gpu_ctx)
 call c_f_pointer(p, msg, [c_strlen(p)])
 write(*, FMT='(A, I4)') "IMCOM ERROR: "//what//" failed with status ", status
 write(*, FMT='(A)', ADVANCE='NO') "IMCOM ERROR: "
@@ -249,6 +306,6 @@ do i = 1, size(msg)
 end do
 write(*, *)
 stop
-END SUBROUTINE imcom_gpu_check
+END SUBROUTINE imcom_stop_with
 
 END MODULE imcom_gpu_iface

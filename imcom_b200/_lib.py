@@ -51,6 +51,11 @@ SIGNATURES = {
     "imcom_gpu_split_pixels": (_i, [_p, _p, _p]),
     "imcom_gpu_build_P_noalloc": (_i, [_p, _ll, _p, _ll, _p, _ll, _i, _i, _p]),
     "imcom_gpu_eigh_jacobi_batched": (_i, [_p, _i, _i, _p, _p, _p, _p]),
+    "imcom_fits_size": (_i, [C.c_char_p, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i)]),
+    "imcom_fits_read": (_i, [C.c_char_p, _i, _i, _p]),
+    "imcom_fits_write": (_i, [C.c_char_p, _i, _i, _p]),
+    "imcom_fits_write_cube": (_i, [C.c_char_p, _i, _i, _i, _p]),
+    "imcom_fits_last_error": (C.c_char_p, []),
     "imcom_gpu_device_buffer": (_i, [_p, C.c_char, C.POINTER(_p), C.POINTER(_ll)]),
     "imcom_gpu_get_stream": (_i, [_p, C.POINTER(_p)]),
     "imcom_gpu_launch_count": (_i, [_p, C.POINTER(_ll)]),
@@ -61,7 +66,7 @@ SIGNATURES = {
 def header_symbols() -> list[str]:
     """Function names declared in include/imcom_gpu.h."""
     txt = open(HEADER).read()
-    return sorted(set(re.findall(r"\b(imcom_gpu_\w+)\s*\(", txt)))
+    return sorted(set(re.findall(r"\b(imcom_(?:gpu|fits)_\w+)\s*\(", txt)))
 
 
 class ImcomError(RuntimeError):

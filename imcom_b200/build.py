@@ -2,7 +2,8 @@
 
 Every ``csrc/*.cu`` is compiled for ``-gencode arch=compute_100a,code=sm_100a``
 and linked with cuFFT (table FFTs) and cuSOLVER (only the comparison-baseline
-eigensolver mode).  Object files go to ``imcom_b200/_build``.
+eigensolver mode); ``csrc/*.cpp`` holds host-only code (FITS files) and is
+compiled with the host C++ compiler.  Object files go to ``imcom_b200/_build``.
 
 Usage: ``python -m imcom_b200.build [--force] [-v]``.
 """
@@ -20,16 +21,18 @@ OUT = os.path.join(HERE, "libimcom_gpu.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
+CXX = os.environ.get("CXX", "g++")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC,
           "--expt-relaxed-constexpr"]
+HOST_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-Wall", "-I" + INCLUDE, "-I" + CSRC]
 # Files whose arithmetic restates the reference operation by operation.
 NO_FMA = {"tables.cu"}
 
 
 def sources():
-    return sorted(f for f in os.listdir(CSRC) if f.endswith(".cu"))
+    return sorted(f for f in os.listdir(CSRC) if f.endswith((".cu", ".cpp")))
 
 
 def _deps_mtime():
@@ -42,16 +45,19 @@ def _deps_mtime():
 
 
 def _compile(src, verbose, extra):
-    obj = os.path.join(BUILD, src[:-3] + ".o")
-    flags = list(COMMON) + ARCH + list(extra)
-    if src in NO_FMA:
-        flags.append("--fmad=false")
-    cmd = [NVCC] + flags + ["-c", os.path.join(CSRC, src), "-o", obj]
+    obj = os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
+    if src.endswith(".cpp"):
+        cmd = [CXX] + HOST_FLAGS + ["-c", os.path.join(CSRC, src), "-o", obj]
+    else:
+        flags = list(COMMON) + ARCH + list(extra)
+        if src in NO_FMA:
+            flags.append("--fmad=false")
+        cmd = [NVCC] + flags + ["-c", os.path.join(CSRC, src), "-o", obj]
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")
+        raise RuntimeError(f"{cmd[0]} failed for {src}:\n{r.stdout}\n{r.stderr}")
     if verbose and (r.stdout or r.stderr):
         print(r.stdout + r.stderr, flush=True)
     return obj

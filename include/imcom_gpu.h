@@ -45,6 +45,7 @@ typedef struct imcom_ctx imcom_ctx;
 #define IMCOM_ERR_NOT_FINITE 7  /* non-finite input                           */
 #define IMCOM_ERR_NOALLOC_SIZE 8 /* problem too large for imcom_gpu_build_P_noalloc */
 #define IMCOM_ERR_SPLIT 9       /* split-precision product unavailable (K too large, pipeline wait ran out) */
+#define IMCOM_ERR_FITS 10       /* FITS file missing, malformed or of another size */
 
 /* Eigensolver selection for imcom_gpu_set_option(IMCOM_OPT_EIGENSOLVER). */
 #define IMCOM_EIGH_DC 0         /* own tridiagonalisation + divide & conquer  */
@@ -306,6 +307,31 @@ int imcom_gpu_build_P_noalloc(const double* dQ, long long ldq, const double* dB,
  * converge in 60 sweeps, IMCOM_ERR_CUDA / IMCOM_ERR_ALLOC. */
 int imcom_gpu_eigh_jacobi_batched(imcom_ctx* ctx, int n, int count, const double* A,
                                   double* Q, double* L, int* sweeps);
+
+/* ---- FITS files without CFITSIO (host only; no context, no GPU) -------- */
+
+/* The primary image of a FITS file, for drivers that get their arrays from
+ * this library and would otherwise link CFITSIO only to read and write them.
+ * Paths are NUL-terminated; arrays are column-major (axis 1 fastest), as
+ * FITS stores them.  Errors return IMCOM_ERR_FITS with the reason in
+ * imcom_fits_last_error() (per host thread); bad arguments return -k. */
+/* imcom_sizefits (imcom_io.f90:338-356): NAXIS1, NAXIS2 (1 for a
+ * one-axis image) and BITPIX. */
+int imcom_fits_size(const char* path, int* naxis1, int* naxis2, int* bitpix);
+/* imcom_readfits (imcom_io.f90:360-403): the image as doubles.  Every BITPIX
+ * is read, with BSCALE and BZERO applied; NaN pixels of floating-point
+ * images and BLANK pixels of integer images become -666, the null value the
+ * reference passes to CFITSIO.  The image must hold naxis1 x naxis2 values
+ * (IMCOM_ERR_FITS otherwise, where the reference stops). */
+int imcom_fits_read(const char* path, int naxis1, int naxis2, double* image);
+/* imcom_writefits (imcom_io.f90:407-457): a BITPIX -64 image; an existing
+ * file is replaced. */
+int imcom_fits_write(const char* path, int naxis1, int naxis2, const double* image);
+/* imcom_writefitscube (imcom_io.f90:460-494): the same with three axes. */
+int imcom_fits_write_cube(const char* path, int naxis1, int naxis2, int naxis3,
+                          const double* cube);
+/* Reason for the last IMCOM_ERR_FITS of this host thread. */
+const char* imcom_fits_last_error(void);
 
 /* ---- device views (for callers that keep data on the GPU) -------------- */
 
