@@ -28,6 +28,10 @@ share of the SMs, concurrency chosen by the autotuner; with N GPUs the
 patches are split across ranks by cost (no data-path collective); patches/s
 and output pixels/s over the slowest rank's wall-clock time.
 
+``t_reuse``: T reused for many image stacks -- H = T^T I for 1, 16 and 64
+stacks in one FP64 GEMM with T resident (imcom_b200/t_reuse.py), run in a
+child process after the timed solves.
+
 ``--impl reference`` times the CPU oracle (the reference's algorithm restated
 in C++ with OpenMP + LAPACK/BLAS) on the same workload, all host cores.
 Multi-GPU (``torchrun``): replicas only -- every rank solves its own
@@ -209,6 +213,25 @@ def batched_patches(npatch=256, sample=16, rank=0, world=1, dist=None, device=No
                                        for (q, tt), v in tune.rates.items()},
             "timing": "wall clock around each rank's thread pool after one warm pass, max "
                       "over ranks"}
+
+
+def t_reuse_child(timeout=300):
+    """H = T^T I for 1, 16 and 64 image stacks at once with T resident
+    (imcom_b200/t_reuse.py), measured in a child process with its own CUDA
+    context, so this line keeps its other numbers whatever that run meets."""
+    try:
+        r = subprocess.run([sys.executable, "-m", "imcom_b200.t_reuse"], cwd=ROOT,
+                           capture_output=True, text=True, timeout=timeout)
+    except subprocess.TimeoutExpired:
+        return {"error": f"no result within {timeout} s"}
+    lines = r.stdout.strip().splitlines()
+    if r.returncode != 0 or not lines:
+        tail = (r.stderr or r.stdout).strip().splitlines()[-3:]
+        return {"error": f"exit {r.returncode}: " + " | ".join(tail)}
+    try:
+        return json.loads(lines[-1])
+    except ValueError:
+        return {"error": "unreadable output: " + lines[-1][:200]}
 
 
 def run_reference(args):
@@ -510,6 +533,10 @@ def run_ours(args):
                "sample": "one full n=4096 solve (C++ restatement of the reference, OpenMP + "
                          "OpenBLAS LAPACK/BLAS), same workload"}
 
+    t_reuse = None
+    if rank == 0 and world == 1 and not args.no_t_reuse:
+        t_reuse = t_reuse_child()
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -539,6 +566,7 @@ def run_ours(args):
             "split_roofline": split_roof,
             "cpu_baseline": cpu,
             "batch": batch_line,
+            "t_reuse": t_reuse,
             "clocks": ck,
         }
         print(json.dumps(line), flush=True)
@@ -559,6 +587,8 @@ def main():
                     help="P and T arithmetic of the fast path")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-patch measurement")
+    ap.add_argument("--no-t-reuse", action="store_true",
+                    help="skip the many-stack H = T^T I measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

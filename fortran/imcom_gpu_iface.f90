@@ -219,6 +219,17 @@ INTERFACE
     INTEGER(C_INT), DIMENSION(count) :: sweeps
   END FUNCTION
 
+  ! imcom_build_image for nstack image stacks sharing the resident T:
+  ! I_stack(n, nstack) -> H(m, nstack), one FP64 GEMM (T read once)
+  INTEGER(C_INT) FUNCTION imcom_gpu_build_images(ctx, nstack, I_stack, H) &
+                                                 BIND(C, NAME="imcom_gpu_build_images")
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: ctx
+    INTEGER(C_INT), VALUE :: nstack
+    REAL(C_DOUBLE), DIMENSION(*), INTENT(IN) :: I_stack
+    REAL(C_DOUBLE), DIMENSION(*) :: H
+  END FUNCTION
+
   ! FITS images without CFITSIO (host only, no context).  Paths are passed
   ! as trim(name)//C_NULL_CHAR.
   ! imcom_sizefits (imcom_io.f90:338-356)

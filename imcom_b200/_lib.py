@@ -41,6 +41,8 @@ SIGNATURES = {
     "imcom_gpu_load_T": (_i, [_p, _p]),
     "imcom_gpu_load_K": (_i, [_p, _p]),
     "imcom_gpu_build_image": (_i, [_p, _p]),
+    "imcom_gpu_build_images": (_i, [_p, _i, _p, _p]),
+    "imcom_gpu_build_images_device": (_i, [_p, _i, _p, _ll, _p, _ll]),
     "imcom_gpu_build_S": (_i, [_p, _p]),
     "imcom_gpu_build_U": (_i, [_p, _d, _p]),
     "imcom_gpu_kappa_features": (_i, [_p, _i, _d, _d, _p]),

@@ -268,6 +268,30 @@ class Solver:
         self._call("imcom_gpu_build_image", _ptr(H))
         return H
 
+    def build_images(self, I_stack, out=True):
+        """H = T^T I for image stacks sharing the resident T's geometry:
+        I_stack is (n, stacks) (or (n,) for one), H is (m, stacks)."""
+        I = _f64(I_stack)
+        if I.ndim == 1:
+            I = I[:, None]
+        if I.ndim != 2 or I.shape[0] != self.n:
+            raise ValueError(f"I_stack must have {self.n} rows (one per input pixel)")
+        I = np.asfortranarray(I)
+        H = np.zeros((self.m, I.shape[1]), order="F") if out else None
+        self._call("imcom_gpu_build_images", int(I.shape[1]), _ptr(I), _ptr(H))
+        return H
+
+    def build_images_device(self, dI, dH):
+        """The same on torch CUDA tensors (column-major: dI of shape
+        (stacks, n), dH (stacks, m), each row a stack), ordered on the library
+        stream and not synchronised."""
+        if dI.dim() != 2 or dI.shape[1] != self.n or dH.shape != (dI.shape[0], self.m):
+            raise ValueError("dI must be (stacks, n) and dH (stacks, m)")
+        if dI.stride(1) != 1 or dH.stride(1) != 1:
+            raise ValueError("dI and dH need unit stride along the pixels")
+        self._call("imcom_gpu_build_images_device", int(dI.shape[0]), dI.data_ptr(),
+                   int(dI.stride(0)), dH.data_ptr(), int(dH.stride(0)))
+
     def build_S(self, out=True):
         S = np.zeros(self.m) if out else None
         self._call("imcom_gpu_build_S", _ptr(S))

@@ -126,6 +126,7 @@ struct imcom_ctx {
   int* sp_list = nullptr;
   size_t sp_margin_bytes = 0, sp_est_bytes = 0, sp_flag_bytes = 0, sp_list_bytes = 0;
   imcom::DMat fbX, fbY;  // gathered columns for the FP64 recomputation
+  imcom::DMat stacks, stack_H;  // image stacks I (n x s) and H = T^T I (m x s)
   double split_info[8] = {};
 
   imcom::EigWork* eig = nullptr;

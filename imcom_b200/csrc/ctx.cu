@@ -313,7 +313,8 @@ int imcom_gpu_destroy(imcom_ctx* ctx) {
                   ctx->Gamma, ctx->Gt, ctx->Gammat, ctx->A.p, ctx->Q.p, ctx->B.p, ctx->P.p,
                   ctx->T.p, ctx->Pt.p, ctx->L, ctx->K, ctx->US, ctx->H, ctx->S, ctx->U,
                   ctx->nev, ctx->flags, ctx->tables, ctx->fftbuf, ctx->mlp.w, ctx->feat,
-                  ctx->gemm_ws, ctx->fb, ctx->train_buf, ctx->band, ctx->jac_buf};
+                  ctx->gemm_ws, ctx->fb, ctx->train_buf, ctx->band, ctx->jac_buf,
+                  ctx->stacks.p, ctx->stack_H.p};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete[] ctx->rot;

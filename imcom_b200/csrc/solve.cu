@@ -335,6 +335,52 @@ extern "C" int imcom_gpu_build_image(imcom_ctx* ctx, double* H_out) {
   return 0;
 }
 
+// H = T^T I for many image stacks that share T's geometry and mask (the
+// production pattern of reusing one T, built or read from the cache, for
+// every stack observed with the same dithers and PSFs).  Per stack it is
+// imcom_build_image (imcom_matrix.f90:754-790); for all stacks together it is
+// one FP64 GEMM (M = m, N = stacks, K = n) in which T crosses HBM once
+// instead of once per stack.
+static int build_images(imcom_ctx* ctx, int nstack, const double* dI, long long ldi,
+                        double* dH, long long ldh) {
+  stage_begin(ctx, ST_EPI);
+  IMC_TRY(dgemm(ctx, 'T', 'N', ctx->m, nstack, ctx->n, 1.0, ctx->T.p, ctx->T.ld, dI, ldi, 0.0,
+                dH, ldh));
+  stage_end(ctx, ST_EPI);
+  return 0;
+}
+
+extern "C" int imcom_gpu_build_images(imcom_ctx* ctx, int nstack, const double* I_stack,
+                                      double* H_out) {
+  if (!ctx) return -1;
+  if (nstack < 0) return -2;
+  if (!I_stack && nstack > 0) return -3;
+  if (!ctx->have_T) return set_err(ctx, IMCOM_ERR_STATE, "T has not been built or loaded");
+  if (nstack == 0) return 0;
+  cudaSetDevice(ctx->device);
+  IMC_TRY(upload_mat(ctx, ctx->stacks, I_stack, ctx->n, nstack));
+  IMC_TRY(ensure_mat(ctx, ctx->stack_H, ctx->m, nstack));
+  IMC_TRY(build_images(ctx, nstack, ctx->stacks.p, ctx->stacks.ld, ctx->stack_H.p,
+                       ctx->stack_H.ld));
+  if (H_out) IMC_TRY(download_mat(ctx, ctx->stack_H, H_out));
+  IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+extern "C" int imcom_gpu_build_images_device(imcom_ctx* ctx, int nstack, const double* dI,
+                                             long long ldi, double* dH, long long ldh) {
+  if (!ctx) return -1;
+  if (nstack < 0) return -2;
+  if (nstack > 0 && !dI) return -3;
+  if (ldi < ctx->n || ldi < 1) return -4;
+  if (nstack > 0 && !dH) return -5;
+  if (ldh < ctx->m || ldh < 1) return -6;
+  if (!ctx->have_T) return set_err(ctx, IMCOM_ERR_STATE, "T has not been built or loaded");
+  if (nstack == 0) return 0;
+  cudaSetDevice(ctx->device);
+  return build_images(ctx, nstack, dI, ldi, dH, ldh);
+}
+
 extern "C" int imcom_gpu_build_S(imcom_ctx* ctx, double* S_out) {
   if (!ctx) return -1;
   if (!ctx->have_T) return set_err(ctx, IMCOM_ERR_STATE, "T has not been built or loaded");

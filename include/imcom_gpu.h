@@ -204,6 +204,19 @@ int imcom_gpu_load_K(imcom_ctx* ctx, const double* K);
 
 /* H = T^T I (imcom_build_image, imcom_matrix.f90:754-790). */
 int imcom_gpu_build_image(imcom_ctx* ctx, double* H_out);
+/* imcom_build_image for nstack image stacks observed with the geometry, mask
+ * and PSFs of the resident T (built, or loaded from the cache with
+ * imcom_gpu_load_T): column s of I_stack (n x nstack, leading dimension n) is
+ * the I_i vector of stack s, column s of H_out (m x nstack, leading
+ * dimension m) its H_a.  One FP64 GEMM H = T^T I, so T is read from HBM once
+ * for all stacks.  Host arrays; H_out may be NULL (result kept on the
+ * device). */
+int imcom_gpu_build_images(imcom_ctx* ctx, int nstack, const double* I_stack, double* H_out);
+/* The same on device arrays the caller owns (dI: n x nstack with leading
+ * dimension ldi >= n; dH: m x nstack, ldh >= m), ordered on the library's
+ * stream (imcom_gpu_get_stream) and not synchronised. */
+int imcom_gpu_build_images_device(imcom_ctx* ctx, int nstack, const double* dI, long long ldi,
+                                  double* dH, long long ldh);
 /* S_a = sum_i T_ia^2 Ndiag_i (imcom_build_S, imcom_matrix.f90:839-877). */
 int imcom_gpu_build_S(imcom_ctx* ctx, double* S_out);
 /* U_a = U(K_a) (imcom_build_U, imcom_matrix.f90:795-835). */

@@ -64,3 +64,13 @@ def test_create_without_gpu_fails_cleanly():
     h = ctypes.c_void_p()
     assert lib.imcom_gpu_create(0, ctypes.byref(h)) != 0
     assert not h.value
+
+
+def test_null_context_is_an_argument_error():
+    """Argument checks come before any device work, so they hold without a GPU."""
+    if not os.path.exists(_lib.LIB_PATH):
+        pytest.skip("libimcom_gpu.so not built")
+    lib = _lib.load()
+    assert lib.imcom_gpu_build_image(None, None) == -1
+    assert lib.imcom_gpu_build_images(None, 2, None, None) == -1
+    assert lib.imcom_gpu_build_images_device(None, 2, None, 1, None, 1) == -1
