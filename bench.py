@@ -28,9 +28,10 @@ share of the SMs, concurrency chosen by the autotuner; with N GPUs the
 patches are split across ranks by cost (no data-path collective); patches/s
 and output pixels/s over the slowest rank's wall-clock time.
 
-``t_reuse``: T reused for many image stacks -- H = T^T I for 1, 16 and 64
-stacks in one FP64 GEMM with T resident (imcom_b200/t_reuse.py), run in a
-child process after the timed solves.
+``t_reuse``: T reused for many image stacks -- H = T^T I for 1, 8, 16 and 64
+stacks at once with T resident (imcom_b200/t_reuse.py), through the FP64 GEMM
+and through the streaming kernel, each in a child process after the timed
+solves.
 
 ``--impl reference`` times the CPU oracle (the reference's algorithm restated
 in C++ with OpenMP + LAPACK/BLAS) on the same workload, all host cores.
@@ -215,13 +216,14 @@ def batched_patches(npatch=256, sample=16, rank=0, world=1, dist=None, device=No
                       "over ranks"}
 
 
-def t_reuse_child(timeout=300):
-    """H = T^T I for 1, 16 and 64 image stacks at once with T resident
-    (imcom_b200/t_reuse.py), measured in a child process with its own CUDA
-    context, so this line keeps its other numbers whatever that run meets."""
+def t_reuse_child(kernel="gemm", timeout=300):
+    """H = T^T I for 1, 8, 16 and 64 image stacks at once with T resident
+    (imcom_b200/t_reuse.py) through the given kernel, measured in a child
+    process with its own CUDA context, so this line keeps its other numbers
+    whatever that run meets."""
     try:
-        r = subprocess.run([sys.executable, "-m", "imcom_b200.t_reuse"], cwd=ROOT,
-                           capture_output=True, text=True, timeout=timeout)
+        r = subprocess.run([sys.executable, "-m", "imcom_b200.t_reuse", "--kernel", kernel],
+                           cwd=ROOT, capture_output=True, text=True, timeout=timeout)
     except subprocess.TimeoutExpired:
         return {"error": f"no result within {timeout} s"}
     lines = r.stdout.strip().splitlines()
@@ -535,7 +537,7 @@ def run_ours(args):
 
     t_reuse = None
     if rank == 0 and world == 1 and not args.no_t_reuse:
-        t_reuse = t_reuse_child()
+        t_reuse = {k: t_reuse_child(k) for k in ("gemm", "stream")}
 
     if rank == 0:
         line = {

@@ -29,6 +29,8 @@ BISECT_AUTO, BISECT_STREAM, BISECT_RESIDENT = 0, 1, 2
 OPT_BISECT_CTAS_PER_SM = 9
 OPT_SM_SHARE = 10
 OPT_TAIL_CTAS = 11
+OPT_STACK_KERNEL = 12
+STACKS_GEMM, STACKS_STREAM = 0, 1
 SPLIT_INFO = ("slices_P", "slices_T", "fp64_pixels_P", "fp64_columns_T", "max_bound_US",
               "max_bound_T_from_P", "max_bound_T_product", "P_split")
 STAGES = ("spectra", "build_A", "eigen_A", "build_B", "build_P", "bisect", "build_T", "epilogue",
@@ -289,8 +291,13 @@ class Solver:
             raise ValueError("dI must be (stacks, n) and dH (stacks, m)")
         if dI.stride(1) != 1 or dH.stride(1) != 1:
             raise ValueError("dI and dH need unit stride along the pixels")
-        self._call("imcom_gpu_build_images_device", int(dI.shape[0]), dI.data_ptr(),
-                   int(dI.stride(0)), dH.data_ptr(), int(dH.stride(0)))
+        # a single stack has no second row, so its row stride is arbitrary
+        # (numpy and torch may give a length-1 axis any stride)
+        one = dI.shape[0] == 1
+        ldi = self.n if one else int(dI.stride(0))
+        ldh = self.m if one else int(dH.stride(0))
+        self._call("imcom_gpu_build_images_device", int(dI.shape[0]), dI.data_ptr(), ldi,
+                   dH.data_ptr(), ldh)
 
     def build_S(self, out=True):
         S = np.zeros(self.m) if out else None

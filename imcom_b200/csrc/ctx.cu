@@ -362,6 +362,10 @@ int imcom_gpu_set_option(imcom_ctx* ctx, int option, long long value) {
       if (value != 0 && value != -1 && value != 8 && value != 16) return -3;
       ctx->tail_ctas = (int)value;
       return 0;
+    case IMCOM_OPT_STACK_KERNEL:
+      if (value != IMCOM_STACKS_GEMM && value != IMCOM_STACKS_STREAM) return -3;
+      ctx->stack_kernel = (int)value;
+      return 0;
     case IMCOM_OPT_BISECT_CTAS_PER_SM:
       if (value < 0 || value > 64) return -3;
       ctx->bisect_ctas = (int)value;

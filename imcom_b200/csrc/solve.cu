@@ -103,6 +103,88 @@ __global__ void eval_kernel(BisectArgs a, PixelSmem plan, double* __restrict__ o
   }
 }
 
+// H(:, s) = T^T I(:, s) for the stacks s0 .. s0+SG-1 of this grid row
+// (blockIdx.y), streaming T once per pass.  Each warp holds STK_CPW columns
+// of T; each lane takes the rows k = k0 + lane + 32 j of a chunk of STK_KC
+// rows and keeps STK_CPW x SG partial sums in registers, so one T value
+// (from HBM) serves SG stacks and one stack value (from shared memory)
+// serves STK_CPW columns.  The chunk of the stacks is staged stack-major
+// (Is[s][k]) so that a warp's 32 lanes read 32 consecutive doubles; rows past
+// n and stacks past S are zero-filled and add nothing.  The next chunk's T
+// values are loaded before the current chunk is summed.
+constexpr int STK_WARPS = 4, STK_CPW = 4, STK_KC = 128, STK_J = STK_KC / 32;
+constexpr int STK_COLS = STK_WARPS * STK_CPW;  // columns of T per CTA
+
+template <int SG>
+__global__ void __launch_bounds__(STK_WARPS * 32, 3)
+stacks_kernel(const double* __restrict__ T, long long ldt, const double* __restrict__ I,
+              long long ldi, double* __restrict__ H, long long ldh, int n, int m, int S) {
+  __shared__ double Is[SG * STK_KC];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int s0 = blockIdx.y * SG;
+  const int sg = min(SG, S - s0);
+  const long long a0 = ((long long)blockIdx.x * STK_WARPS + warp) * STK_CPW;
+  const double* tcol[STK_CPW];
+  bool cv[STK_CPW];
+#pragma unroll
+  for (int c = 0; c < STK_CPW; ++c) {
+    cv[c] = a0 + c < m;
+    tcol[c] = T + (cv[c] ? a0 + c : 0) * ldt;
+  }
+  double acc[STK_CPW][SG];
+#pragma unroll
+  for (int c = 0; c < STK_CPW; ++c)
+#pragma unroll
+    for (int s = 0; s < SG; ++s) acc[c][s] = 0.0;
+
+  double tn[STK_J][STK_CPW];
+  auto load_t = [&](int k0) {
+#pragma unroll
+    for (int j = 0; j < STK_J; ++j) {
+      const int k = k0 + lane + 32 * j;
+#pragma unroll
+      for (int c = 0; c < STK_CPW; ++c) tn[j][c] = (cv[c] && k < n) ? __ldg(tcol[c] + k) : 0.0;
+    }
+  };
+  load_t(0);
+  for (int k0 = 0; k0 < n; k0 += STK_KC) {
+    double tc[STK_J][STK_CPW];
+#pragma unroll
+    for (int j = 0; j < STK_J; ++j)
+#pragma unroll
+      for (int c = 0; c < STK_CPW; ++c) tc[j][c] = tn[j][c];
+    if (k0 + STK_KC < n) load_t(k0 + STK_KC);
+    __syncthreads();  // every warp is done with the previous chunk of Is
+    for (int e = threadIdx.x; e < SG * STK_KC; e += blockDim.x) {
+      const int s = e / STK_KC, kk = e - s * STK_KC;
+      const int k = k0 + kk;
+      Is[e] = (s < sg && k < n) ? I[k + (long long)(s0 + s) * ldi] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < STK_J; ++j) {
+      const int kk = lane + 32 * j;
+#pragma unroll
+      for (int s = 0; s < SG; ++s) {
+        const double iv = Is[s * STK_KC + kk];
+#pragma unroll
+        for (int c = 0; c < STK_CPW; ++c) acc[c][s] = fma(tc[j][c], iv, acc[c][s]);
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < STK_CPW; ++c)
+#pragma unroll
+    for (int s = 0; s < SG; ++s) {
+      double v = acc[c][s];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      // every lane holds the sum; one lane per (column, stack) writes it
+      if (((c * SG + s) & 31) == lane && cv[c] && s < sg)
+        H[(a0 + c) + (long long)(s0 + s) * ldh] = v;
+    }
+}
+
 // H_a = sum_i T_ia I_i and S_a = sum_i T_ia (T_ia Ndiag_i), one warp per a.
 __global__ void image_s_kernel(const double* __restrict__ T, long long ldt,
                                const double* __restrict__ I, const double* __restrict__ Nd,
@@ -341,11 +423,37 @@ extern "C" int imcom_gpu_build_image(imcom_ctx* ctx, double* H_out) {
 // imcom_build_image (imcom_matrix.f90:754-790); for all stacks together it is
 // one FP64 GEMM (M = m, N = stacks, K = n) in which T crosses HBM once
 // instead of once per stack.
+template <int SG>
+static int launch_stacks(imcom_ctx* ctx, int nstack, const double* dI, long long ldi, double* dH,
+                         long long ldh) {
+  const dim3 grid((unsigned)((ctx->m + STK_COLS - 1) / STK_COLS),
+                  (unsigned)((nstack + SG - 1) / SG));
+  stacks_kernel<SG><<<grid, STK_WARPS * 32, 0, ctx->stream>>>(ctx->T.p, ctx->T.ld, dI, ldi, dH,
+                                                              ldh, ctx->n, ctx->m, nstack);
+  IMC_LAUNCH();
+  return 0;
+}
+
 static int build_images(imcom_ctx* ctx, int nstack, const double* dI, long long ldi,
                         double* dH, long long ldh) {
   stage_begin(ctx, ST_EPI);
-  IMC_TRY(dgemm(ctx, 'T', 'N', ctx->m, nstack, ctx->n, 1.0, ctx->T.p, ctx->T.ld, dI, ldi, 0.0,
-                dH, ldh));
+  if (ctx->stack_kernel == IMCOM_STACKS_STREAM) {
+    // passes of at most 8 stacks: 4 x 8 partial sums and two 4 x 4 blocks of
+    // T values per lane fill the register budget of three CTAs per SM
+    if ((nstack + 7) / 8 > 65535)
+      return set_err(ctx, IMCOM_ERR_STATE, "%d stacks exceed one streaming launch", nstack);
+    if (nstack == 1)
+      IMC_TRY(launch_stacks<1>(ctx, nstack, dI, ldi, dH, ldh));
+    else if (nstack == 2)
+      IMC_TRY(launch_stacks<2>(ctx, nstack, dI, ldi, dH, ldh));
+    else if (nstack <= 4)
+      IMC_TRY(launch_stacks<4>(ctx, nstack, dI, ldi, dH, ldh));
+    else
+      IMC_TRY(launch_stacks<8>(ctx, nstack, dI, ldi, dH, ldh));
+  } else {
+    IMC_TRY(dgemm(ctx, 'T', 'N', ctx->m, nstack, ctx->n, 1.0, ctx->T.p, ctx->T.ld, dI, ldi, 0.0,
+                  dH, ldh));
+  }
   stage_end(ctx, ST_EPI);
   return 0;
 }

@@ -6,12 +6,15 @@ same dithers, mask and PSFs, forming H = T^T I per stack (imcom_build_image,
 imcom_matrix.f90:754-790).  One stack is a matrix-vector product that streams
 T (8 n m bytes) from HBM; S stacks at once are one FP64 GEMM (M = m, N = S,
 K = n) that streams T once, so the work per stack falls until the GEMM turns
-compute-bound near S = 4 x (FP64 peak / HBM bandwidth) ~ 20 stacks.
+compute-bound near S = 4 x (FP64 peak / HBM bandwidth) ~ 20 stacks.  The
+streaming kernel (IMCOM_OPT_STACK_KERNEL = 1) does the same sums with FP64
+FMAs in passes of up to 8 stacks, without the GEMM's 128-wide stack tile.
 
-    python -m imcom_b200.t_reuse [--n 4096 --m 4096 --stacks 1 16 64]
+    python -m imcom_b200.t_reuse [--n 4096 --m 4096 --stacks 1 8 16 64]
+                                 [--kernel gemm|stream]
 
-prints one JSON line: per stack count the device time of the GEMM (T
-resident, L2 flushed before each launch, CUDA events on the library stream),
+prints one JSON line: per stack count the device time of the chosen kernel
+(T resident, L2 flushed before each launch, CUDA events on the library stream),
 its HBM and FP64 rooflines, the same work as one per-stack launch per stack,
 the end-to-end rate through the host-array entry point (stack copies in and
 H copies out included), and the largest error against numpy's T^T I as a
@@ -26,7 +29,7 @@ import time
 
 import numpy as np
 
-from .api import EPS, Solver
+from .api import EPS, OPT_STACK_KERNEL, STACKS_GEMM, STACKS_STREAM, Solver
 
 L2_BYTES = 126 * 1024 * 1024
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -60,7 +63,10 @@ def _dgemm_peak(torch, dev):
     return best
 
 
-def measure(n=4096, m=4096, stacks=(1, 16, 64), reps=5, warmup=3, device=0, seed=0):
+def measure(n=4096, m=4096, stacks=(1, 8, 16, 64), reps=5, warmup=3, device=0, seed=0,
+            kernel="gemm"):
+    """kernel: "gemm" (the FP64 GEMM) or "stream" (the streaming kernel of
+    up to 8 stacks per pass over T)."""
     import torch
 
     dev = torch.device("cuda", device)
@@ -69,12 +75,14 @@ def measure(n=4096, m=4096, stacks=(1, 16, 64), reps=5, warmup=3, device=0, seed
     hbm, hbm_src = _hbm_peak()
     f64 = _dgemm_peak(torch, dev)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
-    out = {"workload": f"T resident ({n} inputs x {m} outputs, {8 * n * m / 1e6:.0f} MB), "
+    out = {"kernel": kernel,
+           "workload": f"T resident ({n} inputs x {m} outputs, {8 * n * m / 1e6:.0f} MB), "
                        "H = T^T I for S stacks at once",
            "n": n, "m": m, "hbm_peak_gbs": hbm, "hbm_peak_source": hbm_src,
            "fp64_peak_tflops": f64, "fp64_peak_source": "cuBLAS DGEMM 8192^3 in this run",
            "l2": "flushed before every timed launch (252 MB write)", "runs": []}
     with Solver(device) as s:
+        s.set_option(OPT_STACK_KERNEL, STACKS_STREAM if kernel == "stream" else STACKS_GEMM)
         # the geometry only fixes n and m; T's values do not change the work
         s.set_inputs(rng.uniform(0, 64, n), rng.uniform(0, 64, n), np.ones(n, dtype=np.int32),
                      rng.uniform(0, 64, m), rng.uniform(0, 64, m), I_i=rng.standard_normal(n))
@@ -136,12 +144,13 @@ def main():
     ap = argparse.ArgumentParser(description="H = T^T I for many image stacks (T reuse)")
     ap.add_argument("--n", type=int, default=4096)
     ap.add_argument("--m", type=int, default=4096)
-    ap.add_argument("--stacks", type=int, nargs="+", default=[1, 16, 64])
+    ap.add_argument("--stacks", type=int, nargs="+", default=[1, 8, 16, 64])
+    ap.add_argument("--kernel", choices=["gemm", "stream"], default="gemm")
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--device", type=int, default=0)
     args = ap.parse_args()
-    print(json.dumps(measure(args.n, args.m, tuple(args.stacks), args.reps, device=args.device)),
-          flush=True)
+    print(json.dumps(measure(args.n, args.m, tuple(args.stacks), args.reps, device=args.device,
+                             kernel=args.kernel)), flush=True)
 
 
 if __name__ == "__main__":

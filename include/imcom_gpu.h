@@ -93,6 +93,13 @@ typedef struct imcom_ctx imcom_ctx;
  * side can make wait; smaller clusters hold smaller tails.  Same results to
  * rounding either way. */
 #define IMCOM_OPT_TAIL_CTAS 11
+/* Kernel of imcom_gpu_build_images: 0 = the FP64 GEMM (default), 1 = a
+ * streaming kernel for a few stacks (up to 8 stacks per pass over T, FP64
+ * FMA, each warp holding four columns of T against the stacks of its pass).
+ * Same sums to rounding. */
+#define IMCOM_OPT_STACK_KERNEL 12
+#define IMCOM_STACKS_GEMM 0
+#define IMCOM_STACKS_STREAM 1
 
 /* ---- context ---------------------------------------------------------- */
 

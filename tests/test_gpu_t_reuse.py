@@ -66,6 +66,13 @@ def test_build_images_device_strided():
         Hw = dHw.cpu().numpy()
         check(Hw[:, :m].T, T, I)
         assert np.all(Hw[:, m:] == 7.0)  # nothing written past m
+        # one stack, whatever stride its length-1 axis carries
+        d1 = torch.from_numpy(np.ascontiguousarray(I[:, :1].T)).to("cuda")
+        h1 = torch.empty((1, m), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        s.build_images_device(d1, h1)
+        s.synchronize()
+        check(h1.cpu().numpy().T, T, I[:, :1])
 
 
 def test_build_images_errors():

@@ -74,3 +74,25 @@ def test_null_context_is_an_argument_error():
     assert lib.imcom_gpu_build_image(None, None) == -1
     assert lib.imcom_gpu_build_images(None, 2, None, None) == -1
     assert lib.imcom_gpu_build_images_device(None, 2, None, 1, None, 1) == -1
+
+
+def test_build_images_device_leading_dimensions():
+    """The device entry gets each operand's row stride as its leading
+    dimension; a single stack gets n and m whatever stride its length-1 axis
+    carries."""
+    import torch
+    from imcom_b200.api import Solver
+    s = Solver.__new__(Solver)
+    s.n, s.m = 7, 5
+    calls = []
+    s._call = lambda name, *a: calls.append((name,) + a)
+    one = torch.from_numpy(np.arange(7.0)[None, :])
+    one = one.as_strided((1, 7), (1, 1))  # a length-1 axis with stride 1
+    s.build_images_device(one, torch.zeros((1, 5), dtype=torch.float64))
+    assert calls[-1][1] == 1 and calls[-1][3] == 7 and calls[-1][5] == 5
+    wide_i = torch.zeros((3, 10), dtype=torch.float64)[:, :7]
+    wide_h = torch.zeros((3, 9), dtype=torch.float64)[:, :5]
+    s.build_images_device(wide_i, wide_h)
+    assert calls[-1][1] == 3 and calls[-1][3] == 10 and calls[-1][5] == 9
+    with pytest.raises(ValueError):
+        s.build_images_device(torch.zeros((3, 8), dtype=torch.float64), wide_h)

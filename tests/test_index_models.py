@@ -13,6 +13,9 @@ the GPU against the oracle (test_gpu_*.py).
 * jacobi_kernel (imcom_b200/csrc/eigen_jacobi.cu): the round-robin rounds
   pair every two columns exactly once per sweep, each round with disjoint
   pairs.
+* stacks_kernel (imcom_b200/csrc/solve.cu): every (column, stack) of H is
+  written by exactly one lane, every read stays inside T and the stacks, and
+  the zero-filled chunks sum to T^T I.
 * trd_tail_kernel (imcom_b200/csrc/eigen_dc.cu): the distributed row layout
   and the lazy update order (column j's update applied to row j+1 before its
   reflector and to the other rows in the next pass) give a tridiagonal form
@@ -251,3 +254,74 @@ def test_cluster_tail_order_tridiagonalises(n, ctas):
         Q = Q @ (np.eye(n) - tau[j] * np.outer(V[:, j], V[:, j]))
     T = np.diag(d) + np.diag(e, -1) + np.diag(e, 1)
     assert np.linalg.norm(Q.T @ A @ Q - T) <= 1e-13 * np.linalg.norm(A)
+
+
+# -- many-stack streaming kernel ---------------------------------------------
+
+STK_WARPS, STK_CPW, STK_KC = 4, 4, 128
+
+
+def stacks_model(T, I, SG):
+    """stacks_kernel (imcom_b200/csrc/solve.cu) restated loop for loop:
+    returns H and the number of writes of each element."""
+    n, m = T.shape
+    S = I.shape[1]
+    H = np.full((m, S), np.nan)
+    writes = np.zeros((m, S), dtype=int)
+    gx = (m + STK_WARPS * STK_CPW - 1) // (STK_WARPS * STK_CPW)
+    gy = (S + SG - 1) // SG
+    for by in range(gy):
+        s0 = by * SG
+        sg = min(SG, S - s0)
+        assert sg >= 1
+        for bx in range(gx):
+            acc = np.zeros((STK_WARPS, 32, STK_CPW, SG))
+            for k0 in range(0, n, STK_KC):
+                Is = np.zeros(SG * STK_KC)
+                for e in range(SG * STK_KC):
+                    s, kk = divmod(e, STK_KC)
+                    k = k0 + kk
+                    if s < sg and k < n:
+                        Is[e] = I[k, s0 + s]
+                for w in range(STK_WARPS):
+                    a0 = (bx * STK_WARPS + w) * STK_CPW
+                    for lane in range(32):
+                        for j in range(STK_KC // 32):
+                            k = k0 + lane + 32 * j
+                            kk = lane + 32 * j
+                            for c in range(STK_CPW):
+                                t = T[k, a0 + c] if (a0 + c < m and k < n) else 0.0
+                                for s in range(SG):
+                                    acc[w, lane, c, s] += t * Is[s * STK_KC + kk]
+            for w in range(STK_WARPS):
+                a0 = (bx * STK_WARPS + w) * STK_CPW
+                tot = acc[w].sum(axis=0)  # the butterfly leaves the sum in every lane
+                for lane in range(32):
+                    for c in range(STK_CPW):
+                        for s in range(SG):
+                            if (c * SG + s) % 32 == lane and a0 + c < m and s < sg:
+                                H[a0 + c, s0 + s] = tot[c, s]
+                                writes[a0 + c, s0 + s] += 1
+    return H, writes
+
+
+@pytest.mark.parametrize("n,m,S,SG", [(1, 1, 1, 1), (130, 17, 3, 4), (257, 33, 8, 8),
+                                      (100, 16, 19, 8), (64, 5, 2, 2)])
+def test_stacks_kernel_covers_each_output_once(n, m, S, SG):
+    rng = np.random.default_rng(n * m + S)
+    T = rng.standard_normal((n, m))
+    I = rng.standard_normal((n, S))
+    H, writes = stacks_model(T, I, SG)
+    assert np.all(writes == 1)
+    assert np.allclose(H, T.T @ I, rtol=1e-13, atol=1e-13)
+
+
+def test_stacks_launch_choice():
+    """The launch picks 1, 2, 4 or 8 stacks per pass: one pass up to 8
+    stacks, ceil(S / 8) passes (grid rows) beyond."""
+    def sg(S):
+        return 1 if S == 1 else 2 if S == 2 else 4 if S <= 4 else 8
+    for S in range(1, 70):
+        g, passes = sg(S), -(-S // sg(S))
+        assert g in (1, 2, 4, 8) and g * passes >= S
+        assert passes == (1 if S <= 8 else -(-S // 8))
