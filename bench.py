@@ -31,7 +31,9 @@ and output pixels/s over the slowest rank's wall-clock time.
 ``t_reuse``: T reused for many image stacks -- H = T^T I for 1, 8, 16 and 64
 stacks at once with T resident (imcom_b200/t_reuse.py), through the FP64 GEMM
 and through the streaming kernel, each in a child process after the timed
-solves.
+solves.  ``table_fft``: the n=4096 lookup tables' inverse FFT through the
+library's own pruned, fused transform against embedding + cuFFT + shift
+(imcom_b200/table_fft.py), in a child process too.
 
 ``--impl reference`` times the CPU oracle (the reference's algorithm restated
 in C++ with OpenMP + LAPACK/BLAS) on the same workload, all host cores.
@@ -216,14 +218,14 @@ def batched_patches(npatch=256, sample=16, rank=0, world=1, dist=None, device=No
                       "over ranks"}
 
 
-def t_reuse_child(kernel="gemm", timeout=300):
-    """H = T^T I for 1, 8, 16 and 64 image stacks at once with T resident
-    (imcom_b200/t_reuse.py) through the given kernel, measured in a child
-    process with its own CUDA context, so this line keeps its other numbers
-    whatever that run meets."""
+def child_measure(module, *args, timeout=300):
+    """Run `python -m <module> <args>` (a measurement that prints one JSON
+    line) in a child process with its own CUDA context, so this line keeps
+    its other numbers whatever that run meets; returns its JSON or an
+    {"error": ...} object."""
     try:
-        r = subprocess.run([sys.executable, "-m", "imcom_b200.t_reuse", "--kernel", kernel],
-                           cwd=ROOT, capture_output=True, text=True, timeout=timeout)
+        r = subprocess.run([sys.executable, "-m", module, *args], cwd=ROOT,
+                           capture_output=True, text=True, timeout=timeout)
     except subprocess.TimeoutExpired:
         return {"error": f"no result within {timeout} s"}
     lines = r.stdout.strip().splitlines()
@@ -535,9 +537,14 @@ def run_ours(args):
                "sample": "one full n=4096 solve (C++ restatement of the reference, OpenMP + "
                          "OpenBLAS LAPACK/BLAS), same workload"}
 
-    t_reuse = None
+    # H = T^T I for 1, 8, 16 and 64 stacks with T resident (imcom_b200/t_reuse.py)
+    # through each kernel, and the lookup tables' inverse FFT, own vs cuFFT
+    # (imcom_b200/table_fft.py)
+    t_reuse = table_fft = None
     if rank == 0 and world == 1 and not args.no_t_reuse:
-        t_reuse = {k: t_reuse_child(k) for k in ("gemm", "stream")}
+        t_reuse = {k: child_measure("imcom_b200.t_reuse", "--kernel", k) for k in ("gemm", "stream")}
+    if rank == 0 and world == 1 and not args.no_table_fft:
+        table_fft = child_measure("imcom_b200.table_fft")
 
     if rank == 0:
         line = {
@@ -569,6 +576,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "batch": batch_line,
             "t_reuse": t_reuse,
+            "table_fft": table_fft,
             "clocks": ck,
         }
         print(json.dumps(line), flush=True)
@@ -591,6 +599,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-patch measurement")
     ap.add_argument("--no-t-reuse", action="store_true",
                     help="skip the many-stack H = T^T I measurement")
+    ap.add_argument("--no-table-fft", action="store_true",
+                    help="skip the own-vs-cuFFT lookup-table FFT measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

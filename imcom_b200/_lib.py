@@ -62,6 +62,7 @@ SIGNATURES = {
     "imcom_gpu_get_stream": (_i, [_p, C.POINTER(_p)]),
     "imcom_gpu_launch_count": (_i, [_p, C.POINTER(_ll)]),
     "imcom_gpu_stage_times": (_i, [_p, _p]),
+    "imcom_gpu_table_times": (_i, [_p, _p]),
 }
 
 

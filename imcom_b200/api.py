@@ -31,6 +31,8 @@ OPT_SM_SHARE = 10
 OPT_TAIL_CTAS = 11
 OPT_STACK_KERNEL = 12
 STACKS_GEMM, STACKS_STREAM = 0, 1
+OPT_TABLE_FFT = 13
+TABLE_FFT_CUFFT, TABLE_FFT_OWN = 0, 1
 SPLIT_INFO = ("slices_P", "slices_T", "fp64_pixels_P", "fp64_columns_T", "max_bound_US",
               "max_bound_T_from_P", "max_bound_T_product", "P_split")
 STAGES = ("spectra", "build_A", "eigen_A", "build_B", "build_P", "bisect", "build_T", "epilogue",
@@ -118,6 +120,12 @@ class Solver:
         ms = np.zeros(len(STAGES))
         self._call("imcom_gpu_stage_times", _ptr(ms))
         return dict(zip(STAGES, ms.tolist()))
+
+    def table_times(self) -> dict:
+        """Milliseconds of the last A and B lookup-table builds."""
+        ms = np.zeros(2)
+        self._call("imcom_gpu_table_times", _ptr(ms))
+        return {"A_tables": float(ms[0]), "B_tables": float(ms[1])}
 
     def stream(self) -> int:
         """The context's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""

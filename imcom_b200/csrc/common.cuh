@@ -92,6 +92,10 @@ struct imcom_ctx {
   size_t tables_bytes = 0;
   double2* fftbuf = nullptr;
   size_t fftbuf_bytes = 0;
+  int table_fft = IMCOM_TABLE_FFT_CUFFT;  // inverse FFT of the lookup tables
+  double2* fft_tw = nullptr;              // exp(2 pi i t / L) of the own table FFT
+  size_t fft_tw_bytes = 0;
+  int fft_tw_L = 0;
   // work area bound to the shared cuFFT plans when this context runs them
   void* fft_work = nullptr;
   size_t fft_work_bytes = 0;
@@ -138,6 +142,8 @@ struct imcom_ctx {
   // address of the context field that holds its pointer
   std::unordered_map<void**, size_t> vec_cap;
 
+  cudaEvent_t tab_ev[2][2] = {};  // around the last A (0) and B (1) table build
+  bool tab_used[2] = {};
   cudaEvent_t ev0[imcom::ST_N] = {}, ev1[imcom::ST_N] = {};
   bool ev_used[imcom::ST_N] = {};
 };
@@ -183,6 +189,11 @@ extern unsigned long long g_launches;
 // is already large enough.  ensure_vec likewise keeps a vector whose buffer
 // already holds `count` elements (the contents are not preserved on growth).
 int ensure_mat(imcom_ctx* ctx, DMat& M, long long rows, long long cols);
+// The lookup tables' inverse 2-D FFT in two pruned, fused passes
+// (table_fft.cu); *done is false (and nothing is launched) for sides it does
+// not take, which then go through cuFFT.
+int table_fft_inverse(imcom_ctx* ctx, int nps, int L, int ntab, const int2* dpairs, double2* W,
+                      double* tab, int isB, bool* done);
 int ensure_buf(imcom_ctx* ctx, void** p, size_t& have, size_t need);
 // `batch` contiguous 2-D side x side transforms on the context's stream
 // through the process-wide plan cache: in place complex-to-complex

@@ -314,7 +314,7 @@ int imcom_gpu_destroy(imcom_ctx* ctx) {
                   ctx->T.p, ctx->Pt.p, ctx->L, ctx->K, ctx->US, ctx->H, ctx->S, ctx->U,
                   ctx->nev, ctx->flags, ctx->tables, ctx->fftbuf, ctx->mlp.w, ctx->feat,
                   ctx->gemm_ws, ctx->fb, ctx->train_buf, ctx->band, ctx->jac_buf,
-                  ctx->stacks.p, ctx->stack_H.p};
+                  ctx->stacks.p, ctx->stack_H.p, ctx->fft_tw};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete[] ctx->rot;
@@ -323,6 +323,9 @@ int imcom_gpu_destroy(imcom_ctx* ctx) {
     if (ctx->ev0[s]) cudaEventDestroy(ctx->ev0[s]);
     if (ctx->ev1[s]) cudaEventDestroy(ctx->ev1[s]);
   }
+  for (auto& pair : ctx->tab_ev)
+    for (cudaEvent_t e : pair)
+      if (e) cudaEventDestroy(e);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
   return 0;
@@ -361,6 +364,10 @@ int imcom_gpu_set_option(imcom_ctx* ctx, int option, long long value) {
     case IMCOM_OPT_TAIL_CTAS:
       if (value != 0 && value != -1 && value != 8 && value != 16) return -3;
       ctx->tail_ctas = (int)value;
+      return 0;
+    case IMCOM_OPT_TABLE_FFT:
+      if (value != IMCOM_TABLE_FFT_CUFFT && value != IMCOM_TABLE_FFT_OWN) return -3;
+      ctx->table_fft = (int)value;
       return 0;
     case IMCOM_OPT_STACK_KERNEL:
       if (value != IMCOM_STACKS_GEMM && value != IMCOM_STACKS_STREAM) return -3;
@@ -611,6 +618,22 @@ int imcom_gpu_get_stream(imcom_ctx* ctx, void** stream) {
   if (!ctx) return -1;
   if (!stream) return -2;
   *stream = (void*)ctx->stream;
+  return 0;
+}
+
+int imcom_gpu_table_times(imcom_ctx* ctx, double* ms2) {
+  if (!ctx) return -1;
+  if (!ms2) return -2;
+  cudaSetDevice(ctx->device);
+  IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (int k = 0; k < 2; ++k) {
+    float t = 0.f;
+    ms2[k] = (ctx->tab_used[k] &&
+              cudaEventElapsedTime(&t, ctx->tab_ev[k][0], ctx->tab_ev[k][1]) == cudaSuccess)
+                 ? t
+                 : 0.0;
+  }
+  cudaGetLastError();
   return 0;
 }
 

@@ -1,0 +1,335 @@
+// table_fft.cu -- the lookup tables' inverse 2-D FFT, pruned and fused.
+//
+// imcom_build_Alookup / imcom_build_Blookup (imcom_matrix.f90:400-416,
+// 467-480) embed conj(Gt_e) Gt_f (or conj(Gammat) Gt_e) in the middle of an
+// npad-times larger frequency grid (side L = npad nps), inverse-FFT the grid
+// (imcom_invft_c2c, imcom_proc.f90:498-512, an FFTW backward DFT) and keep the
+// cshifted, scaled real part as the table.  The default path does that as
+// embed_kernel -> cuFFT Z2Z -> shift_scale_kernel (tables.cu).  This file does
+// the same in two passes over HBM, using that only nps of the grid's L lines
+// are non-zero:
+//   pass 1  the nps non-zero lines, computed from the spectra straight into
+//           shared memory and transformed along p; the result W (nps x L per
+//           table) is 1/npad of the grid.
+//   pass 2  TP columns of W at a time, scattered into zero lines of length L,
+//           transformed along q and written as the shifted, scaled real table.
+// Per table element that is ~16/npad bytes written and read back plus the
+// 8-byte table, against a full complex grid written by the embedding, the
+// FFT's passes over it and the shift's read of it.
+//
+// The line transforms are the Stockham autosort formulation (Govindaraju et
+// al., "High performance discrete Fourier transforms on graphics
+// processors", SC 2008), stage by stage in place in shared memory: every
+// thread reads its butterflies' inputs into registers, the block
+// synchronises, and the outputs go to their autosorted places.  Radices 4, 2,
+// 3, 5, 7; the twiddles come from a table of exp(2 pi i t / L) computed on the
+// host in extended precision.  Sides with another prime factor, or longer
+// than a block's shared memory holds, stay on cuFFT.
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+
+namespace imcom {
+
+namespace {
+
+constexpr int FFT_THREADS = 512;
+constexpr int FFT_MAX_ELEMS = 8192;  // TP x LS complex values in shared memory (128 KiB)
+
+// Elements a block may hold when its plan has a stage of radix R: each thread
+// keeps the inputs of cap / (R x FFT_THREADS) butterflies (16, 16, 12, 10 and
+// 7 complex values for R = 2, 4, 3, 5, 7) in registers between a stage's
+// reads and writes, inside the 128 registers of a thread of a 512-thread
+// block.
+constexpr int fft_cap(int R) {
+  return R == 3 ? 6144 : R == 5 ? 5120 : R == 7 ? 3584 : FFT_MAX_ELEMS;
+}
+
+struct FftPlan {
+  int L = 0;   // transform length (grid side)
+  int LS = 0;  // shared-memory stride of a line: L rounded up to odd (no bank conflicts
+               // between the lines of a column read)
+  int TP = 0;  // lines per block (TP x LS <= fft_cap of every radix of the plan)
+  int count[5] = {};  // stages of radix 4, 2, 3, 5, 7 (run in that order)
+};
+
+constexpr int kRadices[5] = {4, 2, 3, 5, 7};
+
+bool make_plan(int L, FftPlan* p) {
+  if (L < 1) return false;
+  p->L = L;
+  p->LS = (L % 2 == 0) ? L + 1 : L;
+  if (p->LS > FFT_MAX_ELEMS) return false;
+  int n = L, cap = FFT_MAX_ELEMS;
+  for (int i = 0; i < 5; ++i) {
+    const int r = kRadices[i];
+    p->count[i] = 0;
+    while (n % r == 0) {
+      ++p->count[i];
+      n /= r;
+    }
+    if (p->count[i] > 0 && fft_cap(r) < cap) cap = fft_cap(r);
+  }
+  if (n != 1) return false;
+  p->TP = cap / p->LS < 8 ? cap / p->LS : 8;
+  return p->TP >= 1;
+}
+
+// Fortran CSHIFT source index (1-based): cshift(X, s)(i) = X(1 + mod(i-1+s, n)).
+__device__ __forceinline__ int cshift_src(int i1, int s, int n) {
+  return 1 + ((i1 - 1 + s) % n + n) % n;
+}
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// The embedded grid value: conj(Gt_e) Gt_f (A) or conj(Gammat) Gt_e (B) times
+// imcom_upsilon2D = (1, 0), rounded step by step as embed_kernel does.
+__device__ __forceinline__ double2 pair_product(const double2* __restrict__ Gt,
+                                                const double2* __restrict__ Gammat, int2 pr,
+                                                size_t s, int nps) {
+  const size_t plane = (size_t)nps * nps;
+  double2 a, b;
+  if (pr.y > 0) {
+    a = Gt[s + (size_t)(pr.x - 1) * plane];
+    b = Gt[s + (size_t)(pr.y - 1) * plane];
+  } else {
+    a = Gammat[s];
+    b = Gt[s + (size_t)(pr.x - 1) * plane];
+  }
+  const double ar = a.x, ai = -a.y;
+  const double xr = __dsub_rn(__dmul_rn(ar, b.x), __dmul_rn(ai, b.y));
+  const double xi = __dadd_rn(__dmul_rn(ar, b.y), __dmul_rn(ai, b.x));
+  return make_double2(__dsub_rn(__dmul_rn(xr, 1.0), __dmul_rn(xi, 0.0)),
+                      __dadd_rn(__dmul_rn(xr, 0.0), __dmul_rn(xi, 1.0)));
+}
+
+// DFT of length R with the + sign, y_r = sum_s v_s exp(2 pi i r s / R),
+// stored to y[r Ns] as each output is formed (no output array is held).  Odd
+// R uses the symmetric pairs: with a_s = v_s + v_{R-s}, b_s = v_s - v_{R-s}
+// (s = 1 .. (R-1)/2), y_r and y_{R-r} = v_0 + sum_s a_s cos(2 pi r s / R)
+// +- i sum_s b_s sin(2 pi r s / R); v is overwritten with the a_s and b_s.
+template <int R>
+__device__ __forceinline__ void dft_store(double2 (&v)[R], const double2* __restrict__ tw, int L,
+                                          double2* y, int Ns) {
+  if constexpr (R == 2) {
+    y[0] = make_double2(v[0].x + v[1].x, v[0].y + v[1].y);
+    y[Ns] = make_double2(v[0].x - v[1].x, v[0].y - v[1].y);
+  } else if constexpr (R == 4) {
+    const double2 s0 = make_double2(v[0].x + v[2].x, v[0].y + v[2].y);
+    const double2 d0 = make_double2(v[0].x - v[2].x, v[0].y - v[2].y);
+    const double2 s1 = make_double2(v[1].x + v[3].x, v[1].y + v[3].y);
+    const double2 d1 = make_double2(v[1].x - v[3].x, v[1].y - v[3].y);
+    y[0] = make_double2(s0.x + s1.x, s0.y + s1.y);
+    y[2 * Ns] = make_double2(s0.x - s1.x, s0.y - s1.y);
+    // d0 +- i d1, i (x, y) = (-y, x)
+    y[Ns] = make_double2(d0.x - d1.y, d0.y + d1.x);
+    y[3 * Ns] = make_double2(d0.x + d1.y, d0.y - d1.x);
+  } else {
+    constexpr int H = (R - 1) / 2;
+    const int step = L / R;
+    double2 y0 = v[0];
+#pragma unroll
+    for (int s = 1; s <= H; ++s) {
+      const double2 a = make_double2(v[s].x + v[R - s].x, v[s].y + v[R - s].y);
+      const double2 b = make_double2(v[s].x - v[R - s].x, v[s].y - v[R - s].y);
+      v[s] = a;
+      v[R - s] = b;
+      y0.x += a.x;
+      y0.y += a.y;
+    }
+    y[0] = y0;
+#pragma unroll
+    for (int r = 1; r <= H; ++r) {
+      double2 A = v[0], B = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int s = 1; s <= H; ++s) {
+        const double2 w = tw[((r * s) % R) * step];  // (cos, sin) of 2 pi r s / R
+        A.x += v[s].x * w.x;
+        A.y += v[s].y * w.x;
+        B.x += v[R - s].x * w.y;
+        B.y += v[R - s].y * w.y;
+      }
+      y[r * Ns] = make_double2(A.x - B.y, A.y + B.x);
+      y[(R - r) * Ns] = make_double2(A.x + B.y, A.y - B.x);
+    }
+  }
+}
+
+// One Stockham stage of radix R over the block's TP lines (span Ns before
+// the stage).  Butterfly j of a line reads x[j + r L/R], multiplies input r by
+// exp(2 pi i k r / (Ns R)) (k = j mod Ns) and writes x[(j div Ns) Ns R + k + r Ns].
+template <int R>
+__device__ __forceinline__ void fft_stage(double2* buf, const FftPlan& plan, int Ns,
+                                          const double2* __restrict__ tw) {
+  // butterflies per thread: TP x L / R <= fft_cap(R) / R = JM x FFT_THREADS
+  constexpr int JM = fft_cap(R) / (R * FFT_THREADS);
+  static_assert(JM * R * FFT_THREADS == fft_cap(R), "cap is a whole number of butterflies");
+  const int L = plan.L, LS = plan.LS;
+  const int per = L / R;
+  const int B = plan.TP * per;
+  double2 v[JM][R];
+#pragma unroll
+  for (int i = 0; i < JM; ++i) {
+    const int b = threadIdx.x + i * FFT_THREADS;
+    if (b < B) {
+      const int line = b / per, j = b - line * per;
+      const double2* x = buf + line * LS + j;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[i][r] = x[r * per];
+    }
+  }
+  __syncthreads();  // every input is in registers before any output lands
+  const int tstep = L / (Ns * R);
+#pragma unroll
+  for (int i = 0; i < JM; ++i) {
+    const int b = threadIdx.x + i * FFT_THREADS;
+    if (b < B) {
+      const int line = b / per, j = b - line * per;
+      const int k = j % Ns;
+      if (Ns > 1) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[i][r] = cmul(v[i][r], tw[k * r * tstep]);
+      }
+      dft_store<R>(v[i], tw, L, buf + line * LS + (j / Ns) * Ns * R + k, Ns);
+    }
+  }
+  __syncthreads();
+}
+
+// The plan's stages in its order (all radix-4 stages, then 2, 3, 5, 7): one
+// counted loop per radix, so each stage body is compiled once.
+__device__ __forceinline__ void run_stages(double2* buf, const FftPlan& plan,
+                                           const double2* __restrict__ tw) {
+  int Ns = 1;
+  for (int i = 0; i < plan.count[0]; ++i, Ns *= 4) fft_stage<4>(buf, plan, Ns, tw);
+  for (int i = 0; i < plan.count[1]; ++i, Ns *= 2) fft_stage<2>(buf, plan, Ns, tw);
+  for (int i = 0; i < plan.count[2]; ++i, Ns *= 3) fft_stage<3>(buf, plan, Ns, tw);
+  for (int i = 0; i < plan.count[3]; ++i, Ns *= 5) fft_stage<5>(buf, plan, Ns, tw);
+  for (int i = 0; i < plan.count[4]; ++i, Ns *= 7) fft_stage<7>(buf, plan, Ns, tw);
+}
+
+// Pass 1: lines u0 .. u0+TP-1 of the nps non-zero grid lines (grid row
+// sq = nmin + u) of table blockIdx.y, transformed along p, into W.
+__global__ void __launch_bounds__(FFT_THREADS, 1)
+table_fft_pass1(FftPlan plan, const double2* __restrict__ Gt, const double2* __restrict__ Gammat,
+                const int2* __restrict__ pairs, const double2* __restrict__ tw,
+                double2* __restrict__ W, int nps) {
+  extern __shared__ double2 buf[];
+  const int L = plan.L, LS = plan.LS, TP = plan.TP;
+  const int t = blockIdx.y;
+  const int u0 = blockIdx.x * TP;
+  const int s = L / 2, nmin = (L - nps) / 2 + 1;
+  const int2 pr = pairs[t];
+  for (int e = threadIdx.x; e < TP * L; e += FFT_THREADS) {
+    const int line = e / L, p0 = e - line * L;
+    const int u = u0 + line;
+    double2 v = make_double2(0.0, 0.0);
+    if (u < nps) {
+      const int sp = cshift_src(p0 + 1, s, L);
+      if (sp >= nmin && sp < nmin + nps) {
+        const int si = cshift_src(sp - nmin + 1, nps / 2, nps);
+        const int sj = cshift_src(u + 1, nps / 2, nps);
+        v = pair_product(Gt, Gammat, pr, (size_t)(si - 1) + (size_t)(sj - 1) * nps, nps);
+      }
+    }
+    buf[line * LS + p0] = v;
+  }
+  __syncthreads();
+  run_stages(buf, plan, tw);
+  for (int e = threadIdx.x; e < TP * L; e += FFT_THREADS) {
+    const int line = e / L, k1 = e - line * L;
+    const int u = u0 + line;
+    if (u < nps) W[((size_t)t * nps + u) * L + k1] = buf[line * LS + k1];
+  }
+}
+
+// Pass 2: columns c0 .. c0+TP-1 of W for table blockIdx.y, each scattered
+// into a zero line of length L at the grid rows of its nps entries,
+// transformed along q and written to the table through the cshifts:
+// tab(p, q) = s Re F(cshift(p), cshift(q)), s = 1/nps^2 (A) or -2/nps^2 (B).
+__global__ void __launch_bounds__(FFT_THREADS, 1)
+table_fft_pass2(FftPlan plan, const double2* __restrict__ W, const double2* __restrict__ tw,
+                double* __restrict__ tab, int nps, int isB) {
+  extern __shared__ double2 buf[];
+  const int L = plan.L, LS = plan.LS, TP = plan.TP;
+  const int t = blockIdx.y;
+  const int c0 = blockIdx.x * TP;
+  const int s = L / 2, nmin = (L - nps) / 2 + 1;
+  for (int e = threadIdx.x; e < TP * L; e += FFT_THREADS) {
+    const int line = e / L, q0 = e - line * L;
+    buf[line * LS + q0] = make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < nps * TP; e += FFT_THREADS) {
+    const int u = e / TP, c = e - u * TP;
+    const int k1 = c0 + c;
+    if (k1 < L) {
+      const int q0 = ((nmin + u - 1 - s) % L + L) % L;
+      buf[c * LS + q0] = W[((size_t)t * nps + u) * L + k1];
+    }
+  }
+  __syncthreads();
+  run_stages(buf, plan, tw);
+  const size_t tbase = (size_t)t * L * L;
+  for (int e = threadIdx.x; e < TP * L; e += FFT_THREADS) {
+    const int k2 = e / TP, c = e - k2 * TP;
+    const int k1 = c0 + c;
+    if (k1 < L) {
+      double v = buf[c * LS + k2].x;
+      if (isB) v = -2.0 * v;
+      const int p0 = ((k1 - s) % L + L) % L, q0 = ((k2 - s) % L + L) % L;
+      tab[tbase + (size_t)q0 * L + p0] = v / (double)nps / (double)nps;
+    }
+  }
+}
+
+// exp(2 pi i t / L), t < L, rounded from extended precision; the parts that
+// are exactly 0 (where 4t is a multiple of L) come out as exact zeros.
+std::vector<double2> twiddles(int L) {
+  const long double two_pi = 6.283185307179586476925286766559005768L;
+  std::vector<double2> tw(L);
+  for (int t = 0; t < L; ++t) {
+    const long double a = two_pi * (long double)t / (long double)L;
+    long double c = cosl(a), s = sinl(a);
+    if (fabsl(c) < 1e-18L) c = 0.0L;
+    if (fabsl(s) < 1e-18L) s = 0.0L;
+    tw[t] = make_double2((double)c, (double)s);
+  }
+  return tw;
+}
+
+}  // namespace
+
+int table_fft_inverse(imcom_ctx* ctx, int nps, int L, int ntab, const int2* dpairs, double2* W,
+                      double* tab, int isB, bool* done) {
+  *done = false;
+  FftPlan plan;
+  if (nps <= 0 || (L - nps) % 2 != 0 || L < nps || !make_plan(L, &plan)) return 0;
+  if (ctx->fft_tw_L != L) {
+    IMC_CUDA(cudaStreamSynchronize(ctx->stream));  // no launch still reads the old table
+    IMC_TRY(ensure_buf(ctx, (void**)&ctx->fft_tw, ctx->fft_tw_bytes, (size_t)L * sizeof(double2)));
+    const std::vector<double2> tw = twiddles(L);
+    IMC_CUDA(cudaMemcpy(ctx->fft_tw, tw.data(), (size_t)L * sizeof(double2),
+                        cudaMemcpyHostToDevice));
+    ctx->fft_tw_L = L;
+  }
+  const int smem = plan.TP * plan.LS * (int)sizeof(double2);
+  IMC_CUDA(cudaFuncSetAttribute(table_fft_pass1, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                smem));
+  IMC_CUDA(cudaFuncSetAttribute(table_fft_pass2, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                smem));
+  const dim3 g1((unsigned)((nps + plan.TP - 1) / plan.TP), (unsigned)ntab);
+  table_fft_pass1<<<g1, FFT_THREADS, smem, ctx->stream>>>(plan, ctx->Gt, ctx->Gammat, dpairs,
+                                                          ctx->fft_tw, W, nps);
+  IMC_LAUNCH();
+  const dim3 g2((unsigned)((L + plan.TP - 1) / plan.TP), (unsigned)ntab);
+  table_fft_pass2<<<g2, FFT_THREADS, smem, ctx->stream>>>(plan, W, ctx->fft_tw, tab, nps, isB);
+  IMC_LAUNCH();
+  *done = true;
+  return 0;
+}
+
+}  // namespace imcom

@@ -242,7 +242,7 @@ int sum_device(imcom_ctx* ctx, const double* a, size_t count, double* dst, doubl
 
 // Build the lookup tables for A (isB = 0: all pairs e <= f, packed index
 // ial = e + f(f-1)/2) or B (isB = 1: one per exposure) into ctx->tables.
-int build_tables(imcom_ctx* ctx, int npad, int isB) {
+static int build_tables_body(imcom_ctx* ctx, int npad, int isB) {
   int nps = ctx->nps, E = ctx->nexppsf;
   int nbig = nps * npad;
   std::vector<int2> pairs;
@@ -262,12 +262,31 @@ int build_tables(imcom_ctx* ctx, int npad, int isB) {
                                          big2 * ntab * sizeof(double2));
   IMC_CUDA(cudaMemcpyAsync(dpairs, pairs.data(), ntab * sizeof(int2), cudaMemcpyHostToDevice,
                            ctx->stream));
+  if (ctx->table_fft == IMCOM_TABLE_FFT_OWN) {
+    bool done = false;
+    IMC_TRY(table_fft_inverse(ctx, nps, nbig, ntab, dpairs, ctx->fftbuf, ctx->tables, isB, &done));
+    if (done) return 0;
+  }
   dim3 blk(128), grd((nbig + 127) / 128, nbig, ntab);
   embed_kernel<<<grd, blk, 0, ctx->stream>>>(ctx->Gt, ctx->Gammat, dpairs, ctx->fftbuf, nps, nbig);
   IMC_LAUNCH();
   IMC_TRY(fft_z2z(ctx, nbig, ntab, ctx->fftbuf, CUFFT_INVERSE));
   shift_scale_kernel<<<grd, blk, 0, ctx->stream>>>(ctx->fftbuf, ctx->tables, nbig, nps, isB);
   IMC_LAUNCH();
+  return 0;
+}
+
+// The table build between two events (imcom_gpu_table_times).
+int build_tables(imcom_ctx* ctx, int npad, int isB) {
+  cudaEvent_t* ev = ctx->tab_ev[isB ? 1 : 0];
+  if (!ev[0]) {
+    IMC_CUDA(cudaEventCreate(&ev[0]));
+    IMC_CUDA(cudaEventCreate(&ev[1]));
+  }
+  IMC_CUDA(cudaEventRecord(ev[0], ctx->stream));
+  IMC_TRY(build_tables_body(ctx, npad, isB));
+  IMC_CUDA(cudaEventRecord(ev[1], ctx->stream));
+  ctx->tab_used[isB ? 1 : 0] = true;
   return 0;
 }
 

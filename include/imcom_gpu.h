@@ -100,6 +100,15 @@ typedef struct imcom_ctx imcom_ctx;
 #define IMCOM_OPT_STACK_KERNEL 12
 #define IMCOM_STACKS_GEMM 0
 #define IMCOM_STACKS_STREAM 1
+/* Inverse 2-D FFT of the lookup tables (imcom_build_Alookup/Blookup): 0 =
+ * embedding, cuFFT and shift as separate steps (default); 1 = the library's
+ * own transform in two passes that skip the grid's zero lines and fuse the
+ * embedding and the shift (sides L = npad nps whose prime factors are 2, 3, 5
+ * and 7, up to 8191, 6143 with a factor 3, 5119 with a 5, 3583 with a 7;
+ * other sides keep cuFFT).  Same tables to rounding. */
+#define IMCOM_OPT_TABLE_FFT 13
+#define IMCOM_TABLE_FFT_CUFFT 0
+#define IMCOM_TABLE_FFT_OWN 1
 
 /* ---- context ---------------------------------------------------------- */
 
@@ -371,6 +380,10 @@ int imcom_gpu_get_stream(imcom_ctx* ctx, void** stream);
  * epilogue, eigen tridiagonalisation, eigen divide and conquer, eigen
  * back-transformation] (11 values). */
 int imcom_gpu_stage_times(imcom_ctx* ctx, double* ms11);
+/* Milliseconds of the last lookup-table build (within build_A and build_B:
+ * embedding, inverse FFT and shift) for the A tables and the B tables
+ * (2 values; 0 where none has run). */
+int imcom_gpu_table_times(imcom_ctx* ctx, double* ms2);
 
 #ifdef __cplusplus
 }

@@ -325,3 +325,186 @@ def test_stacks_launch_choice():
         g, passes = sg(S), -(-S // sg(S))
         assert g in (1, 2, 4, 8) and g * passes >= S
         assert passes == (1 if S <= 8 else -(-S // 8))
+
+
+# -- fused, pruned table FFT ---------------------------------------------------
+
+
+def fft_radices(L):
+    """The factorisation table_fft.cu uses: fours first, then 2, 3, 5, 7."""
+    out = []
+    while L % 4 == 0:
+        out.append(4)
+        L //= 4
+    for r in (2, 3, 5, 7):
+        while L % r == 0:
+            out.append(r)
+            L //= r
+    return out if L == 1 else None
+
+
+def stockham(x, tw):
+    """One line of the kernel's in-place Stockham stages (sign +, natural
+    order out): per stage of radix R and span Ns, butterfly j reads
+    x[j + r L/R], twiddles by tw[k r L/(Ns R)] (k = j mod Ns), and writes
+    x[(j div Ns) Ns R + k + r Ns]."""
+    L = len(x)
+    Ns = 1
+    for R in fft_radices(L):
+        per = L // R
+        v = [[x[j + r * per] for r in range(R)] for j in range(per)]  # all reads first
+        for j in range(per):
+            k = j % Ns
+            vv = [v[j][0]] + [v[j][r] * tw[k * r * (L // (Ns * R))] for r in range(1, R)]
+            base = (j // Ns) * Ns * R + k
+            for r in range(R):
+                x[base + r * Ns] = sum(vv[s] * tw[((r * s) % R) * (L // R)] for s in range(R))
+        Ns *= R
+    return x
+
+
+def cshift_src(i1, s, n):
+    return 1 + ((i1 - 1 + s) % n + n) % n
+
+
+def table_model(Gt, Gammat, pairs, nps, L, isB):
+    """table_fft.cu's two passes: pass 1 transforms the nps non-zero lines
+    of the embedded grid along p into W (nps x L per table); pass 2
+    scatters W's columns into zero lines along q, transforms them and
+    writes the shifted, scaled real table."""
+    s = L // 2
+    nmin = (L - nps) // 2 + 1
+    tw = np.exp(2j * np.pi * np.arange(L) / L)
+    tabs = []
+    for pr in pairs:
+        W = np.zeros((nps, L), complex)
+        for u in range(nps):
+            sj = cshift_src(u + 1, nps // 2, nps)
+            line = np.zeros(L, complex)
+            for p0 in range(L):
+                sp = cshift_src(p0 + 1, s, L)
+                if nmin <= sp < nmin + nps:
+                    si = cshift_src(sp - nmin + 1, nps // 2, nps)
+                    if pr[1] > 0:  # A: conj(Gt_e) Gt_f
+                        a, b = Gt[si - 1, sj - 1, pr[0] - 1], Gt[si - 1, sj - 1, pr[1] - 1]
+                    else:  # B: conj(Gammat) Gt_e
+                        a, b = Gammat[si - 1, sj - 1], Gt[si - 1, sj - 1, pr[0] - 1]
+                    line[p0] = np.conj(a) * b
+            W[u] = stockham(line, tw)
+        tab = np.full((L, L), np.nan)  # tab[p-1, q-1]
+        for k1 in range(L):
+            col = np.zeros(L, complex)
+            for u in range(nps):
+                q0 = (nmin + u - 1 - s) % L  # the line of grid row sq = nmin + u
+                col[q0] = W[u, k1]
+            F = stockham(col, tw)
+            for k2 in range(L):
+                v = F[k2].real
+                if isB:
+                    v = -2.0 * v
+                tab[(k1 - s) % L, (k2 - s) % L] = v / nps / nps
+        tabs.append(tab)
+    return tabs
+
+
+def table_reference(Gt, Gammat, pairs, nps, L, isB):
+    """The cuFFT path restated: embed_kernel, an unnormalised inverse 2-D
+    FFT, shift_scale_kernel."""
+    s = L // 2
+    nmin, nmax = (L - nps) // 2 + 1, (L + nps) // 2
+    tabs = []
+    for pr in pairs:
+        grid = np.zeros((L, L), complex)  # grid[p-1, q-1]
+        for q in range(1, L + 1):
+            for p in range(1, L + 1):
+                sp, sq = cshift_src(p, s, L), cshift_src(q, s, L)
+                if nmin <= sp <= nmax and nmin <= sq <= nmax:
+                    si = cshift_src(sp - nmin + 1, nps // 2, nps)
+                    sj = cshift_src(sq - nmin + 1, nps // 2, nps)
+                    if pr[1] > 0:
+                        a, b = Gt[si - 1, sj - 1, pr[0] - 1], Gt[si - 1, sj - 1, pr[1] - 1]
+                    else:
+                        a, b = Gammat[si - 1, sj - 1], Gt[si - 1, sj - 1, pr[0] - 1]
+                    grid[p - 1, q - 1] = np.conj(a) * b
+        F = np.fft.ifft2(grid) * L * L
+        tab = np.empty((L, L))
+        for q in range(1, L + 1):
+            for p in range(1, L + 1):
+                v = F[cshift_src(p, s, L) - 1, cshift_src(q, s, L) - 1].real
+                tab[p - 1, q - 1] = (-2.0 * v if isB else v) / nps / nps
+        tabs.append(tab)
+    return tabs
+
+
+@pytest.mark.parametrize("nps,npad", [(2, 3), (4, 3), (6, 3), (10, 3), (4, 5), (6, 2)])
+def test_pruned_table_fft_matches_embed_fft_shift(nps, npad):
+    L = nps * npad
+    if fft_radices(L) is None:
+        pytest.skip("size outside the kernel's radices")
+    rng = np.random.default_rng(nps * 10 + npad)
+    E = 2
+    Gt = rng.standard_normal((nps, nps, E)) + 1j * rng.standard_normal((nps, nps, E))
+    Gammat = rng.standard_normal((nps, nps)) + 1j * rng.standard_normal((nps, nps))
+    for isB, pairs in ((0, [(1, 1), (1, 2), (2, 2)]), (1, [(1, 0), (2, 0)])):
+        got = table_model(Gt, Gammat, pairs, nps, L, isB)
+        ref = table_reference(Gt, Gammat, pairs, nps, L, isB)
+        for g, r in zip(got, ref):
+            assert not np.isnan(g).any()
+            assert np.max(np.abs(g - r)) <= 1e-12 * max(1.0, np.max(np.abs(r)))
+
+
+def test_fft_radices_cover_the_workload_sides():
+    assert fft_radices(1728) == [4, 4, 4, 3, 3, 3]  # nps 576 (n = 4096 workload)
+    assert fft_radices(3 * 2 * 11) is None  # a factor 11: cuFFT keeps such sizes
+    for L in range(1, 400):
+        r = fft_radices(L)
+        if r is not None:
+            assert int(np.prod(r)) == L
+
+
+@pytest.mark.parametrize("R", [3, 5, 7])
+def test_symmetric_pair_dft_is_the_dft(R):
+    """dft_store's odd radices: y_r, y_{R-r} = v_0 + sum_s a_s cos(2 pi r s/R)
+    +- i sum_s b_s sin(2 pi r s/R), a_s = v_s + v_{R-s}, b_s = v_s - v_{R-s}."""
+    rng = np.random.default_rng(R)
+    v = rng.standard_normal(R) + 1j * rng.standard_normal(R)
+    H = (R - 1) // 2
+    a = {s: v[s] + v[R - s] for s in range(1, H + 1)}
+    b = {s: v[s] - v[R - s] for s in range(1, H + 1)}
+    y = np.empty(R, complex)
+    y[0] = v[0] + sum(a.values())
+    for r in range(1, H + 1):
+        A = v[0] + sum(a[s] * np.cos(2 * np.pi * r * s / R) for s in a)
+        B = sum(b[s] * np.sin(2 * np.pi * r * s / R) for s in b)
+        y[r], y[R - r] = A + 1j * B, A - 1j * B
+    assert np.allclose(y, np.fft.ifft(v) * R, atol=1e-13)
+
+
+FFT_THREADS = 512
+FFT_CAP = {4: 8192, 2: 8192, 3: 6144, 5: 5120, 7: 3584}
+
+
+def fft_plan(L):
+    """make_plan (table_fft.cu): odd line stride, lines per block from the
+    smallest cap of the plan's radices."""
+    r = fft_radices(L)
+    LS = L + 1 if L % 2 == 0 else L
+    if r is None or LS > 8192:
+        return None
+    cap = min([FFT_CAP[x] for x in r] + [8192])
+    TP = min(8, cap // LS)
+    return (LS, TP, r) if TP >= 1 else None
+
+
+def test_fft_plan_keeps_every_stage_in_its_registers():
+    for L in list(range(1, 700)) + [1728, 2304, 3456, 5120, 6144, 8190]:
+        plan = fft_plan(L)
+        if plan is None:
+            continue
+        LS, TP, radices = plan
+        assert LS % 2 == 1 and LS >= L and TP * LS <= 8192
+        for R in set(radices):
+            JM = FFT_CAP[R] // (R * FFT_THREADS)
+            assert JM * R * FFT_THREADS == FFT_CAP[R]
+            assert TP * (L // R) <= JM * FFT_THREADS  # butterflies fit the register array
+    assert fft_plan(1728)[:2] == (1729, 3)  # radix 3 caps the block at 6144 values
