@@ -6,8 +6,13 @@ files built here by hand in every BITPIX, with BSCALE / BZERO, BLANK and NaN
 pixels (undefined pixels read as -666, the reference's null value,
 imcom_io.f90:366), headers longer than one block and D exponents.  Sizes
 that do not match, missing and malformed files are errors, where the
-reference stops (imcom_io.f90:382-393).
+reference stops (imcom_io.f90:382-393).  Files written by the reference's own
+tooling (its example inputs, tests/golden/fits_examples.npz) read back bit for
+bit and are written again with the same keys, values, data and padding.
 """
+import hashlib
+import os
+
 import numpy as np
 import pytest
 
@@ -15,6 +20,7 @@ from imcom_b200 import fits
 from imcom_b200._lib import ImcomError
 
 IMCOM_ERR_FITS = 10
+EXAMPLES = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "fits_examples.npz")
 
 
 def cards_of(raw):
@@ -200,3 +206,32 @@ def test_errors(tmp_path):
     noend.write_bytes(raw[:80 * 3])
     with pytest.raises(ImcomError, match="END"):
         fits.size(str(noend))
+
+
+@pytest.mark.parametrize("name", ["test1", "x2", "ideal_output"])
+def test_reference_example_files(tmp_path, name):
+    """The reference's example inputs (written by its CFITSIO tooling): the
+    library reads them bit for bit, and its writer reproduces every card's
+    key and value columns, the header padding and the data records byte for
+    byte (only the card comments differ)."""
+    gold = np.load(EXAMPLES)
+    header = gold[f"{name}_header"].tobytes()
+    image = np.asfortranarray(gold[f"{name}_image"])
+    data = image.ravel(order="F").astype(">f8").tobytes()
+    data += b"\0" * ((-len(data)) % 2880)
+    assert hashlib.sha256(data).hexdigest() == str(gold[f"{name}_data_sha256"])
+    p = tmp_path / f"{name}.fits"
+    p.write_bytes(header + data)
+    assert fits.size(str(p)) == (image.shape[0], image.shape[1], -64)
+    got = fits.read(str(p))
+    assert np.array_equal(got.view(np.uint64), image.view(np.uint64))
+    q = str(tmp_path / "again.fits")
+    fits.write(q, got)
+    again = open(q, "rb").read()
+    assert len(again) == len(header) + len(data) and again[2880:] == data
+    for i in range(36):
+        ref, card = header[80 * i:80 * i + 80], again[80 * i:80 * i + 80]
+        assert card[:30] == ref[:30]
+        if ref.startswith(b"END "):
+            break
+    assert again[80 * i:2880] == header[80 * i:2880]
