@@ -219,6 +219,52 @@ INTERFACE
     INTEGER(C_INT), DIMENSION(count) :: sweeps
   END FUNCTION
 
+  ! Wait for the context's queued work; returns the first asynchronous error
+  INTEGER(C_INT) FUNCTION imcom_gpu_synchronize(ctx) BIND(C, NAME="imcom_gpu_synchronize")
+    IMPORT :: C_INT, C_PTR
+    TYPE(C_PTR), VALUE :: ctx
+  END FUNCTION
+
+  ! Kappa map K_a from a previous solve (imcom_data.f90:104)
+  INTEGER(C_INT) FUNCTION imcom_gpu_load_K(ctx, K) BIND(C, NAME="imcom_gpu_load_K")
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: ctx
+    REAL(C_DOUBLE), DIMENSION(*), INTENT(IN) :: K
+  END FUNCTION
+
+  ! Learned-kappa MLP weights (12 -> 64 -> 64 -> 2, real(C_FLOAT) arrays,
+  ! row-major [out][in]) and the feature normalisation (12 means, 12 stds)
+  INTEGER(C_INT) FUNCTION imcom_gpu_mlp_set_weights(ctx, W1, b1, W2, b2, W3, b3, feat_mean, &
+                                                    feat_std) &
+                                                    BIND(C, NAME="imcom_gpu_mlp_set_weights")
+    IMPORT :: C_INT, C_PTR, C_FLOAT
+    TYPE(C_PTR), VALUE :: ctx
+    REAL(C_FLOAT), DIMENSION(*), INTENT(IN) :: W1, b1, W2, b2, W3, b3, feat_mean, feat_std
+  END FUNCTION
+
+  ! Per pixel (m each): 1 where the split audit recomputed the P column (or
+  ! the T column) in FP64
+  INTEGER(C_INT) FUNCTION imcom_gpu_split_pixels(ctx, fp64_P, fp64_T) &
+                                                 BIND(C, NAME="imcom_gpu_split_pixels")
+    IMPORT :: C_INT, C_PTR
+    TYPE(C_PTR), VALUE :: ctx
+    INTEGER(C_INT), DIMENSION(*) :: fp64_P, fp64_T
+  END FUNCTION
+
+  ! GPU milliseconds of the last call of each stage (11 values, order as in
+  ! include/imcom_gpu.h) and of the last A and B table builds (2 values)
+  INTEGER(C_INT) FUNCTION imcom_gpu_stage_times(ctx, ms11) BIND(C, NAME="imcom_gpu_stage_times")
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: ctx
+    REAL(C_DOUBLE), DIMENSION(11) :: ms11
+  END FUNCTION
+
+  INTEGER(C_INT) FUNCTION imcom_gpu_table_times(ctx, ms2) BIND(C, NAME="imcom_gpu_table_times")
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: ctx
+    REAL(C_DOUBLE), DIMENSION(2) :: ms2
+  END FUNCTION
+
   ! imcom_build_image for nstack image stacks sharing the resident T:
   ! I_stack(n, nstack) -> H(m, nstack), one FP64 GEMM (T read once)
   INTEGER(C_INT) FUNCTION imcom_gpu_build_images(ctx, nstack, I_stack, H) &
