@@ -102,6 +102,12 @@ struct imcom_ctx {
 
   int8_t* band = nullptr;   // eigenmode band indices of the learned-kappa features
   size_t band_bytes = 0;
+  int kappa_feat = 0;       // IMCOM_OPT_KAPPA_FEATURES
+  float2* nbr = nullptr;    // per pixel: neighbour count and exposures (valid for these inputs)
+  size_t nbr_bytes = 0;
+  bool nbr_valid = false;
+  int* band_seg = nullptr;  // first eigenmode of bands 0..8, then a non-monotone flag
+  size_t band_seg_bytes = 0;
   int* fb = nullptr;        // per-pixel fallback flags of the learned bisection
   size_t fb_bytes = 0;
   void* train_buf = nullptr;  // MLP training data and state

@@ -314,7 +314,7 @@ int imcom_gpu_destroy(imcom_ctx* ctx) {
                   ctx->T.p, ctx->Pt.p, ctx->L, ctx->K, ctx->US, ctx->H, ctx->S, ctx->U,
                   ctx->nev, ctx->flags, ctx->tables, ctx->fftbuf, ctx->mlp.w, ctx->feat,
                   ctx->gemm_ws, ctx->fb, ctx->train_buf, ctx->band, ctx->jac_buf,
-                  ctx->stacks.p, ctx->stack_H.p, ctx->fft_tw};
+                  ctx->stacks.p, ctx->stack_H.p, ctx->fft_tw, ctx->nbr, ctx->band_seg};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete[] ctx->rot;
@@ -364,6 +364,10 @@ int imcom_gpu_set_option(imcom_ctx* ctx, int option, long long value) {
     case IMCOM_OPT_TAIL_CTAS:
       if (value != 0 && value != -1 && value != 8 && value != 16) return -3;
       ctx->tail_ctas = (int)value;
+      return 0;
+    case IMCOM_OPT_KAPPA_FEATURES:
+      if (value != 0 && value != 1) return -3;
+      ctx->kappa_feat = (int)value;
       return 0;
     case IMCOM_OPT_TABLE_FFT:
       if (value != IMCOM_TABLE_FFT_CUFFT && value != IMCOM_TABLE_FFT_OWN) return -3;
@@ -452,6 +456,7 @@ int imcom_gpu_set_inputs(imcom_ctx* ctx, int n, int m, const double* x_i, const 
   IMC_CUDA(cudaMemcpyAsync(ctx->X, X_a, m * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   IMC_CUDA(cudaMemcpyAsync(ctx->Y, Y_a, m * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   ctx->have_I = I_i != nullptr;
+  ctx->nbr_valid = false;  // the neighbour table belongs to the previous inputs
   ctx->have_N = Ndiag != nullptr;
   if (I_i)
     IMC_CUDA(cudaMemcpyAsync(ctx->I, I_i, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));

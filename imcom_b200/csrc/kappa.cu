@@ -66,11 +66,13 @@ __global__ void band_index_kernel(const double* __restrict__ lam, int n,
   }
 }
 
-// Features of one pixel, every lane gets all 12.
-__device__ void pixel_features(const double* __restrict__ x, const double* __restrict__ y,
-                               const int* __restrict__ expi, int n, double Xa, double Ya,
-                               const double* lam, const int8_t* __restrict__ bidx,
-                               const double* col, double C, double US_max, int lane, float* f) {
+// Neighbour features of one pixel on one warp: the inputs within one pixel
+// in x and y of (Xa, Ya), and the exposures they come from (as a bit mask).
+__device__ __forceinline__ void neighbours(const double* __restrict__ x,
+                                           const double* __restrict__ y,
+                                           const int* __restrict__ expi, int n, double Xa,
+                                           double Ya, int lane, double* cnt_out,
+                                           unsigned* mask_out) {
   double cnt = 0.0;
   unsigned mask = 0u;
   for (int i = lane; i < n; i += 32) {
@@ -83,16 +85,84 @@ __device__ void pixel_features(const double* __restrict__ x, const double* __res
   cnt = wsum(cnt);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) mask |= __shfl_xor_sync(0xffffffffu, mask, o);
+  *cnt_out = cnt;
+  *mask_out = mask;
+}
+
+// The neighbour features of every pixel (one warp each), kept while the
+// inputs stay the same: (count, number of exposures).
+__global__ void neighbour_kernel(const double* __restrict__ x, const double* __restrict__ y,
+                                 const int* __restrict__ expi, int n,
+                                 const double* __restrict__ X, const double* __restrict__ Y,
+                                 int m, float2* __restrict__ nbr) {
+  const int lane = threadIdx.x & 31;
+  const int pix = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (pix >= m) return;
+  double cnt;
+  unsigned mask;
+  neighbours(x, y, expi, n, X[pix], Y[pix], lane, &cnt, &mask);
+  if (lane == 0) nbr[pix] = make_float2((float)cnt, (float)__popc(mask));
+}
+
+// First eigenmode of each band: seg[k] = first p with bidx[p] >= k (k = 0..8,
+// seg[8] = n), for a band index that is non-decreasing in p; seg[9] is set
+// to 1 (it must be 0 before the launch) where it decreases somewhere.  With
+// a non-decreasing index every seg[k] has exactly one writer.
+__global__ void band_segments_kernel(const int8_t* __restrict__ bidx, int n,
+                                     int* __restrict__ seg) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const int b = bidx[p];
+    const int prev = p > 0 ? bidx[p - 1] : -1;
+    if (b < prev) {
+      atomicOr(seg + 9, 1);
+      continue;
+    }
+    for (int k = prev + 1; k <= b; ++k) seg[k] = p;
+    if (p == n - 1)
+      for (int k = b + 1; k <= 8; ++k) seg[k] = n;
+  }
+}
+
+// Features of one pixel, every lane gets all 12.  nbr_pix (may be null):
+// this pixel's entry of the neighbour table; seg (may be null): the band
+// segments of band_segments_kernel, used when the band index was monotone.
+__device__ void pixel_features(const double* __restrict__ x, const double* __restrict__ y,
+                               const int* __restrict__ expi, int n, double Xa, double Ya,
+                               const double* lam, const int8_t* __restrict__ bidx,
+                               const double* col, double C, double US_max, int lane, float* f,
+                               const float2* nbr_pix = nullptr, const int* seg = nullptr) {
+  float cntf, nexpf;
+  if (nbr_pix) {
+    const float2 v = *nbr_pix;
+    cntf = v.x;
+    nexpf = v.y;
+  } else {
+    double cnt;
+    unsigned mask;
+    neighbours(x, y, expi, n, Xa, Ya, lane, &cnt, &mask);
+    cntf = (float)cnt;
+    nexpf = (float)__popc(mask);
+  }
   const double lmax = lam[0];  // eigenvalues are in descending order
   double band[8];
 #pragma unroll
   for (int b = 0; b < 8; ++b) band[b] = 0.0;
-  for (int p = lane; p < n; p += 32) {
-    const double pp = col[p];
-    const int b = bidx[p];
+  if (seg && seg[9] == 0) {
+    // the band index is non-decreasing: band b is the modes seg[b] .. seg[b+1]-1
 #pragma unroll
-    for (int q = 0; q < 8; ++q)
-      if (q == b) band[q] += pp * pp;
+    for (int b = 0; b < 8; ++b) {
+      double s = 0.0;
+      for (int p = seg[b] + lane; p < seg[b + 1]; p += 32) s = fma(col[p], col[p], s);
+      band[b] = s;
+    }
+  } else {
+    for (int p = lane; p < n; p += 32) {
+      const double pp = col[p];
+      const int b = bidx[p];
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        if (q == b) band[q] += pp * pp;
+    }
   }
 #pragma unroll
   for (int b = 0; b < 8; ++b) {
@@ -100,8 +170,8 @@ __device__ void pixel_features(const double* __restrict__ x, const double* __res
     const double lc = lmax * pow(10.0, -(2.0 * b + 1.0));
     f[2 + b] = (float)log10(s / (4.0 * C * (lc > 0.0 ? lc : 1e-300)) + 1e-30);
   }
-  f[0] = (float)cnt;
-  f[1] = (float)__popc(mask);
+  f[0] = cntf;
+  f[1] = nexpf;
   f[10] = (float)log10(fabs(US_max) + 1e-300);
   f[11] = (float)log10(fabs(lmax / C) + 1e-300);
 }
@@ -163,13 +233,14 @@ __device__ void mlp_forward_warp(const float* __restrict__ W, const float* f, in
 __global__ void features_kernel(BisectArgs a, const double* __restrict__ x,
                                 const double* __restrict__ y, const int* __restrict__ expi,
                                 const double* __restrict__ X, const double* __restrict__ Y,
-                                const int8_t* __restrict__ bidx, float* __restrict__ feat) {
+                                const int8_t* __restrict__ bidx, const float2* __restrict__ nbr,
+                                const int* __restrict__ seg, float* __restrict__ feat) {
   const int lane = threadIdx.x & 31;
   const int pix = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (pix >= a.m) return;
   float f[NF];
   pixel_features(x, y, expi, a.n, X[pix], Y[pix], a.L, bidx, a.P + (size_t)pix * a.ldp, a.C,
-                 a.US_max, lane, f);
+                 a.US_max, lane, f, nbr ? nbr + pix : nullptr, seg);
   if (lane < NF) {
 #pragma unroll
     for (int k = 0; k < NF; ++k)
@@ -181,6 +252,8 @@ struct LearnedExtra {
   const double *x, *y, *X, *Y;
   const int* expi;
   const int8_t* bidx;  // band of every eigenmode (band_index_kernel)
+  const float2* nbr;   // neighbour table (IMCOM_OPT_KAPPA_FEATURES = 1) or null
+  const int* seg;      // band segments (IMCOM_OPT_KAPPA_FEATURES = 1) or null
   const float* W;
   int* fallback;
   double half_scale;  // bracket half-width = half_scale * exp(output 1), decades
@@ -199,7 +272,7 @@ __device__ __forceinline__ void learned_pixel(const BisectArgs& a, const Learned
   const bool U = a.UnotS != 0;
   float f[NF], o[NO];
   pixel_features(ex.x, ex.y, ex.expi, a.n, ex.X[pix], ex.Y[pix], lam, ex.bidx, col, a.C,
-                 a.US_max, lane, f);
+                 a.US_max, lane, f, ex.nbr ? ex.nbr + pix : nullptr, ex.seg);
   mlp_forward_warp(sW, f, lane, o);
   double hw = ex.half_scale * exp((double)fminf(fmaxf(o[1], -20.0f), 5.0f));
   hw = fmin(fmax(hw, ex.min_half), 4.0);
@@ -518,6 +591,33 @@ __global__ void adam_kernel(float* __restrict__ params, const float* __restrict_
 
 }  // namespace
 
+// Band index of every eigenmode, and with IMCOM_OPT_KAPPA_FEATURES = 1 the
+// band segments and (once per set of inputs) the neighbour table.
+int feature_tables(imcom_ctx* ctx, const float2** nbr, const int** seg) {
+  IMC_TRY(ensure_buf(ctx, (void**)&ctx->band, ctx->band_bytes, (size_t)ctx->n));
+  band_index_kernel<<<(ctx->n + 255) / 256, 256, 0, ctx->stream>>>(ctx->L, ctx->n, ctx->band);
+  IMC_LAUNCH();
+  *nbr = nullptr;
+  *seg = nullptr;
+  if (!ctx->kappa_feat) return 0;
+  IMC_TRY(ensure_buf(ctx, (void**)&ctx->band_seg, ctx->band_seg_bytes, 10 * sizeof(int)));
+  IMC_CUDA(cudaMemsetAsync(ctx->band_seg, 0, 10 * sizeof(int), ctx->stream));
+  band_segments_kernel<<<(ctx->n + 255) / 256, 256, 0, ctx->stream>>>(ctx->band, ctx->n,
+                                                                      ctx->band_seg);
+  IMC_LAUNCH();
+  if (!ctx->nbr_valid) {
+    IMC_TRY(ensure_buf(ctx, (void**)&ctx->nbr, ctx->nbr_bytes, (size_t)ctx->m * sizeof(float2)));
+    neighbour_kernel<<<(ctx->m + 7) / 8, 256, 0, ctx->stream>>>(ctx->x, ctx->y, ctx->exp_i,
+                                                                ctx->n, ctx->X, ctx->Y, ctx->m,
+                                                                ctx->nbr);
+    IMC_LAUNCH();
+    ctx->nbr_valid = true;
+  }
+  *nbr = ctx->nbr;
+  *seg = ctx->band_seg;
+  return 0;
+}
+
 int fill_learned(imcom_ctx* ctx, LearnedExtra& ex) {
   if (!ctx->mlp.set) return set_err(ctx, IMCOM_ERR_STATE, "imcom_gpu_mlp_set_weights has not run");
   ex.x = ctx->x;
@@ -527,10 +627,8 @@ int fill_learned(imcom_ctx* ctx, LearnedExtra& ex) {
   ex.expi = ctx->exp_i;
   ex.W = ctx->mlp.w;
   ex.fallback = nullptr;
-  // band of every eigenmode for the P2 band features
-  IMC_TRY(ensure_buf(ctx, (void**)&ctx->band, ctx->band_bytes, (size_t)ctx->n));
-  band_index_kernel<<<(ctx->n + 255) / 256, 256, 0, ctx->stream>>>(ctx->L, ctx->n, ctx->band);
-  IMC_LAUNCH();
+  // band of every eigenmode for the P2 band features (+ segments, neighbours)
+  IMC_TRY(feature_tables(ctx, &ex.nbr, &ex.seg));
   ex.bidx = ctx->band;
   ex.half_scale = 3.0;
   ex.min_half = 0.02;
@@ -550,12 +648,12 @@ extern "C" int imcom_gpu_kappa_features(imcom_ctx* ctx, int UnotS, double US_max
   IMC_TRY(fill_bisect_args(ctx, a, UnotS, US_max, 1.0, 1.0, 0.0, 0, C_a));
   cudaSetDevice(ctx->device);
   IMC_TRY(ensure_vec(ctx, &ctx->feat, (size_t)NF * ctx->m));
-  IMC_TRY(ensure_buf(ctx, (void**)&ctx->band, ctx->band_bytes, (size_t)ctx->n));
-  band_index_kernel<<<(ctx->n + 255) / 256, 256, 0, ctx->stream>>>(ctx->L, ctx->n, ctx->band);
-  IMC_LAUNCH();
+  const float2* nbr;
+  const int* seg;
+  IMC_TRY(feature_tables(ctx, &nbr, &seg));
   int blocks = (ctx->m + 7) / 8;
   features_kernel<<<blocks, 256, 0, ctx->stream>>>(a, ctx->x, ctx->y, ctx->exp_i, ctx->X, ctx->Y,
-                                                   ctx->band, ctx->feat);
+                                                   ctx->band, nbr, seg, ctx->feat);
   IMC_LAUNCH();
   IMC_CUDA(cudaMemcpyAsync(feat_out, ctx->feat, (size_t)NF * ctx->m * sizeof(float),
                            cudaMemcpyDeviceToHost, ctx->stream));

@@ -7,11 +7,17 @@ can select one stage's kernels, e.g.
         python -m imcom_b200.stages n4096
 
 Usage: python -m imcom_b200.stages [workload] [--library-eigensolver] [--split]
-                                    [--learned]
+                                    [--learned] [--table-features]
+                                    [--own-table-fft] [--repeat-bisect N]
 
---split    P and T on the split-precision int8 product (IMCOM_PREC_SPLIT)
---learned  learned-kappa bracket (committed weights) instead of the plain
-           bisection
+--split           P and T on the split-precision int8 product (IMCOM_PREC_SPLIT)
+--learned         learned-kappa bracket (committed weights) instead of the plain
+                  bisection
+--table-features  learned-kappa features from the neighbour table and band
+                  segments (IMCOM_OPT_KAPPA_FEATURES = 1)
+--own-table-fft   the library's own inverse FFT for the lookup tables
+                  (IMCOM_OPT_TABLE_FFT = 1)
+--repeat-bisect N run the bisection N more times and print each one's time
 """
 from __future__ import annotations
 
@@ -22,6 +28,7 @@ def main(argv):
     import torch
 
     from . import EIGH_DC, EIGH_LIBRARY, EPS, Solver, synth
+    from .api import OPT_KAPPA_FEATURES, OPT_TABLE_FFT
 
     wl = argv[0] if argv and not argv[0].startswith("-") else "n4096"
     nv = torch.cuda.nvtx
@@ -29,6 +36,8 @@ def main(argv):
     with Solver(0) as s:
         s.set_eigensolver(EIGH_LIBRARY if "--library-eigensolver" in argv else EIGH_DC)
         s.set_precision("--split" in argv)
+        s.set_option(OPT_KAPPA_FEATURES, 1 if "--table-features" in argv else 0)
+        s.set_option(OPT_TABLE_FFT, 1 if "--own-table-fft" in argv else 0)
         learned = "--learned" in argv
         if learned:
             from .kappa_model import DEFAULT_WEIGHTS, KappaModel
@@ -47,15 +56,24 @@ def main(argv):
         stage("EIG", lambda: s.eigen_A(out=False))
         stage("B", lambda: s.build_B(out=False))
         stage("P", lambda: s.build_P(out=False))
-        if learned:
-            stage("BISECT", lambda: s.bisect_kappa_learned(True, 1e-2, C * EPS, C / EPS, 1e-5,
-                                                           53, C, out=False))
-        else:
-            stage("BISECT", lambda: s.bisect_kappa(True, 1e-2, C * EPS, C / EPS, 1e-5, 53, C,
-                                                   out=False))
+        def bisect():
+            if learned:
+                return s.bisect_kappa_learned(True, 1e-2, C * EPS, C / EPS, 1e-5, 53, C,
+                                              out=False)
+            return s.bisect_kappa(True, 1e-2, C * EPS, C / EPS, 1e-5, 53, C, out=False)
+
+        stage("BISECT", bisect)
         stage("T", lambda: s.build_T(out=False))
         stage("EPI", lambda: (s.build_S(out=False), s.build_image(out=False)))
         print({k: round(v, 3) for k, v in s.stage_times().items()})
+        print({k: round(v, 3) for k, v in s.table_times().items()})
+        if "--repeat-bisect" in argv:
+            reps = int(argv[argv.index("--repeat-bisect") + 1])
+            times = []
+            for _ in range(reps):
+                stage("BISECT", bisect)
+                times.append(round(s.stage_times()["bisect"], 3))
+            print({"bisect_ms": times})
 
 
 if __name__ == "__main__":

@@ -109,6 +109,14 @@ typedef struct imcom_ctx imcom_ctx;
 #define IMCOM_OPT_TABLE_FFT 13
 #define IMCOM_TABLE_FFT_CUFFT 0
 #define IMCOM_TABLE_FFT_OWN 1
+/* Features of the learned-kappa bracket: 0 = every pixel scans all inputs
+ * for its neighbours and bins P^2 by eigenmode band element by element
+ * (default); 1 = the neighbour features come from a per-pixel table built
+ * once per set of inputs, and the band sums run over the bands' contiguous
+ * ranges of eigenmodes (the band index is non-decreasing when L is in
+ * descending order; otherwise the element-wise binning is kept).  Same
+ * features to rounding, same kappa. */
+#define IMCOM_OPT_KAPPA_FEATURES 14
 
 /* ---- context ---------------------------------------------------------- */
 

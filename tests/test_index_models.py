@@ -508,3 +508,63 @@ def test_fft_plan_keeps_every_stage_in_its_registers():
             assert JM * R * FFT_THREADS == FFT_CAP[R]
             assert TP * (L // R) <= JM * FFT_THREADS  # butterflies fit the register array
     assert fft_plan(1728)[:2] == (1729, 3)  # radix 3 caps the block at 6144 values
+
+
+# -- learned-kappa band segments ------------------------------------------------
+
+
+def band_segments(bidx):
+    """band_segments_kernel (imcom_b200/csrc/kappa.cu) restated thread for
+    thread: seg[k] = first p with bidx[p] >= k (seg[8] = n), seg[9] = 1 where
+    the index decreases; returns seg and the writes of each seg[k]."""
+    n = len(bidx)
+    seg = [0] * 10
+    writes = [0] * 9
+    for p in range(n):
+        b = int(bidx[p])
+        prev = int(bidx[p - 1]) if p > 0 else -1
+        if b < prev:
+            seg[9] = 1
+            continue
+        for k in range(prev + 1, b + 1):
+            seg[k] = p
+            writes[k] += 1
+        if p == n - 1:
+            for k in range(b + 1, 9):
+                seg[k] = n
+                writes[k] += 1
+    return seg, writes
+
+
+def band_index(lam):
+    lmax = lam[0]
+    out = []
+    for v in lam:
+        r = v / lmax if (v > 0 and lmax > 0) else 0.0
+        b = int(np.floor(-np.log10(r) * 0.5)) if r > 0 else 7
+        out.append(min(max(b, 0), 7))
+    return np.array(out)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_band_segments_are_the_bands(seed):
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(1, 300))
+    lam = np.sort(10.0 ** rng.uniform(-18, 0, n))[::-1]
+    if seed % 2:
+        lam[-min(5, n):] = -np.abs(lam[-min(5, n):])  # tiny negative eigenvalues: band 7
+    bidx = band_index(lam)
+    assert np.all(np.diff(bidx) >= 0)  # descending eigenvalues give a monotone band index
+    seg, writes = band_segments(bidx)
+    assert seg[9] == 0 and writes == [1] * 9 and seg[8] == n
+    P = rng.standard_normal(n)
+    for b in range(8):
+        assert np.array_equal(np.arange(seg[b], seg[b + 1]), np.nonzero(bidx == b)[0])
+        assert np.isclose(np.sum(P[seg[b]:seg[b + 1]] ** 2), np.sum(P[bidx == b] ** 2))
+
+
+def test_band_segments_flag_a_decreasing_index():
+    seg, _ = band_segments(np.array([0, 0, 2, 1, 3]))
+    assert seg[9] == 1
+    seg, writes = band_segments(np.array([5]))
+    assert seg[:9] == [0, 0, 0, 0, 0, 0, 1, 1, 1] and writes == [1] * 9
