@@ -33,7 +33,9 @@ stacks at once with T resident (imcom_b200/t_reuse.py), through the FP64 GEMM
 and through the streaming kernel, each in a child process after the timed
 solves.  ``table_fft``: the n=4096 lookup tables' inverse FFT through the
 library's own pruned, fused transform against embedding + cuFFT + shift
-(imcom_b200/table_fft.py), in a child process too.
+(imcom_b200/table_fft.py), in a child process too.  ``kappa_features``: the
+learned bisection with its features scanned per pixel against the neighbour
+table and band segments (python -m imcom_b200.stages --compare-features).
 
 ``--impl reference`` times the CPU oracle (the reference's algorithm restated
 in C++ with OpenMP + LAPACK/BLAS) on the same workload, all host cores.
@@ -540,11 +542,14 @@ def run_ours(args):
     # H = T^T I for 1, 8, 16 and 64 stacks with T resident (imcom_b200/t_reuse.py)
     # through each kernel, and the lookup tables' inverse FFT, own vs cuFFT
     # (imcom_b200/table_fft.py)
-    t_reuse = table_fft = None
+    t_reuse = table_fft = kappa_features = None
     if rank == 0 and world == 1 and not args.no_t_reuse:
         t_reuse = {k: child_measure("imcom_b200.t_reuse", "--kernel", k) for k in ("gemm", "stream")}
     if rank == 0 and world == 1 and not args.no_table_fft:
         table_fft = child_measure("imcom_b200.table_fft")
+        # learned-kappa features: per-pixel scan vs neighbour table + band segments
+        kappa_features = child_measure("imcom_b200.stages", "n4096", "--split",
+                                       "--compare-features")
 
     if rank == 0:
         line = {
@@ -577,6 +582,7 @@ def run_ours(args):
             "batch": batch_line,
             "t_reuse": t_reuse,
             "table_fft": table_fft,
+            "kappa_features": kappa_features,
             "clocks": ck,
         }
         print(json.dumps(line), flush=True)
@@ -600,7 +606,8 @@ def main():
     ap.add_argument("--no-t-reuse", action="store_true",
                     help="skip the many-stack H = T^T I measurement")
     ap.add_argument("--no-table-fft", action="store_true",
-                    help="skip the own-vs-cuFFT lookup-table FFT measurement")
+                    help="skip the own-vs-cuFFT lookup-table FFT and the learned-kappa "
+                         "features measurements")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

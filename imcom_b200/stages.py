@@ -18,9 +18,13 @@ Usage: python -m imcom_b200.stages [workload] [--library-eigensolver] [--split]
 --own-table-fft   the library's own inverse FFT for the lookup tables
                   (IMCOM_OPT_TABLE_FFT = 1)
 --repeat-bisect N run the bisection N more times and print each one's time
+--compare-features  after the solve, time 5 learned bisections with the scanned
+                  features and 5 with the table-built ones (committed weights),
+                  check that K is identical, and print one JSON line
 """
 from __future__ import annotations
 
+import json
 import sys
 
 
@@ -38,7 +42,8 @@ def main(argv):
         s.set_precision("--split" in argv)
         s.set_option(OPT_KAPPA_FEATURES, 1 if "--table-features" in argv else 0)
         s.set_option(OPT_TABLE_FFT, 1 if "--own-table-fft" in argv else 0)
-        learned = "--learned" in argv
+        compare = "--compare-features" in argv
+        learned = "--learned" in argv or compare
         if learned:
             from .kappa_model import DEFAULT_WEIGHTS, KappaModel
             KappaModel.load(DEFAULT_WEIGHTS).install(s)
@@ -74,6 +79,20 @@ def main(argv):
                 stage("BISECT", bisect)
                 times.append(round(s.stage_times()["bisect"], 3))
             print({"bisect_ms": times})
+        if compare:
+            out = {"workload": wl}
+            K = {}
+            for name, mode in (("scan", 0), ("table", 1)):
+                s.set_option(OPT_KAPPA_FEATURES, mode)
+                K[name] = s.bisect_kappa_learned(True, 1e-2, C * EPS, C / EPS, 1e-5, 53, C)[0]
+                times = []
+                for _ in range(5):
+                    stage("BISECT", bisect)
+                    times.append(s.stage_times()["bisect"])
+                out[f"bisect_ms_{name}"] = sorted(times)[2]
+            out["K_identical"] = bool((K["scan"] == K["table"]).all())
+            out["speedup"] = out["bisect_ms_scan"] / out["bisect_ms_table"]
+            print(json.dumps(out), flush=True)
 
 
 if __name__ == "__main__":
