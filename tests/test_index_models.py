@@ -568,3 +568,122 @@ def test_band_segments_flag_a_decreasing_index():
     assert seg[9] == 1
     seg, writes = band_segments(np.array([5]))
     assert seg[:9] == [0, 0, 0, 0, 0, 0, 1, 1, 1] and writes == [1] * 9
+
+
+def dft_store(v, R, tw, L, y, base, Ns):
+    """dft_store (table_fft.cu) as written: radix 2 and 4 butterflies, odd
+    radices in the symmetric-pair form, outputs stored to y[base + r Ns]."""
+    if R == 2:
+        y[base], y[base + Ns] = v[0] + v[1], v[0] - v[1]
+    elif R == 4:
+        s0, d0, s1, d1 = v[0] + v[2], v[0] - v[2], v[1] + v[3], v[1] - v[3]
+        y[base] = s0 + s1
+        y[base + 2 * Ns] = s0 - s1
+        y[base + Ns] = d0 + 1j * d1
+        y[base + 3 * Ns] = d0 - 1j * d1
+    else:
+        H, step = (R - 1) // 2, L // R
+        v = list(v)
+        y0 = v[0]
+        for s in range(1, H + 1):
+            a, b = v[s] + v[R - s], v[s] - v[R - s]
+            v[s], v[R - s] = a, b
+            y0 += a
+        y[base] = y0
+        for r in range(1, H + 1):
+            A, B = v[0], 0j
+            for s in range(1, H + 1):
+                w = tw[((r * s) % R) * step]
+                A += v[s] * w.real
+                B += v[R - s] * w.imag
+            y[base + r * Ns] = A + 1j * B
+            y[base + (R - r) * Ns] = A - 1j * B
+
+
+def run_stages_block(buf, L, LS, TP, tw):
+    """run_stages over a block's TP lines at stride LS: every butterfly's
+    inputs are read before any output is written (the stage's barrier)."""
+    Ns = 1
+    for R in fft_radices(L):
+        per = L // R
+        B = TP * per
+        v = [[buf[(b // per) * LS + (b % per) + r * per] for r in range(R)] for b in range(B)]
+        tstep = L // (Ns * R)
+        for b in range(B):
+            line, j = divmod(b, per)
+            k = j % Ns
+            vv = [v[b][0]] + [v[b][r] * tw[k * r * tstep] if Ns > 1 else v[b][r]
+                              for r in range(1, R)]
+            dft_store(vv, R, tw, L, buf, line * LS + (j // Ns) * Ns * R + k, Ns)
+        Ns *= R
+
+
+def table_kernels(Gt, Gammat, pairs, nps, L, isB):
+    """table_fft_pass1 and table_fft_pass2 emulated block by block with the
+    plan's line stride and lines per block."""
+    LS, TP, _ = fft_plan(L)
+    s, nmin = L // 2, (L - nps) // 2 + 1
+    tw = np.exp(2j * np.pi * np.arange(L) / L)
+    W = np.full((len(pairs), nps, L), np.nan + 0j)
+    tab = np.full((len(pairs), L * L), np.nan)
+    for t, pr in enumerate(pairs):
+        for bx in range(-(-nps // TP)):
+            u0 = bx * TP
+            buf = np.full(TP * LS, np.nan + 0j)
+            for e in range(TP * L):
+                line, p0 = divmod(e, L)
+                u = u0 + line
+                v = 0j
+                if u < nps:
+                    sp = cshift_src(p0 + 1, s, L)
+                    if nmin <= sp < nmin + nps:
+                        si = cshift_src(sp - nmin + 1, nps // 2, nps)
+                        sj = cshift_src(u + 1, nps // 2, nps)
+                        if pr[1] > 0:
+                            a, b = Gt[si - 1, sj - 1, pr[0] - 1], Gt[si - 1, sj - 1, pr[1] - 1]
+                        else:
+                            a, b = Gammat[si - 1, sj - 1], Gt[si - 1, sj - 1, pr[0] - 1]
+                        v = np.conj(a) * b
+                buf[line * LS + p0] = v
+            run_stages_block(buf, L, LS, TP, tw)
+            for e in range(TP * L):
+                line, k1 = divmod(e, L)
+                if u0 + line < nps:
+                    W[t, u0 + line, k1] = buf[line * LS + k1]
+        for bx in range(-(-L // TP)):
+            c0 = bx * TP
+            buf = np.full(TP * LS, np.nan + 0j)
+            for e in range(TP * L):
+                line, q0 = divmod(e, L)
+                buf[line * LS + q0] = 0j
+            for e in range(nps * TP):
+                u, c = divmod(e, TP)
+                if c0 + c < L:
+                    buf[c * LS + (nmin + u - 1 - s) % L] = W[t, u, c0 + c]
+            run_stages_block(buf, L, LS, TP, tw)
+            for e in range(TP * L):
+                k2, c = divmod(e, TP)
+                k1 = c0 + c
+                if k1 < L:
+                    v = buf[c * LS + k2].real
+                    if isB:
+                        v = -2.0 * v
+                    tab[t, ((k2 - s) % L) * L + (k1 - s) % L] = v / nps / nps
+    return [tt.reshape(L, L).T for tt in tab]  # tab[t][(q-1) L + (p-1)] as (p, q)
+
+
+@pytest.mark.parametrize("nps,npad", [(2, 3), (4, 3), (10, 3), (14, 3), (4, 5), (6, 2)])
+def test_table_kernels_as_written_match_embed_fft_shift(nps, npad):
+    L = nps * npad
+    if fft_plan(L) is None:
+        pytest.skip("size outside the kernel's radices")
+    rng = np.random.default_rng(nps + 100 * npad)
+    E = 2
+    Gt = rng.standard_normal((nps, nps, E)) + 1j * rng.standard_normal((nps, nps, E))
+    Gammat = rng.standard_normal((nps, nps)) + 1j * rng.standard_normal((nps, nps))
+    for isB, pairs in ((0, [(1, 1), (1, 2), (2, 2)]), (1, [(1, 0), (2, 0)])):
+        got = table_kernels(Gt, Gammat, pairs, nps, L, isB)
+        ref = table_reference(Gt, Gammat, pairs, nps, L, isB)
+        for g, r in zip(got, ref):
+            assert not np.isnan(g).any()
+            assert np.max(np.abs(g - r)) <= 1e-12 * max(1.0, np.max(np.abs(r)))
