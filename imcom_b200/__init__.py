@@ -3,8 +3,11 @@
 The compute lives in ``libimcom_gpu.so`` (hand-written CUDA behind the C-ABI of
 ``include/imcom_gpu.h``).  This package holds the ctypes binding
 (``_lib``), a host-side mirror of the reference's solve-path routines
-(``api.Solver``), the problem model (``problem``) and the seeded synthetic
-inputs (``synth``).
+(``api.Solver``), the problem model (``problem``), the seeded synthetic
+inputs (``synth``), FITS images without CFITSIO (``fits``), the many-patch
+driver (``batch``, ``replicas``), the learned-kappa model (``kappa_model``)
+and measurements that print one JSON line (``t_reuse``, ``table_fft``,
+``stages``).
 """
 from .api import (EIGH_DC, EIGH_JACOBI, EIGH_LIBRARY, EPS, ImcomError, SolveResult,  # noqa: F401
                   Solver)
