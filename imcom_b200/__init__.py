@@ -6,8 +6,8 @@ The compute lives in ``libimcom_gpu.so`` (hand-written CUDA behind the C-ABI of
 (``api.Solver``), the problem model (``problem``), the seeded synthetic
 inputs (``synth``), FITS images without CFITSIO (``fits``), the many-patch
 driver (``batch``, ``replicas``), the learned-kappa model (``kappa_model``)
-and measurements that print one JSON line (``t_reuse``, ``table_fft``,
-``stages``).
+measurements that print one JSON line (``t_reuse``, ``table_fft``) and the
+stage-by-stage timer (``stages``).
 """
 from .api import (EIGH_DC, EIGH_JACOBI, EIGH_LIBRARY, EPS, ImcomError, SolveResult,  # noqa: F401
                   Solver)
