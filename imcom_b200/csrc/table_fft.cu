@@ -22,8 +22,8 @@
 // processors", SC 2008), stage by stage in place in shared memory: every
 // thread reads its butterflies' inputs into registers, the block
 // synchronises, and the outputs go to their autosorted places.  Radices 4, 2,
-// 3, 5, 7; the twiddles come from a table of exp(2 pi i t / L) computed on the
-// host in extended precision.  Sides with another prime factor, or longer
+// 3, 5, 7, 11, 13; the twiddles come from a table of exp(2 pi i t / L) computed
+// on the host in extended precision.  Sides with another prime factor, or longer
 // than a block's shared memory holds, stay on cuFFT.
 #include <cmath>
 #include <vector>
@@ -38,12 +38,17 @@ constexpr int FFT_THREADS = 512;
 constexpr int FFT_MAX_ELEMS = 8192;  // TP x LS complex values in shared memory (128 KiB)
 
 // Elements a block may hold when its plan has a stage of radix R: each thread
-// keeps the inputs of cap / (R x FFT_THREADS) butterflies (16, 16, 12, 10 and
-// 7 complex values for R = 2, 4, 3, 5, 7) in registers between a stage's
-// reads and writes, inside the 128 registers of a thread of a 512-thread
-// block.
+// keeps the inputs of cap / (R x FFT_THREADS) butterflies (16, 16, 12, 10, 7,
+// 11 and 13 complex values for R = 2, 4, 3, 5, 7, 11, 13) in registers between
+// a stage's reads and writes, inside the 128 registers of a thread of a
+// 512-thread block.
 constexpr int fft_cap(int R) {
-  return R == 3 ? 6144 : R == 5 ? 5120 : R == 7 ? 3584 : FFT_MAX_ELEMS;
+  return R == 3    ? 6144
+         : R == 5  ? 5120
+         : R == 7  ? 3584
+         : R == 11 ? 5632
+         : R == 13 ? 6656
+                   : FFT_MAX_ELEMS;
 }
 
 struct FftPlan {
@@ -51,10 +56,10 @@ struct FftPlan {
   int LS = 0;  // shared-memory stride of a line: L rounded up to odd (no bank conflicts
                // between the lines of a column read)
   int TP = 0;  // lines per block (TP x LS <= fft_cap of every radix of the plan)
-  int count[5] = {};  // stages of radix 4, 2, 3, 5, 7 (run in that order)
+  int count[7] = {};  // stages of radix 4, 2, 3, 5, 7, 11, 13 (run in that order)
 };
 
-constexpr int kRadices[5] = {4, 2, 3, 5, 7};
+constexpr int kRadices[7] = {4, 2, 3, 5, 7, 11, 13};
 
 bool make_plan(int L, FftPlan* p) {
   if (L < 1) return false;
@@ -62,7 +67,7 @@ bool make_plan(int L, FftPlan* p) {
   p->LS = (L % 2 == 0) ? L + 1 : L;
   if (p->LS > FFT_MAX_ELEMS) return false;
   int n = L, cap = FFT_MAX_ELEMS;
-  for (int i = 0; i < 5; ++i) {
+  for (int i = 0; i < 7; ++i) {
     const int r = kRadices[i];
     p->count[i] = 0;
     while (n % r == 0) {
@@ -199,8 +204,8 @@ __device__ __forceinline__ void fft_stage(double2* buf, const FftPlan& plan, int
   __syncthreads();
 }
 
-// The plan's stages in its order (all radix-4 stages, then 2, 3, 5, 7): one
-// counted loop per radix, so each stage body is compiled once.
+// The plan's stages in its order (all radix-4 stages, then 2, 3, 5, 7, 11,
+// 13): one counted loop per radix, so each stage body is compiled once.
 __device__ __forceinline__ void run_stages(double2* buf, const FftPlan& plan,
                                            const double2* __restrict__ tw) {
   int Ns = 1;
@@ -209,6 +214,8 @@ __device__ __forceinline__ void run_stages(double2* buf, const FftPlan& plan,
   for (int i = 0; i < plan.count[2]; ++i, Ns *= 3) fft_stage<3>(buf, plan, Ns, tw);
   for (int i = 0; i < plan.count[3]; ++i, Ns *= 5) fft_stage<5>(buf, plan, Ns, tw);
   for (int i = 0; i < plan.count[4]; ++i, Ns *= 7) fft_stage<7>(buf, plan, Ns, tw);
+  for (int i = 0; i < plan.count[5]; ++i, Ns *= 11) fft_stage<11>(buf, plan, Ns, tw);
+  for (int i = 0; i < plan.count[6]; ++i, Ns *= 13) fft_stage<13>(buf, plan, Ns, tw);
 }
 
 // Pass 1: lines u0 .. u0+TP-1 of the nps non-zero grid lines (grid row

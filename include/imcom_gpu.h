@@ -103,9 +103,10 @@ typedef struct imcom_ctx imcom_ctx;
 /* Inverse 2-D FFT of the lookup tables (imcom_build_Alookup/Blookup): 0 =
  * embedding, cuFFT and shift as separate steps (default); 1 = the library's
  * own transform in two passes that skip the grid's zero lines and fuse the
- * embedding and the shift (sides L = npad nps whose prime factors are 2, 3, 5
- * and 7, up to 8191, 6143 with a factor 3, 5119 with a 5, 3583 with a 7;
- * other sides keep cuFFT).  Same tables to rounding. */
+ * embedding and the shift (sides L = npad nps whose prime factors are 2, 3, 5,
+ * 7, 11 and 13, up to 8191, 6143 with a factor 3, 5119 with a 5, 3583 with a
+ * 7, 5631 with an 11, 6655 with a 13; other sides keep cuFFT).  Same tables to
+ * rounding. */
 #define IMCOM_OPT_TABLE_FFT 13
 #define IMCOM_TABLE_FFT_CUFFT 0
 #define IMCOM_TABLE_FFT_OWN 1

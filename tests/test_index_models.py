@@ -331,12 +331,12 @@ def test_stacks_launch_choice():
 
 
 def fft_radices(L):
-    """The factorisation table_fft.cu uses: fours first, then 2, 3, 5, 7."""
+    """The factorisation table_fft.cu uses: fours first, then 2, 3, 5, 7, 11, 13."""
     out = []
     while L % 4 == 0:
         out.append(4)
         L //= 4
-    for r in (2, 3, 5, 7):
+    for r in (2, 3, 5, 7, 11, 13):
         while L % r == 0:
             out.append(r)
             L //= r
@@ -455,14 +455,15 @@ def test_pruned_table_fft_matches_embed_fft_shift(nps, npad):
 
 def test_fft_radices_cover_the_workload_sides():
     assert fft_radices(1728) == [4, 4, 4, 3, 3, 3]  # nps 576 (n = 4096 workload)
-    assert fft_radices(3 * 2 * 11) is None  # a factor 11: cuFFT keeps such sizes
+    assert fft_radices(3 * 2 * 11) == [2, 3, 11]
+    assert fft_radices(3 * 2 * 17) is None  # a factor 17: cuFFT keeps such sizes
     for L in range(1, 400):
         r = fft_radices(L)
         if r is not None:
             assert int(np.prod(r)) == L
 
 
-@pytest.mark.parametrize("R", [3, 5, 7])
+@pytest.mark.parametrize("R", [3, 5, 7, 11, 13])
 def test_symmetric_pair_dft_is_the_dft(R):
     """dft_store's odd radices: y_r, y_{R-r} = v_0 + sum_s a_s cos(2 pi r s/R)
     +- i sum_s b_s sin(2 pi r s/R), a_s = v_s + v_{R-s}, b_s = v_s - v_{R-s}."""
@@ -481,7 +482,7 @@ def test_symmetric_pair_dft_is_the_dft(R):
 
 
 FFT_THREADS = 512
-FFT_CAP = {4: 8192, 2: 8192, 3: 6144, 5: 5120, 7: 3584}
+FFT_CAP = {4: 8192, 2: 8192, 3: 6144, 5: 5120, 7: 3584, 11: 5632, 13: 6656}
 
 
 def fft_plan(L):
@@ -672,7 +673,8 @@ def table_kernels(Gt, Gammat, pairs, nps, L, isB):
     return [tt.reshape(L, L).T for tt in tab]  # tab[t][(q-1) L + (p-1)] as (p, q)
 
 
-@pytest.mark.parametrize("nps,npad", [(2, 3), (4, 3), (10, 3), (14, 3), (4, 5), (6, 2)])
+@pytest.mark.parametrize("nps,npad", [(2, 3), (4, 3), (10, 3), (14, 3), (4, 5), (6, 2),
+                                      (22, 3), (26, 2)])
 def test_table_kernels_as_written_match_embed_fft_shift(nps, npad):
     L = nps * npad
     if fft_plan(L) is None:

@@ -2,9 +2,10 @@
 (IMCOM_OPT_TABLE_FFT = 1, imcom_b200/csrc/table_fft.cu), through the C-ABI:
 A and B against the golden fixtures and the oracle at the cuFFT path's bars
 (1e-12 of the largest entry), on table sides that use every radix of the
-transform (L = 288: 4 4 2 3 3; 270: 2 3 3 3 5; 420: 4 3 5 7; 768: 4 4 4 4 3),
-and a side with a prime factor above 7 (L = 330 = 2 3 5 11), which stays on
-cuFFT and so matches the default path bit for bit.  Each test runs its own
+transform (L = 288: 4 4 2 3 3; 270: 2 3 3 3 5; 420: 4 3 5 7; 330: 2 3 5 11;
+390: 2 3 5 13; 768: 4 4 4 4 3), and a side with a prime factor above 13
+(L = 306 = 2 3 3 17), which stays on cuFFT and so matches the default path bit
+for bit.  Each test runs its own
 context so the option does not reach other tests."""
 import os
 import sys
@@ -44,7 +45,8 @@ def test_own_table_fft_golden(case):
 
 
 @pytest.mark.parametrize("workload,stamp,side", [("tiny", 48, 288), ("tiny", 40, 270),
-                                                 ("tiny", 70, 420), ("small", 128, 768)])
+                                                 ("tiny", 70, 420), ("tiny", 55, 330),
+                                                 ("tiny", 65, 390), ("small", 128, 768)])
 def test_own_table_fft_vs_oracle(workload, stamp, side):
     prob = synth.make(workload, 0, psf_stamp=stamp)
     assert 3 * prob.nps == side
@@ -55,8 +57,8 @@ def test_own_table_fft_vs_oracle(workload, stamp, side):
 
 
 def test_side_with_large_prime_stays_on_cufft():
-    prob = synth.make("tiny", 0, psf_stamp=55)
-    assert 3 * prob.nps == 330
+    prob = synth.make("tiny", 0, psf_stamp=51)
+    assert 3 * prob.nps == 306
     A1, B1 = build_AB(prob, TABLE_FFT_OWN)
     A0, B0 = build_AB(prob, TABLE_FFT_CUFFT)
     assert np.array_equal(A1, A0) and np.array_equal(B1, B0)
