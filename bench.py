@@ -63,6 +63,9 @@ WORKLOAD = "n4096"
 UNOTS, US_MAX, US_TOL, MAXNITS = True, 1e-2, 1e-5, 53
 METRIC = "output pixels/s at n=4096 (learned-κ+mixed vs plain FP64 GPU, same U/Σ tol)"
 UNIT = "pixels/s"
+# the same string on both arms' lines
+WORKLOAD_DESC = ("n4096: 4x32x32 inputs (n=4096), rotations U[-5,5] deg, Airy lambda/D=0.5 px "
+                 "PSF, 64x64 output at 0.5 px (m=4096), U mode U<1e-2 tol 1e-5, maxnits 53")
 L2_BYTES = 126 * 1024 * 1024
 
 
@@ -254,8 +257,7 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": "n4096: 4x32x32 inputs (n=4096), 64x64 output (m=4096), "
-                               "U mode U<1e-2 tol 1e-5, maxnits 53", "n": prob.n, "m": prob.m,
+        "config": {"workload": WORKLOAD_DESC, "n": prob.n, "m": prob.m,
                    "nps": prob.nps, "lookup_side": 3 * prob.nps},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": "one full n=4096 solve per step (C++ restatement of the "
@@ -556,9 +558,7 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "n4096: 4x32x32 inputs (n=4096), rotations U[-5,5] deg, Airy "
-                                   "lambda/D=0.5 px PSF, 64x64 output at 0.5 px (m=4096), "
-                                   "U mode U<1e-2 tol 1e-5, maxnits 53",
+            "config": {"workload": WORKLOAD_DESC,
                        "n": n, "m": m, "nps": prob.nps, "lookup_side": 3 * prob.nps,
                        "eigensolver": args.eigensolver, "kappa": args.kappa,
                        "P_T_precision": ("split int8 digits on tcgen05 (7/6 slices), audited, "

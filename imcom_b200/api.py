@@ -21,6 +21,8 @@ from ._lib import ImcomError
 
 EIGH_DC, EIGH_JACOBI, EIGH_LIBRARY = 0, 1, 2
 OPT_EIGENSOLVER, OPT_EIGEN_MAXITER = 1, 2
+OPT_DC_MAXITER, OPT_STALL_TEST = 15, 16
+STALL_SPLIT, STALL_TRIDIAG = 1, 2
 OPT_PRECISION, OPT_SPLIT_SLICES_P, OPT_SPLIT_SLICES_T = 3, 4, 5
 OPT_SPLIT_TOL_US, OPT_SPLIT_TOL_T = 6, 7
 PREC_FP64, PREC_SPLIT = 0, 1

@@ -58,6 +58,8 @@ struct imcom_ctx {
   std::string err;
   int eig_mode = IMCOM_EIGH_DC;
   long long eig_maxiter = 0;
+  int dc_maxiter = 0;     // IMCOM_OPT_DC_MAXITER (0: 100)
+  int stall_test = 0;     // IMCOM_OPT_STALL_TEST bits
 
   // geometry
   int n = 0, m = 0;

@@ -353,6 +353,14 @@ int imcom_gpu_set_option(imcom_ctx* ctx, int option, long long value) {
       if (value < 0) return -3;
       ctx->eig_maxiter = value;
       return 0;
+    case IMCOM_OPT_DC_MAXITER:
+      if (value < 0 || value > 1000000) return -3;
+      ctx->dc_maxiter = (int)value;
+      return 0;
+    case IMCOM_OPT_STALL_TEST:
+      if (value < 0 || value > (IMCOM_STALL_SPLIT | IMCOM_STALL_TRIDIAG)) return -3;
+      ctx->stall_test = (int)value;
+      return 0;
     case IMCOM_OPT_BISECT_KERNEL:
       if (value < IMCOM_BISECT_AUTO || value > IMCOM_BISECT_RESIDENT) return -3;
       ctx->bisect_kernel = (int)value;

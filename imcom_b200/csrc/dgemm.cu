@@ -348,8 +348,13 @@ extern "C" int imcom_gpu_build_P_noalloc(const double* dQ, long long ldq, const 
   if (n <= 0) return -7;
   if (m <= 0) return -8;
   const long long ldo = imcom::pad_ld(n);
-  if ((long long)kNoAllocSplits * ldo * (long long)m > kNoAllocDoubles)
+  // the reduce kernel's grid has one row of blocks per output column, and a
+  // grid's y extent stops at 65,535
+  if ((long long)kNoAllocSplits * ldo * (long long)m > kNoAllocDoubles || m > 65535)
     return IMCOM_ERR_NOALLOC_SIZE;
+  // an error left by the caller's earlier CUDA work is reported, not cleared
+  // (and not mistaken for a failure of this call's launches)
+  if (cudaPeekAtLastError() != cudaSuccess) return IMCOM_ERR_CUDA;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
     cudaGetLastError();

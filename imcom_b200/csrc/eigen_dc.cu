@@ -104,15 +104,16 @@ struct GridSync {
 
 // Arrive with a release add, wait with acquire loads until every CTA of this
 // barrier generation has arrived.  The wait gives up after `limit` polls and
-// sets the error word instead of spinning forever.
-__device__ __forceinline__ bool grid_barrier(GridSync* s, long long limit) {
+// sets the error word instead of spinning forever.  `extra` > 0 (a test of
+// that bound) waits for arrivals that never come.
+__device__ __forceinline__ bool grid_barrier(GridSync* s, long long limit, int extra = 0) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     const unsigned nb = gridDim.x;
     unsigned old;
     asm volatile("atom.add.release.gpu.u32 %0, [%1], 1;" : "=r"(old) : "l"(&s->count) : "memory");
-    const unsigned target = (old / nb + 1) * nb;
+    const unsigned target = (old / nb + 1) * nb + (unsigned)extra;
     int ok = 1;
     long long it = 0;
     while (true) {
@@ -162,6 +163,7 @@ struct TrdArgs {
   GridSync* sync;
   int n, k, b;
   long long spin;
+  int stall;  // test of the bounded barrier: the first barrier never completes
 };
 
 __global__ void __launch_bounds__(TRD_THREADS, 1) trd_panel_kernel(TrdArgs a) {
@@ -199,7 +201,7 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) trd_panel_kernel(TrdArgs a) {
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) a.d[k] = A[k + k * lda];
-  if (!grid_barrier(a.sync, a.spin)) return;
+  if (!grid_barrier(a.sync, a.spin, a.stall)) return;
 
   for (int i = 0; i < a.b; ++i) {
     const int j = k + i;
@@ -1387,7 +1389,7 @@ static int sytrd_launches(imcom_ctx* ctx, DMat& Aw, DMat& Vall, double* d, doubl
     IMC_CUDA(cudaMemsetAsync(accbuf, 0, 2 * sizeof(TrdAcc), ctx->stream));
     static_assert(2 * sizeof(TrdAcc) + 64 + sizeof(GridSync) <= 4096, "panel scratch");
     TrdArgs a{Aw.p, Aw.ld, Vall.p, Vall.ld, W, ldw, d, e, tau, ypart, ycol, ldy, acc, sync, n,
-              k, b, spin};
+              k, b, spin, (ctx->stall_test & IMCOM_STALL_TRIDIAG) ? 1 : 0};
     void* args[] = {&a};
     IMC_CUDA(cudaLaunchCooperativeKernel((void*)trd_panel_kernel, grid, TRD_THREADS, args,
                                          TRD_SMEM, ctx->stream));
@@ -1449,7 +1451,7 @@ static int sytrd_gpu(imcom_ctx* ctx, DMat& Aw, DMat& Vall, double* d, double* e,
                            (long long)(uintptr_t)tau, (long long)(uintptr_t)W, ldw,
                            (long long)(uintptr_t)ypart, (long long)(uintptr_t)ycol, ldy,
                            (long long)(uintptr_t)accbuf, spin, (long long)(uintptr_t)XY,
-                           sm_count(ctx), tail_ctas, tail_max};
+                           sm_count(ctx), tail_ctas, tail_max, ctx->stall_test};
   constexpr int NKEY = (int)(sizeof(key) / sizeof(key[0]));
   static_assert(NKEY <= EigWork::kTrdKey, "graph key size");
   const bool same = std::equal(key, key + NKEY, ew->trd_key);
@@ -1645,7 +1647,9 @@ int eigen_dc(imcom_ctx* ctx, const DMat& A, DMat& Wout, double* wout) {
     dc_rotate_kernel<<<ge, 256, 0, ctx->stream>>>(dnodes, Zcur, ld, wk);
     IMC_LAUNCH();
     dim3 gw((maxnm + 7) / 8, nn_);
-    dc_secular_kernel<<<gw, 256, 0, ctx->stream>>>(dnodes, wk, 100, derr);
+    dc_secular_kernel<<<gw, 256, 0, ctx->stream>>>(dnodes, wk,
+                                                   ctx->dc_maxiter > 0 ? ctx->dc_maxiter : 100,
+                                                   derr);
     IMC_LAUNCH();
     dc_zhat_kernel<<<gw, 256, 0, ctx->stream>>>(dnodes, wk, derr);
     IMC_LAUNCH();

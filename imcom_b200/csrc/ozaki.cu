@@ -312,6 +312,7 @@ struct OzArgs {
   int mblocks, nblocks;
   double alpha;
   int nst;
+  int stall;  // test of the bounded waits: the producer issues no copies
   int* err;
 };
 
@@ -435,6 +436,10 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) oz_gemm_kernel(OzArgs g) {
     uint32_t ph = 0;
     bool ok = true;
     int it = 0;
+    if (g.stall) {  // nothing arrives on the stages: the issuer's wait runs out
+      atomicOr(g.err, 16);
+      ok = false;
+    }
     for (int phase = 0; phase < NPHASE && ok; ++phase) {
       const uint32_t bytes = ((NPHASE == 2 && phase == 0) ? S : H) * SLICE;
       for (int kb = 0; kb < KB; ++kb, ++it) {
@@ -680,6 +685,7 @@ int split_gemm(imcom_ctx* ctx, const SplitOp& a, const SplitOp& b, double alpha,
   g.nblocks = (int)b.rb;
   g.alpha = alpha;
   g.err = err;
+  g.stall = (ctx->stall_test & IMCOM_STALL_SPLIT) != 0;
   switch (a.S) {
     case 2: IMC_TRY(launch_gemm<2>(ctx, g, ctx->stream)); break;
     case 3: IMC_TRY(launch_gemm<3>(ctx, g, ctx->stream)); break;

@@ -118,6 +118,27 @@ typedef struct imcom_ctx imcom_ctx;
  * descending order; otherwise the element-wise binning is kept).  Same
  * features to rounding, same kappa. */
 #define IMCOM_OPT_KAPPA_FEATURES 14
+/* Iteration cap of the divide-and-conquer secular-equation solver (0 = the
+ * default, 100; roots converge in at most about 10).  A root that reaches the
+ * cap makes imcom_gpu_eigen_A return IMCOM_ERR_EIGEN, as DSYEVR's info > 0
+ * stops the reference (imcom_matrix.f90:645-653). */
+#define IMCOM_OPT_DC_MAXITER 15
+/* Tests of the bounded device waits (0 = normal operation, the default).
+ * Each bit makes one wait run out on a flag that nothing sets:
+ *  IMCOM_STALL_SPLIT: the copy producer of the split GEMM (imcom_gpu_build_P
+ *    with IMCOM_PREC_SPLIT) issues no copies, so the MMA issuer's first wait
+ *    (bounded at 2 s) runs out; the kernel drains, frees its tensor memory
+ *    and returns, and the next bisection returns IMCOM_ERR_SPLIT;
+ *  IMCOM_STALL_TRIDIAG: the first grid barrier of the tridiagonalisation
+ *    waits for one arrival more than the grid makes, so it gives up after
+ *    IMCOM_OPT_EIGEN_MAXITER polls and imcom_gpu_eigen_A returns
+ *    IMCOM_ERR_EIGEN (when the tridiagonalisation runs panels: n above the
+ *    cluster tail's size, or IMCOM_OPT_TAIL_CTAS = -1).
+ * The context stays usable: clear the option and the next call runs
+ * normally. */
+#define IMCOM_OPT_STALL_TEST 16
+#define IMCOM_STALL_SPLIT 1
+#define IMCOM_STALL_TRIDIAG 2
 
 /* ---- context ---------------------------------------------------------- */
 
@@ -314,8 +335,11 @@ int imcom_gpu_split_pixels(imcom_ctx* ctx, int* fp64_P, int* fp64_T);
  *
  * Scratch: the split-K partial sums live in a fixed 32 MiB device array that
  * every GPU loading the library holds until the process exits.  Limit:
- * 2 * round_up(n, 32) * m <= 4,194,304 (e.g. n = 2048 with m <= 1024); larger
- * problems return IMCOM_ERR_NOALLOC_SIZE without touching the GPU.  The
+ * 2 * round_up(n, 32) * m <= 4,194,304 (e.g. n = 2048 with m <= 1024) and
+ * m <= 65,535; larger problems return IMCOM_ERR_NOALLOC_SIZE without touching
+ * the GPU.  A CUDA error already pending on the calling thread (from the
+ * caller's earlier work) is returned as IMCOM_ERR_CUDA before anything is
+ * queued, and left pending.  The
  * first call on each device looks the array up and sets the kernel's
  * shared-memory limit, so make that first call before any stream capture.
  * All calls share the array: calls whose GPU work overlaps race.

@@ -10,8 +10,8 @@ alone (big-endian float64 after the header, axis 1 fastest) and the SHA-256
 of the file's data records (the data and its zero padding).  The FITS tests
 rebuild each file from these, read it with the library and write it back.
 
-Usage: ``python tests/golden/make_fits_fixtures.py [reference root]``
-(default /root/reference).
+Usage: ``python tests/golden/make_fits_fixtures.py <reference root>`` (the
+directory holding the reference's ``example/fits``; required).
 """
 from __future__ import annotations
 
@@ -47,4 +47,6 @@ def main(root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_fits_fixtures.py <reference root>")
+    main(sys.argv[1])
