@@ -53,6 +53,7 @@ SIGNATURES = {
     "imcom_gpu_split_pixels": (_i, [_p, _p, _p]),
     "imcom_gpu_build_P_noalloc": (_i, [_p, _ll, _p, _ll, _p, _ll, _i, _i, _p]),
     "imcom_gpu_eigh_jacobi_batched": (_i, [_p, _i, _i, _p, _p, _p, _p]),
+    "imcom_gpu_band_reduce": (_i, [_p, _p, _i]),
     "imcom_fits_size": (_i, [C.c_char_p, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i)]),
     "imcom_fits_read": (_i, [C.c_char_p, _i, _i, _p]),
     "imcom_fits_write": (_i, [C.c_char_p, _i, _i, _p]),

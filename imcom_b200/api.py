@@ -35,6 +35,7 @@ OPT_STACK_KERNEL = 12
 STACKS_GEMM, STACKS_STREAM = 0, 1
 OPT_TABLE_FFT = 13
 OPT_KAPPA_FEATURES = 14
+OPT_KAPPA_START = 17
 TABLE_FFT_CUFFT, TABLE_FFT_OWN = 0, 1
 SPLIT_INFO = ("slices_P", "slices_T", "fp64_pixels_P", "fp64_columns_T", "max_bound_US",
               "max_bound_T_from_P", "max_bound_T_product", "P_split")

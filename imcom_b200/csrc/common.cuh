@@ -98,13 +98,16 @@ struct imcom_ctx {
   double2* fft_tw = nullptr;              // exp(2 pi i t / L) of the own table FFT
   size_t fft_tw_bytes = 0;
   int fft_tw_L = 0;
+  double2* r2c_tw = nullptr;              // exp(2 pi i t / nps) of the own PSF transform
+  size_t r2c_tw_bytes = 0;
+  int r2c_tw_L = 0;
   // work area bound to the shared cuFFT plans when this context runs them
   void* fft_work = nullptr;
   size_t fft_work_bytes = 0;
 
   int8_t* band = nullptr;   // eigenmode band indices of the learned-kappa features
   size_t band_bytes = 0;
-  int kappa_feat = 0;       // IMCOM_OPT_KAPPA_FEATURES
+  int kappa_feat = 1;       // IMCOM_OPT_KAPPA_FEATURES
   float2* nbr = nullptr;    // per pixel: neighbour count and exposures (valid for these inputs)
   size_t nbr_bytes = 0;
   bool nbr_valid = false;
@@ -120,7 +123,7 @@ struct imcom_ctx {
   // split-precision products (IMCOM_PREC_SPLIT)
   int prec = IMCOM_PREC_FP64;
   int bisect_kernel = IMCOM_BISECT_AUTO;
-  int bisect_ctas = 0;  // CTAs per SM of the streaming pixel kernels (0: all pixels at once)
+  int bisect_ctas = 0;  // CTAs per SM of the streaming pixel kernels (0: automatic)
   int sm_share = 0;     // SMs for persistent / cooperative grids (0: the whole device)
   int tail_ctas = 0;    // cluster of the tridiagonalisation tail (0 auto, -1 none, 8, 16)
   int stack_kernel = IMCOM_STACKS_GEMM;  // kernel of imcom_gpu_build_images
@@ -145,6 +148,8 @@ struct imcom_ctx {
   imcom::EigWork* eig = nullptr;
   imcom::MlpWeights mlp;
   float* feat = nullptr;
+  float2* guess = nullptr;  // learned-kappa network outputs per pixel
+  int kappa_nonet = 0;      // IMCOM_OPT_KAPPA_START: 1 = no network (Newton from mid-range)
 
   // capacity in bytes of every buffer grown by ensure_vec, keyed by the
   // address of the context field that holds its pointer
@@ -200,6 +205,12 @@ int ensure_mat(imcom_ctx* ctx, DMat& M, long long rows, long long cols);
 // The lookup tables' inverse 2-D FFT in two pruned, fused passes
 // (table_fft.cu); *done is false (and nothing is launched) for sides it does
 // not take, which then go through cuFFT.
+// The PSF spectra's forward real-to-complex transform of `count` n x n
+// images (in) into half spectra ((n/2 + 1) x n each, k fastest), with H
+// ((n/2 + 1) x n complex per image) as scratch (table_fft.cu); *done is false
+// (and nothing is launched) for sides the own line transforms do not cover.
+int psf_r2c_own(imcom_ctx* ctx, int n, int count, const double* in, double2* H, double2* half,
+                bool* done);
 int table_fft_inverse(imcom_ctx* ctx, int nps, int L, int ntab, const int2* dpairs, double2* W,
                       double* tab, int isB, bool* done);
 int ensure_buf(imcom_ctx* ctx, void** p, size_t& have, size_t need);

@@ -187,6 +187,7 @@ template int ensure_vec<double>(imcom_ctx*, double**, size_t);
 template int ensure_vec<int>(imcom_ctx*, int**, size_t);
 template int ensure_vec<float>(imcom_ctx*, float**, size_t);
 template int ensure_vec<double2>(imcom_ctx*, double2**, size_t);
+template int ensure_vec<float2>(imcom_ctx*, float2**, size_t);
 
 int upload_mat(imcom_ctx* ctx, DMat& M, const double* host, long long rows,
                long long cols) {
@@ -312,9 +313,9 @@ int imcom_gpu_destroy(imcom_ctx* ctx) {
   void* ptrs[] = {ctx->x, ctx->y, ctx->X, ctx->Y, ctx->I, ctx->Nd, ctx->exp_i, ctx->G,
                   ctx->Gamma, ctx->Gt, ctx->Gammat, ctx->A.p, ctx->Q.p, ctx->B.p, ctx->P.p,
                   ctx->T.p, ctx->Pt.p, ctx->L, ctx->K, ctx->US, ctx->H, ctx->S, ctx->U,
-                  ctx->nev, ctx->flags, ctx->tables, ctx->fftbuf, ctx->mlp.w, ctx->feat,
+                  ctx->nev, ctx->flags, ctx->tables, ctx->fftbuf, ctx->mlp.w, ctx->feat, ctx->guess,
                   ctx->gemm_ws, ctx->fb, ctx->train_buf, ctx->band, ctx->jac_buf,
-                  ctx->stacks.p, ctx->stack_H.p, ctx->fft_tw, ctx->nbr, ctx->band_seg};
+                  ctx->stacks.p, ctx->stack_H.p, ctx->fft_tw, ctx->r2c_tw, ctx->nbr, ctx->band_seg};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete[] ctx->rot;
@@ -352,6 +353,10 @@ int imcom_gpu_set_option(imcom_ctx* ctx, int option, long long value) {
     case IMCOM_OPT_EIGEN_MAXITER:
       if (value < 0) return -3;
       ctx->eig_maxiter = value;
+      return 0;
+    case IMCOM_OPT_KAPPA_START:
+      if (value != 0 && value != 1) return -3;
+      ctx->kappa_nonet = (int)value;
       return 0;
     case IMCOM_OPT_DC_MAXITER:
       if (value < 0 || value > 1000000) return -3;

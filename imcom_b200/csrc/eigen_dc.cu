@@ -43,6 +43,7 @@
 #include <cooperative_groups.h>
 
 #include "common.cuh"
+#include "dgemm_tile.cuh"
 #include "eigen.cuh"
 
 namespace imcom {
@@ -1204,6 +1205,23 @@ __global__ void dc_gather_kernel(const Node* nodes, const double* Z, long long l
     G[(s + r) + (long long)(s + jj) * ldg] = Z[(s + r) + (long long)(s + col) * ldz];
 }
 
+// The merge products of one level in one launch: OUT(node) = G(node) U(node)
+// for node z = blockIdx.z, M = its size, N = K = its non-deflated count read
+// on the device, so the level needs no host synchronisation.  CTAs past a
+// node's extent return at once.
+template <int VEC>
+__global__ void __launch_bounds__(gemm::THREADS, 1)
+dc_gemm_kernel(const Node* nodes, const int* kcnt, const double* G, const double* U, double* OUT,
+               long long ld) {
+  const Node nd = nodes[blockIdx.z];
+  const long long k = kcnt[blockIdx.z];
+  const long long m0 = (long long)blockIdx.x * gemm::BM, n0 = (long long)blockIdx.y * gemm::BN;
+  if (m0 >= nd.nm || n0 >= k) return;
+  const size_t off = (size_t)nd.s + (size_t)nd.s * ld;
+  gemm::dgemm_tile<false, true, VEC>(nd.nm, k, k, 1.0, G + off, ld, U + off, ld, 0.0, OUT + off,
+                                     ld, k, m0, n0, 0, 1);
+}
+
 // Rank of each new eigenvalue within its node (stable, O(nm) per element).
 __global__ void dc_rank_kernel(const Node* nodes, DcWork wk) {
   const Node nd = nodes[blockIdx.y];
@@ -1658,16 +1676,28 @@ int eigen_dc(imcom_ctx* ctx, const DMat& A, DMat& Wout, double* wout) {
     dim3 gg((maxnm + 255) / 256, maxnm, nn_);
     dc_gather_kernel<<<gg, 256, 0, ctx->stream>>>(dnodes, Zcur, ld, wk, Gm, UO.ld);
     IMC_LAUNCH();
-    std::vector<int> kh(nn_);
-    IMC_CUDA(cudaMemcpyAsync(kh.data(), wk.kcnt, nn_ * 4, cudaMemcpyDeviceToHost, ctx->stream));
-    IMC_CUDA(cudaStreamSynchronize(ctx->stream));
-    // OUT(node) = G(node) U(node): the new non-deflated eigenvectors
-    for (int b = 0; b < nn_; ++b) {
-      const Node& x = nodes[b];
-      if (kh[b] == 0) continue;
-      IMC_TRY(dgemm(ctx, 'N', 'N', x.nm, kh[b], kh[b], 1.0, Gm + x.s + (size_t)x.s * UO.ld,
-                    UO.ld, Ub + x.s + (size_t)x.s * UO.ld, UO.ld, 0.0,
-                    OUT + x.s + (size_t)x.s * UO.ld, UO.ld));
+    // OUT(node) = G(node) U(node): the new non-deflated eigenvectors, every
+    // node of the level in one launch (16-byte copies when every node block
+    // starts on a 16-byte boundary)
+    {
+      bool even = (UO.ld % 2 == 0) && (((uintptr_t)UO.p & 15) == 0);
+      for (const Node& x : nodes) even = even && (x.s % 2 == 0);
+      const unsigned tiles = (unsigned)((maxnm + gemm::BM - 1) / gemm::BM);
+      dim3 gd(tiles, tiles, nn_);
+      if (even) {
+        IMC_CUDA(cudaFuncSetAttribute(dc_gemm_kernel<2>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)gemm::SMEM_BYTES));
+        dc_gemm_kernel<2><<<gd, gemm::THREADS, gemm::SMEM_BYTES, ctx->stream>>>(
+            dnodes, wk.kcnt, Gm, Ub, OUT, UO.ld);
+      } else {
+        IMC_CUDA(cudaFuncSetAttribute(dc_gemm_kernel<1>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)gemm::SMEM_BYTES));
+        dc_gemm_kernel<1><<<gd, gemm::THREADS, gemm::SMEM_BYTES, ctx->stream>>>(
+            dnodes, wk.kcnt, Gm, Ub, OUT, UO.ld);
+      }
+      IMC_LAUNCH();
     }
     dc_rank_kernel<<<ge, 256, 0, ctx->stream>>>(dnodes, wk);
     IMC_LAUNCH();

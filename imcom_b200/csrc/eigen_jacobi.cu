@@ -161,8 +161,9 @@ int launch_jacobi(imcom_ctx* ctx, const double* A, long long lda, long long stri
     return set_err(ctx, IMCOM_ERR_STATE,
                    "the Jacobi eigensolver takes n <= %d (shared memory); n = %d", JAC_MAX, n);
   const size_t smem = jacobi_smem(n);
+  // the largest size's need: the attribute is process-wide (see usum.cuh)
   IMC_CUDA(cudaFuncSetAttribute(jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem));
+                                (int)jacobi_smem(JAC_MAX)));
   jacobi_kernel<<<count, JAC_THREADS, smem, ctx->stream>>>(A, lda, strideA, n, Q, ldq, strideQ, L,
                                                            strideL, status);
   IMC_LAUNCH();

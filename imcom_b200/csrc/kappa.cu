@@ -176,60 +176,147 @@ __device__ void pixel_features(const double* __restrict__ x, const double* __res
   f[11] = (float)log10(fabs(lmax / C) + 1e-300);
 }
 
-// MLP forward on one warp: lane owns hidden units lane and lane + 32.
-// Shared-memory copy of the weight block for the warp forward: W1 and W2
-// transposed ([in][out]) so that the 32 lanes (consecutive hidden units) read
-// consecutive words; the other parts keep their offsets.
-__device__ __forceinline__ void load_weights_smem(const float* __restrict__ W, float* sW) {
-  for (int q = threadIdx.x; q < NWEIGHT; q += blockDim.x) {
-    float v = W[q];
-    int d = q;
-    if (q >= OFF_W1 && q < OFF_B1) {
-      const int u = (q - OFF_W1) / NF, k = (q - OFF_W1) % NF;
-      d = OFF_W1 + k * NH + u;
-    } else if (q >= OFF_W2 && q < OFF_B2) {
-      const int u = (q - OFF_W2) / NH, v2 = (q - OFF_W2) % NH;
-      d = OFF_W2 + v2 * NH + u;
-    }
-    sW[d] = v;
+// ---------------------------------------------------------------------------
+// MLP inference on the tensor cores: one warp forms the outputs of 16 pixels
+// with mma.sync m16n8k16 (bf16 operands, fp32 accumulation).  Layer 1 is
+// [16 x 16] x [16 x 64] (12 features, zero-padded to K = 16), layer 2
+// [16 x 64] x [64 x 64], layer 3 [16 x 64] x [64 x 8] (2 outputs, zero-padded
+// columns).  The accumulator fragment of one layer is the operand fragment of
+// the next (two 8-column tiles make one 16-wide K step), so activations stay
+// in registers.  Rounding points as the training kernel and the numpy oracle:
+// normalised features, weights and hidden activations in bf16, sums in fp32.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0,
+                                         uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Shared-memory weights of the tensor-core forward: bf16 [out][in] rows
+// (W1 padded to 16 inputs, W3 to 8 outputs), fp32 biases and normalisation.
+struct MlpSmem {
+  __nv_bfloat16 W1[NH][16];
+  __nv_bfloat16 W2[NH][NH];
+  __nv_bfloat16 W3[8][NH];
+  float b1[NH], b2[NH], b3[NO], mean[NF], rstd[NF];
+};
+
+__device__ void load_mlp_smem(const float* __restrict__ W, MlpSmem& S) {
+  for (int q = threadIdx.x; q < NH * 16; q += blockDim.x) {
+    const int u = q / 16, k = q % 16;
+    S.W1[u][k] = __float2bfloat16_rn(k < NF ? W[OFF_W1 + u * NF + k] : 0.0f);
+  }
+  for (int q = threadIdx.x; q < NH * NH; q += blockDim.x)
+    S.W2[q / NH][q % NH] = __float2bfloat16_rn(W[OFF_W2 + q]);
+  for (int q = threadIdx.x; q < 8 * NH; q += blockDim.x) {
+    const int o = q / NH;
+    S.W3[o][q % NH] = __float2bfloat16_rn(o < NO ? W[OFF_W3 + q] : 0.0f);
+  }
+  for (int q = threadIdx.x; q < NH; q += blockDim.x) {
+    S.b1[q] = W[OFF_B1 + q];
+    S.b2[q] = W[OFF_B2 + q];
+  }
+  if (threadIdx.x < NO) S.b3[threadIdx.x] = W[OFF_B3 + threadIdx.x];
+  if (threadIdx.x < NF) {
+    S.mean[threadIdx.x] = W[OFF_MEAN + threadIdx.x];
+    S.rstd[threadIdx.x] = W[OFF_STD + threadIdx.x];
   }
 }
 
-// Forward pass of one pixel on one warp (lane = hidden units lane, lane+32),
-// weights from load_weights_smem.
-__device__ void mlp_forward_warp(const float* __restrict__ W, const float* f, int lane,
-                                 float* out) {
-  float fn[NF];
+__device__ __forceinline__ uint32_t smem_pair(const __nv_bfloat16* p) {
+  return *reinterpret_cast<const uint32_t*>(p);
+}
+
+// Outputs (o0, o1) of pixels p0 .. p0+15 (feature-major feat, m pixels);
+// written for pixels < m.
+__device__ void mlp_forward_16(const MlpSmem& S, const float* __restrict__ feat, int m, int p0,
+                               int lane, float2* __restrict__ out) {
+  const int g = lane >> 2, t = lane & 3;
+  auto x = [&](int row, int k) -> float {
+    const int pix = p0 + row;
+    if (k >= NF || pix >= m) return 0.0f;
+    return (feat[(size_t)k * m + pix] - S.mean[k]) / S.rstd[k];
+  };
+  uint32_t a[4] = {pack_bf16(x(g, 2 * t), x(g, 2 * t + 1)),
+                   pack_bf16(x(g + 8, 2 * t), x(g + 8, 2 * t + 1)),
+                   pack_bf16(x(g, 2 * t + 8), x(g, 2 * t + 9)),
+                   pack_bf16(x(g + 8, 2 * t + 8), x(g + 8, 2 * t + 9))};
+  float h[8][4];
 #pragma unroll
-  for (int k = 0; k < NF; ++k) fn[k] = bf16r((f[k] - W[OFF_MEAN + k]) / W[OFF_STD + k]);
-  float h1[2], h2[2];
+  for (int j = 0; j < 8; ++j) {
+    const float bb0 = S.b1[8 * j + 2 * t], bb1 = S.b1[8 * j + 2 * t + 1];
+    h[j][0] = bb0;
+    h[j][1] = bb1;
+    h[j][2] = bb0;
+    h[j][3] = bb1;
+    mma_bf16(h[j], a, smem_pair(&S.W1[8 * j + g][2 * t]), smem_pair(&S.W1[8 * j + g][2 * t + 8]));
+  }
+  // layer 2: the ReLU'd layer-1 tiles 2kt, 2kt+1 are the operand of K step kt
+  uint32_t a2[4][4];
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int u = lane + 32 * h;
-    float s = W[OFF_B1 + u];
-#pragma unroll
-    for (int k = 0; k < NF; ++k) s = fmaf(W[OFF_W1 + k * NH + u], fn[k], s);
-    h1[h] = bf16r(fmaxf(s, 0.0f));
+  for (int kt = 0; kt < 4; ++kt) {
+    const float* c0 = h[2 * kt];
+    const float* c1 = h[2 * kt + 1];
+    a2[kt][0] = pack_bf16(fmaxf(c0[0], 0.0f), fmaxf(c0[1], 0.0f));
+    a2[kt][1] = pack_bf16(fmaxf(c0[2], 0.0f), fmaxf(c0[3], 0.0f));
+    a2[kt][2] = pack_bf16(fmaxf(c1[0], 0.0f), fmaxf(c1[1], 0.0f));
+    a2[kt][3] = pack_bf16(fmaxf(c1[2], 0.0f), fmaxf(c1[3], 0.0f));
   }
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int u = lane + 32 * h;
-    float s = W[OFF_B2 + u];
-    for (int v = 0; v < NH; ++v) {
-      const float hv = __shfl_sync(0xffffffffu, h1[v >> 5], v & 31);
-      s = fmaf(W[OFF_W2 + v * NH + u], hv, s);
-    }
-    h2[h] = bf16r(fmaxf(s, 0.0f));
+  for (int j = 0; j < 8; ++j) {
+    const float bb0 = S.b2[8 * j + 2 * t], bb1 = S.b2[8 * j + 2 * t + 1];
+    h[j][0] = bb0;
+    h[j][1] = bb1;
+    h[j][2] = bb0;
+    h[j][3] = bb1;
+#pragma unroll
+    for (int kt = 0; kt < 4; ++kt)
+      mma_bf16(h[j], a2[kt], smem_pair(&S.W2[8 * j + g][16 * kt + 2 * t]),
+               smem_pair(&S.W2[8 * j + g][16 * kt + 2 * t + 8]));
   }
+  // layer 3
+  float o[4] = {t == 0 ? S.b3[0] : 0.0f, t == 0 ? S.b3[1] : 0.0f, t == 0 ? S.b3[0] : 0.0f,
+                t == 0 ? S.b3[1] : 0.0f};
 #pragma unroll
-  for (int o = 0; o < NO; ++o) {
-    float s = W[OFF_W3 + o * NH + lane] * h2[0] + W[OFF_W3 + o * NH + lane + 32] * h2[1];
-#pragma unroll
-    for (int q = 16; q > 0; q >>= 1) s += __shfl_xor_sync(0xffffffffu, s, q);
-    out[o] = s + W[OFF_B3 + o];
+  for (int kt = 0; kt < 4; ++kt) {
+    const float* c0 = h[2 * kt];
+    const float* c1 = h[2 * kt + 1];
+    const uint32_t a3[4] = {pack_bf16(fmaxf(c0[0], 0.0f), fmaxf(c0[1], 0.0f)),
+                            pack_bf16(fmaxf(c0[2], 0.0f), fmaxf(c0[3], 0.0f)),
+                            pack_bf16(fmaxf(c1[0], 0.0f), fmaxf(c1[1], 0.0f)),
+                            pack_bf16(fmaxf(c1[2], 0.0f), fmaxf(c1[3], 0.0f))};
+    mma_bf16(o, a3, smem_pair(&S.W3[g][16 * kt + 2 * t]), smem_pair(&S.W3[g][16 * kt + 2 * t + 8]));
+  }
+  // columns 0 and 1 (the two outputs) sit in the lanes with t = 0
+  if (t == 0) {
+    if (p0 + g < m) out[p0 + g] = make_float2(o[0], o[1]);
+    if (p0 + g + 8 < m) out[p0 + g + 8] = make_float2(o[2], o[3]);
   }
 }
 
+constexpr int MLP_WARPS = 4;
+
+__global__ void __launch_bounds__(MLP_WARPS * 32) mlp_infer_kernel(const float* __restrict__ W,
+                                                                   const float* __restrict__ feat,
+                                                                   int m,
+                                                                   float2* __restrict__ out) {
+  __shared__ __align__(16) MlpSmem S;
+  load_mlp_smem(W, S);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int p0 = (blockIdx.x * MLP_WARPS + warp) * 16; p0 < m; p0 += gridDim.x * MLP_WARPS * 16)
+    mlp_forward_16(S, feat, m, p0, lane, out);
+}
+
+// The 12 features of every pixel (one warp each), feature-major.
 __global__ void features_kernel(BisectArgs a, const double* __restrict__ x,
                                 const double* __restrict__ y, const int* __restrict__ expi,
                                 const double* __restrict__ X, const double* __restrict__ Y,
@@ -249,73 +336,149 @@ __global__ void features_kernel(BisectArgs a, const double* __restrict__ x,
 }
 
 struct LearnedExtra {
-  const double *x, *y, *X, *Y;
-  const int* expi;
-  const int8_t* bidx;  // band of every eigenmode (band_index_kernel)
-  const float2* nbr;   // neighbour table (IMCOM_OPT_KAPPA_FEATURES = 1) or null
-  const int* seg;      // band segments (IMCOM_OPT_KAPPA_FEATURES = 1) or null
-  const float* W;
+  const float2* guess;  // MLP outputs per pixel (log10 kappa, log half-width), or null
   int* fallback;
   double half_scale;  // bracket half-width = half_scale * exp(output 1), decades
   double min_half;    // smallest half-width, decades
-  double margin;      // safety margin of the verification tests (units of U or S)
+  double margin;      // safety margin of the known-decision tests (units of U or S)
+  int max_newton;     // Newton steps toward the root before the replay
 };
 
-// One pixel of the learned-bracket bisection: features from lam and the P
-// column `col`, MLP bracket, verification of the bracket ends and the replay
-// of the reference's bisection; ev(k, lane) evaluates U or S.
+// One pixel of the learned-kappa bisection.
+//
+// 1. Start from the network's log10(kappa) (the middle of the range when no
+//    network is given).  When its bracket reaches the start of the range the
+//    reference's first evaluation (kappa_min for U, kappa_max for S) comes
+//    first, and the pixel is done if it returns there.
+// 2. Newton steps in x = log10(kappa) toward f = -w/2 (w = max(tol, C eps)),
+//    the middle of the band in which the bisection stops, each from one
+//    evaluation of f and f' (the same U/S sum as the bisection, bit for bit,
+//    with the derivative summed alongside), safeguarded to the interval the
+//    evaluated points have bracketed.
+// 3. Certificates: the bisection's sequence of midpoints is followed with f
+//    predicted by the tangent at the last Newton point, and the last
+//    midpoint predicted to be accepted and the last predicted to be rejected
+//    before the one predicted to stop it are evaluated.
+// Every evaluated point with f < -(max(tol, C eps) + margin) makes each
+// bisection midpoint on its accept side a known accept that cannot trigger an
+// exit; every point with f >= C eps + margin makes each midpoint on its
+// reject side a known reject.  U(kappa) rises and S(kappa) falls
+// monotonically, and the margin covers the rounding of the computed sums.
+// 4. Replay of the reference's bisection sequence (imcom_bisect.f90:174-267):
+//    known decisions cost nothing, the other midpoints are evaluated.  K_a,
+//    U_a/S_a and the reported value are bit-identical to the plain bisection.
 template <class Eval>
 __device__ __forceinline__ void learned_pixel(const BisectArgs& a, const LearnedExtra& ex,
-                                              const float* sW, const double* lam,
-                                              const double* col, const Eval& ev, int pix,
-                                              int lane) {
+                                              const double* lam, const double* col,
+                                              const Eval& ev, int pix, int lane) {
   const bool U = a.UnotS != 0;
-  float f[NF], o[NO];
-  pixel_features(ex.x, ex.y, ex.expi, a.n, ex.X[pix], ex.Y[pix], lam, ex.bidx, col, a.C,
-                 a.US_max, lane, f, ex.nbr ? ex.nbr + pix : nullptr, ex.seg);
-  mlp_forward_warp(sW, f, lane, o);
-  double hw = ex.half_scale * exp((double)fminf(fmaxf(o[1], -20.0f), 5.0f));
-  hw = fmin(fmax(hw, ex.min_half), 4.0);
-  double bl = (double)o[0] - hw, bh = (double)o[0] + hw;
-  // (lg_min, lg_max) is the reference's search range
-  const double rlo = a.lg_min, rhi = a.lg_max;
-  bl = fmax(bl, rlo);
-  bh = fmin(bh, rhi);
+  const double rlo = a.lg_min, rhi = a.lg_max;  // the reference's search range
+  double x0 = 0.5 * (rlo + rhi), hw = 0.5 * (rhi - rlo);
+  if (ex.guess) {
+    const float2 o = ex.guess[pix];
+    if (isfinite(o.x) && isfinite(o.y)) {
+      x0 = (double)o.x;
+      hw = ex.half_scale * exp((double)fminf(fmaxf(o.y, -20.0f), 5.0f));
+      hw = fmin(fmax(hw, ex.min_half), 4.0);
+    }
+  }
   int nev = 0;
   double k_root = 0.0, us = 0.0;
   const double ceps = __dmul_rn(a.C, a.eps);
-  const double thr = fmax(a.tol, ceps) + ex.margin;
+  const double wband = fmax(a.tol, ceps);
+  const double thr = wband + ex.margin;
   double mg = INFINITY;  // smallest decision margin over the evaluations
-  // One-sided bounds from the evaluated bracket ends.  U rises with kappa:
-  // an end with f < -thr makes every midpoint at or below it a known
-  // accept; an end with f >= C eps (+ margin) makes every midpoint at or
-  // above it a known reject.  S falls with kappa, so the directions flip.
   double accb = U ? -INFINITY : INFINITY;  // known accept beyond this point
   double rejb = U ? INFINITY : -INFINITY;  // known reject beyond this point
-  const double ends[2] = {bl, bh};
-#pragma unroll
-  for (int e = 0; e < 2; ++e) {
-    const double pt = ends[e];
-    if (!(pt > rlo && pt < rhi) || (e == 1 && bh <= bl)) continue;
-    const double fp =
-        __dsub_rn(ev(pow(10.0, pt), lane), a.US_max);
-    ++nev;
+  auto note = [&](double pt, double fp) {
     mg = fmin(mg, fmin(fabs(fp + thr), fabs(fp - (ceps + ex.margin))));
     if (fp < -thr) accb = U ? fmax(accb, pt) : fmin(accb, pt);
     else if (fp >= ceps + ex.margin) rejb = U ? fmin(rejb, pt) : fmax(rejb, pt);
+  };
+  const double k0 = U ? a.k_min : a.k_max;
+  double f0 = 0.0;
+  bool have_f0 = false;
+  // 1. the range start first when the bracket reaches it
+  if (U ? (x0 - hw <= rlo) : (x0 + hw >= rhi)) {
+    us = ev(k0, lane);
+    ++nev;
+    f0 = __dsub_rn(us, a.US_max);
+    have_f0 = true;
+    mg = fmin(mg, fabs(f0));
   }
-  const bool have_acc = U ? (accb > rlo) : (accb < rhi);
-  const bool have_rej = U ? (rejb < rhi) : (rejb > rlo);
-  if (lane == 0 && ex.fallback) ex.fallback[pix] = (have_acc || have_rej) ? 0 : 1;
-  {
-    // The reference first evaluates f0 at the start of the range (kappa_min
-    // for U, kappa_max for S) and returns there if f0 >= 0.  A known accept
-    // point inside the range implies f0 < 0 by monotonicity, so f0 is then
-    // only needed if no later step is accepted.
-    double f0 = 0.0;
-    bool have_f0 = false;
-    if (!have_acc) {
-      const double k0 = U ? a.k_min : a.k_max;
+  if (have_f0 && !(f0 < 0.0)) {
+    k_root = k0;
+  } else {
+    // 2. Newton toward the middle of the stopping band
+    const double ftgt = -0.5 * wband;
+    double x = fmin(fmax(x0, rlo + 1e-9 * (rhi - rlo)), rhi - 1e-9 * (rhi - rlo));
+    double xc = x, fc = 0.0, gc = 0.0;
+    bool conv = false;
+    for (int it = 0; it < ex.max_newton; ++it) {
+      double gd;
+      const double fx = __dsub_rn(ev.eval_d(pow(10.0, x), lane, &gd), a.US_max);
+      ++nev;
+      note(x, fx);
+      xc = x;
+      fc = fx;
+      gc = gd;
+      if (fabs(fx - ftgt) <= 2.0 * wband) {
+        conv = true;
+        break;
+      }
+      // the interval of x the evaluated points leave for the target
+      const double lo_x = U ? fmax(accb, rlo) : fmax(rejb, rlo);
+      const double hi_x = U ? fmin(rejb, rhi) : fmin(accb, rhi);
+      double xn = x - (fx - ftgt) / gd;
+      if (!(gd != 0.0) || !(xn > lo_x && xn < hi_x)) xn = 0.5 * (lo_x + hi_x);
+      if (!(xn > rlo && xn < rhi) || xn == x) break;
+      x = xn;
+    }
+    // 3. certificates: follow the bisection's sequence with f predicted by
+    // the tangent at the last Newton point, up to the midpoint predicted to
+    // stop it; evaluate the last midpoint predicted to be accepted and the
+    // last predicted to be rejected.  If they are (f < -thr, f >= C eps +
+    // margin), every earlier decision of the replay is known.
+    if (conv && gc != 0.0 && isfinite(gc)) {
+      const double lo = U ? a.lg_min : a.lg_max, hi = U ? a.lg_max : a.lg_min;
+      double root = lo, dx = __dsub_rn(hi, lo);
+      double lastA = NAN, lastR = NAN;
+      for (int i = 1; i <= a.maxnits; ++i) {
+        dx = __dmul_rn(0.5, dx);
+        const double mid = __dadd_rn(root, dx);
+        if (U ? (mid <= accb) : (mid >= accb)) {
+          root = mid;
+          continue;
+        }
+        if (U ? (mid >= rejb) : (mid <= rejb)) continue;
+        const double fp = fc + gc * (mid - xc);
+        if (fp < 0.0) {
+          if (fabs(fp) < a.tol) break;
+          root = mid;
+          lastA = mid;
+        } else {
+          if (fabs(fp) < ceps) break;
+          lastR = mid;
+        }
+      }
+      const double pts[2] = {lastA, lastR};
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const double pt = pts[e];
+        if (!(pt > rlo && pt < rhi)) continue;  // none (NaN) or outside the range
+        const double fp = __dsub_rn(ev(pow(10.0, pt), lane), a.US_max);
+        ++nev;
+        note(pt, fp);
+      }
+    }
+    const bool have_acc = U ? (accb > rlo) : (accb < rhi);
+    const bool have_rej = U ? (rejb < rhi) : (rejb > rlo);
+    if (lane == 0 && ex.fallback) ex.fallback[pix] = (have_acc || have_rej) ? 0 : 1;
+    // 4. replay.  The reference evaluates f0 at the start of the range first
+    // and returns there if f0 >= 0; a known accept point inside the range
+    // implies f0 < 0 by monotonicity, so f0 is then only needed if no later
+    // step is accepted.
+    if (!have_acc && !have_f0) {
       us = ev(k0, lane);
       ++nev;
       f0 = __dsub_rn(us, a.US_max);
@@ -323,7 +486,7 @@ __device__ __forceinline__ void learned_pixel(const BisectArgs& a, const Learned
       mg = fmin(mg, fabs(f0));
     }
     if (have_f0 && !(f0 < 0.0)) {
-      k_root = U ? a.k_min : a.k_max;
+      k_root = k0;
     } else {
       const double lo = U ? a.lg_min : a.lg_max, hi = U ? a.lg_max : a.lg_min;
       double root = lo, dx = __dsub_rn(hi, lo);
@@ -340,8 +503,7 @@ __device__ __forceinline__ void learned_pixel(const BisectArgs& a, const Learned
           continue;
         }
         if (known_rej) continue;
-        const double fmid =
-            __dsub_rn(ev(pow(10.0, mid), lane), a.US_max);
+        const double fmid = __dsub_rn(ev(pow(10.0, mid), lane), a.US_max);
         ++nev;
         mg = fmin(mg, decision_margin(fmid, a.tol, ceps));
         if (fmid < 0.0) {
@@ -355,36 +517,35 @@ __device__ __forceinline__ void learned_pixel(const BisectArgs& a, const Learned
       }
       if (!any_acc) {
         if (!have_f0) {
-          const double k0 = U ? a.k_min : a.k_max;
           us = ev(k0, lane);
           ++nev;
           mg = fmin(mg, fabs(__dsub_rn(us, a.US_max)));
         }
       } else if (last_known) {
         // value the reference holds at the last accepted midpoint
-        const double fl =
-            __dsub_rn(ev(pow(10.0, root), lane), a.US_max);
+        const double fl = __dsub_rn(ev(pow(10.0, root), lane), a.US_max);
         ++nev;
         us = __dadd_rn(fl, a.US_max);
       }
       k_root = pow(10.0, root);
     }
   }
+  if (lane == 0 && ex.fallback && have_f0 && !(f0 < 0.0)) ex.fallback[pix] = 0;
   write_pixel(a, lam, col, pix, lane, nev, k_root, us, mg);
 }
 
+// The learned-kappa bisection, one warp per pixel (CTAs of four warps, the
+// plain bisection kernel's shape: the features and the network ran before).
 __global__ void __launch_bounds__(128, 7) learned_bisect_kernel(BisectArgs a, PixelSmem plan,
                                                                 LearnedExtra ex) {
   extern __shared__ __align__(16) double smem[];
-  __shared__ float sW[NWEIGHT];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  load_weights_smem(ex.W, sW);
   const double* lam = a.L;
   if (plan.lam_smem) {
     for (int p = threadIdx.x; p < a.n; p += blockDim.x) smem[p] = a.L[p];
+    __syncthreads();
     lam = smem;
   }
-  __syncthreads();
   double* mycol = plan.col_smem ? smem + (size_t)a.n * (1 + warp) : nullptr;
   for (int pix = blockIdx.x * plan.warps + warp; pix < a.m; pix += gridDim.x * plan.warps) {
     const double* gcol = a.P + (size_t)pix * a.ldp;
@@ -395,38 +556,7 @@ __global__ void __launch_bounds__(128, 7) learned_bisect_kernel(BisectArgs a, Pi
       col = mycol;
     }
     const StreamCol ev{lam, col, a.Nd, a.n, a.UnotS != 0, a.C};
-    learned_pixel(a, ex, sW, lam, col, ev, pix, lane);
-    __syncwarp();
-  }
-}
-
-// Learned-bracket bisection with the pixel's column resident in its warp
-// (n <= RES_MAX_N): one CTA per SM, pixels handed out by an atomic counter.
-__global__ void __launch_bounds__(RES_WARPS_LEARNED * 32, 1) learned_res_kernel(BisectArgs a,
-                                                                               LearnedExtra ex,
-                                                                               int* counter) {
-  extern __shared__ __align__(16) double smem[];
-  __shared__ float sW[NWEIGHT];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  load_weights_smem(ex.W, sW);
-  for (int p = threadIdx.x; p < a.n; p += blockDim.x) smem[p] = a.L[p];
-  __syncthreads();
-  double* smw = smem + RES_MAX_N + (size_t)warp * RES_S * 32;
-  ResCol rc;
-  rc.lam = smem;
-  rc.n = a.n;
-  rc.jn = (a.n + 31) / 32;
-  rc.U = a.UnotS != 0;
-  rc.C = a.C;
-  for (;;) {
-    int t = 0;
-    if (lane == 0) t = atomicAdd(counter, 1);
-    t = __shfl_sync(0xffffffffu, t, 0);
-    if (t >= a.m) break;
-    const double* col = a.P + (size_t)t * a.ldp;
-    rc.load(col, a.Nd, lane, smw);
-    __syncwarp();
-    learned_pixel(a, ex, sW, smem, col, rc, t, lane);
+    learned_pixel(a, ex, lam, gcol, ev, pix, lane);
     __syncwarp();
   }
 }
@@ -618,21 +748,37 @@ int feature_tables(imcom_ctx* ctx, const float2** nbr, const int** seg) {
   return 0;
 }
 
+// Features of every pixel into ctx->feat (12 x m, feature-major) and, with
+// the network installed and selected, its outputs into ctx->guess.
+int kappa_guess(imcom_ctx* ctx, const BisectArgs& a, bool network) {
+  IMC_TRY(ensure_vec(ctx, &ctx->feat, (size_t)NF * ctx->m));
+  IMC_TRY(ensure_vec(ctx, &ctx->guess, (size_t)ctx->m));
+  const float2* nbr;
+  const int* seg;
+  IMC_TRY(feature_tables(ctx, &nbr, &seg));
+  features_kernel<<<(ctx->m + 7) / 8, 256, 0, ctx->stream>>>(a, ctx->x, ctx->y, ctx->exp_i,
+                                                             ctx->X, ctx->Y, ctx->band, nbr, seg,
+                                                             ctx->feat);
+  IMC_LAUNCH();
+  if (network) {
+    const int per_block = MLP_WARPS * 16;
+    const int blocks = std::min((ctx->m + per_block - 1) / per_block, 4 * sm_count(ctx));
+    mlp_infer_kernel<<<blocks, MLP_WARPS * 32, 0, ctx->stream>>>(ctx->mlp.w, ctx->feat, ctx->m,
+                                                                ctx->guess);
+    IMC_LAUNCH();
+  }
+  return 0;
+}
+
 int fill_learned(imcom_ctx* ctx, LearnedExtra& ex) {
-  if (!ctx->mlp.set) return set_err(ctx, IMCOM_ERR_STATE, "imcom_gpu_mlp_set_weights has not run");
-  ex.x = ctx->x;
-  ex.y = ctx->y;
-  ex.X = ctx->X;
-  ex.Y = ctx->Y;
-  ex.expi = ctx->exp_i;
-  ex.W = ctx->mlp.w;
+  if (!ctx->mlp.set && !ctx->kappa_nonet)
+    return set_err(ctx, IMCOM_ERR_STATE, "imcom_gpu_mlp_set_weights has not run");
+  ex.guess = ctx->kappa_nonet ? nullptr : ctx->guess;
   ex.fallback = nullptr;
-  // band of every eigenmode for the P2 band features (+ segments, neighbours)
-  IMC_TRY(feature_tables(ctx, &ex.nbr, &ex.seg));
-  ex.bidx = ctx->band;
   ex.half_scale = 3.0;
   ex.min_half = 0.02;
   ex.margin = 1e-10;
+  ex.max_newton = 8;
   return 0;
 }
 
@@ -647,14 +793,7 @@ extern "C" int imcom_gpu_kappa_features(imcom_ctx* ctx, int UnotS, double US_max
   BisectArgs a;
   IMC_TRY(fill_bisect_args(ctx, a, UnotS, US_max, 1.0, 1.0, 0.0, 0, C_a));
   cudaSetDevice(ctx->device);
-  IMC_TRY(ensure_vec(ctx, &ctx->feat, (size_t)NF * ctx->m));
-  const float2* nbr;
-  const int* seg;
-  IMC_TRY(feature_tables(ctx, &nbr, &seg));
-  int blocks = (ctx->m + 7) / 8;
-  features_kernel<<<blocks, 256, 0, ctx->stream>>>(a, ctx->x, ctx->y, ctx->exp_i, ctx->X, ctx->Y,
-                                                   ctx->band, nbr, seg, ctx->feat);
-  IMC_LAUNCH();
+  IMC_TRY(kappa_guess(ctx, a, false));
   IMC_CUDA(cudaMemcpyAsync(feat_out, ctx->feat, (size_t)NF * ctx->m * sizeof(float),
                            cudaMemcpyDeviceToHost, ctx->stream));
   IMC_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -713,20 +852,12 @@ extern "C" int imcom_gpu_bisect_kappa_learned(imcom_ctx* ctx, int UnotS, double 
   IMC_TRY(ensure_buf(ctx, (void**)&ctx->fb, ctx->fb_bytes, (size_t)ctx->m * sizeof(int)));
   ex.fallback = ctx->fb;
   if (ctx->p_split) IMC_TRY(split_margin_buffer(ctx, a));
-  if (use_resident(ctx->bisect_kernel, ctx->n)) {
-    int* counter = ctx->flags + 24;
-    IMC_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), ctx->stream));
-    const size_t bytes = res_smem_bytes(RES_WARPS_LEARNED);
-    IMC_CUDA(cudaFuncSetAttribute(learned_res_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)bytes));
-    const int grid =
-        std::min(sm_count(ctx), (ctx->m + RES_WARPS_LEARNED - 1) / RES_WARPS_LEARNED);
-    learned_res_kernel<<<grid, RES_WARPS_LEARNED * 32, bytes, ctx->stream>>>(a, ex, counter);
-    IMC_LAUNCH();
-  } else {
+  if (!ctx->kappa_nonet) IMC_TRY(kappa_guess(ctx, a, true));
+  {
     PixelSmem plan = plan_pixel_smem(ctx->n);
     IMC_CUDA(cudaFuncSetAttribute(learned_bisect_kernel,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.bytes));
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kPixelSmemMax));
     learned_bisect_kernel<<<pixel_grid(ctx, plan, ctx->m), plan.warps * 32, plan.bytes,
                             ctx->stream>>>(a, plan, ex);
     IMC_LAUNCH();

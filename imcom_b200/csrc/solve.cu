@@ -250,9 +250,19 @@ int fill_bisect_args(imcom_ctx* ctx, BisectArgs& a, int UnotS, double US_max, do
   return 0;
 }
 
+// Pixels in flight: every pixel's warp streams its P column at each U/S
+// evaluation, so the columns of the pixels resident at once should fit in L2
+// (an explicit IMCOM_OPT_BISECT_CTAS_PER_SM wins).
+constexpr double kPixelL2Budget = 80.0 * 1024 * 1024;
+
 int pixel_grid(imcom_ctx* ctx, const PixelSmem& plan, int m) {
   int blocks = (m + plan.warps - 1) / plan.warps;
-  if (ctx->bisect_ctas > 0) blocks = std::min(blocks, ctx->bisect_ctas * sm_count(ctx));
+  int per_sm = ctx->bisect_ctas;
+  if (per_sm <= 0 && !plan.col_smem) {
+    const double col = (double)ctx->n * sizeof(double) * plan.warps;  // one CTA's columns
+    per_sm = std::max(1, (int)(kPixelL2Budget / (col * sm_count(ctx))));
+  }
+  if (per_sm > 0) blocks = std::min(blocks, per_sm * sm_count(ctx));
   return blocks;
 }
 
@@ -272,7 +282,7 @@ int launch_bisect(imcom_ctx* ctx, const BisectArgs& a) {
   }
   PixelSmem plan = plan_pixel_smem(ctx->n);
   IMC_CUDA(cudaFuncSetAttribute(bisect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)plan.bytes));
+                                (int)kPixelSmemMax));
   bisect_kernel<<<pixel_grid(ctx, plan, total), plan.warps * 32, plan.bytes, ctx->stream>>>(a,
                                                                                           plan);
   IMC_LAUNCH();
@@ -516,7 +526,7 @@ extern "C" int imcom_gpu_build_U(imcom_ctx* ctx, double C_a, double* U_out) {
   plan.col_smem = false;
   plan.bytes = plan.lam_smem ? (size_t)ctx->n * sizeof(double) : 0;
   IMC_CUDA(cudaFuncSetAttribute(eval_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)plan.bytes));
+                                (int)kPixelSmemMax));
   eval_kernel<<<pixel_grid(ctx, plan, ctx->m), plan.warps * 32, plan.bytes, ctx->stream>>>(
       a, plan, ctx->U);
   IMC_LAUNCH();

@@ -293,6 +293,72 @@ table_fft_pass2(FftPlan plan, const double2* __restrict__ W, const double2* __re
   }
 }
 
+// ---------------------------------------------------------------------------
+// The PSF spectra's real-to-complex transform (imcom_ft_r2c,
+// imcom_proc.f90:433-475: FFTW's forward r2c of an nps x nps image, the first
+// axis halved to nps/2 + 1), in two passes with the same line transforms.
+// The forward transform is the conjugate of the backward one of the
+// conjugated input: pass 1 transforms the real lines along the first axis and
+// keeps k = 0 .. nps/2 (stored column-major by k, H[b][k][j]), pass 2
+// transforms those columns along the second axis and writes the half
+// spectrum half[b][j][k] (k fastest), the layout the Hermitian fill reads.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(FFT_THREADS, 1)
+r2c_pass1(FftPlan plan, const double* __restrict__ in, const double2* __restrict__ tw,
+          double2* __restrict__ H) {
+  extern __shared__ double2 buf[];
+  const int n = plan.L, LS = plan.LS, TP = plan.TP;
+  const int nh = n / 2 + 1;
+  const int b = blockIdx.y;
+  const int j0 = blockIdx.x * TP;
+  const double* src = in + (size_t)b * n * n;
+  for (int e = threadIdx.x; e < TP * n; e += FFT_THREADS) {
+    const int line = e / n, k = e - line * n;
+    const int j = j0 + line;
+    buf[line * LS + k] = make_double2(j < n ? src[(size_t)j * n + k] : 0.0, 0.0);
+  }
+  __syncthreads();
+  run_stages(buf, plan, tw);
+  for (int e = threadIdx.x; e < TP * nh; e += FFT_THREADS) {
+    const int k = e / TP, line = e - k * TP;
+    const int j = j0 + line;
+    if (j < n) {
+      const double2 v = buf[line * LS + k];
+      H[((size_t)b * nh + k) * n + j] = make_double2(v.x, -v.y);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(FFT_THREADS, 1)
+r2c_pass2(FftPlan plan, const double2* __restrict__ H, const double2* __restrict__ tw,
+          double2* __restrict__ half) {
+  extern __shared__ double2 buf[];
+  const int n = plan.L, LS = plan.LS, TP = plan.TP;
+  const int nh = n / 2 + 1;
+  const int b = blockIdx.y;
+  const int k0 = blockIdx.x * TP;
+  for (int e = threadIdx.x; e < TP * n; e += FFT_THREADS) {
+    const int line = e / n, j = e - line * n;
+    const int k = k0 + line;
+    double2 v = make_double2(0.0, 0.0);
+    if (k < nh) {
+      v = H[((size_t)b * nh + k) * n + j];
+      v.y = -v.y;
+    }
+    buf[line * LS + j] = v;
+  }
+  __syncthreads();
+  run_stages(buf, plan, tw);
+  for (int e = threadIdx.x; e < TP * n; e += FFT_THREADS) {
+    const int j = e / TP, line = e - j * TP;
+    const int k = k0 + line;
+    if (k < nh) {
+      const double2 v = buf[line * LS + j];
+      half[((size_t)b * n + j) * nh + k] = make_double2(v.x, -v.y);
+    }
+  }
+}
+
 // exp(2 pi i t / L), t < L, rounded from extended precision; the parts that
 // are exactly 0 (where 4t is a multiple of L) come out as exact zeros.
 std::vector<double2> twiddles(int L) {
@@ -310,6 +376,36 @@ std::vector<double2> twiddles(int L) {
 
 }  // namespace
 
+int psf_r2c_own(imcom_ctx* ctx, int n, int count, const double* in, double2* H, double2* half,
+                bool* done) {
+  *done = false;
+  FftPlan plan;
+  if (n < 2 || !make_plan(n, &plan)) return 0;
+  if (ctx->r2c_tw_L != n) {
+    IMC_CUDA(cudaStreamSynchronize(ctx->stream));  // no launch still reads the old table
+    IMC_TRY(ensure_buf(ctx, (void**)&ctx->r2c_tw, ctx->r2c_tw_bytes, (size_t)n * sizeof(double2)));
+    const std::vector<double2> tw = twiddles(n);
+    IMC_CUDA(cudaMemcpy(ctx->r2c_tw, tw.data(), (size_t)n * sizeof(double2),
+                        cudaMemcpyHostToDevice));
+    ctx->r2c_tw_L = n;
+  }
+  const int smem = plan.TP * plan.LS * (int)sizeof(double2);
+  // limits set to the largest plan's need: the attribute is process-wide and
+  // contexts on several host threads must not lower it under each other
+  constexpr int kMax = FFT_MAX_ELEMS * (int)sizeof(double2);
+  IMC_CUDA(cudaFuncSetAttribute(r2c_pass1, cudaFuncAttributeMaxDynamicSharedMemorySize, kMax));
+  IMC_CUDA(cudaFuncSetAttribute(r2c_pass2, cudaFuncAttributeMaxDynamicSharedMemorySize, kMax));
+  const int nh = n / 2 + 1;
+  const dim3 g1((unsigned)((n + plan.TP - 1) / plan.TP), (unsigned)count);
+  r2c_pass1<<<g1, FFT_THREADS, smem, ctx->stream>>>(plan, in, ctx->r2c_tw, H);
+  IMC_LAUNCH();
+  const dim3 g2((unsigned)((nh + plan.TP - 1) / plan.TP), (unsigned)count);
+  r2c_pass2<<<g2, FFT_THREADS, smem, ctx->stream>>>(plan, H, ctx->r2c_tw, half);
+  IMC_LAUNCH();
+  *done = true;
+  return 0;
+}
+
 int table_fft_inverse(imcom_ctx* ctx, int nps, int L, int ntab, const int2* dpairs, double2* W,
                       double* tab, int isB, bool* done) {
   *done = false;
@@ -324,10 +420,11 @@ int table_fft_inverse(imcom_ctx* ctx, int nps, int L, int ntab, const int2* dpai
     ctx->fft_tw_L = L;
   }
   const int smem = plan.TP * plan.LS * (int)sizeof(double2);
+  constexpr int kMax = FFT_MAX_ELEMS * (int)sizeof(double2);  // see psf_r2c_own
   IMC_CUDA(cudaFuncSetAttribute(table_fft_pass1, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                smem));
+                                kMax));
   IMC_CUDA(cudaFuncSetAttribute(table_fft_pass2, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                smem));
+                                kMax));
   const dim3 g1((unsigned)((nps + plan.TP - 1) / plan.TP), (unsigned)ntab);
   table_fft_pass1<<<g1, FFT_THREADS, smem, ctx->stream>>>(plan, ctx->Gt, ctx->Gammat, dpairs,
                                                           ctx->fft_tw, W, nps);

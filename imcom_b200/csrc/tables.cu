@@ -5,7 +5,7 @@
 // imcom_proc.f90 / imcom_matrix.f90 operation by operation.  The FFTs are
 // cuFFT (the reference calls FFTW for the same transforms).
 //
-//   rotate_psf_kernel     imcom_rotate_image   imcom_proc.f90:184-250
+//   rotate_psf_kernel     imcom_rotate_image   imcom_proc.f90:184-250 (Lagrange form)
 //   hermitian_fill_kernel imcom_ft_r2c         imcom_proc.f90:433-475
 //   csum_kernel           imcom_calc_C         imcom_matrix.f90:546-552
 //   embed_kernel          imcom_build_Alookup  imcom_matrix.f90:395-411
@@ -19,54 +19,50 @@
 namespace imcom {
 namespace {
 
-// Neville on at most 16 points: imcom_polint (imcom_proc.f90:351-394),
-// step for step.  Returns nonzero on the duplicate-abscissa trap.
-__device__ int polint_dev(const double* xa, const double* ya, int n, double x,
-                          double* y, double eps) {
-  double c[16], d[16], den[16], ho[16];
-  for (int i = 0; i < n; ++i) {
-    c[i] = ya[i];
-    d[i] = ya[i];
-    ho[i] = xa[i] - x;
+// Lagrange weights of the m consecutive integer nodes x0, x0+1, ... at t:
+// w_k = prod_{j != k} (t - x_j) / prod_{j != k} (k - j), from prefix and
+// suffix products (the denominators are exact integers); a node hit exactly
+// gets weight 1 and the others 0.
+__device__ __forceinline__ void lagrange_weights(double t, int x0, int m, double (&w)[16]) {
+  double sv[16], pre[16];
+  bool node = false;
+  double acc = 1.0;
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    sv[j] = (j < m) ? t - (double)(x0 + j) : 1.0;
+    node |= (j < m) && (sv[j] == 0.0);
+    pre[j] = acc;
+    acc = acc * sv[j];
   }
-  int ns = 1;
-  double best = fabs(x - xa[0]);
-  for (int i = 1; i < n; ++i) {
-    double v = fabs(x - xa[i]);
-    if (v < best) {
-      best = v;
-      ns = i + 1;
-    }
+  acc = 1.0;
+#pragma unroll
+  for (int k = 15; k >= 0; --k) {
+    // prod_{j != k} (k - j) = (-1)^(m-1-k) k! (m-1-k)!
+    double den = 1.0;
+    for (int q = 2; q <= k; ++q) den = den * (double)q;
+    for (int q = 2; q <= m - 1 - k; ++q) den = den * (double)q;
+    if ((m - 1 - k) & 1) den = -den;
+    w[k] = (k < m) ? pre[k] * acc / den : 0.0;
+    acc = acc * sv[k];
   }
-  double yy = ya[ns - 1], dy;
-  ns = ns - 1;
-  for (int m = 1; m <= n - 1; ++m) {
-    for (int i = 1; i <= n - m; ++i) den[i - 1] = ho[i - 1] - ho[i + m - 1];
-    for (int i = 1; i <= n - m; ++i)
-      if (fabs(den[i - 1]) <= eps) return 1;
-    for (int i = 1; i <= n - m; ++i) den[i - 1] = (c[i] - d[i - 1]) / den[i - 1];
-    for (int i = 1; i <= n - m; ++i) {
-      d[i - 1] = ho[i + m - 1] * den[i - 1];
-      c[i - 1] = ho[i - 1] * den[i - 1];
-    }
-    if (2 * ns < n - m) {
-      dy = c[ns];
-    } else {
-      dy = d[ns - 1];
-      ns = ns - 1;
-    }
-    yy = yy + dy;
+  if (node) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) w[k] = (k < m && sv[k] == 0.0) ? 1.0 : 0.0;
   }
-  *y = yy;
-  return 0;
 }
 
 // One output pixel of imcom_rotate_image per thread.  cost/sint come from
-// the host (same libm as the reference's runtime), so the source coordinate
-// and its floor/ceiling are bit-identical.
+// the host (same libm as the reference's runtime), so the source coordinate,
+// its floor/ceiling and the interpolation window [floor - npm, ceil + npm]
+// clipped to the image are bit-identical.  The reference interpolates on that
+// window with imcom_polin2 (Neville's tableau along the second axis for each
+// window row, then along the first; imcom_proc.f90:351-429); the
+// interpolating polynomial on those nodes is unique, and this kernel
+// evaluates it in Lagrange form, f = sum_j wx_j sum_k wy_k in(x_j, y_k):
+// equal up to rounding, with no divisions by data.  Neville's
+// duplicate-abscissa trap cannot fire on distinct integer nodes.
 __global__ void rotate_psf_kernel(const double* __restrict__ in, double* __restrict__ out,
-                                  int nim, int npm, double cost, double sint,
-                                  double eps, int* flags) {
+                                  int nim, int npm, double cost, double sint) {
   int iout = blockIdx.x * blockDim.x + threadIdx.x + 1;
   int jout = blockIdx.y + 1;
   if (iout > nim) return;
@@ -82,17 +78,21 @@ __global__ void rotate_psf_kernel(const double* __restrict__ in, double* __restr
     int imin = max(1, is_floor - npm), jmin = max(1, js_floor - npm);
     int imax = min(nim, is_ceil + npm), jmax = min(nim, js_ceil + npm);
     int m1 = imax - imin + 1, m2 = jmax - jmin + 1;
-    double x1a[16], x2a[16], ymtmp[16], yntmp[16];
-    for (int ii = 0; ii < m1; ++ii) x1a[ii] = (double)(imin + ii);
-    for (int jj = 0; jj < m2; ++jj) x2a[jj] = (double)(jmin + jj);
-    int bad = 0;
-    for (int j = 0; j < m1; ++j) {
-      for (int k = 0; k < m2; ++k)
-        yntmp[k] = in[(size_t)(imin - 1 + j) + (size_t)(jmin - 1 + k) * nim];
-      bad |= polint_dev(x2a, yntmp, m2, ys, &ymtmp[j], eps);
+    double wx[16], wy[16];
+    lagrange_weights(xs, imin, m1, wx);
+    lagrange_weights(ys, jmin, m2, wy);
+    const double* base = in + (size_t)(imin - 1) + (size_t)(jmin - 1) * nim;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      if (k < m2) {
+        const double* row = base + (size_t)k * nim;
+        double g = 0.0;
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+          if (j < m1) g = g + wx[j] * __ldg(row + j);
+        f = f + wy[k] * g;
+      }
     }
-    bad |= polint_dev(x1a, ymtmp, m1, xs, &f, eps);
-    if (bad) atomicOr(flags, 1);
   }
   out[(size_t)(iout - 1) + (size_t)(jout - 1) * nim] = f;
 }
@@ -310,7 +310,9 @@ extern "C" int imcom_gpu_psf_spectra(imcom_ctx* ctx, int npoly_in, double* C_out
   // each region starts on a 256-byte boundary (complex data needs 16 bytes)
   size_t real_b = ((E + 1) * ps2 * sizeof(double) + 255) / 256 * 256;
   size_t half_b = ((size_t)(E + 1) * nh * nps * sizeof(double2) + 255) / 256 * 256;
-  size_t need = real_b + half_b + 8192;
+  // own transform: its intermediate (same size as the half spectra) follows
+  const bool own = ctx->table_fft == IMCOM_TABLE_FFT_OWN;
+  size_t need = real_b + half_b + 8192 + (own ? half_b : 0);
   stage_begin(ctx, ST_SPECTRA);
   IMC_TRY(ensure_buf(ctx, (void**)&ctx->fftbuf, ctx->fftbuf_bytes, need));
   double* rin = reinterpret_cast<double*>(ctx->fftbuf);
@@ -328,8 +330,7 @@ extern "C" int imcom_gpu_psf_spectra(imcom_ctx* ctx, int npoly_in, double* C_out
       double theta_rad = std::fmod(ang, 360.0) * pi / 180.0;
       double cost = std::cos(theta_rad), sint = std::sin(theta_rad);
       dim3 blk(128), grd((nps + 127) / 128, nps);
-      rotate_psf_kernel<<<grd, blk, 0, ctx->stream>>>(src, dst, nps, npm, cost, sint, eps,
-                                                       ctx->flags);
+      rotate_psf_kernel<<<grd, blk, 0, ctx->stream>>>(src, dst, nps, npm, cost, sint);
       IMC_LAUNCH();
       IMC_TRY(sum_device(ctx, src, ps2, sums + 0, scratch));
       IMC_TRY(sum_device(ctx, dst, ps2, sums + 1, scratch + 256));
@@ -342,7 +343,13 @@ extern "C" int imcom_gpu_psf_spectra(imcom_ctx* ctx, int npoly_in, double* C_out
   }
   IMC_CUDA(cudaMemcpyAsync(rin + (size_t)E * ps2, ctx->Gamma, ps2 * sizeof(double),
                            cudaMemcpyDeviceToDevice, ctx->stream));
-  IMC_TRY(fft_d2z(ctx, nps, E + 1, rin, half));
+  bool done = false;
+  if (own) {
+    double2* H = reinterpret_cast<double2*>(reinterpret_cast<char*>(ctx->fftbuf) + real_b +
+                                            half_b + 8192);
+    IMC_TRY(psf_r2c_own(ctx, nps, E + 1, rin, H, half, &done));
+  }
+  if (!done) IMC_TRY(fft_d2z(ctx, nps, E + 1, rin, half));
   {
     dim3 blk(128), grd((nps + 127) / 128, nps, E);
     hermitian_fill_kernel<<<grd, blk, 0, ctx->stream>>>(half, ctx->Gt, nps, nps);

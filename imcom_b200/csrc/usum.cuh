@@ -48,6 +48,26 @@ __device__ __forceinline__ double sterm(double l, double pp, double nd, double k
   return __dmul_rn(__dmul_rn(nd, p2), rcp_nr(__dmul_rn(t, t)));
 }
 
+// The same terms with the kappa derivative's term added to *d: P2 / (L + k)^3
+// (U mode) or Nd P2 / (L + k)^3 (S mode).  The returned term is the one
+// uterm / sterm return, formed by the same operations.
+__device__ __forceinline__ double uterm_d(double l, double pp, double k, double k2, double* d) {
+  const double p2 = __dmul_rn(pp, pp);
+  const double t = __dadd_rn(l, k);
+  const double r = rcp_nr(__dmul_rn(t, t));
+  *d = fma(p2 * r, t * r, *d);
+  return __dmul_rn(__dmul_rn(__dadd_rn(l, k2), p2), r);
+}
+
+__device__ __forceinline__ double sterm_d(double l, double pp, double nd, double k, double* d) {
+  const double p2 = __dmul_rn(pp, pp);
+  const double t = __dadd_rn(l, k);
+  const double r = rcp_nr(__dmul_rn(t, t));
+  const double v = __dmul_rn(__dmul_rn(nd, p2), r);
+  *d = fma(v, t * r, *d);
+  return v;
+}
+
 __device__ __forceinline__ double warp_reduce_sum(double s) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) s = __dadd_rn(s, __shfl_xor_sync(0xffffffffu, s, o));
@@ -56,10 +76,15 @@ __device__ __forceinline__ double warp_reduce_sum(double s) {
 
 // Modes p = lane + 32 j go to partial sum j mod 4, in increasing j; blocks
 // of eight modes per lane keep eight column loads in flight.
-__device__ __forceinline__ double warp_usum(const double* lam, const double* col, int n,
-                                            double k, int lane) {
+// D = true also sums the derivative terms into *dsum (every lane gets the
+// total); the U sum is formed by exactly the same operations either way.
+template <bool D>
+__device__ __forceinline__ double warp_usum_t(const double* lam, const double* col, int n,
+                                              double k, int lane, double* dsum) {
   const double k2 = __dmul_rn(2.0, k);
   double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  double dd = 0.0;
+#define UT(l_, c_) (D ? uterm_d(l_, c_, k, k2, &dd) : uterm(l_, c_, k, k2))
   int p = lane;
   for (; p + 224 < n; p += 256) {
     double c[8], l[8];
@@ -68,30 +93,41 @@ __device__ __forceinline__ double warp_usum(const double* lam, const double* col
       c[q] = col[p + 32 * q];
       l[q] = lam[p + 32 * q];
     }
-    s0 = __dadd_rn(s0, uterm(l[0], c[0], k, k2));
-    s1 = __dadd_rn(s1, uterm(l[1], c[1], k, k2));
-    s2 = __dadd_rn(s2, uterm(l[2], c[2], k, k2));
-    s3 = __dadd_rn(s3, uterm(l[3], c[3], k, k2));
-    s0 = __dadd_rn(s0, uterm(l[4], c[4], k, k2));
-    s1 = __dadd_rn(s1, uterm(l[5], c[5], k, k2));
-    s2 = __dadd_rn(s2, uterm(l[6], c[6], k, k2));
-    s3 = __dadd_rn(s3, uterm(l[7], c[7], k, k2));
+    s0 = __dadd_rn(s0, UT(l[0], c[0]));
+    s1 = __dadd_rn(s1, UT(l[1], c[1]));
+    s2 = __dadd_rn(s2, UT(l[2], c[2]));
+    s3 = __dadd_rn(s3, UT(l[3], c[3]));
+    s0 = __dadd_rn(s0, UT(l[4], c[4]));
+    s1 = __dadd_rn(s1, UT(l[5], c[5]));
+    s2 = __dadd_rn(s2, UT(l[6], c[6]));
+    s3 = __dadd_rn(s3, UT(l[7], c[7]));
   }
   for (; p + 96 < n; p += 128) {
-    s0 = __dadd_rn(s0, uterm(lam[p], col[p], k, k2));
-    s1 = __dadd_rn(s1, uterm(lam[p + 32], col[p + 32], k, k2));
-    s2 = __dadd_rn(s2, uterm(lam[p + 64], col[p + 64], k, k2));
-    s3 = __dadd_rn(s3, uterm(lam[p + 96], col[p + 96], k, k2));
+    s0 = __dadd_rn(s0, UT(lam[p], col[p]));
+    s1 = __dadd_rn(s1, UT(lam[p + 32], col[p + 32]));
+    s2 = __dadd_rn(s2, UT(lam[p + 64], col[p + 64]));
+    s3 = __dadd_rn(s3, UT(lam[p + 96], col[p + 96]));
   }
-  if (p < n) s0 = __dadd_rn(s0, uterm(lam[p], col[p], k, k2));
-  if (p + 32 < n) s1 = __dadd_rn(s1, uterm(lam[p + 32], col[p + 32], k, k2));
-  if (p + 64 < n) s2 = __dadd_rn(s2, uterm(lam[p + 64], col[p + 64], k, k2));
+  if (p < n) s0 = __dadd_rn(s0, UT(lam[p], col[p]));
+  if (p + 32 < n) s1 = __dadd_rn(s1, UT(lam[p + 32], col[p + 32]));
+  if (p + 64 < n) s2 = __dadd_rn(s2, UT(lam[p + 64], col[p + 64]));
+#undef UT
+  if (D) *dsum = warp_reduce_sum(dd);
   return warp_reduce_sum(__dadd_rn(__dadd_rn(s0, s1), __dadd_rn(s2, s3)));
 }
 
-__device__ __forceinline__ double warp_ssum(const double* lam, const double* col,
-                                            const double* nd, int n, double k, int lane) {
+__device__ __forceinline__ double warp_usum(const double* lam, const double* col, int n,
+                                            double k, int lane) {
+  return warp_usum_t<false>(lam, col, n, k, lane, nullptr);
+}
+
+template <bool D>
+__device__ __forceinline__ double warp_ssum_t(const double* lam, const double* col,
+                                              const double* nd, int n, double k, int lane,
+                                              double* dsum) {
   double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  double dd = 0.0;
+#define ST(l_, c_, w_) (D ? sterm_d(l_, c_, w_, k, &dd) : sterm(l_, c_, w_, k))
   int p = lane;
   for (; p + 224 < n; p += 256) {
     double c[8], l[8], w[8];
@@ -101,25 +137,32 @@ __device__ __forceinline__ double warp_ssum(const double* lam, const double* col
       l[q] = lam[p + 32 * q];
       w[q] = nd[p + 32 * q];
     }
-    s0 = __dadd_rn(s0, sterm(l[0], c[0], w[0], k));
-    s1 = __dadd_rn(s1, sterm(l[1], c[1], w[1], k));
-    s2 = __dadd_rn(s2, sterm(l[2], c[2], w[2], k));
-    s3 = __dadd_rn(s3, sterm(l[3], c[3], w[3], k));
-    s0 = __dadd_rn(s0, sterm(l[4], c[4], w[4], k));
-    s1 = __dadd_rn(s1, sterm(l[5], c[5], w[5], k));
-    s2 = __dadd_rn(s2, sterm(l[6], c[6], w[6], k));
-    s3 = __dadd_rn(s3, sterm(l[7], c[7], w[7], k));
+    s0 = __dadd_rn(s0, ST(l[0], c[0], w[0]));
+    s1 = __dadd_rn(s1, ST(l[1], c[1], w[1]));
+    s2 = __dadd_rn(s2, ST(l[2], c[2], w[2]));
+    s3 = __dadd_rn(s3, ST(l[3], c[3], w[3]));
+    s0 = __dadd_rn(s0, ST(l[4], c[4], w[4]));
+    s1 = __dadd_rn(s1, ST(l[5], c[5], w[5]));
+    s2 = __dadd_rn(s2, ST(l[6], c[6], w[6]));
+    s3 = __dadd_rn(s3, ST(l[7], c[7], w[7]));
   }
   for (; p + 96 < n; p += 128) {
-    s0 = __dadd_rn(s0, sterm(lam[p], col[p], nd[p], k));
-    s1 = __dadd_rn(s1, sterm(lam[p + 32], col[p + 32], nd[p + 32], k));
-    s2 = __dadd_rn(s2, sterm(lam[p + 64], col[p + 64], nd[p + 64], k));
-    s3 = __dadd_rn(s3, sterm(lam[p + 96], col[p + 96], nd[p + 96], k));
+    s0 = __dadd_rn(s0, ST(lam[p], col[p], nd[p]));
+    s1 = __dadd_rn(s1, ST(lam[p + 32], col[p + 32], nd[p + 32]));
+    s2 = __dadd_rn(s2, ST(lam[p + 64], col[p + 64], nd[p + 64]));
+    s3 = __dadd_rn(s3, ST(lam[p + 96], col[p + 96], nd[p + 96]));
   }
-  if (p < n) s0 = __dadd_rn(s0, sterm(lam[p], col[p], nd[p], k));
-  if (p + 32 < n) s1 = __dadd_rn(s1, sterm(lam[p + 32], col[p + 32], nd[p + 32], k));
-  if (p + 64 < n) s2 = __dadd_rn(s2, sterm(lam[p + 64], col[p + 64], nd[p + 64], k));
+  if (p < n) s0 = __dadd_rn(s0, ST(lam[p], col[p], nd[p]));
+  if (p + 32 < n) s1 = __dadd_rn(s1, ST(lam[p + 32], col[p + 32], nd[p + 32]));
+  if (p + 64 < n) s2 = __dadd_rn(s2, ST(lam[p + 64], col[p + 64], nd[p + 64]));
+#undef ST
+  if (D) *dsum = warp_reduce_sum(dd);
   return warp_reduce_sum(__dadd_rn(__dadd_rn(s0, s1), __dadd_rn(s2, s3)));
+}
+
+__device__ __forceinline__ double warp_ssum(const double* lam, const double* col,
+                                            const double* nd, int n, double k, int lane) {
+  return warp_ssum_t<false>(lam, col, nd, n, k, lane, nullptr);
 }
 
 // U or S at kappa k.
@@ -143,6 +186,20 @@ struct StreamCol {
   double C;
   __device__ __forceinline__ double operator()(double k, int lane) const {
     return warp_us(U, lam, col, nd, n, k, C, lane);
+  }
+  // U or S at kappa k (the value operator() returns, bit for bit) and its
+  // derivative with respect to x = log10(kappa) in *dx.
+  __device__ __forceinline__ double eval_d(double k, int lane, double* dx) const {
+    constexpr double LN10 = 2.302585092994046;
+    double d;
+    if (U) {
+      const double usum = warp_usum_t<true>(lam, col, n, k, lane, &d);
+      *dx = LN10 * k * k / (2.0 * C) * d;
+      return __ddiv_rn(__dsub_rn(C, __ddiv_rn(usum, 4.0)), C);
+    }
+    const double ssum = warp_ssum_t<true>(lam, col, nd, n, k, lane, &d);
+    *dx = -0.5 * LN10 * k * d;
+    return __ddiv_rn(ssum, 4.0);
   }
 };
 
@@ -224,7 +281,6 @@ struct ResCol {
 // register-resident weights; with 3 warps on a sub-partition the limit drops
 // to 168 and the column spills.
 constexpr int RES_WARPS_PLAIN = 8;    // 32 KB + 8 x 16 KB = 160 KB
-constexpr int RES_WARPS_LEARNED = 8;  // + 20 KB of MLP weights
 // Resident kernel for this problem?  mode: IMCOM_BISECT_* option value.
 // Automatic choice: streaming.  With the Newton reciprocal the per-term
 // chain is short and the streaming kernel's ~28 warps per SM hide L2
@@ -253,7 +309,12 @@ struct PixelSmem {
 // least 4 CTAs (16 pixel warps) per SM.  Otherwise nothing is staged: the
 // eigenvalues (read by every warp) stay in L1, the columns stream from L2,
 // and ~28 pixel warps per SM run the n = m = 4096 case in a single wave.
-inline PixelSmem plan_pixel_smem(int n, size_t limit = 52 * 1024) {
+// The pixel kernels' dynamic shared-memory limit is set once to this ceiling
+// (the attribute is process-wide: contexts solving on several host threads
+// must not set it under one another's launches).
+constexpr size_t kPixelSmemMax = 52 * 1024;
+
+inline PixelSmem plan_pixel_smem(int n, size_t limit = kPixelSmemMax) {
   PixelSmem p;
   const size_t col = (size_t)n * sizeof(double);
   p.warps = 4;

@@ -75,9 +75,10 @@ typedef struct imcom_ctx imcom_ctx;
 #define IMCOM_BISECT_AUTO 0
 #define IMCOM_BISECT_STREAM 1
 #define IMCOM_BISECT_RESIDENT 2
-/* CTAs (of 4 pixel warps) per SM of the streaming bisection kernels; 0 puts
- * every pixel in flight at once.  Fewer pixels in flight keep their P columns
- * in L2 across their U/S evaluations. */
+/* CTAs (of 4 pixel warps) per SM of the streaming bisection kernels: 1..64
+ * that many; 0 (default) = automatic, as many as keep the P columns of the
+ * pixels in flight within 80 MB, so that they stay in L2 across their U/S
+ * evaluations instead of being read from HBM again at every evaluation. */
 #define IMCOM_OPT_BISECT_CTAS_PER_SM 9
 /* Number of SMs this context sizes its persistent and cooperative grids for
  * (the tridiagonalisation panel kernel, the resident bisection, split-K
@@ -111,13 +112,18 @@ typedef struct imcom_ctx imcom_ctx;
 #define IMCOM_TABLE_FFT_CUFFT 0
 #define IMCOM_TABLE_FFT_OWN 1
 /* Features of the learned-kappa bracket: 0 = every pixel scans all inputs
- * for its neighbours and bins P^2 by eigenmode band element by element
- * (default); 1 = the neighbour features come from a per-pixel table built
+ * for its neighbours and bins P^2 by eigenmode band element by element;
+ * 1 (default) = the neighbour features come from a per-pixel table built
  * once per set of inputs, and the band sums run over the bands' contiguous
  * ranges of eigenmodes (the band index is non-decreasing when L is in
  * descending order; otherwise the element-wise binning is kept).  Same
  * features to rounding, same kappa. */
 #define IMCOM_OPT_KAPPA_FEATURES 14
+/* Starting point of imcom_gpu_bisect_kappa_learned's Newton steps: 0
+ * (default) = the network's prediction; 1 = no network, the middle of the
+ * search range (the comparison that shows what the network saves).  Same
+ * kappa either way. */
+#define IMCOM_OPT_KAPPA_START 17
 /* Iteration cap of the divide-and-conquer secular-equation solver (0 = the
  * default, 100; roots converge in at most about 10).  A root that reaches the
  * cap makes imcom_gpu_eigen_A return IMCOM_ERR_EIGEN, as DSYEVR's info > 0
@@ -227,10 +233,14 @@ int imcom_gpu_bisect_kappa(imcom_ctx* ctx, int UnotS, double US_max,
 
 /* Same contract and bit-identical K as imcom_gpu_bisect_kappa, with the
  * learned-kappa bracket: an MLP (imcom_gpu_mlp_set_weights) predicts
- * log10(kappa) and a bracket half-width per pixel; the bracket is verified
- * with two evaluations and the bisection steps it decides are skipped.
- * Pixels whose bracket fails run the plain bisection.  No reference
- * counterpart; replaces imcom_bisect_kappa (imcom_bisect.f90:78-170). */
+ * log10(kappa) and a bracket half-width per pixel; Newton steps in
+ * log10(kappa) from that prediction, each one evaluation of U (or S) and its
+ * derivative, and two probes find points on either side of the band where
+ * the bisection stops; the bisection steps those points decide are skipped
+ * and the rest are evaluated, so K_a and U_a (S_a) equal the plain
+ * bisection's bit for bit.  fallback_out (m, may be NULL): 1 where no point
+ * bounded the bisection.  No reference counterpart; replaces
+ * imcom_bisect_kappa (imcom_bisect.f90:78-170). */
 int imcom_gpu_bisect_kappa_learned(imcom_ctx* ctx, int UnotS, double US_max,
                                    double k_min, double k_max, double tol,
                                    int maxnits, double C_a, double* K_out,
@@ -369,6 +379,17 @@ int imcom_gpu_build_P_noalloc(const double* dQ, long long ldq, const double* dB,
  * converge in 60 sweeps, IMCOM_ERR_CUDA / IMCOM_ERR_ALLOC. */
 int imcom_gpu_eigh_jacobi_batched(imcom_ctx* ctx, int n, int count, const double* A,
                                   double* Q, double* L, int* sweeps);
+
+/* ---- two-stage reduction (diagnostic) --------------------------------- */
+
+/* First stage of the two-stage tridiagonalisation alone: the resident A
+ * (built or loaded) reduced to a symmetric band matrix of bandwidth 32 by
+ * blocked Householder transformations, returned as its 33 lower diagonals in
+ * band storage, AB_out[d + c * ldb] = B(c + d, c) (ldb >= 33, n columns).
+ * The band matrix has A's eigenvalues.  No reference counterpart (the
+ * reference reduces A to tridiagonal form inside DSYEVR,
+ * imcom_matrix.f90:617-643). */
+int imcom_gpu_band_reduce(imcom_ctx* ctx, double* AB_out, int ldb);
 
 /* ---- FITS files without CFITSIO (host only; no context, no GPU) -------- */
 

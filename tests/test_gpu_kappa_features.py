@@ -1,6 +1,6 @@
 """The learned-kappa features from the neighbour table and the band segments
-(IMCOM_OPT_KAPPA_FEATURES = 1, imcom_b200/csrc/kappa.cu) against the default
-per-pixel scan and element-wise binning, through the C-ABI: the neighbour
+(IMCOM_OPT_KAPPA_FEATURES = 1, the default; imcom_b200/csrc/kappa.cu) against
+the per-pixel scan and element-wise binning (option 0), through the C-ABI: the neighbour
 count and exposure count equal, the eight band features equal to float
 rounding; and the bracketed bisection's contract -- K and U bit-identical to
 the plain bisection -- with the table-built features, also after the inputs
@@ -29,6 +29,7 @@ def system(s, prob):
 def test_table_features_equal_scanned_features(seed):
     with Solver(0) as s:
         C = system(s, synth.make("small", seed))
+        s.set_option(OPT_KAPPA_FEATURES, 0)
         F0 = s.kappa_features(True, 1e-6, C)
         s.set_option(OPT_KAPPA_FEATURES, 1)
         F1 = s.kappa_features(True, 1e-6, C)

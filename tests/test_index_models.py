@@ -689,3 +689,99 @@ def test_table_kernels_as_written_match_embed_fft_shift(nps, npad):
         for g, r in zip(got, ref):
             assert not np.isnan(g).any()
             assert np.max(np.abs(g - r)) <= 1e-12 * max(1.0, np.max(np.abs(r)))
+
+
+# -- the PSF spectra's own real-to-complex transform ------------------------------
+
+
+def r2c_kernels(images):
+    """r2c_pass1 and r2c_pass2 (table_fft.cu) emulated block by block: the
+    half spectra half[b][j][k] (k fastest, n/2 + 1 per row) of n x n real
+    images stored x fastest."""
+    count, n = images.shape[0], images.shape[1]
+    LS, TP, _ = fft_plan(n)
+    nh = n // 2 + 1
+    tw = np.exp(2j * np.pi * np.arange(n) / n)
+    src = [im.T.ravel() for im in images]  # element (k, j) at j n + k
+    H = np.full((count, nh, n), np.nan + 0j)
+    half = np.full((count, n, nh), np.nan + 0j)
+    for b in range(count):
+        for bx in range(-(-n // TP)):
+            j0 = bx * TP
+            buf = np.full(TP * LS, np.nan + 0j)
+            for e in range(TP * n):
+                line, k = divmod(e, n)
+                j = j0 + line
+                buf[line * LS + k] = src[b][j * n + k] if j < n else 0.0
+            run_stages_block(buf, n, LS, TP, tw)
+            for e in range(TP * nh):
+                k, line = divmod(e, TP)
+                if j0 + line < n:
+                    H[b, k, j0 + line] = np.conj(buf[line * LS + k])
+        for bx in range(-(-nh // TP)):
+            k0 = bx * TP
+            buf = np.full(TP * LS, np.nan + 0j)
+            for e in range(TP * n):
+                line, j = divmod(e, n)
+                k = k0 + line
+                buf[line * LS + j] = np.conj(H[b, k, j]) if k < nh else 0j
+            run_stages_block(buf, n, LS, TP, tw)
+            for e in range(TP * n):
+                j, line = divmod(e, TP)
+                if k0 + line < nh:
+                    half[b, j, k0 + line] = np.conj(buf[line * LS + j])
+    return half
+
+
+@pytest.mark.parametrize("n", [4, 6, 12, 18, 20, 24, 28])
+def test_r2c_kernels_as_written_match_rfft2(n):
+    """The half spectrum imcom_ft_r2c keeps (FFTW's r2c: the first axis
+    halved), as numpy's rfft along the first axis and fft along the second."""
+    rng = np.random.default_rng(n)
+    images = rng.standard_normal((2, n, n))  # images[b][x][y], x the first axis
+    got = r2c_kernels(images)
+    for b in range(2):
+        ref = np.fft.fft(np.fft.rfft(images[b], axis=0), axis=1)  # (nh, n): [k][j]
+        assert not np.isnan(got[b]).any()
+        assert np.max(np.abs(got[b].T - ref)) <= 1e-12 * np.max(np.abs(ref))
+
+
+# -- Lagrange weights of the PSF rotation ------------------------------------------
+
+
+def lagrange_weights(t, x0, m):
+    """lagrange_weights (tables.cu) as written: prefix/suffix products over
+    16 slots and the integer denominators (-1)^(m-1-k) k! (m-1-k)!."""
+    sv = [t - (x0 + j) if j < m else 1.0 for j in range(16)]
+    node = any(j < m and sv[j] == 0.0 for j in range(16))
+    pre, acc = [], 1.0
+    for j in range(16):
+        pre.append(acc)
+        acc *= sv[j]
+    w, acc = [0.0] * 16, 1.0
+    for k in range(15, -1, -1):
+        den = float(np.prod(np.arange(2, k + 1), dtype=float)) * float(
+            np.prod(np.arange(2, m - k), dtype=float))
+        if (m - 1 - k) % 2:
+            den = -den
+        w[k] = pre[k] * acc / den if k < m else 0.0
+        acc *= sv[k]
+    if node:
+        w = [1.0 if (k < m and sv[k] == 0.0) else 0.0 for k in range(16)]
+    return np.array(w)
+
+
+@pytest.mark.parametrize("m", [1, 2, 5, 7, 8, 9, 16])
+def test_lagrange_weights_reproduce_polynomials(m):
+    """Weights on m consecutive integer nodes reproduce every polynomial of
+    degree < m (so they interpolate as Neville's tableau does), also at a node."""
+    rng = np.random.default_rng(m)
+    x0 = 17
+    nodes = x0 + np.arange(m)
+    coef = rng.standard_normal(m)
+    vals = np.polyval(coef, nodes - x0 - 0.5 * (m - 1))
+    for t in [x0 + 0.37 * (m - 1), x0 + m - 1.0, x0 + 0.5, float(x0)]:
+        w = lagrange_weights(t, x0, m)
+        ref = np.polyval(coef, t - x0 - 0.5 * (m - 1))
+        assert abs(w[:m] @ vals - ref) <= 1e-9 * max(1.0, np.abs(vals).max())
+        assert np.all(w[m:] == 0.0)
