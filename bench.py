@@ -47,6 +47,7 @@ independent patch (seed = rank); value = all ranks' pixels / max rank time.
 from __future__ import annotations
 
 import argparse
+import faulthandler
 import json
 import os
 import statistics
@@ -665,6 +666,8 @@ def run_ours(args):
 
 
 def main():
+    # a crash in native code prints the Python stack of every thread to stderr
+    faulthandler.enable(all_threads=True)
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)

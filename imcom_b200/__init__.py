@@ -9,7 +9,8 @@ driver (``batch``, ``replicas``), the learned-kappa model (``kappa_model``)
 measurements that print one JSON line (``t_reuse``, ``table_fft``) and the
 stage-by-stage timer (``stages``).
 """
-from .api import (EIGH_DC, EIGH_JACOBI, EIGH_LIBRARY, EPS, ImcomError, SolveResult,  # noqa: F401
-                  Solver)
+from .api import (EIGH_DC, EIGH_JACOBI, EIGH_LIBRARY, EIGH_TWOSTAGE, EPS,  # noqa: F401
+                  ImcomError, SolveResult, Solver)
 
-__all__ = ["Solver", "SolveResult", "ImcomError", "EIGH_DC", "EIGH_JACOBI", "EIGH_LIBRARY", "EPS"]
+__all__ = ["Solver", "SolveResult", "ImcomError", "EIGH_DC", "EIGH_JACOBI", "EIGH_LIBRARY",
+           "EIGH_TWOSTAGE", "EPS"]

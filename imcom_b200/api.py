@@ -19,7 +19,7 @@ import numpy as np
 from . import _lib
 from ._lib import ImcomError
 
-EIGH_DC, EIGH_JACOBI, EIGH_LIBRARY = 0, 1, 2
+EIGH_DC, EIGH_JACOBI, EIGH_LIBRARY, EIGH_TWOSTAGE = 0, 1, 2, 3
 OPT_EIGENSOLVER, OPT_EIGEN_MAXITER = 1, 2
 OPT_DC_MAXITER, OPT_STALL_TEST = 15, 16
 STALL_SPLIT, STALL_TRIDIAG = 1, 2

@@ -346,7 +346,8 @@ int imcom_gpu_set_option(imcom_ctx* ctx, int option, long long value) {
   if (!ctx) return -1;
   switch (option) {
     case IMCOM_OPT_EIGENSOLVER:
-      if (value != IMCOM_EIGH_DC && value != IMCOM_EIGH_JACOBI && value != IMCOM_EIGH_LIBRARY)
+      if (value != IMCOM_EIGH_DC && value != IMCOM_EIGH_JACOBI && value != IMCOM_EIGH_LIBRARY &&
+          value != IMCOM_EIGH_TWOSTAGE)
         return -3;
       ctx->eig_mode = (int)value;
       return 0;

@@ -2,12 +2,15 @@
 //
 // The reference calls LAPACK DSYEVR('V', 'A', 'U') and reverses the result
 // into descending eigenvalue order (:656-662), then reports
-// condition = max(L) / min(L) (:664-671).  Three solvers sit behind one entry
+// condition = max(L) / min(L) (:664-671).  Four solvers sit behind one entry
 // point (imcom_gpu_set_option(IMCOM_OPT_EIGENSOLVER)):
 //   IMCOM_EIGH_DC       own FP64 blocked Householder tridiagonalisation +
 //                       divide and conquer + back-transformation (eigen_dc.cu)
 //   IMCOM_EIGH_JACOBI   own FP64 one-sided Jacobi for small systems, n <= 112
 //                       (eigen_jacobi.cu)
+//   IMCOM_EIGH_TWOSTAGE the same divide and conquer and back-transformation
+//                       after a two-stage reduction, dense -> band -> tridiagonal
+//                       (eigen_2s.cu)
 //   IMCOM_EIGH_LIBRARY  cuSOLVER syevd, kept only as a comparison baseline.
 // All of them return ascending eigenpairs in a work matrix; reverse_kernel
 // writes them to Q and L in the reference's descending order.

@@ -29,6 +29,14 @@ int eig_buf(imcom_ctx* ctx, size_t bytes);
 int copy_mat(imcom_ctx* ctx, const double* A, long long lda, double* B, long long ldb, int rows,
              int cols);
 
+// Two-stage tridiagonalisation (eigen_2s.cu): scratch bytes for order n,
+// the reduction of Aw to (d, e) with the stage-1 reflectors in Vall/tau and
+// the stage-2 ones in scratch, and the stage-2 back-transformation Z <- Q2 Z.
+size_t twostage_bytes(int n);
+int twostage_tridiag(imcom_ctx* ctx, DMat& Aw, DMat& Vall, double* d, double* e, double* tau,
+                     double* W, long long ldw, double* XY, void* scratch, long long spin);
+int twostage_backtransform2(imcom_ctx* ctx, int n, void* scratch, double* Z, long long ldz);
+
 // Keep-if-large-enough vector allocation.
 template <class T>
 inline int ensure_vec_keep(imcom_ctx* ctx, T** p, size_t& cap, size_t count) {

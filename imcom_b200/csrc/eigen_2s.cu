@@ -53,6 +53,11 @@ struct PanelArgs {
 //   beta = -sign(alpha) sqrt(alpha^2 + S_j), tau = (beta - alpha) / beta,
 //   v = [1; P(j+1:, j) / (alpha - beta)],  w_c = tau (R_c + S_c / (alpha - beta)),
 // and the later columns are updated, P(:, c) -= v w_c.
+// STAGED: the CTA's rows are copied into shared memory first (panels of up to
+// a few hundred rows per CTA); otherwise the columns are updated in place in
+// global memory (stride lda), which only the reduction buffers need shared
+// memory for.
+template <bool STAGED>
 __global__ void __launch_bounds__(SB_THREADS, 1) sb_panel_kernel(PanelArgs a) {
   namespace cg = cooperative_groups;
   cg::cluster_group cl = cg::this_cluster();
@@ -62,22 +67,25 @@ __global__ void __launch_bounds__(SB_THREADS, 1) sb_panel_kernel(PanelArgs a) {
   const int rb = q * per, nr = max(0, min(per, N - rb));
   const int jmax = min(SB, N);
   extern __shared__ __align__(16) double psm[];
-  double* P = psm;                                   // [SB][per]
-  double* part = P + (size_t)SB * per;               // [2][SB_CTAS][2 SB] from every CTA
-  double* red = part + 2 * SB_CTAS * 2 * SB;         // [SB_SLICES][2 SB]
-  double* fin = red + SB_SLICES * 2 * SB;            // [2 SB] cluster totals
-  const int c = threadIdx.x & (SB - 1), slice = threadIdx.x / SB;
   const size_t row0 = (size_t)a.k + SB + rb;
-  for (int e = threadIdx.x; e < SB * nr; e += SB_THREADS) {
-    const int cc = e / nr, i = e - cc * nr;
-    P[(size_t)cc * per + i] = a.A[row0 + i + (size_t)(a.k + cc) * a.lda];
-  }
+  // P(i, c) = P[c * ldp + i]: the CTA's rows of the panel
+  const long long ldp = STAGED ? per : a.lda;
+  double* P = STAGED ? psm : a.A + row0 + (size_t)a.k * a.lda;
+  double* part = psm + (STAGED ? (size_t)SB * per : 0);  // [2][SB_CTAS][2 SB] from every CTA
+  double* red = part + 2 * SB_CTAS * 2 * SB;              // [SB_SLICES][2 SB]
+  double* fin = red + SB_SLICES * 2 * SB;                 // [2 SB] cluster totals
+  const int c = threadIdx.x & (SB - 1), slice = threadIdx.x / SB;
+  if (STAGED)
+    for (int e = threadIdx.x; e < SB * nr; e += SB_THREADS) {
+      const int cc = e / nr, i = e - cc * nr;
+      P[(size_t)cc * per + i] = a.A[row0 + i + (size_t)(a.k + cc) * a.lda];
+    }
   cl.sync();  // every CTA runs before any stores into its shared memory
   for (int j = 0; j < jmax; ++j) {
     double sdot = 0.0, rowv = 0.0;
     if (c >= j) {
-      const double* pj = P + (size_t)j * per;
-      const double* pc = P + (size_t)c * per;
+      const double* pj = P + (size_t)j * ldp;
+      const double* pc = P + (size_t)c * ldp;
       for (int i = slice; i < nr; i += SB_SLICES) {
         const int gi = rb + i;
         if (gi > j) sdot = fma(pj[i], pc[i], sdot);
@@ -109,8 +117,8 @@ __global__ void __launch_bounds__(SB_THREADS, 1) sb_panel_kernel(PanelArgs a) {
     }
     if (c > j) {
       const double w = t * (fin[SB + c] + scl * fin[c]);
-      const double* pj = P + (size_t)j * per;
-      double* pc = P + (size_t)c * per;
+      const double* pj = P + (size_t)j * ldp;
+      double* pc = P + (size_t)c * ldp;
       for (int i = slice; i < nr; i += SB_SLICES) {
         const int gi = rb + i;
         if (gi > j) pc[i] -= (pj[i] * scl) * w;
@@ -120,7 +128,7 @@ __global__ void __launch_bounds__(SB_THREADS, 1) sb_panel_kernel(PanelArgs a) {
     __syncthreads();
     if (c == j) {
       // column j: v below the pivot (kept in P until the write-back), beta on it
-      double* pj = P + (size_t)j * per;
+      double* pj = P + (size_t)j * ldp;
       for (int i = slice; i < nr; i += SB_SLICES) {
         const int gi = rb + i;
         if (gi > j) pj[i] *= scl;
@@ -135,15 +143,16 @@ __global__ void __launch_bounds__(SB_THREADS, 1) sb_panel_kernel(PanelArgs a) {
   for (int e = threadIdx.x; e < SB * nr; e += SB_THREADS) {
     const int cc = e / nr, i = e - cc * nr;
     const int gi = rb + i;
-    const double p = P[(size_t)cc * per + i];
+    const double p = P[(size_t)cc * ldp + i];
     const size_t col = (size_t)(a.k + cc);
     a.A[row0 + i + col * a.lda] = gi <= cc ? p : 0.0;
     a.V[row0 + i + col * a.ldv] = gi < cc ? 0.0 : (gi == cc ? 1.0 : p);
   }
 }
 
-inline size_t panel_smem(int per) {
-  return ((size_t)SB * per + 2 * SB_CTAS * 2 * SB + SB_SLICES * 2 * SB + 2 * SB) * sizeof(double);
+inline size_t panel_smem(int per, bool staged) {
+  return ((staged ? (size_t)SB * per : 0) + 2 * SB_CTAS * 2 * SB + SB_SLICES * 2 * SB + 2 * SB) *
+         sizeof(double);
 }
 
 // T (upper triangular, ld SB) of the panel's block reflector from its Gram
@@ -177,6 +186,375 @@ __global__ void band_extract_kernel(const double* __restrict__ A, long long lda,
     AB[d + (size_t)c * ldb] = (d <= SB && c + d < n) ? A[(c + d) + (size_t)c * lda] : 0.0;
 }
 
+
+// ---- Stage 2: band -> tridiagonal by bulge chasing ------------------------
+// The band (bandwidth SB, lower) is reduced column by column (LAPACK
+// dsb2st's scheme): sweep s annihilates A(s+2 :, s) with a reflector on rows
+// s+1 .. s+SB (task 0), whose right application fills a triangle below the
+// band; task t > 0 of the sweep annihilates the first column of that bulge
+// (column r0 - SB, rows r0 = s + 1 + t SB ..) and applies its reflector from
+// the left to the bulge's other columns, two-sidedly to the diagonal block
+// and from the right to the rows below, pushing the bulge SB rows further.
+// Task (s, t) touches columns s + 1 + (t-1) SB .. s + (t+2) SB only, so task
+// t of sweep s + 1 may run beside task t + 3 of sweep s: a warp per sweep,
+// CH_K consecutive sweeps per CTA ("group") in lock step, each warp CH_LAG
+// tasks behind the one before it.  The group's live columns sit in a
+// circular shared-memory window (band and bulge, 2 SB rows per column);
+// columns it has finished are written back to AB and published by a
+// watermark, which the next group waits for before it loads them.
+constexpr int CH_K = 4;                 // sweeps per group, one warp each
+constexpr int CH_THREADS = 32 * CH_K;
+constexpr int CH_LAG = 3;               // tasks between consecutive sweeps
+constexpr int CH_LDB = 2 * SB;          // rows of band storage: band and bulge
+constexpr int CH_WCOLS = 12 * SB;       // columns of the window (a group spans < 11 SB)
+constexpr size_t CH_SMEM = (size_t)CH_WCOLS * CH_LDB * sizeof(double);
+
+struct ChaseArgs {
+  double* AB;       // AB[d + c * CH_LDB] = A(c + d, c)
+  int n, ngroups;
+  double* V;        // V[(t n + s) SB + i]: reflector of task t of sweep s, V[0] = 1
+  double* tau;      // tau[t n + s]
+  int* wm;          // wm[g]: AB holds group g's final values of columns < wm[g]
+  int* next_group;  // groups are taken in order
+  int* err;         // a wait ran out
+  long long spin;   // polls per wait
+};
+
+__host__ __device__ __forceinline__ int chase_ntasks(int n, int s) {
+  return (n - s - 3) >= 0 ? (n - s - 3) / SB + 1 : 0;
+}
+
+// A(r, c), r >= c, in the window
+__device__ __forceinline__ double& wb_at(double* W, int r, int c) {
+  return W[(size_t)(c % CH_WCOLS) * CH_LDB + (r - c)];
+}
+
+// One task, by one warp (lane i: row r0 + i of the reflector).
+__device__ void chase_task(const ChaseArgs& a, double* W, int s, int t, int lane, double* sv,
+                           double* sw) {
+  const int n = a.n;
+  const int r0 = s + 1 + t * SB;
+  const int c0 = t == 0 ? s : r0 - SB;
+  const int L = min(SB, n - r0);
+  // reflector from A(r0 : r0 + L, c0) (dlarfg)
+  const double x = lane < L ? wb_at(W, r0 + lane, c0) : 0.0;
+  double sig2 = lane >= 1 ? x * x : 0.0;
+#pragma unroll
+  for (int o = 16; o; o >>= 1) sig2 += __shfl_xor_sync(0xffffffffu, sig2, o);
+  const double alpha = __shfl_sync(0xffffffffu, x, 0);
+  double beta = alpha, tau = 0.0, scl = 0.0;
+  if (sig2 != 0.0) {
+    beta = -copysign(sqrt(alpha * alpha + sig2), alpha);
+    tau = (beta - alpha) / beta;
+    scl = 1.0 / (alpha - beta);
+  }
+  const double v = lane == 0 ? 1.0 : (lane < L ? x * scl : 0.0);
+  sv[lane] = v;
+  if (lane < L) wb_at(W, r0 + lane, c0) = lane == 0 ? beta : 0.0;
+  a.V[((size_t)t * n + s) * SB + lane] = v;
+  if (lane == 0) a.tau[(size_t)t * n + s] = tau;
+  __syncwarp();
+  if (tau == 0.0) return;
+  // left: the bulge's other columns c0 + 1 .. r0 - 1, rows r0 .. r0 + L - 1
+  if (t > 0 && lane < SB - 1) {
+    const int c = c0 + 1 + lane;
+    double w = 0.0;
+    for (int i = 0; i < L; ++i) w = fma(sv[i], wb_at(W, r0 + i, c), w);
+    w *= tau;
+    for (int i = 0; i < L; ++i) wb_at(W, r0 + i, c) -= sv[i] * w;
+  }
+  // two-sided on the diagonal block D: D - v w^T - w v^T,
+  // p = tau D v, w = p - tau/2 (p^T v) v (dlarfy)
+  double y = 0.0;
+  if (lane < L)
+    for (int j = 0; j < L; ++j) {
+      const double dij = j <= lane ? wb_at(W, r0 + lane, r0 + j) : wb_at(W, r0 + j, r0 + lane);
+      y = fma(dij, sv[j], y);
+    }
+  const double p = tau * y;
+  double pv = p * v;
+#pragma unroll
+  for (int o = 16; o; o >>= 1) pv += __shfl_xor_sync(0xffffffffu, pv, o);
+  const double wv = p - 0.5 * tau * pv * v;
+  sw[lane] = wv;
+  __syncwarp();
+  if (lane < L)
+    for (int j = 0; j <= lane; ++j) wb_at(W, r0 + lane, r0 + j) -= v * sw[j] + wv * sv[j];
+  // right: rows r0 + L .. r0 + L + L2 - 1 (the new bulge), columns r0 .. r0 + L - 1
+  const int L2 = min(SB, n - (r0 + L));
+  if (lane < L2) {
+    const int r = r0 + L + lane;
+    double z = 0.0;
+    for (int j = 0; j < L; ++j) z = fma(wb_at(W, r, r0 + j), sv[j], z);
+    z *= tau;
+    for (int j = 0; j < L; ++j) wb_at(W, r, r0 + j) -= z * sv[j];
+  }
+  __syncwarp();
+}
+
+// Columns [lo, hi) group g's tasks at step tau touch; lo also covers the
+// group's sweeps that have not started (they begin at their own column).
+__device__ __forceinline__ void chase_span(const ChaseArgs& a, int g, int step, int& lo,
+                                           int& hi) {
+  lo = 0x7fffffff;
+  hi = 0;
+  for (int k = 0; k < CH_K; ++k) {
+    const int s = g * CH_K + k;
+    if (s > a.n - 3) break;
+    const int t = step - CH_LAG * k;
+    if (t < 0) {
+      lo = min(lo, s);
+      continue;
+    }
+    if (t >= chase_ntasks(a.n, s)) continue;
+    const int r0 = s + 1 + t * SB;
+    lo = min(lo, t == 0 ? s : r0 - SB);
+    hi = max(hi, min(a.n, r0 + SB));
+  }
+}
+
+// Waits (bounded) until group g has published columns below need.
+__device__ bool wait_wm(const ChaseArgs& a, int g, int need) {
+  if (g < 0) return true;
+  for (long long it = 0;; ++it) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(a.wm + g) : "memory");
+    if (v >= need) return true;
+    if (*(volatile int*)a.err) return false;
+    if (it >= a.spin) {
+      atomicExch(a.err, 1);
+      return false;
+    }
+    __nanosleep(100);
+  }
+}
+
+__device__ __forceinline__ void publish_wm(const ChaseArgs& a, int g, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(a.wm + g), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ void window_store(const ChaseArgs& a, const double* W, int c_lo,
+                                             int c_hi) {
+  for (int e = threadIdx.x; e < (c_hi - c_lo) * CH_LDB; e += CH_THREADS) {
+    const int c = c_lo + e / CH_LDB, d = e % CH_LDB;
+    a.AB[(size_t)c * CH_LDB + d] = W[(size_t)(c % CH_WCOLS) * CH_LDB + d];
+  }
+}
+
+// Persistent: every CTA takes groups in order until none is left.  Launched
+// cooperatively, so all CTAs are resident and the group a CTA waits for is
+// always held by a running CTA.
+__global__ void __launch_bounds__(CH_THREADS, 1) chase_kernel(ChaseArgs a) {
+  extern __shared__ __align__(16) double W[];
+  __shared__ double sv[CH_K][SB], sw[CH_K][SB];
+  __shared__ int s_g, s_ok;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  while (true) {
+    if (threadIdx.x == 0) s_g = atomicAdd(a.next_group, 1);
+    __syncthreads();
+    const int g = s_g;
+    if (g >= a.ngroups) return;
+    const int s0 = g * CH_K;
+    int loaded = s0, lo_prev = s0, steps = 0;
+    for (int k = 0; k < CH_K && s0 + k <= a.n - 3; ++k)
+      steps = max(steps, CH_LAG * k + chase_ntasks(a.n, s0 + k));
+    for (int step = 0; step < steps; ++step) {
+      int lo, hi;
+      chase_span(a, g, step, lo, hi);
+      if (hi > loaded) {
+        if (threadIdx.x == 0) s_ok = wait_wm(a, g - 1, hi);
+        __syncthreads();
+        if (!s_ok) return;
+        for (int e = threadIdx.x; e < (hi - loaded) * CH_LDB; e += CH_THREADS) {
+          const int c = loaded + e / CH_LDB, d = e % CH_LDB;
+          W[(size_t)(c % CH_WCOLS) * CH_LDB + d] = __ldcg(a.AB + (size_t)c * CH_LDB + d);
+        }
+        loaded = hi;
+        __syncthreads();
+      }
+      {
+        const int s = s0 + warp, t = step - CH_LAG * warp;
+        if (s <= a.n - 3 && t >= 0 && t < chase_ntasks(a.n, s))
+          chase_task(a, W, s, t, lane, sv[warp], sw[warp]);
+      }
+      __syncthreads();
+      int lo_next, hi_next;
+      chase_span(a, g, step + 1, lo_next, hi_next);
+      lo_next = min(lo_next, loaded);
+      if (lo_next > lo_prev) {
+        window_store(a, W, lo_prev, lo_next);
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) publish_wm(a, g, lo_next);
+        lo_prev = lo_next;
+      }
+    }
+    window_store(a, W, lo_prev, loaded);
+    __threadfence();
+    __syncthreads();
+    // columns this group never loaded are final once the previous group's are
+    if (threadIdx.x == 0) {
+      s_ok = wait_wm(a, g - 1, a.n);
+      if (s_ok) publish_wm(a, g, a.n);
+    }
+    __syncthreads();
+    if (!s_ok) return;
+  }
+}
+
+__global__ void band_tridiag_kernel(const double* __restrict__ AB, int n, double* __restrict__ d,
+                                    double* __restrict__ e) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  d[c] = AB[(size_t)c * CH_LDB];
+  e[c] = c + 1 < n ? AB[(size_t)c * CH_LDB + 1] : 0.0;
+}
+
+// ---- Q2 back-transformation ----------------------------------------------
+// Z <- Q2 Z with Q2 the product of all tasks' reflectors in the order they
+// were applied.  Block B(g, t) holds task t of the BT_G consecutive sweeps
+// g BT_G .. g BT_G + BT_G - 1: sweep j of the block reflects rows
+// R0 + j .. R0 + j + SB - 1 (R0 = g BT_G + 1 + t SB), so V of the block is a
+// parallelogram of BT_H rows, and H_j ... H_{j+G-1} = I - V T V^T (forward
+// dlarft).  Reflectors of different t within a block range never overlap
+// and later sweeps act below earlier ones, so the blocks apply in the order
+// g descending, t ascending.  Every CTA owns a strip of BT_CW columns of Z
+// and applies all blocks to it; no CTA waits for another.
+constexpr int BT_G = SB;
+constexpr int BT_H = SB + BT_G - 1;
+constexpr int BT_CW = 32;
+constexpr int BT_THREADS = 256;
+constexpr int BT_ROWS = 64;  // BT_H rounded up: 8 rows per thread in the update
+constexpr size_t BT_SMEM =
+    ((size_t)BT_G * SB + (size_t)BT_G * (BT_G + 1) + (size_t)BT_ROWS * (BT_CW + 1) +
+     2 * (size_t)BT_G * (BT_CW + 1)) * sizeof(double);
+
+__host__ __device__ __forceinline__ int bt_ntasks(int n, int g) { return chase_ntasks(n, g * BT_G); }
+
+// T of block (t, g) = (blockIdx.x, blockIdx.y), column-major BT_G x BT_G.
+__global__ void bt_tfactor_kernel(const double* __restrict__ V, const double* __restrict__ tau,
+                                  int n, int tmax, double* __restrict__ T) {
+  const int t = blockIdx.x, g = blockIdx.y, lane = threadIdx.x;
+  if (t >= bt_ntasks(n, g)) return;
+  __shared__ double sv[BT_G][SB + 1];
+  __shared__ double sT[BT_G][BT_G + 1];
+  __shared__ double stau[BT_G], sg[BT_G];
+  for (int j = 0; j < BT_G; ++j) {
+    const int s = g * BT_G + j;
+    const bool ok = s <= n - 3 && t < chase_ntasks(n, s);
+    sv[j][lane] = ok ? V[((size_t)t * n + s) * SB + lane] : 0.0;
+    if (lane == 0) stau[j] = ok ? tau[(size_t)t * n + s] : 0.0;
+  }
+  __syncwarp();
+  for (int j = 0; j < BT_G; ++j) {
+    // G(h, j) = v_h^T v_j over the rows both reach (h < j): rows j .. h + SB - 1
+    double gv = 0.0;
+    if (lane < j)
+      for (int r = j; r < lane + SB; ++r) gv = fma(sv[lane][r - lane], sv[j][r - j], gv);
+    sg[lane] = gv;
+    __syncwarp();
+    double x = 0.0;
+    if (lane < j)
+      for (int h = lane; h < j; ++h) x = fma(sT[lane][h], sg[h], x);
+    sT[lane][j] = lane < j ? -stau[j] * x : (lane == j ? stau[j] : 0.0);
+    __syncwarp();
+  }
+  double* Tb = T + ((size_t)g * tmax + t) * BT_G * BT_G;
+  for (int c = 0; c < BT_G; ++c) Tb[(size_t)c * BT_G + lane] = sT[lane][c];
+}
+
+__global__ void __launch_bounds__(BT_THREADS) bt_apply_kernel(
+    const double* __restrict__ V, const double* __restrict__ T, int n, int ngroups, int tmax,
+    double* __restrict__ Z, long long ldz) {
+  extern __shared__ __align__(16) double bsm[];
+  double* sv = bsm;                               // [BT_G][SB]
+  double* sT = sv + BT_G * SB;                    // [BT_G][BT_G + 1], sT[i][h] = T(i, h)
+  double* sZ = sT + BT_G * (BT_G + 1);            // [BT_ROWS][BT_CW + 1]
+  double* sY = sZ + BT_ROWS * (BT_CW + 1);        // [BT_G][BT_CW + 1]
+  double* sY2 = sY + BT_G * (BT_CW + 1);          // [BT_G][BT_CW + 1]
+  const int c0 = blockIdx.x * BT_CW;
+  const int tid = threadIdx.x, col = tid & (BT_CW - 1), grp = tid / BT_CW;  // 8 groups
+  for (int g = ngroups - 1; g >= 0; --g) {
+    const int nt = bt_ntasks(n, g);
+    for (int t = 0; t < nt; ++t) {
+      const int R0 = g * BT_G + 1 + t * SB;
+      for (int e = tid; e < BT_G * SB; e += BT_THREADS) {
+        const int j = e / SB, i = e % SB, s = g * BT_G + j;
+        const bool ok = s <= n - 3 && t < chase_ntasks(n, s);
+        sv[e] = ok ? V[((size_t)t * n + s) * SB + i] : 0.0;
+      }
+      const double* Tb = T + ((size_t)g * tmax + t) * BT_G * BT_G;
+      for (int e = tid; e < BT_G * BT_G; e += BT_THREADS) {
+        const int h = e / BT_G, i = e % BT_G;
+        sT[i * (BT_G + 1) + h] = Tb[e];
+      }
+      for (int e = tid; e < BT_ROWS * BT_CW; e += BT_THREADS) {
+        const int r = e % BT_ROWS, c = e / BT_ROWS;
+        const int gr = R0 + r, gc = c0 + c;
+        sZ[r * (BT_CW + 1) + c] =
+            (r < BT_H && gr < n && gc < n) ? Z[(size_t)gc * ldz + gr] : 0.0;
+      }
+      __syncthreads();
+      // Y = V^T Z: rows j = 4 grp .. 4 grp + 3 of column col
+      {
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        const int j0 = 4 * grp;
+        for (int rr = 0; rr < SB + 3; ++rr) {
+          const int r = j0 + rr;
+          const double z = sZ[r * (BT_CW + 1) + col];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int i = rr - q;
+            if (i >= 0 && i < SB) acc[q] = fma(sv[(j0 + q) * SB + i], z, acc[q]);
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) sY[(j0 + q) * (BT_CW + 1) + col] = acc[q];
+      }
+      __syncthreads();
+      // Y2 = T Y (T upper triangular)
+      {
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        const int i0 = 4 * grp;
+        for (int h = i0; h < BT_G; ++h) {
+          const double y = sY[h * (BT_CW + 1) + col];
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (h >= i0 + q) acc[q] = fma(sT[(i0 + q) * (BT_G + 1) + h], y, acc[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) sY2[(i0 + q) * (BT_CW + 1) + col] = acc[q];
+      }
+      __syncthreads();
+      // Z -= V Y2: rows 8 grp .. 8 grp + 7
+      {
+        const int q0 = 8 * grp;
+        double acc[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) acc[q] = sZ[(q0 + q) * (BT_CW + 1) + col];
+        const int jlo = max(0, q0 - SB + 1), jhi = min(BT_G - 1, q0 + 7);
+        for (int j = jlo; j <= jhi; ++j) {
+          const double y = sY2[j * (BT_CW + 1) + col];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const int i = q0 + q - j;
+            if (i >= 0 && i < SB) acc[q] = fma(-sv[j * SB + i], y, acc[q]);
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) sZ[(q0 + q) * (BT_CW + 1) + col] = acc[q];
+      }
+      __syncthreads();
+      for (int e = tid; e < BT_ROWS * BT_CW; e += BT_THREADS) {
+        const int r = e % BT_ROWS, c = e / BT_ROWS;
+        const int gr = R0 + r, gc = c0 + c;
+        if (r < BT_H && gr < n && gc < n) Z[(size_t)gc * ldz + gr] = sZ[r * (BT_CW + 1) + c];
+      }
+      __syncthreads();
+    }
+  }
+}
+
 }  // namespace
 
 // X = [V(:, k:k+b) | W(:, 0:b)], Y = [W | V] (eigen_dc.cu)
@@ -185,36 +563,48 @@ __global__ void pack_update_kernel(const double* __restrict__ V, long long ldv,
                                    int b, double* __restrict__ X, double* __restrict__ Y,
                                    long long ldx);
 
+// Sets the panel kernel's attributes (non-portable cluster size; the device's
+// shared-memory ceiling, since the attribute is process-wide) and tells
+// whether a cluster of cs CTAs with smem bytes each can be placed.
+template <bool STAGED>
+static bool panel_cluster_fits(imcom_ctx* ctx, int cs, size_t smem, int optin) {
+  if (cudaFuncSetAttribute(sb_panel_kernel<STAGED>,
+                           cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess ||
+      cudaFuncSetAttribute(sb_panel_kernel<STAGED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           optin - 1024) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = cs;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(cs);
+  cfg.blockDim = dim3(SB_THREADS);
+  cfg.dynamicSmemBytes = smem;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  int nc = 0;
+  const bool ok = cudaOccupancyMaxActiveClusters(&nc, (void*)sb_panel_kernel<STAGED>, &cfg) ==
+                      cudaSuccess && nc >= 1;
+  cudaGetLastError();
+  (void)ctx;
+  return ok;
+}
+
 // Cluster size for the panel kernel: 16 CTAs where the device can place them
-// (non-portable size), else 8.
-static int panel_cluster(imcom_ctx* ctx, int per, int* ctas) {
-  const size_t smem = panel_smem(per);
-  IMC_CUDA(cudaFuncSetAttribute(sb_panel_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-  int optin = 0;
-  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
-  // the device's ceiling, not this panel's need: the attribute is process-wide
-  IMC_CUDA(cudaFuncSetAttribute(sb_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                optin - 1024));
+// (a non-portable size), else 8.  Placement is checked at the largest shared
+// memory either variant asks for.
+static int panel_cluster(imcom_ctx* ctx, int optin, int* ctas) {
   for (int cs : {16, 8}) {
-    cudaLaunchConfig_t cfg = {};
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = cs;
-    at[0].val.clusterDim.y = 1;
-    at[0].val.clusterDim.z = 1;
-    cfg.gridDim = dim3(cs);
-    cfg.blockDim = dim3(SB_THREADS);
-    cfg.dynamicSmemBytes = smem;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    int nc = 0;
-    if (cudaOccupancyMaxActiveClusters(&nc, (void*)sb_panel_kernel, &cfg) == cudaSuccess &&
-        nc >= 1) {
+    if (panel_cluster_fits<true>(ctx, cs, optin - 1024, optin) &&
+        panel_cluster_fits<false>(ctx, cs, panel_smem(0, false), optin)) {
       *ctas = cs;
       return 0;
     }
   }
-  cudaGetLastError();
   return set_err(ctx, IMCOM_ERR_CUDA, "the band reduction's panel cluster cannot be placed");
 }
 
@@ -228,26 +618,18 @@ int sy2sb_gpu(imcom_ctx* ctx, DMat& Aw, DMat& V, double* tau, double* Tf, double
   const int n = (int)Aw.rows;
   const long long ld = Aw.ld;
   IMC_CUDA(cudaMemsetAsync(V.p, 0, V.bytes(), ctx->stream));
-  // cluster shape for the largest panel (rows per CTA fixed by it)
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
   int ctas = 16;
-  const int Nmax = std::max(0, n - SB);
-  int per = std::max(1, (Nmax + 15) / 16);
-  {
-    int optin = 0;
-    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
-    if (panel_smem(per) > (size_t)optin - 1024)
-      return set_err(ctx, IMCOM_ERR_CUDA, "band reduction: panel of %d rows does not fit", Nmax);
-  }
-  IMC_TRY(panel_cluster(ctx, per, &ctas));
-  if (ctas != 16) per = std::max(1, (Nmax + ctas - 1) / ctas);
-  if (ctas != 16 && panel_smem(per) > 227 * 1024 - 1024)
-    return set_err(ctx, IMCOM_ERR_CUDA, "band reduction: panel of %d rows does not fit", Nmax);
+  IMC_TRY(panel_cluster(ctx, optin, &ctas));
   double* G = Tf + (size_t)((n + SB - 1) / SB) * SB * SB;  // SB x SB Gram scratch
   double* M = G + SB * SB;                                   // SB x SB
   double* M2 = M + SB * SB;
   for (int k = 0; k + SB < n - 1; k += SB) {
     const int N = n - k - SB;
     const int pc = std::max(1, (N + ctas - 1) / ctas);
+    // panels whose slices fit are staged in shared memory, taller ones run in place
+    const bool staged = panel_smem(pc, true) <= (size_t)optin - 1024;
     PanelArgs pa{Aw.p, ld, V.p, V.ld, tau, n, k, pc};
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute at[1];
@@ -257,11 +639,14 @@ int sy2sb_gpu(imcom_ctx* ctx, DMat& Aw, DMat& V, double* tau, double* Tf, double
     at[0].val.clusterDim.z = 1;
     cfg.gridDim = dim3(ctas);
     cfg.blockDim = dim3(SB_THREADS);
-    cfg.dynamicSmemBytes = panel_smem(pc);
+    cfg.dynamicSmemBytes = panel_smem(pc, staged);
     cfg.stream = ctx->stream;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    IMC_CUDA(cudaLaunchKernelEx(&cfg, sb_panel_kernel, pa));
+    if (staged)
+      IMC_CUDA(cudaLaunchKernelEx(&cfg, sb_panel_kernel<true>, pa));
+    else
+      IMC_CUDA(cudaLaunchKernelEx(&cfg, sb_panel_kernel<false>, pa));
     IMC_LAUNCH();
     const size_t r0 = (size_t)k + SB;
     const double* Vp = V.p + r0 + (size_t)k * V.ld;  // N x SB
@@ -289,6 +674,110 @@ int sy2sb_gpu(imcom_ctx* ctx, DMat& Aw, DMat& V, double* tau, double* Tf, double
     IMC_TRY(dgemm(ctx, 'N', 'T', N, N, 2 * SB, -1.0, X, ldw, Y, ldw, 1.0, A22, ld));
   }
   band_extract_kernel<<<n, 128, 0, ctx->stream>>>(Aw.p, ld, n, AB, ldb);
+  IMC_LAUNCH();
+  return 0;
+}
+
+
+// ---- two-stage driver -----------------------------------------------------
+
+namespace {
+
+struct TwoStage {
+  double* AB;    // band + bulge storage, CH_LDB x n
+  double* V2;    // stage-2 reflectors, tmax x n x SB
+  double* tau2;  // tmax x n
+  double* T2;    // T factors of the Q2 blocks, ng_bt x tmax x BT_G^2
+  int* sync;     // [0] group counter, [1] error, [16 ..] watermarks
+  double* Tf;    // stage-1 T factors and scratch
+  int tmax, ng_chase, ng_bt;
+};
+
+inline size_t r256(size_t b) { return (b + 255) / 256 * 256; }
+
+inline void twostage_dims(int n, int& tmax, int& ng_chase, int& ng_bt) {
+  tmax = std::max(1, chase_ntasks(n, 0));
+  ng_chase = std::max(1, (n - 2 + CH_K - 1) / CH_K);
+  ng_bt = std::max(1, (n - 2 + BT_G - 1) / BT_G);
+}
+
+TwoStage carve(int n, void* scratch) {
+  TwoStage ts;
+  twostage_dims(n, ts.tmax, ts.ng_chase, ts.ng_bt);
+  char* p = (char*)scratch;
+  auto take = [&](size_t bytes) {
+    char* r = p;
+    p += r256(bytes);
+    return r;
+  };
+  ts.AB = (double*)take((size_t)CH_LDB * n * 8);
+  ts.V2 = (double*)take((size_t)ts.tmax * n * SB * 8);
+  ts.tau2 = (double*)take((size_t)ts.tmax * n * 8);
+  ts.T2 = (double*)take((size_t)ts.ng_bt * ts.tmax * BT_G * BT_G * 8);
+  ts.sync = (int*)take((size_t)ts.ng_chase * 4 + 64);
+  ts.Tf = (double*)take(((size_t)(n / SB + 1) * SB * SB + 3 * SB * SB) * 8);
+  return ts;
+}
+
+}  // namespace
+
+size_t twostage_bytes(int n) {
+  int tmax, ngc, ngb;
+  twostage_dims(n, tmax, ngc, ngb);
+  return r256((size_t)CH_LDB * n * 8) + r256((size_t)tmax * n * SB * 8) +
+         r256((size_t)tmax * n * 8) + r256((size_t)ngb * tmax * BT_G * BT_G * 8) +
+         r256((size_t)ngc * 4 + 64) + r256(((size_t)(n / SB + 1) * SB * SB + 3 * SB * SB) * 8);
+}
+
+// Tridiagonal (d, e) of the full symmetric Aw through the band: the stage-1
+// reflectors go to Vall (column c, unit at row c + SB) and tau, so the
+// one-stage back-transformation applies Q1 unchanged; the stage-2
+// reflectors stay in scratch for twostage_backtransform2.
+int twostage_tridiag(imcom_ctx* ctx, DMat& Aw, DMat& Vall, double* d, double* e, double* tau,
+                     double* W, long long ldw, double* XY, void* scratch, long long spin) {
+  const int n = (int)Aw.rows;
+  TwoStage ts = carve(n, scratch);
+  IMC_CUDA(cudaMemsetAsync(tau, 0, (size_t)n * 8, ctx->stream));
+  IMC_TRY(sy2sb_gpu(ctx, Aw, Vall, tau, ts.Tf, W, ldw, XY, ts.AB, CH_LDB));
+  IMC_CUDA(cudaMemsetAsync(ts.sync, 0, (size_t)ts.ng_chase * 4 + 64, ctx->stream));
+  if (n >= 3) {
+    IMC_CUDA(cudaMemsetAsync(ts.V2, 0, (size_t)ts.tmax * n * SB * 8, ctx->stream));
+    IMC_CUDA(cudaMemsetAsync(ts.tau2, 0, (size_t)ts.tmax * n * 8, ctx->stream));
+    IMC_CUDA(cudaFuncSetAttribute(chase_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)CH_SMEM));
+    int per_sm = 0;
+    IMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chase_kernel, CH_THREADS,
+                                                           CH_SMEM));
+    if (per_sm < 1)
+      return set_err(ctx, IMCOM_ERR_CUDA, "bulge chasing: the kernel cannot be placed");
+    const int grid = std::min(sm_count(ctx) * per_sm, ts.ng_chase);
+    ChaseArgs ca{ts.AB, n, ts.ng_chase, ts.V2, ts.tau2, ts.sync + 16, ts.sync, ts.sync + 1,
+                 std::min<long long>(spin, 4000000LL)};
+    void* args[] = {&ca};
+    IMC_CUDA(cudaLaunchCooperativeKernel((void*)chase_kernel, dim3(grid), dim3(CH_THREADS), args,
+                                         CH_SMEM, ctx->stream));
+    IMC_LAUNCH();
+  }
+  band_tridiag_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(ts.AB, n, d, e);
+  IMC_LAUNCH();
+  int h = 0;
+  IMC_CUDA(cudaMemcpyAsync(&h, ts.sync + 1, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  IMC_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (h) return set_err(ctx, IMCOM_ERR_EIGEN, "bulge chasing: a wait between sweep groups timed out");
+  return 0;
+}
+
+// Z <- Q2 Z (n x n, ld ldz) with the reflectors twostage_tridiag left in scratch.
+int twostage_backtransform2(imcom_ctx* ctx, int n, void* scratch, double* Z, long long ldz) {
+  if (n < 3) return 0;
+  TwoStage ts = carve(n, scratch);
+  bt_tfactor_kernel<<<dim3(ts.tmax, ts.ng_bt), 32, 0, ctx->stream>>>(ts.V2, ts.tau2, n, ts.tmax,
+                                                                     ts.T2);
+  IMC_LAUNCH();
+  IMC_CUDA(cudaFuncSetAttribute(bt_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)BT_SMEM));
+  bt_apply_kernel<<<(n + BT_CW - 1) / BT_CW, BT_THREADS, BT_SMEM, ctx->stream>>>(
+      ts.V2, ts.T2, n, ts.ng_bt, ts.tmax, Z, ldz);
   IMC_LAUNCH();
   return 0;
 }

@@ -1557,6 +1557,8 @@ int eigen_dc(imcom_ctx* ctx, const DMat& A, DMat& Wout, double* wout) {
   size_t o_T = take(npair_bt * 4 * NBB * NBB * 8), o_G = take(npair_bt * 4 * NBB * NBB * 8);
   size_t o_X = take((size_t)2 * NBB * ld * 8 * 2);
   size_t o_err = take(64);
+  const bool two = ctx->eig_mode == IMCOM_EIGH_TWOSTAGE;
+  size_t o_2s = take(two ? twostage_bytes(n) : 0);
   IMC_TRY(eig_buf(ctx, off + 256));
   char* base = (char*)ew->buf;
   double* d = (double*)(base + o_d);
@@ -1578,8 +1580,12 @@ int eigen_dc(imcom_ctx* ctx, const DMat& A, DMat& Wout, double* wout) {
   IMC_TRY(copy_mat(ctx, A.p, A.ld, Aw.p, Aw.ld, n, n));
   IMC_CUDA(cudaMemsetAsync(Vall.p, 0, Vall.bytes(), ctx->stream));
   IMC_CUDA(cudaMemsetAsync(Wp, 0, (size_t)ldw * NB * 8, ctx->stream));
-  IMC_TRY(sytrd_gpu(ctx, Aw, Vall, d, e, tau, Wp, ldw, yp, yp + (size_t)ldy * nch, ldy,
-                    base + o_acc, spin, (double*)(base + o_XY)));
+  if (two)
+    IMC_TRY(twostage_tridiag(ctx, Aw, Vall, d, e, tau, Wp, ldw, (double*)(base + o_XY),
+                             base + o_2s, spin));
+  else
+    IMC_TRY(sytrd_gpu(ctx, Aw, Vall, d, e, tau, Wp, ldw, yp, yp + (size_t)ldy * nch, ldy,
+                      base + o_acc, spin, (double*)(base + o_XY)));
   stage_end(ctx, ST_EIG_TRD);
   stage_begin(ctx, ST_EIG_DC);
 
@@ -1717,6 +1723,9 @@ int eigen_dc(imcom_ctx* ctx, const DMat& A, DMat& Wout, double* wout) {
   stage_end(ctx, ST_EIG_DC);
   // ---- 3. back-transformation Z <- Q_T Z (Q_T = H_0 H_1 ... H_{n-2}) ----
   stage_begin(ctx, ST_EIG_BT);
+  // two-stage: Z <- Q2 Z first; Q1 (reflectors in Vall, unit at row c + SB
+  // of column c) then applies like the one-stage Q
+  if (two) IMC_TRY(twostage_backtransform2(ctx, n, base + o_2s, Zcur, ld));
   const int nref = n - 1;
   const int nblk = (nref + NBB - 1) / NBB;
   const int NB2 = 2 * NBB, npair = (nblk + 1) / 2;

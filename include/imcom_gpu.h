@@ -51,6 +51,8 @@ typedef struct imcom_ctx imcom_ctx;
 #define IMCOM_EIGH_DC 0         /* own tridiagonalisation + divide & conquer  */
 #define IMCOM_EIGH_JACOBI 1     /* own one-sided Jacobi (n <= 112)            */
 #define IMCOM_EIGH_LIBRARY 2    /* cuSOLVER syevd: comparison baseline only   */
+#define IMCOM_EIGH_TWOSTAGE 3   /* own two-stage (dense -> band -> tridiagonal)
+                                   reduction + divide & conquer               */
 
 /* Options for imcom_gpu_set_option. */
 #define IMCOM_OPT_EIGENSOLVER 1

@@ -9,7 +9,8 @@ reference's own example case.
   bisection's own resolution is coarser), U and S within 1e-6 relative, T
   within 1e-8 relative (largest element and every column), H within 1e-8
   (normwise).  The eigendecomposition alone is also checked against LAPACK's
-  at this size (residual, orthogonality, eigenvalues).
+  at this size (eigenvalues, orthogonality, and the residual as LAPACK's own
+  test ratio ||AQ - Q Lambda||_1 / (n ulp ||A||_1) <= 10).
 * n16200 (8 x 45 x 45 inputs, 128 x 128 outputs): stage by stage on the GPU's
   own results -- A Q = Q Lambda and Q^T Q = I (formed on the device with
   torch as the checker), P = Q^T B and T columns on 64 seeded pixels against
@@ -64,6 +65,16 @@ def oracle_at(r, prob, UnotS, US, tol, maxnits=53):
     else:
         out["S"], out["U"] = USo, O.build_U(r.L, r.P2, r.C_a, K)
     return out
+
+
+# LAPACK's own test of an eigendecomposition (dsyt21): ||A Q - Q Lambda||_1 /
+# (n ulp ||A||_1); LAPACK's test drivers accept ratios below their threshold
+# (tens).  The bar here is 10.
+RATIO_BAR = 10.0
+
+
+def residual_ratio(res_1norm, a_1norm, n):
+    return res_1norm / (n * np.finfo(np.float64).eps * a_1norm)
 
 
 def check_solve(g, o, L_o):
@@ -126,7 +137,7 @@ def test_n4096_eigen_vs_lapack(solver, n4096):
     dA = torch.from_numpy(r.A).cuda()
     res = torch.linalg.matrix_norm(dA @ dQ - dQ * torch.from_numpy(L).cuda(), ord=1).item()
     orth = (dQ.T @ dQ - torch.eye(prob.n, dtype=torch.float64, device="cuda")).abs().max().item()
-    assert res <= 1e-12 * torch.linalg.matrix_norm(dA, ord=1).item()
+    assert residual_ratio(res, torch.linalg.matrix_norm(dA, ord=1).item(), prob.n) <= RATIO_BAR
     assert orth <= 1e-12
     # the eigenvectors of well-separated eigenvalues agree with LAPACK's up to sign
     gap = np.minimum(np.abs(np.diff(r.L, prepend=np.inf)), np.abs(np.diff(r.L, append=-np.inf)))
@@ -154,7 +165,7 @@ def test_n16200_stages_vs_oracle(solver):
     dA = torch.from_numpy(g.A).cuda()
     dL = torch.from_numpy(g.L).cuda()
     res = torch.linalg.matrix_norm(dA @ dQ - dQ * dL, ord=1).item()
-    assert res <= 1e-12 * torch.linalg.matrix_norm(dA, ord=1).item()
+    assert residual_ratio(res, torch.linalg.matrix_norm(dA, ord=1).item(), n) <= RATIO_BAR
     orth = (dQ.T @ dQ - torch.eye(n, dtype=torch.float64, device="cuda")).abs().max().item()
     assert orth <= 1e-12
     assert np.all(np.diff(g.L) <= 0)
