@@ -201,12 +201,18 @@ __global__ void band_extract_kernel(const double* __restrict__ A, long long lda,
 // tasks behind the one before it.  The group's live columns sit in a
 // circular shared-memory window (band and bulge, 2 SB rows per column);
 // columns it has finished are written back to AB and published by a
-// watermark, which the next group waits for before it loads them.
+// watermark, which the next group waits for before it loads them.  Two
+// more warps move the columns while the four task warps compute: in step
+// tau one writes back and publishes the columns the previous step finished,
+// the other fetches the columns step tau + 1 adds, so the global round trips
+// stay off the tasks' path; one barrier per step.
 constexpr int CH_K = 4;                 // sweeps per group, one warp each
-constexpr int CH_THREADS = 32 * CH_K;
+constexpr int CH_THREADS = 32 * (CH_K + 2);  // + a storing and a loading warp
 constexpr int CH_LAG = 3;               // tasks between consecutive sweeps
 constexpr int CH_LDB = 2 * SB;          // rows of band storage: band and bulge
-constexpr int CH_WCOLS = 12 * SB;       // columns of the window (a group spans < 11 SB)
+// columns of the window: a group's tasks span < 11 SB columns; the columns
+// being written back (one step behind) and fetched (one step ahead) add 2 SB
+constexpr int CH_WCOLS = 13 * SB;
 constexpr size_t CH_SMEM = (size_t)CH_WCOLS * CH_LDB * sizeof(double);
 
 struct ChaseArgs {
@@ -325,7 +331,6 @@ __device__ bool wait_wm(const ChaseArgs& a, int g, int need) {
       atomicExch(a.err, 1);
       return false;
     }
-    __nanosleep(100);
   }
 }
 
@@ -333,69 +338,102 @@ __device__ __forceinline__ void publish_wm(const ChaseArgs& a, int g, int v) {
   asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(a.wm + g), "r"(v) : "memory");
 }
 
-__device__ __forceinline__ void window_store(const ChaseArgs& a, const double* W, int c_lo,
-                                             int c_hi) {
-  for (int e = threadIdx.x; e < (c_hi - c_lo) * CH_LDB; e += CH_THREADS) {
+// Columns [c_lo, c_hi) of the window back to AB, by one warp.
+__device__ __forceinline__ void window_store_warp(const ChaseArgs& a, const double* W, int c_lo,
+                                                  int c_hi, int lane) {
+  for (int e = lane; e < (c_hi - c_lo) * CH_LDB; e += 32) {
     const int c = c_lo + e / CH_LDB, d = e % CH_LDB;
     a.AB[(size_t)c * CH_LDB + d] = W[(size_t)(c % CH_WCOLS) * CH_LDB + d];
   }
 }
 
+// Columns [c_lo, c_hi) of AB into the window, by one warp.
+__device__ __forceinline__ void window_load_warp(const ChaseArgs& a, double* W, int c_lo,
+                                                 int c_hi, int lane) {
+  for (int e = lane; e < (c_hi - c_lo) * CH_LDB; e += 32) {
+    const int c = c_lo + e / CH_LDB, d = e % CH_LDB;
+    W[(size_t)(c % CH_WCOLS) * CH_LDB + d] = __ldcg(a.AB + (size_t)c * CH_LDB + d);
+  }
+}
+
 // Persistent: every CTA takes groups in order until none is left.  Launched
 // cooperatively, so all CTAs are resident and the group a CTA waits for is
-// always held by a running CTA.
+// always held by a running CTA.  Warps 0 .. CH_K-1 run the sweeps' tasks,
+// warp CH_K writes back and publishes, warp CH_K + 1 fetches.
 __global__ void __launch_bounds__(CH_THREADS, 1) chase_kernel(ChaseArgs a) {
   extern __shared__ __align__(16) double W[];
   __shared__ double sv[CH_K][SB], sw[CH_K][SB];
   __shared__ int s_g, s_ok;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int STORER = CH_K, LOADER = CH_K + 1;
   while (true) {
-    if (threadIdx.x == 0) s_g = atomicAdd(a.next_group, 1);
+    if (threadIdx.x == 0) {
+      s_g = atomicAdd(a.next_group, 1);
+      s_ok = 1;
+    }
     __syncthreads();
     const int g = s_g;
     if (g >= a.ngroups) return;
     const int s0 = g * CH_K;
-    int loaded = s0, lo_prev = s0, steps = 0;
+    int steps = 0;
     for (int k = 0; k < CH_K && s0 + k <= a.n - 3; ++k)
       steps = max(steps, CH_LAG * k + chase_ntasks(a.n, s0 + k));
-    for (int step = 0; step < steps; ++step) {
+    int loaded = s0, lo_prev = s0;
+    {
       int lo, hi;
-      chase_span(a, g, step, lo, hi);
-      if (hi > loaded) {
-        if (threadIdx.x == 0) s_ok = wait_wm(a, g - 1, hi);
-        __syncthreads();
-        if (!s_ok) return;
-        for (int e = threadIdx.x; e < (hi - loaded) * CH_LDB; e += CH_THREADS) {
-          const int c = loaded + e / CH_LDB, d = e % CH_LDB;
-          W[(size_t)(c % CH_WCOLS) * CH_LDB + d] = __ldcg(a.AB + (size_t)c * CH_LDB + d);
-        }
-        loaded = hi;
-        __syncthreads();
+      chase_span(a, g, 0, lo, hi);
+      if (warp == LOADER && hi > loaded) {
+        bool ok = true;
+        if (lane == 0) ok = wait_wm(a, g - 1, hi);
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (ok) window_load_warp(a, W, loaded, hi, lane);
+        else if (lane == 0) s_ok = 0;
       }
-      {
+      loaded = max(loaded, hi);
+    }
+    __syncthreads();
+    if (!s_ok) return;
+    for (int step = 0; step < steps; ++step) {
+      int lo, hi, lo1, hi1;
+      chase_span(a, g, step, lo, hi);
+      chase_span(a, g, step + 1, lo1, hi1);
+      const int lo_next = min(lo, loaded);
+      if (warp < CH_K) {
         const int s = s0 + warp, t = step - CH_LAG * warp;
         if (s <= a.n - 3 && t >= 0 && t < chase_ntasks(a.n, s))
           chase_task(a, W, s, t, lane, sv[warp], sw[warp]);
+      } else if (warp == STORER) {
+        // columns the previous step finished: no task of this step touches them
+        if (lo_next > lo_prev) {
+          window_store_warp(a, W, lo_prev, lo_next, lane);
+          __threadfence();
+          __syncwarp();
+          if (lane == 0) publish_wm(a, g, lo_next);
+        }
+      } else if (hi1 > loaded) {
+        // the columns the next step adds: beyond every column in use, and
+        // their slots held columns already written back
+        bool ok = true;
+        if (lane == 0) ok = wait_wm(a, g - 1, hi1);
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (ok) window_load_warp(a, W, loaded, hi1, lane);
+        else if (lane == 0) s_ok = 0;
       }
+      if (lo_next > lo_prev) lo_prev = lo_next;
+      loaded = max(loaded, hi1);
       __syncthreads();
-      int lo_next, hi_next;
-      chase_span(a, g, step + 1, lo_next, hi_next);
-      lo_next = min(lo_next, loaded);
-      if (lo_next > lo_prev) {
-        window_store(a, W, lo_prev, lo_next);
-        __threadfence();
-        __syncthreads();
-        if (threadIdx.x == 0) publish_wm(a, g, lo_next);
-        lo_prev = lo_next;
-      }
+      if (!s_ok) return;
     }
-    window_store(a, W, lo_prev, loaded);
-    __threadfence();
-    __syncthreads();
-    // columns this group never loaded are final once the previous group's are
-    if (threadIdx.x == 0) {
-      s_ok = wait_wm(a, g - 1, a.n);
-      if (s_ok) publish_wm(a, g, a.n);
+    // the rest of the window; columns this group never loaded are final once
+    // the previous group's are
+    if (warp == STORER) {
+      window_store_warp(a, W, lo_prev, loaded, lane);
+      __threadfence();
+      __syncwarp();
+      if (lane == 0) {
+        if (wait_wm(a, g - 1, a.n)) publish_wm(a, g, a.n);
+        else s_ok = 0;
+      }
     }
     __syncthreads();
     if (!s_ok) return;
@@ -415,20 +453,14 @@ __global__ void band_tridiag_kernel(const double* __restrict__ AB, int n, double
 // were applied.  Block B(g, t) holds task t of the BT_G consecutive sweeps
 // g BT_G .. g BT_G + BT_G - 1: sweep j of the block reflects rows
 // R0 + j .. R0 + j + SB - 1 (R0 = g BT_G + 1 + t SB), so V of the block is a
-// parallelogram of BT_H rows, and H_j ... H_{j+G-1} = I - V T V^T (forward
+// parallelogram of SB + BT_G - 1 rows, and H_j ... H_{j+G-1} = I - V T V^T (forward
 // dlarft).  Reflectors of different t within a block range never overlap
 // and later sweeps act below earlier ones, so the blocks apply in the order
 // g descending, t ascending.  Every CTA owns a strip of BT_CW columns of Z
 // and applies all blocks to it; no CTA waits for another.
 constexpr int BT_G = SB;
-constexpr int BT_H = SB + BT_G - 1;
 constexpr int BT_CW = 32;
 constexpr int BT_THREADS = 256;
-constexpr int BT_ROWS = 64;  // BT_H rounded up: 8 rows per thread in the update
-constexpr size_t BT_SMEM =
-    ((size_t)BT_G * SB + (size_t)BT_G * (BT_G + 1) + (size_t)BT_ROWS * (BT_CW + 1) +
-     2 * (size_t)BT_G * (BT_CW + 1)) * sizeof(double);
-
 __host__ __device__ __forceinline__ int bt_ntasks(int n, int g) { return chase_ntasks(n, g * BT_G); }
 
 // T of block (t, g) = (blockIdx.x, blockIdx.y), column-major BT_G x BT_G.
@@ -463,95 +495,220 @@ __global__ void bt_tfactor_kernel(const double* __restrict__ V, const double* __
   for (int c = 0; c < BT_G; ++c) Tb[(size_t)c * BT_G + lane] = sT[lane][c];
 }
 
-__global__ void __launch_bounds__(BT_THREADS) bt_apply_kernel(
+__device__ __forceinline__ void dmma(double (&d)[4], double a0, double a1, double b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+      "{%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a0), "d"(a1), "d"(b));
+}
+
+// Row strides of the shared tiles (doubles), chosen so that the DMMA operand
+// loads of a half-warp (4 x 4 lanes) hit 16 distinct 8-byte banks.
+constexpr int BT_SVS = 37;  // sv[j][i]: V(j) element i; (S - 1) = 4 mod 16
+constexpr int BT_TS = 36;   // sT[i][h] = T(i, h)
+constexpr int BT_YS = 36;   // sY[j][c]
+constexpr int BT_ZS = 36;   // sZ[slot][row][c]
+constexpr size_t BT_SMEM =
+    ((size_t)BT_G * BT_SVS + (size_t)BT_G * BT_TS + 2 * (size_t)BT_G * BT_YS +
+     2 * 32 * (size_t)BT_ZS) * sizeof(double);
+
+// One CTA (8 warps) per strip of BT_CW = 32 columns of Z.  For block (g, tb)
+// the 64 rows R0 .. R0 + 63 of the strip sit in shared memory as two 32-row
+// segments (segment k of the sweep group: rows g G + 1 + 32 k ..); block tb
+// uses segments tb and tb + 1, so after it segment tb is final and is
+// written back and segment tb + 2 takes its slot.  The next block's V, T and
+// new segment are loaded into registers while this block computes.  The three
+// products are FP64 DMMA tiles (m16n8k4):
+//   Y = V^T Z (32 x 32, K over the parallelogram's 47 rows per 16-row tile),
+//   -Y2 = -T Y (T upper triangular), Z += V (-Y2) (64 x 32).
+__global__ void __launch_bounds__(BT_THREADS, 2) bt_apply_kernel(
     const double* __restrict__ V, const double* __restrict__ T, int n, int ngroups, int tmax,
     double* __restrict__ Z, long long ldz) {
   extern __shared__ __align__(16) double bsm[];
-  double* sv = bsm;                               // [BT_G][SB]
-  double* sT = sv + BT_G * SB;                    // [BT_G][BT_G + 1], sT[i][h] = T(i, h)
-  double* sZ = sT + BT_G * (BT_G + 1);            // [BT_ROWS][BT_CW + 1]
-  double* sY = sZ + BT_ROWS * (BT_CW + 1);        // [BT_G][BT_CW + 1]
-  double* sY2 = sY + BT_G * (BT_CW + 1);          // [BT_G][BT_CW + 1]
+  double* sv = bsm;                        // [BT_G][BT_SVS]
+  double* sT = sv + BT_G * BT_SVS;         // [BT_G][BT_TS]
+  double* sY = sT + BT_G * BT_TS;          // [BT_G][BT_YS]
+  double* sY2 = sY + BT_G * BT_YS;         // [BT_G][BT_YS], holds -Y2
+  double* sZ = sY2 + BT_G * BT_YS;         // [2][32][BT_ZS]
   const int c0 = blockIdx.x * BT_CW;
-  const int tid = threadIdx.x, col = tid & (BT_CW - 1), grp = tid / BT_CW;  // 8 groups
-  for (int g = ngroups - 1; g >= 0; --g) {
-    const int nt = bt_ntasks(n, g);
-    for (int t = 0; t < nt; ++t) {
-      const int R0 = g * BT_G + 1 + t * SB;
-      for (int e = tid; e < BT_G * SB; e += BT_THREADS) {
-        const int j = e / SB, i = e % SB, s = g * BT_G + j;
-        const bool ok = s <= n - 3 && t < chase_ntasks(n, s);
-        sv[e] = ok ? V[((size_t)t * n + s) * SB + i] : 0.0;
-      }
-      const double* Tb = T + ((size_t)g * tmax + t) * BT_G * BT_G;
-      for (int e = tid; e < BT_G * BT_G; e += BT_THREADS) {
-        const int h = e / BT_G, i = e % BT_G;
-        sT[i * (BT_G + 1) + h] = Tb[e];
-      }
-      for (int e = tid; e < BT_ROWS * BT_CW; e += BT_THREADS) {
-        const int r = e % BT_ROWS, c = e / BT_ROWS;
-        const int gr = R0 + r, gc = c0 + c;
-        sZ[r * (BT_CW + 1) + c] =
-            (r < BT_H && gr < n && gc < n) ? Z[(size_t)gc * ldz + gr] : 0.0;
-      }
-      __syncthreads();
-      // Y = V^T Z: rows j = 4 grp .. 4 grp + 3 of column col
-      {
-        double acc[4] = {0.0, 0.0, 0.0, 0.0};
-        const int j0 = 4 * grp;
-        for (int rr = 0; rr < SB + 3; ++rr) {
-          const int r = j0 + rr;
-          const double z = sZ[r * (BT_CW + 1) + col];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int gq = lane >> 2, tq = lane & 3;
+  // element e = tid + 256 q (q < 4) of a 32 x 32 tile: (row e % 32, column e / 32)
+  auto vload = [&](int g, int tb, double (&r)[4]) {
 #pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const int i = rr - q;
-            if (i >= 0 && i < SB) acc[q] = fma(sv[(j0 + q) * SB + i], z, acc[q]);
-          }
-        }
-#pragma unroll
-        for (int q = 0; q < 4; ++q) sY[(j0 + q) * (BT_CW + 1) + col] = acc[q];
-      }
-      __syncthreads();
-      // Y2 = T Y (T upper triangular)
-      {
-        double acc[4] = {0.0, 0.0, 0.0, 0.0};
-        const int i0 = 4 * grp;
-        for (int h = i0; h < BT_G; ++h) {
-          const double y = sY[h * (BT_CW + 1) + col];
-#pragma unroll
-          for (int q = 0; q < 4; ++q)
-            if (h >= i0 + q) acc[q] = fma(sT[(i0 + q) * (BT_G + 1) + h], y, acc[q]);
-        }
-#pragma unroll
-        for (int q = 0; q < 4; ++q) sY2[(i0 + q) * (BT_CW + 1) + col] = acc[q];
-      }
-      __syncthreads();
-      // Z -= V Y2: rows 8 grp .. 8 grp + 7
-      {
-        const int q0 = 8 * grp;
-        double acc[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) acc[q] = sZ[(q0 + q) * (BT_CW + 1) + col];
-        const int jlo = max(0, q0 - SB + 1), jhi = min(BT_G - 1, q0 + 7);
-        for (int j = jlo; j <= jhi; ++j) {
-          const double y = sY2[j * (BT_CW + 1) + col];
-#pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            const int i = q0 + q - j;
-            if (i >= 0 && i < SB) acc[q] = fma(-sv[j * SB + i], y, acc[q]);
-          }
-        }
-#pragma unroll
-        for (int q = 0; q < 8; ++q) sZ[(q0 + q) * (BT_CW + 1) + col] = acc[q];
-      }
-      __syncthreads();
-      for (int e = tid; e < BT_ROWS * BT_CW; e += BT_THREADS) {
-        const int r = e % BT_ROWS, c = e / BT_ROWS;
-        const int gr = R0 + r, gc = c0 + c;
-        if (r < BT_H && gr < n && gc < n) Z[(size_t)gc * ldz + gr] = sZ[r * (BT_CW + 1) + c];
-      }
-      __syncthreads();
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + BT_THREADS * q, jj = e >> 5, i = e & 31, sw = g * BT_G + jj;
+      r[q] = (sw <= n - 3 && tb < chase_ntasks(n, sw)) ? V[((size_t)tb * n + sw) * SB + i] : 0.0;
     }
+  };
+  auto tload = [&](int g, int tb, double (&r)[4]) {
+    const double* Tb = T + ((size_t)g * tmax + tb) * BT_G * BT_G;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) r[q] = Tb[tid + BT_THREADS * q];
+  };
+  // rows row0 .. row0 + 31 of the strip (zero beyond n)
+  auto zload = [&](int row0, double (&r)[4]) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + BT_THREADS * q, rr = e & 31, c = e >> 5;
+      const int gr = row0 + rr, gc = c0 + c;
+      r[q] = (gr < n && gc < n) ? Z[(size_t)gc * ldz + gr] : 0.0;
+    }
+  };
+  auto zput = [&](int slot, const double (&r)[4]) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + BT_THREADS * q;
+      sZ[((size_t)slot * 32 + (e & 31)) * BT_ZS + (e >> 5)] = r[q];
+    }
+  };
+  auto zstore = [&](int slot, int row0) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + BT_THREADS * q, rr = e & 31, c = e >> 5;
+      const int gr = row0 + rr, gc = c0 + c;
+      if (gr < n && gc < n) Z[(size_t)gc * ldz + gr] = sZ[((size_t)slot * 32 + rr) * BT_ZS + c];
+    }
+  };
+  auto vput = [&](const double (&r)[4]) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + BT_THREADS * q;
+      sv[(e >> 5) * BT_SVS + (e & 31)] = r[q];
+    }
+  };
+  auto tput = [&](const double (&r)[4]) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + BT_THREADS * q;  // T(i, h) at column-major e = h 32 + i
+      sT[(e & 31) * BT_TS + (e >> 5)] = r[q];
+    }
+  };
+  // the first block
+  int g = ngroups - 1, tb = 0;
+  {
+    double rv[4], rt[4], z0[4], z1[4];
+    vload(g, tb, rv);
+    tload(g, tb, rt);
+    zload(g * BT_G + 1, z0);
+    zload(g * BT_G + 1 + 32, z1);
+    vput(rv);
+    tput(rt);
+    zput(0, z0);
+    zput(1, z1);
+  }
+  __syncthreads();
+  while (g >= 0) {
+    const int nt = bt_ntasks(n, g);
+    const int R0 = g * BT_G + 1 + tb * SB;
+    const bool last = tb + 1 >= nt;
+    const int ng = last ? g - 1 : g, ntb = last ? 0 : tb + 1;  // the next block
+    // prefetch: the next block's V and T, and the segment it adds (for the
+    // next sweep group its first segment, which this group never touches;
+    // its second is this group's first and is read after the write-back)
+    double pv[4], pt[4], pz[4];
+    if (ng >= 0) {
+      vload(ng, ntb, pv);
+      tload(ng, ntb, pt);
+      zload(last ? ng * BT_G + 1 : R0 + 64, pz);
+    }
+    const int slot0 = tb & 1, slot1 = (tb + 1) & 1;
+    auto zrow = [&](int r) { return sZ + ((size_t)((r >> 5) ? slot1 : slot0) * 32 + (r & 31)) * BT_ZS; };
+    // Y = V^T Z: warp -> 16 x 8 tile (rows 16 mt of Y, columns 8 nt)
+    {
+      const int mt = warp & 1, nt8 = warp >> 1, m0 = 16 * mt, n0 = 8 * nt8;
+      double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int kb = 0; kb < 48; kb += 4) {
+        const int r = m0 + kb + tq;
+        const int i0 = r - (m0 + gq), i1 = i0 - 8;
+        const double a0 = (i0 >= 0 && i0 < SB) ? sv[(m0 + gq) * BT_SVS + i0] : 0.0;
+        const double a1 = (i1 >= 0 && i1 < SB) ? sv[(m0 + gq + 8) * BT_SVS + i1] : 0.0;
+        dmma(acc, a0, a1, zrow(r)[n0 + gq]);
+      }
+      double* y0 = sY + (m0 + gq) * BT_YS + n0 + 2 * tq;
+      y0[0] = acc[0];
+      y0[1] = acc[1];
+      y0[8 * BT_YS] = acc[2];
+      y0[8 * BT_YS + 1] = acc[3];
+    }
+    __syncthreads();
+    // -Y2 = -T Y
+    {
+      const int mt = warp & 1, nt8 = warp >> 1, m0 = 16 * mt, n0 = 8 * nt8;
+      double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int kb = 0; kb < 32; kb += 4) {
+        if (kb + 4 <= m0) continue;  // T(i, h) = 0 for h < i
+        dmma(acc, sT[(m0 + gq) * BT_TS + kb + tq], sT[(m0 + gq + 8) * BT_TS + kb + tq],
+             sY[(kb + tq) * BT_YS + n0 + gq]);
+      }
+      double* y0 = sY2 + (m0 + gq) * BT_YS + n0 + 2 * tq;
+      y0[0] = -acc[0];
+      y0[1] = -acc[1];
+      y0[8 * BT_YS] = -acc[2];
+      y0[8 * BT_YS + 1] = -acc[3];
+    }
+    __syncthreads();
+    // Z += V (-Y2): warp -> rows 16 mt, two 8-column tiles
+    {
+      const int mt = warp & 3, m0 = 16 * mt, n0 = 16 * (warp >> 2);
+      double acc[2][4];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const double* zr0 = zrow(m0 + gq);
+        const double* zr1 = zrow(m0 + gq + 8);
+        const int cc = n0 + 8 * h + 2 * tq;
+        acc[h][0] = zr0[cc];
+        acc[h][1] = zr0[cc + 1];
+        acc[h][2] = zr1[cc];
+        acc[h][3] = zr1[cc + 1];
+      }
+      const int jlo = m0 >= SB ? m0 - SB + 1 : 0, jhi = min(BT_G - 1, m0 + 15);
+#pragma unroll
+      for (int kb = 0; kb < 32; kb += 4) {
+        if (kb + 3 < jlo || kb > jhi) continue;
+        const int jj = kb + tq;
+        const int i0 = m0 + gq - jj, i1 = i0 + 8;
+        const double a0 = (i0 >= 0 && i0 < SB) ? sv[jj * BT_SVS + i0] : 0.0;
+        const double a1 = (i1 >= 0 && i1 < SB) ? sv[jj * BT_SVS + i1] : 0.0;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) dmma(acc[h], a0, a1, sY2[jj * BT_YS + n0 + 8 * h + gq]);
+      }
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        double* zr0 = zrow(m0 + gq);
+        double* zr1 = zrow(m0 + gq + 8);
+        const int cc = n0 + 8 * h + 2 * tq;
+        zr0[cc] = acc[h][0];
+        zr0[cc + 1] = acc[h][1];
+        zr1[cc] = acc[h][2];
+        zr1[cc + 1] = acc[h][3];
+      }
+    }
+    __syncthreads();
+    // segment tb is final; the next block's operands take the freed space
+    // (each thread writes back and refills the same elements: no barrier)
+    zstore(slot0, R0);
+    if (last) zstore(slot1, R0 + 32);
+    if (ng >= 0) {
+      vput(pv);
+      tput(pt);
+      if (last) {
+        // rows ng G + 33 .. ng G + 64 are this group's first segment, written
+        // back by this thread (at block 0, or just above when nt = 1)
+        double pz2[4];
+        zload(ng * BT_G + 1 + 32, pz2);
+        zput(0, pz);
+        zput(1, pz2);
+      } else {
+        zput(slot0, pz);
+      }
+    }
+    __syncthreads();
+    g = ng;
+    tb = ntb;
   }
 }
 

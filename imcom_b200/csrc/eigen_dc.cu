@@ -83,7 +83,6 @@ __device__ __forceinline__ void cp_async8(double* dst, const double* src, int by
                : "memory");
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_wait_2() { asm volatile("cp.async.wait_group 2;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_wait_0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 

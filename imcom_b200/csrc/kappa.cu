@@ -1,17 +1,18 @@
-// kappa.cu -- learned-kappa bracket for the per-pixel bisection.
+// kappa.cu -- learned kappa for the per-pixel bisection.
 //
 // The reference finds kappa per output pixel by log-space bisection
 // (imcom_bisect_by_U / _by_S, imcom_bisect.f90:174-267).  Here a small MLP
 // predicts log10(kappa) and a bracket half-width from 12 cheap per-pixel
-// features.  Because U(kappa) rises and S(kappa) falls monotonically in
-// kappa, f = U - U_max (or S - S_max) evaluated at the two bracket ends
-// gives one-sided bounds: an end with f < -max(tol, C eps) makes every
-// bisection midpoint on its accept side a known accept that cannot trigger an
-// exit test; an end with f >= C eps makes every midpoint on its reject side a
-// known reject.  The kernel replays the reference's bisection sequence and
-// evaluates U/S only at midpoints between the bounds, so K_a and U_a/S_a are
-// bit-identical to the plain bisection (same evaluator, same operations).
-// A bracket that yields neither bound costs two extra evaluations.
+// features; Newton steps in log10(kappa) from that start home in on the
+// band where the bisection stops, two certificate evaluations cover the
+// bisection's path there, and the reference's bisection sequence is then
+// replayed with every decision the evaluated points settle taken for free.
+// Because U(kappa) rises and S(kappa) falls monotonically in kappa, a point
+// with f = U - U_max (or S - S_max) below -max(tol, C eps) settles every
+// midpoint on its accept side and a point with f >= C eps every midpoint on
+// its reject side (learned_pixel gives the details).  Only undecided
+// midpoints are evaluated, with the plain bisection's evaluator, so K_a and
+// U_a/S_a are bit-identical to the plain bisection.
 //
 // Features (feature-major, 12 x m, float):
 //   0  inputs within a 2 x 2 px box around (X_a, Y_a)
@@ -367,10 +368,13 @@ struct LearnedExtra {
 // 4. Replay of the reference's bisection sequence (imcom_bisect.f90:174-267):
 //    known decisions cost nothing, the other midpoints are evaluated.  K_a,
 //    U_a/S_a and the reported value are bit-identical to the plain bisection.
+// The nw warps that share the evaluator run it in lock step (same values,
+// same branches); warp wid 0 writes the scalars.
 template <class Eval>
 __device__ __forceinline__ void learned_pixel(const BisectArgs& a, const LearnedExtra& ex,
                                               const double* lam, const double* col,
-                                              const Eval& ev, int pix, int lane) {
+                                              const Eval& ev, int pix, int lane, int wid = 0,
+                                              int nw = 1) {
   const bool U = a.UnotS != 0;
   const double rlo = a.lg_min, rhi = a.lg_max;  // the reference's search range
   double x0 = 0.5 * (rlo + rhi), hw = 0.5 * (rhi - rlo);
@@ -473,7 +477,7 @@ __device__ __forceinline__ void learned_pixel(const BisectArgs& a, const Learned
     }
     const bool have_acc = U ? (accb > rlo) : (accb < rhi);
     const bool have_rej = U ? (rejb < rhi) : (rejb > rlo);
-    if (lane == 0 && ex.fallback) ex.fallback[pix] = (have_acc || have_rej) ? 0 : 1;
+    if (lane == 0 && wid == 0 && ex.fallback) ex.fallback[pix] = (have_acc || have_rej) ? 0 : 1;
     // 4. replay.  The reference evaluates f0 at the start of the range first
     // and returns there if f0 >= 0; a known accept point inside the range
     // implies f0 < 0 by monotonicity, so f0 is then only needed if no later
@@ -530,35 +534,28 @@ __device__ __forceinline__ void learned_pixel(const BisectArgs& a, const Learned
       k_root = pow(10.0, root);
     }
   }
-  if (lane == 0 && ex.fallback && have_f0 && !(f0 < 0.0)) ex.fallback[pix] = 0;
-  write_pixel(a, lam, col, pix, lane, nev, k_root, us, mg);
+  if (lane == 0 && wid == 0 && ex.fallback && have_f0 && !(f0 < 0.0)) ex.fallback[pix] = 0;
+  write_pixel(a, lam, col, pix, lane, nev, k_root, us, mg, wid, nw);
 }
 
-// The learned-kappa bisection, one warp per pixel (CTAs of four warps, the
-// plain bisection kernel's shape: the features and the network ran before).
-__global__ void __launch_bounds__(128, 7) learned_bisect_kernel(BisectArgs a, PixelSmem plan,
-                                                                LearnedExtra ex) {
-  extern __shared__ __align__(16) double smem[];
+// The learned-kappa bisection: one CTA of four warps per pixel sharing each
+// U/S evaluation (CtaCol), one pixel per CTA, so the block scheduler hands
+// the next pixel to whichever CTA finishes first -- the evaluation counts
+// vary from pixel to pixel (network start, Newton steps), and with about
+// one resident warp per pixel a kernel of one-warp pixels lasts as long as
+// its slowest pixels.
+constexpr int LB_WARPS = 4;
+static_assert(LB_WARPS == 4, "CtaCol splits the four partial sums of the one-warp evaluator");
+
+__global__ void __launch_bounds__(LB_WARPS * 32, 7) learned_bisect_kernel(BisectArgs a,
+                                                                          LearnedExtra ex) {
+  __shared__ double red[2 * 2 * LB_WARPS * 32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const double* lam = a.L;
-  if (plan.lam_smem) {
-    for (int p = threadIdx.x; p < a.n; p += blockDim.x) smem[p] = a.L[p];
-    __syncthreads();
-    lam = smem;
-  }
-  double* mycol = plan.col_smem ? smem + (size_t)a.n * (1 + warp) : nullptr;
-  for (int pix = blockIdx.x * plan.warps + warp; pix < a.m; pix += gridDim.x * plan.warps) {
-    const double* gcol = a.P + (size_t)pix * a.ldp;
-    const double* col = gcol;
-    if (mycol) {
-      for (int p = lane; p < a.n; p += 32) mycol[p] = gcol[p];
-      __syncwarp();
-      col = mycol;
-    }
-    const StreamCol ev{lam, col, a.Nd, a.n, a.UnotS != 0, a.C};
-    learned_pixel(a, ex, lam, gcol, ev, pix, lane);
-    __syncwarp();
-  }
+  const int pix = blockIdx.x;
+  if (pix >= a.m) return;
+  const double* col = a.P + (size_t)pix * a.ldp;
+  const CtaCol ev{a.L, col, a.Nd, a.n, a.UnotS != 0, a.C, red, warp, 0};
+  learned_pixel(a, ex, a.L, col, ev, pix, lane, warp, LB_WARPS);
 }
 
 // ---------------------------------------------------------------------------
@@ -853,15 +850,8 @@ extern "C" int imcom_gpu_bisect_kappa_learned(imcom_ctx* ctx, int UnotS, double 
   ex.fallback = ctx->fb;
   if (ctx->p_split) IMC_TRY(split_margin_buffer(ctx, a));
   if (!ctx->kappa_nonet) IMC_TRY(kappa_guess(ctx, a, true));
-  {
-    PixelSmem plan = plan_pixel_smem(ctx->n);
-    IMC_CUDA(cudaFuncSetAttribute(learned_bisect_kernel,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)kPixelSmemMax));
-    learned_bisect_kernel<<<pixel_grid(ctx, plan, ctx->m), plan.warps * 32, plan.bytes,
-                            ctx->stream>>>(a, plan, ex);
-    IMC_LAUNCH();
-  }
+  learned_bisect_kernel<<<ctx->m, LB_WARPS * 32, 0, ctx->stream>>>(a, ex);
+  IMC_LAUNCH();
   if (ctx->p_split) IMC_TRY(split_audit(ctx, a));
   stage_end(ctx, ST_BISECT);
   ctx->have_K = true;

@@ -79,9 +79,12 @@ __device__ __forceinline__ void bisect_pixel(const BisectArgs& a, const Eval& ev
   *mg_out = mg;
 }
 
+// Outputs of one pixel, written by the nw warps that solved it together
+// (warp wid of them; one warp: wid 0, nw 1).
 __device__ __forceinline__ void write_pixel(const BisectArgs& a, const double* lam, const double* col, int pix,
-                            int lane, int nev, double k, double us, double mg) {
-  if (lane == 0) {
+                            int lane, int nev, double k, double us, double mg, int wid = 0,
+                            int nw = 1) {
+  if (lane == 0 && wid == 0) {
     a.K[pix] = k;
     a.US[pix] = us;
     if (a.nev) a.nev[pix] = nev;
@@ -89,7 +92,8 @@ __device__ __forceinline__ void write_pixel(const BisectArgs& a, const double* l
   }
   if (a.Pt) {
     double* dst = a.Pt + (size_t)pix * a.ldt;
-    for (int p = lane; p < a.n; p += 32) dst[p] = __ddiv_rn(col[p], __dadd_rn(lam[p], k));
+    for (int p = lane + 32 * wid; p < a.n; p += 32 * nw)
+      dst[p] = __ddiv_rn(col[p], __dadd_rn(lam[p], k));
   }
 }
 

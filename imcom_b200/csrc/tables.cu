@@ -127,6 +127,136 @@ __global__ void finish_sum_kernel(const double* __restrict__ partial, int np, do
   if (threadIdx.x == 0) *out = sh[0];
 }
 
+// Sum of |z_k|^2 = re^2 + im^2 over k = 0 .. count-1 with the rounding of the
+// sequential loop s = s + |z_k|^2 (Fortran's SUM without reassociation, as
+// in imcom_calc_C, imcom_matrix.f90:546-552), in parallel.  While s stays in
+// one binade [2^(E-1), 2^E), every step rounds to a multiple of the same ulp
+// u = 2^(E-53): s_k = s_(k-1) + rint(t_k / u) u, unless t_k / u is exactly
+// half-way (a tie, decided by the parity of s) or s leaves the binade.  The
+// terms are non-negative, so s only grows: a block of terms whose rounded
+// quotients sum to Q with s / u + Q < 2^53 and no tie advances s by Q u
+// exactly.  One CTA walks the terms in chunks of SQ_CHUNK; a chunk that
+// crosses a binade or holds a tie is split into 32-term sub-chunks and only
+// those sub-chunks are added term by term.  Result bit-identical to the
+// sequential loop (a binade's worth of terms is an exact integer sum).
+constexpr int SQ_THREADS = 1024, SQ_PER = 4, SQ_CHUNK = SQ_THREADS * SQ_PER, SQ_SUB = 32;
+constexpr int SQ_NSUB = SQ_CHUNK / SQ_SUB;
+
+__global__ void __launch_bounds__(SQ_THREADS, 1)
+    seq_abs2_sum_kernel(const double2* __restrict__ z, size_t count, double* __restrict__ out) {
+  __shared__ double st[SQ_CHUNK];     // the chunk's terms in order
+  __shared__ double sq[SQ_NSUB];      // rounded-quotient sums per sub-chunk
+  __shared__ int stie[SQ_NSUB];       // a tie in the sub-chunk
+  __shared__ double sS;               // the running sum
+  __shared__ int s_start, s_done;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const double two53 = 9007199254740992.0, tiny = 4.450147717014403e-308;  // 2^53, 2^-1021
+  if (tid == 0) sS = 0.0;
+  for (size_t base = 0; base < count; base += SQ_CHUNK) {
+    // term r * 1024 + tid of the chunk (coalesced); sub-chunk r * 32 + warp
+    double t[SQ_PER];
+#pragma unroll
+    for (int r = 0; r < SQ_PER; ++r) {
+      const size_t k = base + (size_t)r * SQ_THREADS + tid;
+      t[r] = 0.0;
+      if (k < count) {
+        const double2 v = z[k];
+        t[r] = __dadd_rn(__dmul_rn(v.x, v.x), __dmul_rn(v.y, v.y));
+      }
+      st[r * SQ_THREADS + tid] = t[r];
+    }
+    if (tid == 0) s_start = 0;
+    __syncthreads();
+    while (true) {
+      const double S = sS;
+      const int start = s_start;
+      const bool normal = S >= tiny;
+      int E = 0;
+      if (normal) frexp(S, &E);
+#pragma unroll
+      for (int r = 0; r < SQ_PER; ++r) {
+        const int sub = r * 32 + warp;
+        double q = 0.0;
+        int tie = 0;
+        if (sub >= start) {
+          if (normal) {
+            const double x = ldexp(t[r], 53 - E);
+            q = rint(x);
+            tie = (x - floor(x) == 0.5) ? 1 : 0;
+          } else {
+            tie = 1;  // no binade yet: term by term
+          }
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+          q += __shfl_xor_sync(0xffffffffu, q, o);
+          tie |= __shfl_xor_sync(0xffffffffu, tie, o);
+        }
+        if (lane == 0) {
+          sq[sub] = q;
+          stie[sub] = tie;
+        }
+      }
+      __syncthreads();
+      if (warp == 0) {
+        // the whole chunk at once when it stays in the binade without a tie
+        double tot = 0.0;
+        int anytie = 0;
+#pragma unroll
+        for (int r = 0; r < SQ_NSUB / 32; ++r) {
+          tot += sq[r * 32 + lane];
+          anytie |= stie[r * 32 + lane];
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+          tot += __shfl_xor_sync(0xffffffffu, tot, o);
+          anytie |= __shfl_xor_sync(0xffffffffu, anytie, o);
+        }
+        if (lane == 0) {
+          s_done = 1;
+          const double M = normal ? ldexp(S, 53 - E) : 0.0;
+          if (normal && !anytie && M + tot < two53) {
+            sS = ldexp(M + tot, E - 53);
+          } else {
+            // sub-chunk walk
+            double Mw = M, Sw = S;
+            int Ew = E;
+            bool nw = normal;
+            for (int idx = start; idx < SQ_NSUB; ++idx) {
+              if (nw && !stie[idx] && Mw + sq[idx] < two53) {
+                Mw += sq[idx];
+                continue;
+              }
+              if (nw) Sw = ldexp(Mw, Ew - 53);
+              for (int i = 0; i < SQ_SUB; ++i) Sw = __dadd_rn(Sw, st[idx * SQ_SUB + i]);
+              if (Sw >= tiny) {
+                int E2;
+                frexp(Sw, &E2);
+                if (!nw || E2 != Ew) {
+                  // a new binade: the later sub-chunks' quotients are stale
+                  if (idx + 1 < SQ_NSUB) {
+                    s_start = idx + 1;
+                    s_done = 0;
+                  }
+                  nw = false;  // Sw is authoritative
+                  break;
+                }
+                Mw = ldexp(Sw, 53 - Ew);
+              } else {
+                nw = false;
+              }
+            }
+            sS = nw ? ldexp(Mw, Ew - 53) : Sw;
+          }
+        }
+      }
+      __syncthreads();
+      if (s_done) break;
+    }
+  }
+  if (tid == 0) *out = sS;
+}
+
 // im_out = sum(im_in) * im_out / sum(im_out)  (imcom_proc.f90:249)
 __global__ void flux_scale_kernel(double* __restrict__ out, size_t count,
                                   const double* __restrict__ sums) {
@@ -157,24 +287,6 @@ __global__ void hermitian_fill_kernel(const double2* __restrict__ half, double2*
   full[(size_t)b * n1 * n2 + (size_t)j * n1 + k] = v;
 }
 
-// Partial sums of |z|^2 computed as a*a - b*(-b) (Re(z conj(z))).
-__global__ void abs2_partial_kernel(const double2* __restrict__ z, size_t count,
-                                    double* __restrict__ partial) {
-  __shared__ double sh[256];
-  double s = 0.0;
-  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < count;
-       k += (size_t)gridDim.x * blockDim.x) {
-    double2 v = z[k];
-    s += v.x * v.x - v.y * (-v.y);
-  }
-  sh[threadIdx.x] = s;
-  __syncthreads();
-  for (int w = 128; w > 0; w >>= 1) {
-    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
-}
 
 // Fortran CSHIFT source index (1-based): cshift(X, s)(i) = X(1 + mod(i-1+s, n)).
 __device__ __forceinline__ int cshift_src(int i1, int s, int n) {
@@ -359,9 +471,9 @@ extern "C" int imcom_gpu_psf_spectra(imcom_ctx* ctx, int npoly_in, double* C_out
                                                          ctx->Gammat, nps, nps);
     IMC_LAUNCH();
   }
-  abs2_partial_kernel<<<256, 256, 0, ctx->stream>>>(ctx->Gammat, ps2, scratch);
-  IMC_LAUNCH();
-  finish_sum_kernel<<<1, 256, 0, ctx->stream>>>(scratch, 256, sums + 2);
+  // C_a's sum in the reference's order: its rounding moves U by about
+  // count * eps / 2 relative at U ~ 1e-6 (about 1e-12 absolute)
+  seq_abs2_sum_kernel<<<1, SQ_THREADS, 0, ctx->stream>>>(ctx->Gammat, ps2, sums + 2);
   IMC_LAUNCH();
   double hs[3];
   int flag = 0;

@@ -77,14 +77,16 @@ __device__ __forceinline__ double warp_reduce_sum(double s) {
 // Modes p = lane + 32 j go to partial sum j mod 4, in increasing j; blocks
 // of eight modes per lane keep eight column loads in flight.
 // D = true also sums the derivative terms into *dsum (every lane gets the
-// total); the U sum is formed by exactly the same operations either way.
+// total) in four partials of their own, so they add no dependent chain; the
+// derivative only steers the Newton steps, so its summation order is free.
+// The U sum is formed by exactly the same operations either way.
 template <bool D>
 __device__ __forceinline__ double warp_usum_t(const double* lam, const double* col, int n,
                                               double k, int lane, double* dsum) {
   const double k2 = __dmul_rn(2.0, k);
   double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-  double dd = 0.0;
-#define UT(l_, c_) (D ? uterm_d(l_, c_, k, k2, &dd) : uterm(l_, c_, k, k2))
+  double d0 = 0.0, d1 = 0.0, d2 = 0.0, d3 = 0.0;  // derivative partials
+#define UT(l_, c_, d_) (D ? uterm_d(l_, c_, k, k2, &d_) : uterm(l_, c_, k, k2))
   int p = lane;
   for (; p + 224 < n; p += 256) {
     double c[8], l[8];
@@ -93,26 +95,26 @@ __device__ __forceinline__ double warp_usum_t(const double* lam, const double* c
       c[q] = col[p + 32 * q];
       l[q] = lam[p + 32 * q];
     }
-    s0 = __dadd_rn(s0, UT(l[0], c[0]));
-    s1 = __dadd_rn(s1, UT(l[1], c[1]));
-    s2 = __dadd_rn(s2, UT(l[2], c[2]));
-    s3 = __dadd_rn(s3, UT(l[3], c[3]));
-    s0 = __dadd_rn(s0, UT(l[4], c[4]));
-    s1 = __dadd_rn(s1, UT(l[5], c[5]));
-    s2 = __dadd_rn(s2, UT(l[6], c[6]));
-    s3 = __dadd_rn(s3, UT(l[7], c[7]));
+    s0 = __dadd_rn(s0, UT(l[0], c[0], d0));
+    s1 = __dadd_rn(s1, UT(l[1], c[1], d1));
+    s2 = __dadd_rn(s2, UT(l[2], c[2], d2));
+    s3 = __dadd_rn(s3, UT(l[3], c[3], d3));
+    s0 = __dadd_rn(s0, UT(l[4], c[4], d0));
+    s1 = __dadd_rn(s1, UT(l[5], c[5], d1));
+    s2 = __dadd_rn(s2, UT(l[6], c[6], d2));
+    s3 = __dadd_rn(s3, UT(l[7], c[7], d3));
   }
   for (; p + 96 < n; p += 128) {
-    s0 = __dadd_rn(s0, UT(lam[p], col[p]));
-    s1 = __dadd_rn(s1, UT(lam[p + 32], col[p + 32]));
-    s2 = __dadd_rn(s2, UT(lam[p + 64], col[p + 64]));
-    s3 = __dadd_rn(s3, UT(lam[p + 96], col[p + 96]));
+    s0 = __dadd_rn(s0, UT(lam[p], col[p], d0));
+    s1 = __dadd_rn(s1, UT(lam[p + 32], col[p + 32], d1));
+    s2 = __dadd_rn(s2, UT(lam[p + 64], col[p + 64], d2));
+    s3 = __dadd_rn(s3, UT(lam[p + 96], col[p + 96], d3));
   }
-  if (p < n) s0 = __dadd_rn(s0, UT(lam[p], col[p]));
-  if (p + 32 < n) s1 = __dadd_rn(s1, UT(lam[p + 32], col[p + 32]));
-  if (p + 64 < n) s2 = __dadd_rn(s2, UT(lam[p + 64], col[p + 64]));
+  if (p < n) s0 = __dadd_rn(s0, UT(lam[p], col[p], d0));
+  if (p + 32 < n) s1 = __dadd_rn(s1, UT(lam[p + 32], col[p + 32], d1));
+  if (p + 64 < n) s2 = __dadd_rn(s2, UT(lam[p + 64], col[p + 64], d2));
 #undef UT
-  if (D) *dsum = warp_reduce_sum(dd);
+  if (D) *dsum = warp_reduce_sum((d0 + d1) + (d2 + d3));
   return warp_reduce_sum(__dadd_rn(__dadd_rn(s0, s1), __dadd_rn(s2, s3)));
 }
 
@@ -126,8 +128,8 @@ __device__ __forceinline__ double warp_ssum_t(const double* lam, const double* c
                                               const double* nd, int n, double k, int lane,
                                               double* dsum) {
   double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-  double dd = 0.0;
-#define ST(l_, c_, w_) (D ? sterm_d(l_, c_, w_, k, &dd) : sterm(l_, c_, w_, k))
+  double d0 = 0.0, d1 = 0.0, d2 = 0.0, d3 = 0.0;  // derivative partials
+#define ST(l_, c_, w_, d_) (D ? sterm_d(l_, c_, w_, k, &d_) : sterm(l_, c_, w_, k))
   int p = lane;
   for (; p + 224 < n; p += 256) {
     double c[8], l[8], w[8];
@@ -137,26 +139,26 @@ __device__ __forceinline__ double warp_ssum_t(const double* lam, const double* c
       l[q] = lam[p + 32 * q];
       w[q] = nd[p + 32 * q];
     }
-    s0 = __dadd_rn(s0, ST(l[0], c[0], w[0]));
-    s1 = __dadd_rn(s1, ST(l[1], c[1], w[1]));
-    s2 = __dadd_rn(s2, ST(l[2], c[2], w[2]));
-    s3 = __dadd_rn(s3, ST(l[3], c[3], w[3]));
-    s0 = __dadd_rn(s0, ST(l[4], c[4], w[4]));
-    s1 = __dadd_rn(s1, ST(l[5], c[5], w[5]));
-    s2 = __dadd_rn(s2, ST(l[6], c[6], w[6]));
-    s3 = __dadd_rn(s3, ST(l[7], c[7], w[7]));
+    s0 = __dadd_rn(s0, ST(l[0], c[0], w[0], d0));
+    s1 = __dadd_rn(s1, ST(l[1], c[1], w[1], d1));
+    s2 = __dadd_rn(s2, ST(l[2], c[2], w[2], d2));
+    s3 = __dadd_rn(s3, ST(l[3], c[3], w[3], d3));
+    s0 = __dadd_rn(s0, ST(l[4], c[4], w[4], d0));
+    s1 = __dadd_rn(s1, ST(l[5], c[5], w[5], d1));
+    s2 = __dadd_rn(s2, ST(l[6], c[6], w[6], d2));
+    s3 = __dadd_rn(s3, ST(l[7], c[7], w[7], d3));
   }
   for (; p + 96 < n; p += 128) {
-    s0 = __dadd_rn(s0, ST(lam[p], col[p], nd[p]));
-    s1 = __dadd_rn(s1, ST(lam[p + 32], col[p + 32], nd[p + 32]));
-    s2 = __dadd_rn(s2, ST(lam[p + 64], col[p + 64], nd[p + 64]));
-    s3 = __dadd_rn(s3, ST(lam[p + 96], col[p + 96], nd[p + 96]));
+    s0 = __dadd_rn(s0, ST(lam[p], col[p], nd[p], d0));
+    s1 = __dadd_rn(s1, ST(lam[p + 32], col[p + 32], nd[p + 32], d1));
+    s2 = __dadd_rn(s2, ST(lam[p + 64], col[p + 64], nd[p + 64], d2));
+    s3 = __dadd_rn(s3, ST(lam[p + 96], col[p + 96], nd[p + 96], d3));
   }
-  if (p < n) s0 = __dadd_rn(s0, ST(lam[p], col[p], nd[p]));
-  if (p + 32 < n) s1 = __dadd_rn(s1, ST(lam[p + 32], col[p + 32], nd[p + 32]));
-  if (p + 64 < n) s2 = __dadd_rn(s2, ST(lam[p + 64], col[p + 64], nd[p + 64]));
+  if (p < n) s0 = __dadd_rn(s0, ST(lam[p], col[p], nd[p], d0));
+  if (p + 32 < n) s1 = __dadd_rn(s1, ST(lam[p + 32], col[p + 32], nd[p + 32], d1));
+  if (p + 64 < n) s2 = __dadd_rn(s2, ST(lam[p + 64], col[p + 64], nd[p + 64], d2));
 #undef ST
-  if (D) *dsum = warp_reduce_sum(dd);
+  if (D) *dsum = warp_reduce_sum((d0 + d1) + (d2 + d3));
   return warp_reduce_sum(__dadd_rn(__dadd_rn(s0, s1), __dadd_rn(s2, s3)));
 }
 
@@ -200,6 +202,97 @@ struct StreamCol {
     const double ssum = warp_ssum_t<true>(lam, col, nd, n, k, lane, &d);
     *dx = -0.5 * LN10 * k * d;
     return __ddiv_rn(ssum, 4.0);
+  }
+};
+
+// U/S evaluator shared by the four warps of a CTA: warp w sums the modes
+// p = lane + 32 j with j = w (mod 4), in increasing j -- exactly partial sum
+// s_w of warp_usum_t / warp_ssum_t --, the partials meet in shared memory and
+// every warp combines them as (s0 + s1) + (s2 + s3) and the lane butterfly.
+// So every warp gets the one-warp evaluator's value bit for bit, with a
+// quarter of the terms in each warp's dependent chain.  One barrier per
+// evaluation (double-buffered partials); all four warps must call it with
+// the same arguments.
+template <bool D, bool U>
+__device__ __forceinline__ double cta_partial(const double* lam, const double* col,
+                                              const double* nd, int n, double k, int lane,
+                                              int w, double* dpart) {
+  constexpr int B = U ? 6 : 4;  // terms whose loads are in flight together
+  const double k2 = __dmul_rn(2.0, k);
+  double s = 0.0, d0 = 0.0, d1 = 0.0;
+  int j = w;
+  for (; lane + 32 * (j + 4 * (B - 1)) < n; j += 4 * B) {
+    double c[B], l[B], wv[B];
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      const int p = lane + 32 * (j + 4 * q);
+      c[q] = col[p];
+      l[q] = lam[p];
+      if (!U) wv[q] = nd[p];
+    }
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      double t;
+      if (U)
+        t = D ? uterm_d(l[q], c[q], k, k2, (q & 1) ? &d1 : &d0) : uterm(l[q], c[q], k, k2);
+      else
+        t = D ? sterm_d(l[q], c[q], wv[q], k, (q & 1) ? &d1 : &d0) : sterm(l[q], c[q], wv[q], k);
+      s = __dadd_rn(s, t);
+    }
+  }
+  for (; lane + 32 * j < n; j += 4) {
+    const int p = lane + 32 * j;
+    double t;
+    if (U)
+      t = D ? uterm_d(lam[p], col[p], k, k2, &d0) : uterm(lam[p], col[p], k, k2);
+    else
+      t = D ? sterm_d(lam[p], col[p], nd[p], k, &d0) : sterm(lam[p], col[p], nd[p], k);
+    s = __dadd_rn(s, t);
+  }
+  if (D) *dpart = d0 + d1;
+  return s;
+}
+
+struct CtaCol {
+  const double* lam;
+  const double* col;
+  const double* nd;
+  int n;
+  bool U;
+  double C;
+  double* red;  // shared, 2 x 2 x 4 x 32 doubles: buffer, value/derivative, warp, lane
+  int warp;
+  mutable int buf;
+
+  template <bool D>
+  __device__ __forceinline__ double sum(double k, int lane, double* dsum) const {
+    double dw = 0.0;
+    const double sw = U ? cta_partial<D, true>(lam, col, nd, n, k, lane, warp, &dw)
+                        : cta_partial<D, false>(lam, col, nd, n, k, lane, warp, &dw);
+    double* r = red + buf * 256;
+    buf ^= 1;
+    r[warp * 32 + lane] = sw;
+    if (D) r[128 + warp * 32 + lane] = dw;
+    __syncthreads();
+    const double tot = __dadd_rn(__dadd_rn(r[lane], r[32 + lane]), __dadd_rn(r[64 + lane], r[96 + lane]));
+    if (D) *dsum = warp_reduce_sum((r[128 + lane] + r[160 + lane]) + (r[192 + lane] + r[224 + lane]));
+    return warp_reduce_sum(tot);
+  }
+  __device__ __forceinline__ double operator()(double k, int lane) const {
+    if (U) return __ddiv_rn(__dsub_rn(C, __ddiv_rn(sum<false>(k, lane, nullptr), 4.0)), C);
+    return __ddiv_rn(sum<false>(k, lane, nullptr), 4.0);
+  }
+  // the value operator() returns, bit for bit, and d/dx at x = log10(kappa)
+  __device__ __forceinline__ double eval_d(double k, int lane, double* dx) const {
+    constexpr double LN10 = 2.302585092994046;
+    double d;
+    const double s = sum<true>(k, lane, &d);
+    if (U) {
+      *dx = LN10 * k * k / (2.0 * C) * d;
+      return __ddiv_rn(__dsub_rn(C, __ddiv_rn(s, 4.0)), C);
+    }
+    *dx = -0.5 * LN10 * k * d;
+    return __ddiv_rn(s, 4.0);
   }
 };
 

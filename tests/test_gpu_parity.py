@@ -54,6 +54,25 @@ def test_psf_spectra(gs, case):
     assert np.array_equal(Gt[n1 // 2 + 1:, 0, 0], np.conj(Gt[n1 // 2 - 1:0:-1, 0, 0]))
 
 
+@pytest.mark.parametrize("workload", ["small", "n4096"])
+def test_C_is_summed_in_the_reference_order(gs, workload):
+    """C_a = sum(|Gammat|^2) / nps^2 rounded as the reference's sequential
+    SUM (imcom_matrix.f90:549): the oracle's sequential loop over the GPU's
+    own Gammat gives the GPU's C bit for bit (the GPU sums in parallel by
+    binades).  At n4096 (nps = 576, 331776 terms) the sequential and the exact
+    sums differ by far more than one rounding, so the order is what is
+    tested."""
+    import math
+    prob = synth.make(workload, 0)
+    gs.set_problem(prob)
+    C, _, Gm = gs.psf_spectra(spectra=True)
+    assert C == O.calc_C(Gm)
+    t = (Gm.real * Gm.real + Gm.imag * Gm.imag).reshape(-1, order="F")
+    exact = math.fsum(t) / prob.nps / prob.nps
+    if workload == "n4096":
+        assert C != exact
+
+
 @pytest.mark.parametrize("case", ["tiny_u", "tiny_rot"])
 def test_build_A_B(gs, case):
     prob, d = make_golden.load(case)

