@@ -9,7 +9,8 @@
 // Q = I - V T V^T; R goes into the band below the diagonal block, and the
 // trailing matrix A22 = A(k+SB:, k+SB:) (full symmetric storage) becomes
 // Q^T A22 Q through
-//     W = A22 V T,  W <- W - 1/2 V (T^T (V^T W)),  A22 <- A22 - V W^T - W V^T.
+//     W = A22 V T,  W <- W - 1/2 V (T^T (V^T W)),  A22 <- A22 - V W^T - W V^T,
+// the last on the lower tiles only, its upper triangle mirrored after.
 // The panel QR runs in one thread-block cluster: each CTA holds a slice of
 // the panel's rows in shared memory, and every column needs one cluster-wide
 // exchange of its partial sums (the column's norm below the pivot, its dot
@@ -30,8 +31,10 @@ namespace {
 
 constexpr int SB = 32;            // bandwidth of the first stage (panel width)
 constexpr int SB_CTAS = 16;       // CTAs of the panel cluster (8 where 16 cannot be placed)
-constexpr int SB_THREADS = 256;   // 32 columns x 8 row slices
-constexpr int SB_SLICES = SB_THREADS / SB;
+// threads of the panel kernel: 32 columns x 8 row slices with the panel
+// staged in shared memory, x 32 row slices when it is updated in place in
+// global memory (more loads in flight per column)
+__host__ __device__ constexpr int sb_threads(bool staged) { return staged ? 256 : 1024; }
 
 struct PanelArgs {
   double* A;       // full symmetric working matrix
@@ -58,7 +61,8 @@ struct PanelArgs {
 // global memory (stride lda), which only the reduction buffers need shared
 // memory for.
 template <bool STAGED>
-__global__ void __launch_bounds__(SB_THREADS, 1) sb_panel_kernel(PanelArgs a) {
+__global__ void __launch_bounds__(sb_threads(STAGED), 1) sb_panel_kernel(PanelArgs a) {
+  constexpr int SB_THREADS = sb_threads(STAGED), SB_SLICES = SB_THREADS / SB;
   namespace cg = cooperative_groups;
   cg::cluster_group cl = cg::this_cluster();
   const int q = (int)cl.block_rank(), nct = (int)cl.num_blocks();
@@ -151,7 +155,8 @@ __global__ void __launch_bounds__(SB_THREADS, 1) sb_panel_kernel(PanelArgs a) {
 }
 
 inline size_t panel_smem(int per, bool staged) {
-  return ((staged ? (size_t)SB * per : 0) + 2 * SB_CTAS * 2 * SB + SB_SLICES * 2 * SB + 2 * SB) *
+  return ((staged ? (size_t)SB * per : 0) + 2 * SB_CTAS * 2 * SB +
+          (size_t)(sb_threads(staged) / SB) * 2 * SB + 2 * SB) *
          sizeof(double);
 }
 
@@ -161,20 +166,131 @@ inline size_t panel_smem(int per, bool staged) {
 __global__ void sb_larft_kernel(const double* __restrict__ G, const double* __restrict__ tau,
                                 double* __restrict__ T) {
   __shared__ double sT[SB][SB + 1];
+  __shared__ double sG[SB][SB + 1];  // sG[j][h] = G(h, j)
+  __shared__ double stau[SB];
   const int r = threadIdx.x;
-  for (int cc = 0; cc < SB; ++cc) sT[r][cc] = 0.0;
+  for (int cc = 0; cc < SB; ++cc) {
+    sT[r][cc] = 0.0;
+    sG[cc][r] = G[r + cc * SB];
+  }
+  stau[r] = tau[r];
   __syncwarp();
   for (int j = 0; j < SB; ++j) {
-    const double tj = tau[j];
+    const double tj = stau[j];
     double s = 0.0;
     if (r < j)
-      for (int h = r; h < j; ++h) s += sT[r][h] * G[h + j * SB];
+      for (int h = r; h < j; ++h) s += sT[r][h] * sG[j][h];
     __syncwarp();
     if (r < j) sT[r][j] = -tj * s;
     if (r == j) sT[j][j] = tj;
     __syncwarp();
   }
   for (int cc = 0; cc < SB; ++cc) T[r + cc * SB] = sT[r][cc];
+}
+
+// The panel's two-sided update factors from X1 = A22 V (N x SB):
+//   W = X1 T - 1/2 V M2,  M2 = T^T (V^T X1) T     (V^T W = (V^T X1) T),
+// in three launches.  wy_partial_kernel: S_b = V_b^T X1_b for blocks b of
+// WY_ROWS rows.  wy_m2_kernel (one CTA): S = sum_b S_b in a fixed order and
+// M2.  wy_finish_kernel: for its rows, W and the packed operands of the
+// update A22 -= X Y^T, X = [V | W] and Y = [W | V] (ld ldx, 2 SB columns),
+// written over X1's storage (the block's rows of X1 are read first; X1 lives
+// in X's first SB columns).
+constexpr int WY_ROWS = 48, WY_THREADS = 256;
+
+__global__ void __launch_bounds__(WY_THREADS) wy_partial_kernel(
+    const double* __restrict__ V, long long ldv, const double* __restrict__ X1, long long ldx,
+    int N, double* __restrict__ Spart) {
+  __shared__ double sV[WY_ROWS][SB + 1], sX[WY_ROWS][SB + 1];
+  const int r0 = blockIdx.x * WY_ROWS;
+  for (int e = threadIdx.x; e < WY_ROWS * SB; e += WY_THREADS) {
+    const int r = e % WY_ROWS, c = e / WY_ROWS;
+    const bool in = r0 + r < N;
+    sV[r][c] = in ? V[(size_t)(r0 + r) + (size_t)c * ldv] : 0.0;
+    sX[r][c] = in ? X1[(size_t)(r0 + r) + (size_t)c * ldx] : 0.0;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < SB * SB; e += WY_THREADS) {
+    const int i = e % SB, j = e / SB;
+    double acc = 0.0;
+    for (int r = 0; r < WY_ROWS; ++r) acc = fma(sV[r][i], sX[r][j], acc);
+    Spart[(size_t)blockIdx.x * SB * SB + e] = acc;
+  }
+}
+
+// One CTA of SB * SB threads: M2 = T^T S T (column-major, ld SB).
+__global__ void __launch_bounds__(SB * SB) wy_m2_kernel(const double* __restrict__ Spart, int nb,
+                                                        const double* __restrict__ T,
+                                                        double* __restrict__ M2) {
+  __shared__ double sS[SB][SB + 1], sT[SB][SB + 1], sU[SB][SB + 1];
+  const int e = threadIdx.x, i = e % SB, j = e / SB;
+  double acc = 0.0;
+  for (int b = 0; b < nb; ++b) acc += Spart[(size_t)b * SB * SB + e];
+  sS[i][j] = acc;
+  sT[i][j] = T[e];  // T(i, j) at i + j SB, upper triangular
+  __syncthreads();
+  double u = 0.0;
+  for (int h = 0; h <= j; ++h) u = fma(sS[i][h], sT[h][j], u);
+  sU[i][j] = u;
+  __syncthreads();
+  double m = 0.0;
+  for (int h = 0; h <= i; ++h) m = fma(sT[h][i], sU[h][j], m);
+  M2[e] = m;
+}
+
+__global__ void __launch_bounds__(WY_THREADS) wy_finish_kernel(
+    const double* __restrict__ T, const double* __restrict__ M2, const double* __restrict__ V,
+    long long ldv, double* __restrict__ XY, long long ldx, int N) {
+  __shared__ double sT[SB][SB + 1], sM[SB][SB + 1];
+  __shared__ double sV[WY_ROWS][SB + 1], sX[WY_ROWS][SB + 1];
+  const int r0 = blockIdx.x * WY_ROWS;
+  for (int e = threadIdx.x; e < SB * SB; e += WY_THREADS) {
+    sT[e % SB][e / SB] = T[e];
+    sM[e % SB][e / SB] = M2[e];
+  }
+  for (int e = threadIdx.x; e < WY_ROWS * SB; e += WY_THREADS) {
+    const int r = e % WY_ROWS, c = e / WY_ROWS;
+    const bool in = r0 + r < N;
+    sV[r][c] = in ? V[(size_t)(r0 + r) + (size_t)c * ldv] : 0.0;
+    sX[r][c] = in ? XY[(size_t)(r0 + r) + (size_t)c * ldx] : 0.0;
+  }
+  __syncthreads();
+  double* X = XY;
+  double* Y = XY + (size_t)ldx * 2 * SB;
+  for (int e = threadIdx.x; e < WY_ROWS * SB; e += WY_THREADS) {
+    const int r = e % WY_ROWS, j = e / WY_ROWS;
+    if (r0 + r >= N) continue;
+    double w1 = 0.0, w2 = 0.0;
+    for (int h = 0; h <= j; ++h) w1 = fma(sX[r][h], sT[h][j], w1);
+    for (int h = 0; h < SB; ++h) w2 = fma(sV[r][h], sM[h][j], w2);
+    const double w = w1 - 0.5 * w2;
+    const double v = sV[r][j];
+    const size_t row = (size_t)(r0 + r);
+    X[row + (size_t)j * ldx] = v;
+    X[row + (size_t)(SB + j) * ldx] = w;
+    Y[row + (size_t)j * ldx] = w;
+    Y[row + (size_t)(SB + j) * ldx] = v;
+  }
+}
+
+// A(i, j) = A(j, i) for i < j: the strictly upper triangle of the N x N
+// matrix at ld from its lower triangle, through 32 x 32 shared tiles
+// (block (x, y) writes tile row y, tile column x >= y; reads only the lower
+// tile (x, y), so blocks never touch each other's data).
+__global__ void mirror_lower_kernel(double* __restrict__ A, long long ld, int N) {
+  __shared__ double t[32][33];
+  const int bi = blockIdx.y, bj = blockIdx.x;
+  if (bi > bj) return;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int k = ty; k < 32; k += 8) {
+    const int r = bj * 32 + tx, c = bi * 32 + k;  // source A(r, c), r >= c
+    t[k][tx] = (r < N && c < N) ? A[r + (size_t)c * ld] : 0.0;
+  }
+  __syncthreads();
+  for (int k = ty; k < 32; k += 8) {
+    const int r = bi * 32 + tx, c = bj * 32 + k;  // destination A(r, c) = A(c, r)
+    if (r < c && c < N) A[r + (size_t)c * ld] = t[tx][k];
+  }
 }
 
 // Band storage for the second stage: AB[d + c * ldb] = A(c + d, c) for
@@ -739,7 +855,7 @@ static bool panel_cluster_fits(imcom_ctx* ctx, int cs, size_t smem, int optin) {
   at[0].val.clusterDim.y = 1;
   at[0].val.clusterDim.z = 1;
   cfg.gridDim = dim3(cs);
-  cfg.blockDim = dim3(SB_THREADS);
+  cfg.blockDim = dim3(sb_threads(STAGED));
   cfg.dynamicSmemBytes = smem;
   cfg.attrs = at;
   cfg.numAttrs = 1;
@@ -780,8 +896,8 @@ int sy2sb_gpu(imcom_ctx* ctx, DMat& Aw, DMat& V, double* tau, double* Tf, double
   int ctas = 16;
   IMC_TRY(panel_cluster(ctx, optin, &ctas));
   double* G = Tf + (size_t)((n + SB - 1) / SB) * SB * SB;  // SB x SB Gram scratch
-  double* M = G + SB * SB;                                   // SB x SB
-  double* M2 = M + SB * SB;
+  double* M2 = G + SB * SB;                                  // SB x SB
+  double* Spart = W;  // per-block partials of V^T X1: ceil(N / WY_ROWS) SB^2 <= SB ldw
   for (int k = 0; k + SB < n - 1; k += SB) {
     const int N = n - k - SB;
     const int pc = std::max(1, (N + ctas - 1) / ctas);
@@ -795,7 +911,7 @@ int sy2sb_gpu(imcom_ctx* ctx, DMat& Aw, DMat& V, double* tau, double* Tf, double
     at[0].val.clusterDim.y = 1;
     at[0].val.clusterDim.z = 1;
     cfg.gridDim = dim3(ctas);
-    cfg.blockDim = dim3(SB_THREADS);
+    cfg.blockDim = dim3(sb_threads(staged));
     cfg.dynamicSmemBytes = panel_smem(pc, staged);
     cfg.stream = ctx->stream;
     cfg.attrs = at;
@@ -813,22 +929,30 @@ int sy2sb_gpu(imcom_ctx* ctx, DMat& Aw, DMat& V, double* tau, double* Tf, double
     IMC_TRY(dgemm(ctx, 'T', 'N', SB, SB, N, 1.0, Vp, V.ld, Vp, V.ld, 0.0, G, SB));
     sb_larft_kernel<<<1, SB, 0, ctx->stream>>>(G, tau + k, T);
     IMC_LAUNCH();
-    // W = A22 V T (the first product into XY as scratch)
+    // X1 = A22 V into the first SB columns of XY, then W and the packed
+    // operands X = [V | W], Y = [W | V] of the update A22 -= X Y^T
     double* X1 = XY;
     IMC_TRY(dgemm(ctx, 'N', 'N', N, SB, N, 1.0, A22, ld, Vp, V.ld, 0.0, X1, ldw));
-    IMC_TRY(dgemm(ctx, 'N', 'N', N, SB, SB, 1.0, X1, ldw, T, SB, 0.0, W, ldw));
-    // W -= 1/2 V (T^T (V^T W))
-    IMC_TRY(dgemm(ctx, 'T', 'N', SB, SB, N, 1.0, Vp, V.ld, W, ldw, 0.0, M, SB));
-    IMC_TRY(dgemm(ctx, 'T', 'N', SB, SB, SB, 1.0, T, SB, M, SB, 0.0, M2, SB));
-    IMC_TRY(dgemm(ctx, 'N', 'N', N, SB, SB, -0.5, Vp, V.ld, M2, SB, 1.0, W, ldw));
-    // A22 -= [V W] [W V]^T
+    const int nb = (N + WY_ROWS - 1) / WY_ROWS;
+    wy_partial_kernel<<<nb, WY_THREADS, 0, ctx->stream>>>(Vp, V.ld, X1, ldw, N, Spart);
+    IMC_LAUNCH();
+    wy_m2_kernel<<<1, SB * SB, 0, ctx->stream>>>(Spart, nb, T, M2);
+    IMC_LAUNCH();
+    wy_finish_kernel<<<nb, WY_THREADS, 0, ctx->stream>>>(T, M2, Vp, V.ld, XY, ldw, N);
+    IMC_LAUNCH();
     double* X = XY;
     double* Y = XY + (size_t)ldw * 2 * SB;
-    dim3 grd((N + 255) / 256, SB);
-    pack_update_kernel<<<grd, 256, 0, ctx->stream>>>(Vp - r0, V.ld, W - r0, ldw, (int)r0, n, SB,
-                                                     X - r0, Y - r0, ldw);
-    IMC_LAUNCH();
-    IMC_TRY(dgemm(ctx, 'N', 'T', N, N, 2 * SB, -1.0, X, ldw, Y, ldw, 1.0, A22, ld));
+    // the update on the tiles on and below the diagonal only; the next panel's
+    // product A22 V reads the whole trailing matrix, so its upper triangle is
+    // then mirrored from the lower
+    IMC_TRY(dgemm_lower_nt(ctx, N, 2 * SB, -1.0, X, ldw, Y, ldw, 1.0, A22, ld));
+    const int Nn = N - SB;  // the next trailing matrix
+    if (k + 2 * SB < n - 1 && Nn > 0) {
+      dim3 grd((Nn + 31) / 32, (Nn + 31) / 32);
+      mirror_lower_kernel<<<grd, dim3(32, 8), 0, ctx->stream>>>(A22 + SB + (size_t)SB * ld, ld,
+                                                                Nn);
+      IMC_LAUNCH();
+    }
   }
   band_extract_kernel<<<n, 128, 0, ctx->stream>>>(Aw.p, ld, n, AB, ldb);
   IMC_LAUNCH();

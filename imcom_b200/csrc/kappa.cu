@@ -370,16 +370,17 @@ struct LearnedExtra {
 //    U_a/S_a and the reported value are bit-identical to the plain bisection.
 // The nw warps that share the evaluator run it in lock step (same values,
 // same branches); warp wid 0 writes the scalars.
+// guess: this pixel's network outputs, or null (start from the middle).
 template <class Eval>
 __device__ __forceinline__ void learned_pixel(const BisectArgs& a, const LearnedExtra& ex,
                                               const double* lam, const double* col,
-                                              const Eval& ev, int pix, int lane, int wid = 0,
-                                              int nw = 1) {
+                                              const Eval& ev, int pix, int lane, int wid,
+                                              int nw, const float2* guess) {
   const bool U = a.UnotS != 0;
   const double rlo = a.lg_min, rhi = a.lg_max;  // the reference's search range
   double x0 = 0.5 * (rlo + rhi), hw = 0.5 * (rhi - rlo);
-  if (ex.guess) {
-    const float2 o = ex.guess[pix];
+  if (guess) {
+    const float2 o = *guess;
     if (isfinite(o.x) && isfinite(o.y)) {
       x0 = (double)o.x;
       hw = ex.half_scale * exp((double)fminf(fmaxf(o.y, -20.0f), 5.0f));
@@ -555,7 +556,87 @@ __global__ void __launch_bounds__(LB_WARPS * 32, 7) learned_bisect_kernel(Bisect
   if (pix >= a.m) return;
   const double* col = a.P + (size_t)pix * a.ldp;
   const CtaCol ev{a.L, col, a.Nd, a.n, a.UnotS != 0, a.C, red, warp, 0};
-  learned_pixel(a, ex, a.L, col, ev, pix, lane, warp, LB_WARPS);
+  learned_pixel(a, ex, a.L, col, ev, pix, lane, warp, LB_WARPS,
+                ex.guess ? ex.guess + pix : nullptr);
+}
+
+// The same with the features and the network in the pixel's CTA (the table
+// features, IMCOM_OPT_KAPPA_FEATURES = 1): the CTA sums the column's band
+// masses in its first pass over the column -- which leaves the column in L2
+// for the evaluations that follow --, warp 0 forms the 12 features and runs
+// the tensor-core forward (mlp_forward_16, one valid row) on weights staged
+// in shared memory, and the Newton steps start from its outputs.  This
+// replaces a separate pass of the features kernel over all of P and two
+// launches.
+struct FusedTables {
+  const float2* nbr;      // neighbour count and exposures per pixel
+  const int8_t* bidx;     // band index per eigenmode
+  const int* seg;         // band segments (seg[9] != 0: the index is not monotone)
+  const float* weights;   // the network (device weight block)
+};
+
+__global__ void __launch_bounds__(LB_WARPS * 32, 7) learned_fused_kernel(BisectArgs a,
+                                                                         LearnedExtra ex,
+                                                                         FusedTables ft) {
+  __shared__ double red[2 * 2 * LB_WARPS * 32];
+  __shared__ __align__(16) MlpSmem S;
+  __shared__ double sband[LB_WARPS][8];
+  __shared__ float sfeat[16];
+  __shared__ float2 sguess;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, tid = threadIdx.x;
+  const int pix = blockIdx.x;
+  if (pix >= a.m) return;
+  const double* col = a.P + (size_t)pix * a.ldp;
+  load_mlp_smem(ft.weights, S);
+  double band[8];
+#pragma unroll
+  for (int b = 0; b < 8; ++b) band[b] = 0.0;
+  if (ft.seg[9] == 0) {
+#pragma unroll
+    for (int b = 0; b < 8; ++b)
+      for (int p = ft.seg[b] + tid; p < ft.seg[b + 1]; p += LB_WARPS * 32)
+        band[b] = fma(col[p], col[p], band[b]);
+  } else {
+    for (int p = tid; p < a.n; p += LB_WARPS * 32) {
+      const double pp = col[p];
+      const int bb = ft.bidx[p];
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        if (q == bb) band[q] += pp * pp;
+    }
+  }
+#pragma unroll
+  for (int b = 0; b < 8; ++b) {
+    const double v = wsum(band[b]);
+    if (lane == 0) sband[warp][b] = v;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const double lmax = a.L[0];  // eigenvalues are in descending order
+    if (lane < 16) {
+      float f = 0.0f;
+      if (lane == 0) f = ft.nbr[pix].x;
+      else if (lane == 1) f = ft.nbr[pix].y;
+      else if (lane < 10) {
+        const int b = lane - 2;
+        double sb = 0.0;
+#pragma unroll
+        for (int w = 0; w < LB_WARPS; ++w) sb += sband[w][b];
+        const double lc = lmax * pow(10.0, -(2.0 * b + 1.0));
+        f = (float)log10(sb / (4.0 * a.C * (lc > 0.0 ? lc : 1e-300)) + 1e-30);
+      } else if (lane == 10) {
+        f = (float)log10(fabs(a.US_max) + 1e-300);
+      } else if (lane == 11) {
+        f = (float)log10(fabs(lmax / a.C) + 1e-300);
+      }
+      sfeat[lane] = f;
+    }
+    __syncwarp();
+    mlp_forward_16(S, sfeat, 1, 0, lane, &sguess);
+  }
+  __syncthreads();
+  const CtaCol ev{a.L, col, a.Nd, a.n, a.UnotS != 0, a.C, red, warp, 0};
+  learned_pixel(a, ex, a.L, col, ev, pix, lane, warp, LB_WARPS, &sguess);
 }
 
 // ---------------------------------------------------------------------------
@@ -770,7 +851,7 @@ int kappa_guess(imcom_ctx* ctx, const BisectArgs& a, bool network) {
 int fill_learned(imcom_ctx* ctx, LearnedExtra& ex) {
   if (!ctx->mlp.set && !ctx->kappa_nonet)
     return set_err(ctx, IMCOM_ERR_STATE, "imcom_gpu_mlp_set_weights has not run");
-  ex.guess = ctx->kappa_nonet ? nullptr : ctx->guess;
+  ex.guess = nullptr;  // set by the caller once kappa_guess has sized ctx->guess
   ex.fallback = nullptr;
   ex.half_scale = 3.0;
   ex.min_half = 0.02;
@@ -849,8 +930,20 @@ extern "C" int imcom_gpu_bisect_kappa_learned(imcom_ctx* ctx, int UnotS, double 
   IMC_TRY(ensure_buf(ctx, (void**)&ctx->fb, ctx->fb_bytes, (size_t)ctx->m * sizeof(int)));
   ex.fallback = ctx->fb;
   if (ctx->p_split) IMC_TRY(split_margin_buffer(ctx, a));
-  if (!ctx->kappa_nonet) IMC_TRY(kappa_guess(ctx, a, true));
-  learned_bisect_kernel<<<ctx->m, LB_WARPS * 32, 0, ctx->stream>>>(a, ex);
+  const bool fused = !ctx->kappa_nonet && ctx->kappa_feat;
+  if (!ctx->kappa_nonet && !fused) {
+    IMC_TRY(kappa_guess(ctx, a, true));
+    ex.guess = ctx->guess;  // after kappa_guess: it may have grown the buffer
+  }
+  if (fused) {
+    const float2* nbr;
+    const int* seg;
+    IMC_TRY(feature_tables(ctx, &nbr, &seg));
+    FusedTables ft{nbr, ctx->band, seg, ctx->mlp.w};
+    learned_fused_kernel<<<ctx->m, LB_WARPS * 32, 0, ctx->stream>>>(a, ex, ft);
+  } else {
+    learned_bisect_kernel<<<ctx->m, LB_WARPS * 32, 0, ctx->stream>>>(a, ex);
+  }
   IMC_LAUNCH();
   if (ctx->p_split) IMC_TRY(split_audit(ctx, a));
   stage_end(ctx, ST_BISECT);
