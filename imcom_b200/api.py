@@ -32,7 +32,7 @@ OPT_BISECT_CTAS_PER_SM = 9
 OPT_SM_SHARE = 10
 OPT_TAIL_CTAS = 11
 OPT_STACK_KERNEL = 12
-STACKS_GEMM, STACKS_STREAM = 0, 1
+STACKS_GEMM, STACKS_STREAM, STACKS_AUTO = 0, 1, 2
 OPT_TABLE_FFT = 13
 OPT_KAPPA_FEATURES = 14
 OPT_KAPPA_START = 17

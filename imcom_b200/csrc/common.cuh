@@ -126,7 +126,7 @@ struct imcom_ctx {
   int bisect_ctas = 0;  // CTAs per SM of the streaming pixel kernels (0: automatic)
   int sm_share = 0;     // SMs for persistent / cooperative grids (0: the whole device)
   int tail_ctas = 0;    // cluster of the tridiagonalisation tail (0 auto, -1 none, 8, 16)
-  int stack_kernel = IMCOM_STACKS_GEMM;  // kernel of imcom_gpu_build_images
+  int stack_kernel = IMCOM_STACKS_AUTO;  // kernel of imcom_gpu_build_images
   void* jac_buf = nullptr;  // batched Jacobi: matrices, vectors, values, status
   size_t jac_bytes = 0;
   int split_SP = 7, split_ST = 6;        // digit slices of the P and T products

@@ -388,7 +388,8 @@ int imcom_gpu_set_option(imcom_ctx* ctx, int option, long long value) {
       ctx->table_fft = (int)value;
       return 0;
     case IMCOM_OPT_STACK_KERNEL:
-      if (value != IMCOM_STACKS_GEMM && value != IMCOM_STACKS_STREAM) return -3;
+      if (value != IMCOM_STACKS_GEMM && value != IMCOM_STACKS_STREAM && value != IMCOM_STACKS_AUTO)
+        return -3;
       ctx->stack_kernel = (int)value;
       return 0;
     case IMCOM_OPT_BISECT_CTAS_PER_SM:

@@ -447,7 +447,11 @@ static int launch_stacks(imcom_ctx* ctx, int nstack, const double* dI, long long
 static int build_images(imcom_ctx* ctx, int nstack, const double* dI, long long ldi,
                         double* dH, long long ldh) {
   stage_begin(ctx, ST_EPI);
-  if (ctx->stack_kernel == IMCOM_STACKS_STREAM) {
+  // the streaming kernel passes over T once per 8 stacks (~45 us each at
+  // n = m = 4096), the GEMM's time is flat at ~215 us up to 64 stacks
+  const bool stream = ctx->stack_kernel == IMCOM_STACKS_STREAM ||
+                      (ctx->stack_kernel == IMCOM_STACKS_AUTO && nstack <= IMCOM_STACKS_STREAM_MAX);
+  if (stream) {
     // passes of at most 8 stacks: 4 x 8 partial sums and two 4 x 4 blocks of
     // T values per lane fill the register budget of three CTAs per SM
     if ((nstack + 7) / 8 > 65535)

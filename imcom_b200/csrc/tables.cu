@@ -152,18 +152,25 @@ __global__ void __launch_bounds__(SQ_THREADS, 1)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const double two53 = 9007199254740992.0, tiny = 4.450147717014403e-308;  // 2^53, 2^-1021
   if (tid == 0) sS = 0.0;
+  // term r * 1024 + tid of a chunk (coalesced); sub-chunk r * 32 + warp.  The
+  // next chunk's values are loaded while this one is reduced.
+  double2 vn[SQ_PER];
+#pragma unroll
+  for (int r = 0; r < SQ_PER; ++r) {
+    const size_t k = (size_t)r * SQ_THREADS + tid;
+    vn[r] = k < count ? z[k] : make_double2(0.0, 0.0);
+  }
   for (size_t base = 0; base < count; base += SQ_CHUNK) {
-    // term r * 1024 + tid of the chunk (coalesced); sub-chunk r * 32 + warp
     double t[SQ_PER];
 #pragma unroll
     for (int r = 0; r < SQ_PER; ++r) {
-      const size_t k = base + (size_t)r * SQ_THREADS + tid;
-      t[r] = 0.0;
-      if (k < count) {
-        const double2 v = z[k];
-        t[r] = __dadd_rn(__dmul_rn(v.x, v.x), __dmul_rn(v.y, v.y));
-      }
+      t[r] = __dadd_rn(__dmul_rn(vn[r].x, vn[r].x), __dmul_rn(vn[r].y, vn[r].y));
       st[r * SQ_THREADS + tid] = t[r];
+    }
+#pragma unroll
+    for (int r = 0; r < SQ_PER; ++r) {
+      const size_t k = base + SQ_CHUNK + (size_t)r * SQ_THREADS + tid;
+      vn[r] = k < count ? z[k] : make_double2(0.0, 0.0);
     }
     if (tid == 0) s_start = 0;
     __syncthreads();

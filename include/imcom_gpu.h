@@ -96,13 +96,17 @@ typedef struct imcom_ctx imcom_ctx;
  * side can make wait; smaller clusters hold smaller tails.  Same results to
  * rounding either way. */
 #define IMCOM_OPT_TAIL_CTAS 11
-/* Kernel of imcom_gpu_build_images: 0 = the FP64 GEMM (default), 1 = a
- * streaming kernel for a few stacks (up to 8 stacks per pass over T, FP64
- * FMA, each warp holding four columns of T against the stacks of its pass).
- * Same sums to rounding. */
+/* Kernel of imcom_gpu_build_images: 0 = the FP64 GEMM, 1 = a streaming
+ * kernel for a few stacks (up to 8 stacks per pass over T, FP64 FMA, each
+ * warp holding four columns of T against the stacks of its pass), 2 = the
+ * streaming kernel up to IMCOM_STACKS_STREAM_MAX stacks and the GEMM above
+ * (default).  Same sums to rounding. */
 #define IMCOM_OPT_STACK_KERNEL 12
 #define IMCOM_STACKS_GEMM 0
 #define IMCOM_STACKS_STREAM 1
+#define IMCOM_STACKS_AUTO 2      /* default: streaming up to IMCOM_STACKS_STREAM_MAX
+                                   stacks, the GEMM above (measured crossover) */
+#define IMCOM_STACKS_STREAM_MAX 32
 /* Inverse 2-D FFT of the lookup tables (imcom_build_Alookup/Blookup): 0 =
  * embedding, cuFFT and shift as separate steps (default); 1 = the library's
  * own transform in two passes that skip the grid's zero lines and fuse the
