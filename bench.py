@@ -579,10 +579,16 @@ def run_ours(args):
         t_ms = avg.get("eig_tridiag") or avg[dom]
         ach = byts / (t_ms * 1e-3) / 1e9
         pk = peaks.get("hbm_gbs", 6650.0)
+        # DRAM bytes of the 108 panel launches of one tridiagonalisation at n = 4096
+        # (profiles/trd_traffic_n4096.md): the trailing matrix stays in L2
+        traffic = 3.024e9 if n == 4096 else None
         roof = {"kernel": "trd_panel_kernel (eigen_A tridiagonalisation)", "bound": "hbm",
                 "achieved": ach, "peak": pk, "unit": "GB/s", "frac": ach / pk,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
-                "algorithmic_bytes": byts, "traffic": None}
+                "algorithmic_bytes": byts, "traffic": traffic,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum over all "
+                                  "panel launches of one tridiagonalisation "
+                                  "(profiles/trd_traffic_n4096.md)"}
     else:
         byts = {"build_A": 8.0 * n * n, "build_B": 8.0 * n * m}.get(dom, 8.0 * n * m)
         ach = byts / (avg[dom] * 1e-3) / 1e9

@@ -351,26 +351,15 @@ __device__ __forceinline__ double& wb_at(double* W, int r, int c) {
   return W[(size_t)(c % CH_WCOLS) * CH_LDB + (r - c)];
 }
 
-// Slot of window column c0 + j given the slot s0 of c0 (j < CH_WCOLS).
-__device__ __forceinline__ int wslot(int s0, int j) {
-  const int sl = s0 + j;
-  return sl >= CH_WCOLS ? sl - CH_WCOLS : sl;
-}
-
-// One task, by one warp (lane i: row r0 + i of the reflector).  The dot
-// products run as four interleaved partial sums (shorter dependent chains).
+// One task, by one warp (lane i: row r0 + i of the reflector).
 __device__ void chase_task(const ChaseArgs& a, double* W, int s, int t, int lane, double* sv,
                            double* sw) {
   const int n = a.n;
   const int r0 = s + 1 + t * SB;
   const int c0 = t == 0 ? s : r0 - SB;
   const int L = min(SB, n - r0);
-  const int s0 = r0 % CH_WCOLS;  // slot of column r0
-  // A(r, r0 + j) = W[wslot(s0, j) * CH_LDB + r - r0 - j]
-  auto dcol = [&](int j) { return W + (size_t)wslot(s0, j) * CH_LDB - (r0 + j); };
   // reflector from A(r0 : r0 + L, c0) (dlarfg)
-  double* colc0 = W + (size_t)(c0 % CH_WCOLS) * CH_LDB - c0;
-  const double x = lane < L ? colc0[r0 + lane] : 0.0;
+  const double x = lane < L ? wb_at(W, r0 + lane, c0) : 0.0;
   double sig2 = lane >= 1 ? x * x : 0.0;
 #pragma unroll
   for (int o = 16; o; o >>= 1) sig2 += __shfl_xor_sync(0xffffffffu, sig2, o);
@@ -383,7 +372,7 @@ __device__ void chase_task(const ChaseArgs& a, double* W, int s, int t, int lane
   }
   const double v = lane == 0 ? 1.0 : (lane < L ? x * scl : 0.0);
   sv[lane] = v;
-  if (lane < L) colc0[r0 + lane] = lane == 0 ? beta : 0.0;
+  if (lane < L) wb_at(W, r0 + lane, c0) = lane == 0 ? beta : 0.0;
   a.V[((size_t)t * n + s) * SB + lane] = v;
   if (lane == 0) a.tau[(size_t)t * n + s] = tau;
   __syncwarp();
@@ -391,37 +380,19 @@ __device__ void chase_task(const ChaseArgs& a, double* W, int s, int t, int lane
   // left: the bulge's other columns c0 + 1 .. r0 - 1, rows r0 .. r0 + L - 1
   if (t > 0 && lane < SB - 1) {
     const int c = c0 + 1 + lane;
-    double* col = W + (size_t)(c % CH_WCOLS) * CH_LDB - c;
-    double w0 = 0.0, w1 = 0.0, w2 = 0.0, w3 = 0.0;
-    int i = 0;
-    for (; i + 3 < L; i += 4) {
-      w0 = fma(sv[i], col[r0 + i], w0);
-      w1 = fma(sv[i + 1], col[r0 + i + 1], w1);
-      w2 = fma(sv[i + 2], col[r0 + i + 2], w2);
-      w3 = fma(sv[i + 3], col[r0 + i + 3], w3);
-    }
-    for (; i < L; ++i) w0 = fma(sv[i], col[r0 + i], w0);
-    const double w = tau * ((w0 + w1) + (w2 + w3));
-    for (int i2 = 0; i2 < L; ++i2) col[r0 + i2] -= sv[i2] * w;
+    double w = 0.0;
+    for (int i = 0; i < L; ++i) w = fma(sv[i], wb_at(W, r0 + i, c), w);
+    w *= tau;
+    for (int i = 0; i < L; ++i) wb_at(W, r0 + i, c) -= sv[i] * w;
   }
   // two-sided on the diagonal block D: D - v w^T - w v^T,
   // p = tau D v, w = p - tau/2 (p^T v) v (dlarfy)
   double y = 0.0;
-  if (lane < L) {
-    const double* own = dcol(lane);  // column r0 + lane: D(j, lane) for j >= lane
-    double y0 = 0.0, y1 = 0.0, y2 = 0.0, y3 = 0.0;
+  if (lane < L)
     for (int j = 0; j < L; ++j) {
-      const double dij = j <= lane ? dcol(j)[r0 + lane] : own[r0 + j];
-      const double t_ = dij * sv[j];
-      switch (j & 3) {
-        case 0: y0 += t_; break;
-        case 1: y1 += t_; break;
-        case 2: y2 += t_; break;
-        default: y3 += t_; break;
-      }
+      const double dij = j <= lane ? wb_at(W, r0 + lane, r0 + j) : wb_at(W, r0 + j, r0 + lane);
+      y = fma(dij, sv[j], y);
     }
-    y = (y0 + y1) + (y2 + y3);
-  }
   const double p = tau * y;
   double pv = p * v;
 #pragma unroll
@@ -430,22 +401,15 @@ __device__ void chase_task(const ChaseArgs& a, double* W, int s, int t, int lane
   sw[lane] = wv;
   __syncwarp();
   if (lane < L)
-    for (int j = 0; j <= lane; ++j) dcol(j)[r0 + lane] -= v * sw[j] + wv * sv[j];
+    for (int j = 0; j <= lane; ++j) wb_at(W, r0 + lane, r0 + j) -= v * sw[j] + wv * sv[j];
   // right: rows r0 + L .. r0 + L + L2 - 1 (the new bulge), columns r0 .. r0 + L - 1
   const int L2 = min(SB, n - (r0 + L));
   if (lane < L2) {
     const int r = r0 + L + lane;
-    double z0 = 0.0, z1 = 0.0, z2 = 0.0, z3 = 0.0;
-    int j = 0;
-    for (; j + 3 < L; j += 4) {
-      z0 = fma(dcol(j)[r], sv[j], z0);
-      z1 = fma(dcol(j + 1)[r], sv[j + 1], z1);
-      z2 = fma(dcol(j + 2)[r], sv[j + 2], z2);
-      z3 = fma(dcol(j + 3)[r], sv[j + 3], z3);
-    }
-    for (; j < L; ++j) z0 = fma(dcol(j)[r], sv[j], z0);
-    const double z = tau * ((z0 + z1) + (z2 + z3));
-    for (int j2 = 0; j2 < L; ++j2) dcol(j2)[r] -= z * sv[j2];
+    double z = 0.0;
+    for (int j = 0; j < L; ++j) z = fma(wb_at(W, r, r0 + j), sv[j], z);
+    z *= tau;
+    for (int j = 0; j < L; ++j) wb_at(W, r, r0 + j) -= z * sv[j];
   }
   __syncwarp();
 }
