@@ -241,6 +241,9 @@ int sm_count(imcom_ctx* ctx);
 // K x N) or 'T' (B is N x K).
 // C (M x M, lower triangle and the tiles crossing the diagonal) = alpha A B^T
 // + beta C with A, B M x K column-major (the symmetric rank-2k update).
+// C (M x 32) = A (M x K) B (K x 32), 'N', 'N' (a tile for 32 output columns).
+int dgemm_nn_skinny32(imcom_ctx* ctx, long long M, long long K, const double* A, long long lda,
+                      const double* B, long long ldb, double* C, long long ldc);
 int dgemm_lower_nt(imcom_ctx* ctx, long long M, long long K, double alpha, const double* A,
                    long long lda, const double* B, long long ldb, double beta, double* C,
                    long long ldc);

@@ -81,6 +81,143 @@ int launch(imcom_ctx* ctx, long long M, long long N, long long K, double alpha, 
   return 0;
 }
 
+// ---------------------------------------------------------------------------
+// C (M x 32) = A (M x K) B (K x 32), A and B column-major ('N', 'N'): the
+// tall-skinny product of a symmetric trailing matrix and a panel's 32
+// reflectors.  The general tile is 128 x 128, so with 32 output columns six
+// of its eight warps would compute nothing; this tile is 128 x 32 with every
+// warp on 16 rows x all 32 columns (four m16n8k4 DMMA tiles), K in steps of
+// SK_BK through a 3-stage cp.async pipeline, split over K into partial
+// slices that splitk_reduce_kernel sums.
+// Shared strides: A stored [k][r] (stride SK_SA), B stored [n][k] (stride
+// SK_SB); both = 4 (mod 16) doubles, so the fragment loads of a half-warp
+// (4 x 4 lanes) hit distinct 8-byte banks.
+// ---------------------------------------------------------------------------
+constexpr int SK_BM = 128, SK_BN = 32, SK_BK = 32, SK_STAGES = 3, SK_THREADS = 256;
+constexpr int SK_SA = SK_BM + 4, SK_SB = SK_BK + 4;
+constexpr int SK_STAGE = SK_BK * SK_SA + SK_BN * SK_SB;
+constexpr size_t SK_SMEM = (size_t)SK_STAGES * SK_STAGE * sizeof(double);
+
+template <int VEC>
+__global__ void __launch_bounds__(SK_THREADS) skinny32_kernel(long long M, long long K,
+                                                              const double* __restrict__ A,
+                                                              long long lda,
+                                                              const double* __restrict__ B,
+                                                              long long ldb, double* __restrict__ C,
+                                                              long long ldc, long long kchunk) {
+  using namespace gemm;
+  extern __shared__ __align__(16) double sk[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const long long m0 = (long long)blockIdx.x * SK_BM;
+  const long long kb = (long long)blockIdx.y * kchunk, ke = min(K, kb + kchunk);
+  C += (size_t)blockIdx.y * (size_t)ldc * SK_BN;  // partial slice
+  const int nk = ke > kb ? (int)((ke - kb + SK_BK - 1) / SK_BK) : 0;
+  auto sA = [&](int st) { return sk + st * SK_STAGE; };
+  auto sB = [&](int st) { return sk + st * SK_STAGE + SK_BK * SK_SA; };
+  auto load = [&](int st, long long k0) {
+    double* a = sA(st);
+    for (int c = threadIdx.x; c < SK_BM * SK_BK / VEC; c += SK_THREADS) {
+      const int kk = c / (SK_BM / VEC), rr = (c % (SK_BM / VEC)) * VEC;
+      const long long r = m0 + rr, k = k0 + kk;
+      const int valid = (k < ke) ? (int)min((long long)VEC, max(0LL, M - r)) : 0;
+      cp_async(a + kk * SK_SA + rr, valid ? A + r + k * lda : A, valid * 8, VEC);
+    }
+    double* b = sB(st);
+    for (int c = threadIdx.x; c < SK_BN * SK_BK / VEC; c += SK_THREADS) {
+      const int nn = c / (SK_BK / VEC), kk = (c % (SK_BK / VEC)) * VEC;
+      const long long k = k0 + kk;
+      const int valid = (int)min((long long)VEC, max(0LL, ke - k));
+      cp_async(b + nn * SK_SB + kk, valid ? B + k + nn * ldb : B, valid * 8, VEC);
+    }
+  };
+  double acc[4][4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+#pragma unroll
+    for (int r = 0; r < 4; ++r) acc[j][r] = 0.0;
+#pragma unroll
+  for (int st = 0; st < SK_STAGES - 1; ++st) {
+    if (st < nk) load(st, kb + (long long)st * SK_BK);
+    cp_commit();
+  }
+  const int mr = warp * 16 + g;
+  for (int kt = 0; kt < nk; ++kt) {
+    cp_wait<SK_STAGES - 2>();
+    __syncthreads();
+    const double* a = sA(kt % SK_STAGES);
+    const double* b = sB(kt % SK_STAGES);
+#pragma unroll
+    for (int kk = 0; kk < SK_BK; kk += 4) {
+      const double a0 = a[(kk + t) * SK_SA + mr], a1 = a[(kk + t) * SK_SA + mr + 8];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const double bv = b[(8 * j + g) * SK_SB + kk + t];
+        asm volatile(
+            "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+            "{%0,%1,%2,%3};\n"
+            : "+d"(acc[j][0]), "+d"(acc[j][1]), "+d"(acc[j][2]), "+d"(acc[j][3])
+            : "d"(a0), "d"(a1), "d"(bv));
+      }
+    }
+    const int nxt = kt + SK_STAGES - 1;
+    if (nxt < nk) load(nxt % SK_STAGES, kb + (long long)nxt * SK_BK);
+    cp_commit();
+  }
+  cp_wait<0>();
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const long long row = m0 + mr + ((r >> 1) ? 8 : 0);
+      const int col = 8 * j + 2 * t + (r & 1);
+      if (row < M) C[row + (size_t)col * ldc] = acc[j][r];
+    }
+}
+
+int dgemm_nn_skinny32(imcom_ctx* ctx, long long M, long long K, const double* A, long long lda,
+                      const double* B, long long ldb, double* C, long long ldc) {
+  if (M <= 0) return 0;
+  const long long gm = (M + SK_BM - 1) / SK_BM;
+  const int sms = sm_count(ctx);
+  int splits = (int)std::max<long long>(1, std::min<long long>((3LL * sms + gm - 1) / gm,
+                                                               K / (2 * SK_BK)));
+  splits = std::min(splits, 32);
+  long long kchunk = (K + splits - 1) / splits;
+  kchunk = std::max<long long>(SK_BK, (kchunk + SK_BK - 1) / SK_BK * SK_BK);
+  splits = (int)std::max<long long>(1, (K + kchunk - 1) / kchunk);
+  double* out = C;
+  long long ldo = ldc;
+  if (splits > 1) {
+    ldo = pad_ld(M);
+    IMC_TRY(ensure_buf(ctx, &ctx->gemm_ws, ctx->gemm_ws_bytes,
+                       (size_t)splits * (size_t)ldo * SK_BN * sizeof(double)));
+    out = (double*)ctx->gemm_ws;
+  }
+  auto al16 = [](const void* p) { return ((uintptr_t)p & 15) == 0; };
+  const bool v2 = al16(A) && al16(B) && lda % 2 == 0 && ldb % 2 == 0;
+  dim3 grd((unsigned)gm, (unsigned)splits);
+  if (v2) {
+    IMC_CUDA(cudaFuncSetAttribute(skinny32_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)SK_SMEM));
+    skinny32_kernel<2><<<grd, SK_THREADS, SK_SMEM, ctx->stream>>>(M, K, A, lda, B, ldb, out, ldo,
+                                                                  kchunk);
+  } else {
+    IMC_CUDA(cudaFuncSetAttribute(skinny32_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)SK_SMEM));
+    skinny32_kernel<1><<<grd, SK_THREADS, SK_SMEM, ctx->stream>>>(M, K, A, lda, B, ldb, out, ldo,
+                                                                  kchunk);
+  }
+  IMC_LAUNCH();
+  if (splits > 1) {
+    dim3 g2((unsigned)std::min<long long>((M + 255) / 256, 64), (unsigned)SK_BN);
+    splitk_reduce_kernel<<<g2, 256, 0, ctx->stream>>>(out, ldo, splits, M, SK_BN, 1.0, 0.0, C,
+                                                      ldc);
+    IMC_LAUNCH();
+  }
+  return 0;
+}
+
 int dgemm_lower_nt(imcom_ctx* ctx, long long M, long long K, double alpha, const double* A,
                    long long lda, const double* B, long long ldb, double beta, double* C,
                    long long ldc) {

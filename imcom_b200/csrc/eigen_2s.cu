@@ -160,34 +160,6 @@ inline size_t panel_smem(int per, bool staged) {
          sizeof(double);
 }
 
-// T (upper triangular, ld SB) of the panel's block reflector from its Gram
-// matrix G = V^T V (ld SB) and tau (LAPACK dlarft, forward, columnwise):
-// T(j,j) = tau_j, T(0:j, j) = -tau_j T(0:j, 0:j) G(0:j, j).  One warp.
-__global__ void sb_larft_kernel(const double* __restrict__ G, const double* __restrict__ tau,
-                                double* __restrict__ T) {
-  __shared__ double sT[SB][SB + 1];
-  __shared__ double sG[SB][SB + 1];  // sG[j][h] = G(h, j)
-  __shared__ double stau[SB];
-  const int r = threadIdx.x;
-  for (int cc = 0; cc < SB; ++cc) {
-    sT[r][cc] = 0.0;
-    sG[cc][r] = G[r + cc * SB];
-  }
-  stau[r] = tau[r];
-  __syncwarp();
-  for (int j = 0; j < SB; ++j) {
-    const double tj = stau[j];
-    double s = 0.0;
-    if (r < j)
-      for (int h = r; h < j; ++h) s += sT[r][h] * sG[j][h];
-    __syncwarp();
-    if (r < j) sT[r][j] = -tj * s;
-    if (r == j) sT[j][j] = tj;
-    __syncwarp();
-  }
-  for (int cc = 0; cc < SB; ++cc) T[r + cc * SB] = sT[r][cc];
-}
-
 // The panel's two-sided update factors from X1 = A22 V (N x SB):
 //   W = X1 T - 1/2 V M2,  M2 = T^T (V^T X1) T     (V^T W = (V^T X1) T),
 // in three launches.  wy_partial_kernel: S_b = V_b^T X1_b for blocks b of
@@ -236,6 +208,39 @@ __global__ void __launch_bounds__(SB * SB) wy_m2_kernel(const double* __restrict
   double m = 0.0;
   for (int h = 0; h <= i; ++h) m = fma(sT[h][i], sU[h][j], m);
   M2[e] = m;
+}
+
+// One CTA of SB * SB threads: G = sum_b Spart_b (the panel's Gram matrix
+// V^T V from wy_partial_kernel's blocks, in a fixed order) and T from G and
+// tau (LAPACK dlarft, forward, columnwise: T(j,j) = tau_j,
+// T(0:j, j) = -tau_j T(0:j, 0:j) G(0:j, j)), by warp 0.
+__global__ void __launch_bounds__(SB * SB) gram_larft_kernel(const double* __restrict__ Spart,
+                                                             int nb,
+                                                             const double* __restrict__ tau,
+                                                             double* __restrict__ T) {
+  __shared__ double sG[SB][SB + 1];  // sG[j][h] = G(h, j)
+  __shared__ double sT[SB][SB + 1];
+  const int e = threadIdx.x, i = e % SB, j = e / SB;
+  double acc = 0.0;
+  for (int b = 0; b < nb; ++b) acc += Spart[(size_t)b * SB * SB + e];
+  sG[j][i] = acc;
+  sT[i][j] = 0.0;
+  __syncthreads();
+  if (threadIdx.x < SB) {
+    const int r = threadIdx.x;
+    for (int jj = 0; jj < SB; ++jj) {
+      const double tj = tau[jj];
+      double sum = 0.0;
+      if (r < jj)
+        for (int h = r; h < jj; ++h) sum += sT[r][h] * sG[jj][h];
+      __syncwarp();
+      if (r < jj) sT[r][jj] = -tj * sum;
+      if (r == jj) sT[jj][jj] = tj;
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  T[e] = sT[i][j];  // column-major: T(i, j) at i + j SB
 }
 
 __global__ void __launch_bounds__(WY_THREADS) wy_finish_kernel(
@@ -625,6 +630,7 @@ constexpr int BT_SVS = 37;  // sv[j][i]: V(j) element i; (S - 1) = 4 mod 16
 constexpr int BT_TS = 36;   // sT[i][h] = T(i, h)
 constexpr int BT_YS = 36;   // sY[j][c]
 constexpr int BT_ZS = 36;   // sZ[slot][row][c]
+
 constexpr size_t BT_SMEM =
     ((size_t)BT_G * BT_SVS + (size_t)BT_G * BT_TS + 2 * (size_t)BT_G * BT_YS +
      2 * 32 * (size_t)BT_ZS) * sizeof(double);
@@ -734,15 +740,19 @@ __global__ void __launch_bounds__(BT_THREADS, 2) bt_apply_kernel(
     // Y = V^T Z: warp -> 16 x 8 tile (rows 16 mt of Y, columns 8 nt)
     {
       const int mt = warp & 1, nt8 = warp >> 1, m0 = 16 * mt, n0 = 8 * nt8;
-      double acc[4] = {0.0, 0.0, 0.0, 0.0};
+      // two independent accumulation chains (halves of K), added at the end
+      double acc[4] = {0.0, 0.0, 0.0, 0.0}, accb[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
       for (int kb = 0; kb < 48; kb += 4) {
         const int r = m0 + kb + tq;
         const int i0 = r - (m0 + gq), i1 = i0 - 8;
         const double a0 = (i0 >= 0 && i0 < SB) ? sv[(m0 + gq) * BT_SVS + i0] : 0.0;
         const double a1 = (i1 >= 0 && i1 < SB) ? sv[(m0 + gq + 8) * BT_SVS + i1] : 0.0;
-        dmma(acc, a0, a1, zrow(r)[n0 + gq]);
+        if (kb < 24) dmma(acc, a0, a1, zrow(r)[n0 + gq]);
+        else dmma(accb, a0, a1, zrow(r)[n0 + gq]);
       }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[q] += accb[q];
       double* y0 = sY + (m0 + gq) * BT_YS + n0 + 2 * tq;
       y0[0] = acc[0];
       y0[1] = acc[1];
@@ -753,13 +763,19 @@ __global__ void __launch_bounds__(BT_THREADS, 2) bt_apply_kernel(
     // -Y2 = -T Y
     {
       const int mt = warp & 1, nt8 = warp >> 1, m0 = 16 * mt, n0 = 8 * nt8;
-      double acc[4] = {0.0, 0.0, 0.0, 0.0};
+      double acc[4] = {0.0, 0.0, 0.0, 0.0}, accb[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
       for (int kb = 0; kb < 32; kb += 4) {
         if (kb + 4 <= m0) continue;  // T(i, h) = 0 for h < i
-        dmma(acc, sT[(m0 + gq) * BT_TS + kb + tq], sT[(m0 + gq + 8) * BT_TS + kb + tq],
-             sY[(kb + tq) * BT_YS + n0 + gq]);
+        if ((kb >> 2) & 1)
+          dmma(accb, sT[(m0 + gq) * BT_TS + kb + tq], sT[(m0 + gq + 8) * BT_TS + kb + tq],
+               sY[(kb + tq) * BT_YS + n0 + gq]);
+        else
+          dmma(acc, sT[(m0 + gq) * BT_TS + kb + tq], sT[(m0 + gq + 8) * BT_TS + kb + tq],
+               sY[(kb + tq) * BT_YS + n0 + gq]);
       }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[q] += accb[q];
       double* y0 = sY2 + (m0 + gq) * BT_YS + n0 + 2 * tq;
       y0[0] = -acc[0];
       y0[1] = -acc[1];
@@ -782,6 +798,7 @@ __global__ void __launch_bounds__(BT_THREADS, 2) bt_apply_kernel(
         acc[h][3] = zr1[cc + 1];
       }
       const int jlo = m0 >= SB ? m0 - SB + 1 : 0, jhi = min(BT_G - 1, m0 + 15);
+      double accb[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
 #pragma unroll
       for (int kb = 0; kb < 32; kb += 4) {
         if (kb + 3 < jlo || kb > jhi) continue;
@@ -790,8 +807,15 @@ __global__ void __launch_bounds__(BT_THREADS, 2) bt_apply_kernel(
         const double a0 = (i0 >= 0 && i0 < SB) ? sv[jj * BT_SVS + i0] : 0.0;
         const double a1 = (i1 >= 0 && i1 < SB) ? sv[jj * BT_SVS + i1] : 0.0;
 #pragma unroll
-        for (int h = 0; h < 2; ++h) dmma(acc[h], a0, a1, sY2[jj * BT_YS + n0 + 8 * h + gq]);
+        for (int h = 0; h < 2; ++h) {
+          if ((kb >> 2) & 1) dmma(accb[h], a0, a1, sY2[jj * BT_YS + n0 + 8 * h + gq]);
+          else dmma(acc[h], a0, a1, sY2[jj * BT_YS + n0 + 8 * h + gq]);
+        }
       }
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[h][q] += accb[h][q];
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         double* zr0 = zrow(m0 + gq);
@@ -895,8 +919,7 @@ int sy2sb_gpu(imcom_ctx* ctx, DMat& Aw, DMat& V, double* tau, double* Tf, double
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
   int ctas = 16;
   IMC_TRY(panel_cluster(ctx, optin, &ctas));
-  double* G = Tf + (size_t)((n + SB - 1) / SB) * SB * SB;  // SB x SB Gram scratch
-  double* M2 = G + SB * SB;                                  // SB x SB
+  double* M2 = Tf + (size_t)((n + SB - 1) / SB) * SB * SB;  // SB x SB scratch after the T factors
   double* Spart = W;  // per-block partials of V^T X1: ceil(N / WY_ROWS) SB^2 <= SB ldw
   for (int k = 0; k + SB < n - 1; k += SB) {
     const int N = n - k - SB;
@@ -925,14 +948,16 @@ int sy2sb_gpu(imcom_ctx* ctx, DMat& Aw, DMat& V, double* tau, double* Tf, double
     const double* Vp = V.p + r0 + (size_t)k * V.ld;  // N x SB
     double* T = Tf + (size_t)(k / SB) * SB * SB;
     double* A22 = Aw.p + r0 + r0 * (size_t)ld;
-    // T from G = V^T V
-    IMC_TRY(dgemm(ctx, 'T', 'N', SB, SB, N, 1.0, Vp, V.ld, Vp, V.ld, 0.0, G, SB));
-    sb_larft_kernel<<<1, SB, 0, ctx->stream>>>(G, tau + k, T);
+    // T from the Gram matrix V^T V (block partials, then one CTA)
+    const int nbg = (N + WY_ROWS - 1) / WY_ROWS;
+    wy_partial_kernel<<<nbg, WY_THREADS, 0, ctx->stream>>>(Vp, V.ld, Vp, V.ld, N, Spart);
+    IMC_LAUNCH();
+    gram_larft_kernel<<<1, SB * SB, 0, ctx->stream>>>(Spart, nbg, tau + k, T);
     IMC_LAUNCH();
     // X1 = A22 V into the first SB columns of XY, then W and the packed
     // operands X = [V | W], Y = [W | V] of the update A22 -= X Y^T
     double* X1 = XY;
-    IMC_TRY(dgemm(ctx, 'N', 'N', N, SB, N, 1.0, A22, ld, Vp, V.ld, 0.0, X1, ldw));
+    IMC_TRY(dgemm_nn_skinny32(ctx, N, N, A22, ld, Vp, V.ld, X1, ldw));
     const int nb = (N + WY_ROWS - 1) / WY_ROWS;
     wy_partial_kernel<<<nb, WY_THREADS, 0, ctx->stream>>>(Vp, V.ld, X1, ldw, N, Spart);
     IMC_LAUNCH();
