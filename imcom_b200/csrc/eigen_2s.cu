@@ -740,19 +740,15 @@ __global__ void __launch_bounds__(BT_THREADS, 2) bt_apply_kernel(
     // Y = V^T Z: warp -> 16 x 8 tile (rows 16 mt of Y, columns 8 nt)
     {
       const int mt = warp & 1, nt8 = warp >> 1, m0 = 16 * mt, n0 = 8 * nt8;
-      // two independent accumulation chains (halves of K), added at the end
-      double acc[4] = {0.0, 0.0, 0.0, 0.0}, accb[4] = {0.0, 0.0, 0.0, 0.0};
+      double acc[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
       for (int kb = 0; kb < 48; kb += 4) {
         const int r = m0 + kb + tq;
         const int i0 = r - (m0 + gq), i1 = i0 - 8;
         const double a0 = (i0 >= 0 && i0 < SB) ? sv[(m0 + gq) * BT_SVS + i0] : 0.0;
         const double a1 = (i1 >= 0 && i1 < SB) ? sv[(m0 + gq + 8) * BT_SVS + i1] : 0.0;
-        if (kb < 24) dmma(acc, a0, a1, zrow(r)[n0 + gq]);
-        else dmma(accb, a0, a1, zrow(r)[n0 + gq]);
+        dmma(acc, a0, a1, zrow(r)[n0 + gq]);
       }
-#pragma unroll
-      for (int q = 0; q < 4; ++q) acc[q] += accb[q];
       double* y0 = sY + (m0 + gq) * BT_YS + n0 + 2 * tq;
       y0[0] = acc[0];
       y0[1] = acc[1];
@@ -763,19 +759,13 @@ __global__ void __launch_bounds__(BT_THREADS, 2) bt_apply_kernel(
     // -Y2 = -T Y
     {
       const int mt = warp & 1, nt8 = warp >> 1, m0 = 16 * mt, n0 = 8 * nt8;
-      double acc[4] = {0.0, 0.0, 0.0, 0.0}, accb[4] = {0.0, 0.0, 0.0, 0.0};
+      double acc[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
       for (int kb = 0; kb < 32; kb += 4) {
         if (kb + 4 <= m0) continue;  // T(i, h) = 0 for h < i
-        if ((kb >> 2) & 1)
-          dmma(accb, sT[(m0 + gq) * BT_TS + kb + tq], sT[(m0 + gq + 8) * BT_TS + kb + tq],
-               sY[(kb + tq) * BT_YS + n0 + gq]);
-        else
-          dmma(acc, sT[(m0 + gq) * BT_TS + kb + tq], sT[(m0 + gq + 8) * BT_TS + kb + tq],
-               sY[(kb + tq) * BT_YS + n0 + gq]);
+        dmma(acc, sT[(m0 + gq) * BT_TS + kb + tq], sT[(m0 + gq + 8) * BT_TS + kb + tq],
+             sY[(kb + tq) * BT_YS + n0 + gq]);
       }
-#pragma unroll
-      for (int q = 0; q < 4; ++q) acc[q] += accb[q];
       double* y0 = sY2 + (m0 + gq) * BT_YS + n0 + 2 * tq;
       y0[0] = -acc[0];
       y0[1] = -acc[1];
@@ -798,7 +788,6 @@ __global__ void __launch_bounds__(BT_THREADS, 2) bt_apply_kernel(
         acc[h][3] = zr1[cc + 1];
       }
       const int jlo = m0 >= SB ? m0 - SB + 1 : 0, jhi = min(BT_G - 1, m0 + 15);
-      double accb[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
 #pragma unroll
       for (int kb = 0; kb < 32; kb += 4) {
         if (kb + 3 < jlo || kb > jhi) continue;
@@ -807,15 +796,8 @@ __global__ void __launch_bounds__(BT_THREADS, 2) bt_apply_kernel(
         const double a0 = (i0 >= 0 && i0 < SB) ? sv[jj * BT_SVS + i0] : 0.0;
         const double a1 = (i1 >= 0 && i1 < SB) ? sv[jj * BT_SVS + i1] : 0.0;
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          if ((kb >> 2) & 1) dmma(accb[h], a0, a1, sY2[jj * BT_YS + n0 + 8 * h + gq]);
-          else dmma(acc[h], a0, a1, sY2[jj * BT_YS + n0 + 8 * h + gq]);
-        }
+        for (int h = 0; h < 2; ++h) dmma(acc[h], a0, a1, sY2[jj * BT_YS + n0 + 8 * h + gq]);
       }
-#pragma unroll
-      for (int h = 0; h < 2; ++h)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) acc[h][q] += accb[h][q];
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         double* zr0 = zrow(m0 + gq);
