@@ -218,14 +218,118 @@ int dgemm_nn_skinny32(imcom_ctx* ctx, long long M, long long K, const double* A,
   return 0;
 }
 
+// ---------------------------------------------------------------------------
+// C = alpha (alpha C + A B^T), alpha = +-1, on the tiles on and below the
+// diagonal, K <= 64: the rank-2b update of a trailing matrix kept in its
+// lower triangle (LAPACK dsyr2k 'L' with A = [V W], B = [W V], alpha = -1).
+// With K this short the 128 x 128 tile is bound by its C round trip and the
+// start of its operand pipeline (a lone tile takes ~27 us for ~9 us of
+// MMAs), and a small trailing matrix has fewer 128-row tiles than SMs.  Here
+// the tile is 64 x 64 (four warps of 32 x 32), all of K is loaded at once,
+// only the lower tiles are launched (a diagonal tile's upper-right quarter is
+// skipped), and three CTAs share an SM so that one's loads overlap another's
+// MMAs.  The accumulators start from alpha C and take the k-steps of 4 in
+// the general tile's order (zero-filled up to a multiple of its BK), so the
+// result is bit-identical to it.
+// ---------------------------------------------------------------------------
+constexpr int LU_T = 64, LU_KMAX = 64, LU_THREADS = 128, LU_S = LU_T + 4;
+constexpr size_t LU_SMEM = (size_t)2 * LU_KMAX * LU_S * sizeof(double);
+
+template <int VEC>
+__global__ void __launch_bounds__(LU_THREADS, 3)
+    lower_update_kernel(long long M, int K, int KP, double alpha, const double* __restrict__ A,
+                        long long lda, const double* __restrict__ B, long long ldb,
+                        double* __restrict__ C, long long ldc) {
+  extern __shared__ __align__(16) double lu[];
+  double* sA = lu;                   // sA[k][r]
+  double* sB = lu + LU_KMAX * LU_S;  // sB[k][c]
+  // lower tile (ti, tj), ti >= tj, from the linear block index
+  const int b = (int)blockIdx.x;
+  int ti = (int)((sqrtf(8.0f * (float)b + 1.0f) - 1.0f) * 0.5f);
+  while ((ti + 1) * (ti + 2) / 2 <= b) ++ti;
+  while (ti > 0 && ti * (ti + 1) / 2 > b) --ti;
+  const int tj = b - ti * (ti + 1) / 2;
+  const long long m0 = (long long)ti * LU_T, n0 = (long long)tj * LU_T;
+  for (int c = threadIdx.x; c < KP * (LU_T / VEC); c += LU_THREADS) {
+    const int kk = c / (LU_T / VEC), rr = (c % (LU_T / VEC)) * VEC;
+    const long long ra = m0 + rr, rb = n0 + rr;
+    const int va = kk < K ? (int)min((long long)VEC, max(0LL, M - ra)) : 0;
+    const int vb = kk < K ? (int)min((long long)VEC, max(0LL, M - rb)) : 0;
+    cp_async(sA + kk * LU_S + rr, va ? A + ra + (long long)kk * lda : A, va * 8, VEC);
+    cp_async(sB + kk * LU_S + rr, vb ? B + rb + (long long)kk * ldb : B, vb * 8, VEC);
+  }
+  cp_commit();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wm = warp & 1, wn = warp >> 1, g = lane >> 2, t = lane & 3;
+  const bool skip = ti == tj && wm < wn;  // above the diagonal
+  double acc[2][4][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const long long row = m0 + wm * 32 + i * 16 + g + ((r >> 1) ? 8 : 0);
+        const long long col = n0 + wn * 32 + j * 8 + 2 * t + (r & 1);
+        acc[i][j][r] = (!skip && row < M && col < M) ? alpha * C[row + col * ldc] : 0.0;
+      }
+  cp_wait<0>();
+  __syncthreads();
+  if (skip) return;
+#pragma unroll 4
+  for (int kk = 0; kk < KP; kk += 4) {
+    double af[2][2], bf[4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int mr = wm * 32 + i * 16 + g;
+      af[i][0] = sA[(kk + t) * LU_S + mr];
+      af[i][1] = sA[(kk + t) * LU_S + mr + 8];
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) bf[j] = sB[(kk + t) * LU_S + wn * 32 + j * 8 + g];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        asm volatile(
+            "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+            "{%0,%1,%2,%3};\n"
+            : "+d"(acc[i][j][0]), "+d"(acc[i][j][1]), "+d"(acc[i][j][2]), "+d"(acc[i][j][3])
+            : "d"(af[i][0]), "d"(af[i][1]), "d"(bf[j]));
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const long long row = m0 + wm * 32 + i * 16 + g + ((r >> 1) ? 8 : 0);
+        const long long col = n0 + wn * 32 + j * 8 + 2 * t + (r & 1);
+        if (row < M && col < M) C[row + col * ldc] = alpha * acc[i][j][r];
+      }
+}
+
 int dgemm_lower_nt(imcom_ctx* ctx, long long M, long long K, double alpha, const double* A,
                    long long lda, const double* B, long long ldb, double beta, double* C,
                    long long ldc) {
   if (M <= 0 || K <= 0) return 0;
+  auto al16 = [](const void* p) { return ((uintptr_t)p & 15) == 0; };
+  const bool v2 = al16(A) && al16(B) && lda % 2 == 0 && ldb % 2 == 0;
+  if (K <= LU_KMAX && beta == 1.0 && (alpha == 1.0 || alpha == -1.0)) {
+    const long long nt = (M + LU_T - 1) / LU_T;
+    const unsigned tiles = (unsigned)(nt * (nt + 1) / 2);
+    const int KP = (int)((K + BK - 1) / BK * BK);
+    auto k = v2 ? lower_update_kernel<2> : lower_update_kernel<1>;
+    IMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LU_SMEM));
+    IMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  (int)cudaSharedmemCarveoutMaxShared));
+    k<<<tiles, LU_THREADS, LU_SMEM, ctx->stream>>>(M, (int)K, KP, alpha, A, lda, B, ldb, C, ldc);
+    IMC_LAUNCH();
+    return 0;
+  }
   const long long g = (M + BM - 1) / BM;
   dim3 grd((unsigned)g, (unsigned)g, 1);
-  auto al16 = [](const void* p) { return ((uintptr_t)p & 15) == 0; };
-  if (al16(A) && al16(B) && lda % 2 == 0 && ldb % 2 == 0) {
+  if (v2) {
     auto k = dgemm_kernel<false, false, 2, true>;
     IMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES));
     k<<<grd, THREADS, SMEM_BYTES, ctx->stream>>>(M, M, K, alpha, A, lda, B, ldb, beta, C, ldc, K);

@@ -221,26 +221,34 @@ EXAMPLE_RMS = 5e-5
 
 
 def lapack_spread(r, prob, ref):
-    """How far the reference's own results move with the LAPACK driver: the
-    same solve on dsyevd's eigenpairs (numpy) instead of dsyevr's, per run,
-    as (S relmax, T column relmax) over the pixels at kappa_min.  There U and
-    T are set by eigenmodes whose eigenvalues are at the rounding level of A,
-    which no two eigensolvers share."""
+    """How far the reference's own results move with the eigensolver: the
+    same solve on dsyevd's eigenpairs (numpy) instead of dsyevr's, of A and of
+    A plus a seeded symmetric perturbation with ||dA||_1 = n eps ||A||_1 (the
+    backward error of a solver at LAPACK's test ratio 1), per run, as the
+    larger (S relmax, T column relmax) over the pixels at kappa_min.  There U
+    and T are set by eigenmodes whose eigenvalues are at the rounding level of
+    A, which no two eigensolvers share; the GPU solver's own result there
+    varies between runs (its reductions add partial sums in arrival order)."""
     from types import SimpleNamespace
-    w, V = np.linalg.eigh(r.A)
-    L2, Q2 = w[::-1].copy(), V[:, ::-1].copy()
-    P2 = Q2.T @ r.B
-    alt = SimpleNamespace(L=L2, Q=Q2, P=P2, P2=P2 * P2, Ndiag=r.Ndiag, C_a=r.C_a,
-                          kappa_min=r.kappa_min, kappa_max=r.kappa_max)
-    out = {}
-    for k, v in EXAMPLE_RUNS.items():
-        a, o = oracle_at(alt, prob, *v), ref[k]
-        at_min = o["K"] <= r.kappa_min
-        if at_min.any():
-            out[k] = (relmax(a["S"][at_min], o["S"][at_min]),
-                      column_rel(a["T"][:, at_min], o["T"][:, at_min]))
-        else:
-            out[k] = (0.0, 0.0)
+    n = r.A.shape[0]
+    rng = np.random.default_rng(11)
+    E = rng.standard_normal((n, n))
+    E = E + E.T
+    norm1 = lambda M: np.abs(M).sum(axis=0).max()
+    E *= n * np.finfo(np.float64).eps * norm1(r.A) / norm1(E)
+    out = {k: (0.0, 0.0) for k in EXAMPLE_RUNS}
+    for A in (r.A, r.A + E):
+        w, V = np.linalg.eigh(A)
+        L2, Q2 = w[::-1].copy(), V[:, ::-1].copy()
+        P2 = Q2.T @ r.B
+        alt = SimpleNamespace(L=L2, Q=Q2, P=P2, P2=P2 * P2, Ndiag=r.Ndiag, C_a=r.C_a,
+                              kappa_min=r.kappa_min, kappa_max=r.kappa_max)
+        for k, v in EXAMPLE_RUNS.items():
+            a, o = oracle_at(alt, prob, *v), ref[k]
+            at_min = o["K"] <= r.kappa_min
+            if at_min.any():
+                out[k] = (max(out[k][0], relmax(a["S"][at_min], o["S"][at_min])),
+                          max(out[k][1], column_rel(a["T"][:, at_min], o["T"][:, at_min])))
     return out
 
 
@@ -275,9 +283,11 @@ def central_rms(H, ideal):
 @pytest.mark.parametrize("fast", [False, True], ids=["plain_fp64", "split"])
 def test_example_solve_vs_oracle(solver, example, fast, run):
     """The bars on every pixel with kappa > kappa_min; at kappa_min (129
-    pixels of the U < 1e-6 run) S and T within twice the spread between two
-    LAPACK drivers on the same A (1.1e-4 and 5.2e-4 when measured), where
-    the reference itself is not reproducible to the bars."""
+    pixels of the U < 1e-6 run) S and T within the spread of the reference's
+    own results between two LAPACK drivers and under a backward error of
+    n eps ||A||_1 (S 1.8e-3, T 1.0e-2 when measured; the two drivers alone,
+    which share one Householder reduction, differ by 4e-5 to 1.1e-4 and
+    5e-4), where the reference itself is not reproducible to the bars."""
     prob, r, ref, ideal, spread = example
     UnotS, US, tol = EXAMPLE_RUNS[run]
     from imcom_b200 import EIGH_DC
@@ -298,8 +308,8 @@ def test_example_solve_vs_oracle(solver, example, fast, run):
     assert relmax(g.K, o["K"]) <= 1e-6 and relmax(g.U, o["U"]) <= 1e-6
     if at_min.any():
         s_spread, t_spread = spread[run]
-        assert relmax(g.S[at_min], o["S"][at_min]) <= max(1e-6, 2 * s_spread)
-        assert column_rel(g.T[:, at_min], o["T"][:, at_min]) <= max(1e-8, 2 * t_spread)
+        assert relmax(g.S[at_min], o["S"][at_min]) <= max(1e-6, s_spread)
+        assert column_rel(g.T[:, at_min], o["T"][:, at_min]) <= max(1e-8, t_spread)
     # every accepted kappa keeps U (or Sigma) below the target
     assert np.all(g.US[g.nevals > 1] < US)
     if UnotS:
