@@ -42,11 +42,25 @@ int launch(imcom_ctx* ctx, long long M, long long N, long long K, double alpha, 
            int vec) {
   long long gm = (M + BM - 1) / BM, gn = (N + BN - 1) / BN;
   int sms = sm_count(ctx);
-  // Split K when the output tiles cannot fill the GPU and K is long.
+  // Split K when the output tiles cannot fill the GPU and K is long: the
+  // number of slices (<= 16, >= 4 k-steps each) that minimises waves x
+  // k-steps per CTA (one CTA per SM), plus the reduction's pass over the
+  // slices and its launch in the same units (a k-step is ~2.2 us, the
+  // reduction moves ~6 GB/s per us).
   int splits = 1;
   if (gm * gn < sms && K >= 8 * BK) {
-    splits = (int)std::min<long long>((2LL * sms + gm * gn - 1) / (gm * gn), K / (4 * BK));
-    splits = std::max(1, std::min(splits, 16));
+    const long long tiles = gm * gn, ksteps = (K + BK - 1) / BK;
+    double best = 0.0;
+    for (int s = 1; s <= 16 && ksteps >= 4LL * s; ++s) {
+      const long long waves = (tiles * s + sms - 1) / sms;
+      const long long per = (ksteps + s - 1) / s;
+      double cost = (double)(waves * per);
+      if (s > 1) cost += 1.5 + (double)(s + 1) * (double)M * (double)N * 8.0 / 6e3 / 2.2e3;
+      if (s == 1 || cost < best) {
+        best = cost;
+        splits = s;
+      }
+    }
   }
   long long kchunk = (K + splits - 1) / splits;
   kchunk = (kchunk + BK - 1) / BK * BK;

@@ -995,12 +995,22 @@ __global__ void __launch_bounds__(256) dc_deflate_kernel(const Node* nodes, DcWo
           pp = pj;
           continue;
         }
-        double sv = zp, cv = zj;
-        const double tau = hypot(cv, sv);
         const double t = dj - dp;
-        cv /= tau;
-        sv = -sv / tau;
-        if (fabs(t * cv * sv) <= tol) {
+        // |t c s| = |t zj zp| / (zj^2 + zp^2).  Far above tol (the usual
+        // case) the pair is kept without the square root and divisions; the
+        // factor 4 covers the rounding of both sides (a normal right-hand
+        // side keeps the products out of the subnormal range), so the
+        // decision is the one the exact test below makes.
+        const double far = 4.0 * tol * fma(zj, zj, zp * zp);
+        bool rotate = false;
+        double cv = zj, sv = zp, tau = 0.0;
+        if (!(far >= 2.2250738585072014e-308 && fabs(t * zj * zp) > far)) {
+          tau = hypot(cv, sv);
+          cv /= tau;
+          sv = -sv / tau;
+          rotate = fabs(t * cv * sv) <= tol;
+        }
+        if (rotate) {
           wk.rcol[s + nrot] = make_int2(pp, pj);
           wk.rcs[s + nrot] = make_double2(cv, sv);
           ++nrot;
