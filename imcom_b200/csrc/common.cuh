@@ -7,6 +7,7 @@
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -214,6 +215,13 @@ int psf_r2c_own(imcom_ctx* ctx, int n, int count, const double* in, double2* H, 
 int table_fft_inverse(imcom_ctx* ctx, int nps, int L, int ntab, const int2* dpairs, double2* W,
                       double* tab, int isB, bool* done);
 int ensure_buf(imcom_ctx* ctx, void** p, size_t& have, size_t need);
+// Held around every device allocation and free, every cuFFT plan creation
+// and every stream capture of the process.  cudaFree synchronises the device
+// and cuFFT's planning allocates and frees; either one in a thread while
+// another thread captures a graph can fail or invalidate the capture, so
+// contexts on several host threads take turns at them.  Recursive: a capture
+// may allocate.
+std::recursive_mutex& alloc_mutex();
 // `batch` contiguous 2-D side x side transforms on the context's stream
 // through the process-wide plan cache: in place complex-to-complex
 // (dir = CUFFT_FORWARD / CUFFT_INVERSE), or real side^2 -> side*(side/2+1)

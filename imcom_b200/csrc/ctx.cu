@@ -23,8 +23,14 @@ int set_err(imcom_ctx* c, int code, const char* fmt, ...) {
   return code;
 }
 
+std::recursive_mutex& alloc_mutex() {
+  static std::recursive_mutex mu;
+  return mu;
+}
+
 int ensure_buf(imcom_ctx* ctx, void** p, size_t& have, size_t need) {
   if (*p && have >= need) return 0;
+  std::lock_guard<std::recursive_mutex> lk(alloc_mutex());
   if (*p) cudaFree(*p);
   *p = nullptr;
   have = 0;
@@ -71,6 +77,7 @@ int fft_exec(imcom_ctx* ctx, cufftType type, int side, int batch, void* in, void
     if (f.dev == ctx->device && f.type == (int)type && f.side == side && f.batch == batch) hit = i;
   }
   if (hit == g_fft_plans.size()) {
+    std::lock_guard<std::recursive_mutex> lk_alloc(alloc_mutex());
     if (g_fft_plans.size() >= kMaxPlans) {
       size_t lru = 0;
       for (size_t i = 1; i < g_fft_plans.size(); ++i)
@@ -129,10 +136,12 @@ void fft_free(imcom_ctx* ctx) {
     std::lock_guard<std::mutex> lk(g_fft_mu);
     if (--g_fft_contexts == 0) {
       // every context's stream has drained (destroy synchronises first)
+      std::lock_guard<std::recursive_mutex> lk_alloc(alloc_mutex());
       for (auto& f : g_fft_plans) cufftDestroy(f.h);
       g_fft_plans.clear();
     }
   }
+  std::lock_guard<std::recursive_mutex> lk(alloc_mutex());
   if (ctx->fft_work) cudaFree(ctx->fft_work);
   ctx->fft_work = nullptr;
   ctx->fft_work_bytes = 0;
@@ -148,6 +157,7 @@ int ensure_mat(imcom_ctx* ctx, DMat& M, long long rows, long long cols) {
     M.ld = ld;
     return 0;
   }
+  std::lock_guard<std::recursive_mutex> lk(alloc_mutex());
   if (M.p) cudaFree(M.p);
   M.p = nullptr;
   M.cap = 0;
@@ -170,6 +180,7 @@ int ensure_vec(imcom_ctx* ctx, T** p, size_t count) {
   const size_t need = count * sizeof(T) + 256;
   size_t& cap = ctx->vec_cap[reinterpret_cast<void**>(p)];
   if (*p && cap >= need) return 0;
+  std::lock_guard<std::recursive_mutex> lk(alloc_mutex());
   if (*p) cudaFree(*p);
   *p = nullptr;
   cap = 0;
@@ -292,14 +303,22 @@ int imcom_gpu_create(int device, imcom_ctx** out) {
     delete ctx;
     return IMCOM_ERR_CUDA;
   }
-  if (cudaMalloc(&ctx->flags, 64 * sizeof(int)) != cudaSuccess) {
-    cudaGetLastError();
-    cudaStreamDestroy(ctx->stream);
-    delete ctx;
-    return IMCOM_ERR_ALLOC;
+  {
+    std::lock_guard<std::recursive_mutex> lk(alloc_mutex());
+    if (cudaMalloc(&ctx->flags, 64 * sizeof(int)) != cudaSuccess) {
+      cudaGetLastError();
+      cudaStreamDestroy(ctx->stream);
+      delete ctx;
+      return IMCOM_ERR_ALLOC;
+    }
   }
-  cudaMemset(ctx->flags, 0, 64 * sizeof(int));
   fft_attach();
+  if (cudaMemsetAsync(ctx->flags, 0, 64 * sizeof(int), ctx->stream) != cudaSuccess ||
+      cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+    cudaGetLastError();
+    imcom_gpu_destroy(ctx);
+    return IMCOM_ERR_CUDA;
+  }
   *out = ctx;
   return 0;
 }
@@ -308,16 +327,20 @@ int imcom_gpu_destroy(imcom_ctx* ctx) {
   if (!ctx) return 0;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
-  eig_free(ctx);
-  split_release(ctx);
-  void* ptrs[] = {ctx->x, ctx->y, ctx->X, ctx->Y, ctx->I, ctx->Nd, ctx->exp_i, ctx->G,
-                  ctx->Gamma, ctx->Gt, ctx->Gammat, ctx->A.p, ctx->Q.p, ctx->B.p, ctx->P.p,
-                  ctx->T.p, ctx->Pt.p, ctx->L, ctx->K, ctx->US, ctx->H, ctx->S, ctx->U,
-                  ctx->nev, ctx->flags, ctx->tables, ctx->fftbuf, ctx->mlp.w, ctx->feat, ctx->guess,
-                  ctx->gemm_ws, ctx->fb, ctx->train_buf, ctx->band, ctx->jac_buf,
-                  ctx->stacks.p, ctx->stack_H.p, ctx->fft_tw, ctx->r2c_tw, ctx->nbr, ctx->band_seg};
-  for (void* p : ptrs)
-    if (p) cudaFree(p);
+  {
+    // released before fft_free, which takes the plan cache's lock first
+    std::lock_guard<std::recursive_mutex> lk(alloc_mutex());
+    eig_free(ctx);
+    split_release(ctx);
+    void* ptrs[] = {ctx->x, ctx->y, ctx->X, ctx->Y, ctx->I, ctx->Nd, ctx->exp_i, ctx->G,
+                    ctx->Gamma, ctx->Gt, ctx->Gammat, ctx->A.p, ctx->Q.p, ctx->B.p, ctx->P.p,
+                    ctx->T.p, ctx->Pt.p, ctx->L, ctx->K, ctx->US, ctx->H, ctx->S, ctx->U,
+                    ctx->nev, ctx->flags, ctx->tables, ctx->fftbuf, ctx->mlp.w, ctx->feat, ctx->guess,
+                    ctx->gemm_ws, ctx->fb, ctx->train_buf, ctx->band, ctx->jac_buf,
+                    ctx->stacks.p, ctx->stack_H.p, ctx->fft_tw, ctx->r2c_tw, ctx->nbr, ctx->band_seg};
+    for (void* p : ptrs)
+      if (p) cudaFree(p);
+  }
   delete[] ctx->rot;
   fft_free(ctx);
   for (int s = 0; s < ST_N; ++s) {
@@ -595,6 +618,7 @@ int imcom_gpu_free_AB(imcom_ctx* ctx) {
   if (!ctx) return -1;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  std::lock_guard<std::recursive_mutex> lk(alloc_mutex());
   if (ctx->A.p) cudaFree(ctx->A.p);
   if (ctx->B.p) cudaFree(ctx->B.p);
   ctx->A = DMat();

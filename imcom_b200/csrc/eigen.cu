@@ -58,6 +58,7 @@ int copy_mat(imcom_ctx* ctx, const double* A, long long lda, double* B, long lon
 void eig_free(imcom_ctx* ctx) {
   if (!ctx->eig) return;
   EigWork* w = ctx->eig;
+  std::lock_guard<std::recursive_mutex> lk(alloc_mutex());
   if (w->W.p) cudaFree(w->W.p);
   if (w->w) cudaFree(w->w);
   if (w->Z.p) cudaFree(w->Z.p);

@@ -1494,12 +1494,17 @@ static int sytrd_gpu(imcom_ctx* ctx, DMat& Aw, DMat& Vall, double* d, double* e,
     // second call at this key: capture, instantiate, launch
     cudaGraph_t graph = nullptr;
     const unsigned long long l0 = __atomic_load_n(&g_launches, __ATOMIC_RELAXED);
-    bool ok = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed) == cudaSuccess;
-    int st = 0;
-    if (ok) {
-      st = sytrd_launches(ctx, Aw, Vall, d, e, tau, W, ldw, ypart, ycol, ldy, accbuf, spin, XY,
-                          tail_ctas, tail_max, true);
-      ok = cudaStreamEndCapture(ctx->stream, &graph) == cudaSuccess && st == 0 && graph;
+    bool ok;
+    {
+      // no other thread frees, allocates or plans while this stream captures
+      std::lock_guard<std::recursive_mutex> lk(alloc_mutex());
+      ok = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed) == cudaSuccess;
+      int st = 0;
+      if (ok) {
+        st = sytrd_launches(ctx, Aw, Vall, d, e, tau, W, ldw, ypart, ycol, ldy, accbuf, spin,
+                            XY, tail_ctas, tail_max, true);
+        ok = cudaStreamEndCapture(ctx->stream, &graph) == cudaSuccess && st == 0 && graph;
+      }
     }
     cudaGraphExec_t exec = nullptr;
     if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;

@@ -703,6 +703,7 @@ int split_check_error(imcom_ctx* ctx) {
 }
 
 void split_free(SplitOp& op) {
+  std::lock_guard<std::recursive_mutex> lk(alloc_mutex());
   if (op.dig) cudaFree(op.dig);
   if (op.scale) cudaFree(op.scale);
   if (op.exps) cudaFree(op.exps);

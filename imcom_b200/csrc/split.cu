@@ -378,6 +378,7 @@ int build_T_split(imcom_ctx* ctx) {
 }
 
 void split_release(imcom_ctx* ctx) {
+  std::lock_guard<std::recursive_mutex> lk(alloc_mutex());
   split_free(ctx->sq_P);
   split_free(ctx->sq_T);
   split_free(ctx->sb_P);

@@ -385,8 +385,9 @@ int psf_r2c_own(imcom_ctx* ctx, int n, int count, const double* in, double2* H, 
     IMC_CUDA(cudaStreamSynchronize(ctx->stream));  // no launch still reads the old table
     IMC_TRY(ensure_buf(ctx, (void**)&ctx->r2c_tw, ctx->r2c_tw_bytes, (size_t)n * sizeof(double2)));
     const std::vector<double2> tw = twiddles(n);
-    IMC_CUDA(cudaMemcpy(ctx->r2c_tw, tw.data(), (size_t)n * sizeof(double2),
-                        cudaMemcpyHostToDevice));
+    IMC_CUDA(cudaMemcpyAsync(ctx->r2c_tw, tw.data(), (size_t)n * sizeof(double2),
+                             cudaMemcpyHostToDevice, ctx->stream));
+    IMC_CUDA(cudaStreamSynchronize(ctx->stream));
     ctx->r2c_tw_L = n;
   }
   const int smem = plan.TP * plan.LS * (int)sizeof(double2);
@@ -415,8 +416,9 @@ int table_fft_inverse(imcom_ctx* ctx, int nps, int L, int ntab, const int2* dpai
     IMC_CUDA(cudaStreamSynchronize(ctx->stream));  // no launch still reads the old table
     IMC_TRY(ensure_buf(ctx, (void**)&ctx->fft_tw, ctx->fft_tw_bytes, (size_t)L * sizeof(double2)));
     const std::vector<double2> tw = twiddles(L);
-    IMC_CUDA(cudaMemcpy(ctx->fft_tw, tw.data(), (size_t)L * sizeof(double2),
-                        cudaMemcpyHostToDevice));
+    IMC_CUDA(cudaMemcpyAsync(ctx->fft_tw, tw.data(), (size_t)L * sizeof(double2),
+                             cudaMemcpyHostToDevice, ctx->stream));
+    IMC_CUDA(cudaStreamSynchronize(ctx->stream));
     ctx->fft_tw_L = L;
   }
   const int smem = plan.TP * plan.LS * (int)sizeof(double2);
