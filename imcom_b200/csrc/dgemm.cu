@@ -6,11 +6,12 @@
 // eigensolver's blocked updates.
 //
 // sm_100a has no tcgen05 kind for f64, so the FP64 tensor instruction is the
-// warp-level DMMA  mma.sync.m16n8k4.f64.  CTA tile 128 x 128 x 16, 8 warps
+// warp-level DMMA  mma.sync.m16n8k4.f64.  CTA tile 128 x 128 x 32, 8 warps
 // as 2 (M) x 4 (N), warp tile 64 x 32 = 4 x 4 MMAs per k-step of 4.
-// Operands stream through a 3-stage cp.async shared-memory pipeline; the
-// shared layouts are padded so every fragment load is bank-conflict free
-// (stride 20 doubles for k-contiguous tiles, 132 for m/n-contiguous ones).
+// Operands stream through a 3-stage cp.async shared-memory pipeline (216 KB,
+// one CTA per SM, one barrier per 32 of K); the shared layouts are padded so
+// every fragment load is bank-conflict free (stride 36 doubles for
+// k-contiguous tiles, 132 for m/n-contiguous ones).
 #include <algorithm>
 
 #include "common.cuh"
@@ -45,8 +46,8 @@ int launch(imcom_ctx* ctx, long long M, long long N, long long K, double alpha, 
   // Split K when the output tiles cannot fill the GPU and K is long: the
   // number of slices (<= 16, >= 4 k-steps each) that minimises waves x
   // k-steps per CTA (one CTA per SM), plus the reduction's pass over the
-  // slices and its launch in the same units (a k-step is ~2.2 us, the
-  // reduction moves ~6 GB/s per us).
+  // slices and its launch in the same units (a k-step of BK is ~0.14 BK us,
+  // the reduction moves ~6 GB/s per us).
   int splits = 1;
   if (gm * gn < sms && K >= 8 * BK) {
     const long long tiles = gm * gn, ksteps = (K + BK - 1) / BK;
@@ -55,7 +56,8 @@ int launch(imcom_ctx* ctx, long long M, long long N, long long K, double alpha, 
       const long long waves = (tiles * s + sms - 1) / sms;
       const long long per = (ksteps + s - 1) / s;
       double cost = (double)(waves * per);
-      if (s > 1) cost += 1.5 + (double)(s + 1) * (double)M * (double)N * 8.0 / 6e3 / 2.2e3;
+      const double step_us = 0.14 * BK;
+      if (s > 1) cost += (3.3 + (double)(s + 1) * (double)M * (double)N * 8.0 / 6e6) / step_us;
       if (s == 1 || cost < best) {
         best = cost;
         splits = s;

@@ -8,10 +8,10 @@
 namespace imcom {
 namespace gemm {
 
-constexpr int BM = 128, BN = 128, BK = 16, STAGES = 3, THREADS = 256;
+constexpr int BM = 128, BN = 128, BK = 32, STAGES = 3, THREADS = 256;
 constexpr int SKC = BK + 4;   // stride of a k-contiguous tile row
 constexpr int SMC = BM + 4;   // stride of an m/n-contiguous tile row
-constexpr int TILE_DBL = (BM * SKC > BK * SMC) ? BM * SKC : BK * SMC;  // 2560
+constexpr int TILE_DBL = (BM * SKC > BK * SMC) ? BM * SKC : BK * SMC;  // 4608
 constexpr int STAGE_DBL = 2 * TILE_DBL;
 constexpr size_t SMEM_BYTES = (size_t)STAGES * STAGE_DBL * sizeof(double);
 
