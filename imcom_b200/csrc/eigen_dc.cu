@@ -166,6 +166,7 @@ struct TrdArgs {
   int stall;  // test of the bounded barrier: the first barrier never completes
 };
 
+template <bool CACHED>
 __global__ void __launch_bounds__(TRD_THREADS, 1) trd_panel_kernel(TrdArgs a) {
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   constexpr int WPB = TRD_THREADS / 32;
@@ -208,9 +209,16 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) trd_panel_kernel(TrdArgs a) {
     const int par = i & 1;
     TrdAcc* cur = a.acc + par;
     TrdAcc* nxt = a.acc + (par ^ 1);
+    // The tiles cover the trailing matrix of column jg: this column, or for
+    // the cached variant the panel's first column k, so that every warp
+    // keeps the same tiles (in its shared-memory slots) through the panel
+    // and only x changes; x is zero left of and above column j+1 there, and
+    // the chunks wholly left of it (ch < chf) are skipped.
+    const long long jg = CACHED ? k : j;
+    const long long chf = (j - jg) / CW;
     // rows handled in pairs from an even base row so the loads are 16-byte
-    const long long rbase = (j + 1) & ~1LL;
-    const long long R = n - (j + 1);
+    const long long rbase = (jg + 1) & ~1LL;
+    const long long R = n - (jg + 1);
     const long long RB = (n - rbase + TR - 1) / TR, NC = (R + CW - 1) / CW;
     // Tiles on or below the diagonal: row block rb (TR rows from rbase +
     // TR rb) with column chunks ch < min(NC, CPB (rb + 1)), counted row block
@@ -241,9 +249,22 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) trd_panel_kernel(TrdArgs a) {
         ch = (int)(t2 - qq * nc);
       }
     };
+    // x's segments for tile (rb, ch): rows r, r + 1 and columns c0 ..
+    auto issue_x = [&](int rb, int ch, int slot) {
+      const long long r = rbase + (long long)rb * TR + 2 * lane;
+      const long long c0 = jg + 1 + (long long)ch * CW, c1 = min((long long)n, c0 + CW);
+      double* dst = wbuf + slot * TRD_SLOT + 2 * lane;
+      const bool okr = r < n;
+      cp_async16(dst + CW * TR, okr ? colj + r : A, okr ? (r + 1 < n ? 16 : 8) : 0);
+      if (lane < CW) {
+        const bool okc = c0 + lane < c1;
+        cp_async8(wbuf + slot * TRD_SLOT + CW * TR + TR + lane, okc ? colj + c0 + lane : A,
+                  okc ? 8 : 0);
+      }
+    };
     auto issue = [&](int rb, int ch, int slot) {
       const long long r = rbase + (long long)rb * TR + 2 * lane;
-      const long long c0 = j + 1 + (long long)ch * CW, c1 = min((long long)n, c0 + CW);
+      const long long c0 = jg + 1 + (long long)ch * CW, c1 = min((long long)n, c0 + CW);
       double* dst = wbuf + slot * TRD_SLOT + 2 * lane;
 #pragma unroll
       for (int u = 0; u < CW; ++u) {
@@ -268,16 +289,29 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) trd_panel_kernel(TrdArgs a) {
     // tile loop.
     // decoded indices of this warp's next two tiles
     int rb_n = 0, ch_n = 0, rb_m = 0, ch_m = 0;
-    if (gw < ntiles) {
-      decode((int)gw, rb_n, ch_n);
-      issue(rb_n, ch_n, 0);
+    if constexpr (CACHED) {
+      // the warp's tiles (at most TRD_SLOTS) sit in slots 0, 1, .. for the
+      // whole panel: the first column loads them, every column its x
+      int q = 0;
+      for (long long tile = gw; tile < ntiles; tile += GW, ++q) {
+        int rb, ch;
+        decode((int)tile, rb, ch);
+        if (i == 0) issue(rb, ch, q);
+        else issue_x(rb, ch, q);
+      }
+      cp_commit();
+    } else {
+      if (gw < ntiles) {
+        decode((int)gw, rb_n, ch_n);
+        issue(rb_n, ch_n, 0);
+      }
+      cp_commit();
+      if (gw + GW < ntiles) {
+        decode((int)(gw + GW), rb_m, ch_m);
+        issue(rb_m, ch_m, 1);
+      }
+      cp_commit();
     }
-    cp_commit();
-    if (gw + GW < ntiles) {
-      decode((int)(gw + GW), rb_m, ch_m);
-      issue(rb_m, ch_m, 1);
-    }
-    cp_commit();
     const double alpha = ld_cg(A + (j + 1) + (long long)j * lda);
     const double xn2 = ld_cg(&cur->nrm);
     // A(j+1, j+1) before this column's phase B rewrites column j+1
@@ -306,25 +340,19 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) trd_panel_kernel(TrdArgs a) {
     // kinds.  x^T A22 x is summed per warp, then per CTA, and added with one
     // atomic per CTA. ----
     double vty_part = 0.0;
-    int slot = 0;
-    for (long long tile = gw; tile < ntiles; tile += GW, slot = (slot + 1) % TRD_SLOTS) {
-      const int rb = rb_n, ch = ch_n;
-      rb_n = rb_m;
-      ch_n = ch_m;
-      if (tile + 2 * GW < ntiles) {
-        decode((int)(tile + 2 * GW), rb_m, ch_m);
-        issue(rb_m, ch_m, (slot + 2) % TRD_SLOTS);
-      }
-      cp_commit();
-      cp_wait_2();
+    // Tile (rb, ch) in `slot`: row sums to ypart[ch], column sums to
+    // ycol[rb], its share of x^T A22 x to vty_part.
+    auto sum_tile = [&](int rb, int ch, int slot) {
       const long long r = rbase + (long long)rb * TR + 2 * lane;
-      const long long c0 = j + 1 + (long long)ch * CW, c1 = min((long long)n, c0 + CW);
+      const long long c0 = jg + 1 + (long long)ch * CW, c1 = min((long long)n, c0 + CW);
       const double* sl = wbuf + slot * TRD_SLOT;
       const double2 vraw = reinterpret_cast<const double2*>(sl + CW * TR)[lane];
       // raw column-j values at rows r, r + 1 and at columns c0 .. c0 + CW - 1
-      // (zero-filled past row n); only row j (when rbase = j) lies above x
+      // (zero-filled past row n); rows at or above j lie above x (only row j
+      // when rbase = j; the cached tiles' columns at or left of j are zeroed
+      // before the tile is summed)
       const double* vcol = sl + CW * TR + TR;
-      const double v0 = (r <= j) ? 0.0 : vraw.x, v1 = vraw.y;
+      const double v0 = (r <= j) ? 0.0 : vraw.x, v1 = (r + 1 <= j) ? 0.0 : vraw.y;
       const double2* av = reinterpret_cast<const double2*>(sl) + lane;
       const int dr = (int)(r - c0);  // this lane's first row relative to column c0
       double acc0 = 0.0, acc1 = 0.0, vtz = 0.0;
@@ -376,6 +404,35 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) trd_panel_kernel(TrdArgs a) {
       if (r >= j + 1 && r < n) a.ypart[(long long)ch * a.ldy + r] = acc0;
       if (r + 1 >= j + 1 && r + 1 < n) a.ypart[(long long)ch * a.ldy + r + 1] = acc1;
       vty_part += v0 * acc0 + v1 * acc1 + vtz;
+    };
+    if constexpr (CACHED) {
+      cp_wait_0();
+      __syncwarp();
+      int q = 0;
+      for (long long tile = gw; tile < ntiles; tile += GW, ++q) {
+        int rb, ch;
+        decode((int)tile, rb, ch);
+        if (ch < chf) continue;  // every column left of j+1: x is zero
+        const long long c0 = jg + 1 + (long long)ch * CW;
+        double* vc = wbuf + q * TRD_SLOT + CW * TR + TR;
+        if (lane < CW && c0 + lane <= j) vc[lane] = 0.0;
+        __syncwarp();
+        sum_tile(rb, ch, q);
+      }
+    } else {
+      int slot = 0;
+      for (long long tile = gw; tile < ntiles; tile += GW, slot = (slot + 1) % TRD_SLOTS) {
+        const int rb = rb_n, ch = ch_n;
+        rb_n = rb_m;
+        ch_n = ch_m;
+        if (tile + 2 * GW < ntiles) {
+          decode((int)(tile + 2 * GW), rb_m, ch_m);
+          issue(rb_m, ch_m, (slot + 2) % TRD_SLOTS);
+        }
+        cp_commit();
+        cp_wait_2();
+        sum_tile(rb, ch, slot);
+      }
     }
     cp_wait_0();
     // Householder reflector of x = A(j+1:n, j) (LAPACK dlarfg)
@@ -419,7 +476,8 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) trd_panel_kernel(TrdArgs a) {
     // block's partial sums
     double y1 = 0.0;
     if (wib == 0) {
-      if (lane < min(NC, (long long)CPB)) y1 = __ldcg(a.ypart + lane * a.ldy + (j + 1));
+      if (lane >= chf && lane < min(NC, (long long)CPB))
+        y1 = __ldcg(a.ypart + lane * a.ldy + (j + 1));
       for (long long q = lane; q < RB; q += 32) y1 += __ldcg(a.ycol + q * a.ldy + (j + 1));
     }
     for (long long rb = blockIdx.x; j + 1 + rb * 32 < n; rb += gridDim.x) {
@@ -433,9 +491,9 @@ __global__ void __launch_bounds__(TRD_THREADS, 1) trd_panel_kernel(TrdArgs a) {
         // row sums of the chunks its row block covers, column sums of the
         // row blocks below its chunk
         const long long ncr = min(NC, (long long)CPB * ((r - rbase) / TR + 1));
-        const long long rb0 = (r - (j + 1)) / CW / CPB;
+        const long long rb0 = (r - (jg + 1)) / CW / CPB;
 #pragma unroll 4
-        for (long long ch = wib; ch < ncr; ch += WPB) ys += __ldcg(a.ypart + ch * a.ldy + r);
+        for (long long ch = chf + wib; ch < ncr; ch += WPB) ys += __ldcg(a.ypart + ch * a.ldy + r);
 #pragma unroll 4
         for (long long q = rb0 + wib; q < RB; q += WPB) ys += __ldcg(a.ycol + q * a.ldy + r);
 #pragma unroll
@@ -1418,8 +1476,17 @@ static int sytrd_launches(imcom_ctx* ctx, DMat& Aw, DMat& Vall, double* d, doubl
     TrdArgs a{Aw.p, Aw.ld, Vall.p, Vall.ld, W, ldw, d, e, tau, ypart, ycol, ldy, acc, sync, n,
               k, b, spin, (ctx->stall_test & IMCOM_STALL_TRIDIAG) ? 1 : 0};
     void* args[] = {&a};
-    IMC_CUDA(cudaLaunchCooperativeKernel((void*)trd_panel_kernel, grid, TRD_THREADS, args,
-                                         TRD_SMEM, ctx->stream));
+    // Tiles of the panel's first trailing matrix: when every warp has at
+    // most TRD_SLOTS of them, they stay in shared memory for the panel's
+    // columns (read from L2 once per panel instead of once per column).
+    const long long rbase = (k + 1) & ~1LL, R = n - (k + 1);
+    const long long RB = (n - rbase + TR - 1) / TR, NC = (R + CW - 1) / CW;
+    const long long rbc = std::min(RB, std::max(0LL, (NC - 1) / CPB));
+    const long long ntiles = (long long)CPB * rbc * (rbc + 1) / 2 + (RB - rbc) * NC;
+    const bool cached = ntiles <= (long long)TRD_SLOTS * grid * (TRD_THREADS / 32);
+    IMC_CUDA(cudaLaunchCooperativeKernel(
+        cached ? (void*)trd_panel_kernel<true> : (void*)trd_panel_kernel<false>, grid,
+        TRD_THREADS, args, TRD_SMEM, ctx->stream));
     IMC_LAUNCH();
     const int t0 = k + b, rem = n - t0;
     if (rem > 0) {
@@ -1463,12 +1530,17 @@ static int sytrd_gpu(imcom_ctx* ctx, DMat& Aw, DMat& Vall, double* d, double* e,
   int dev = ctx->device, coop = 0;
   cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
   if (!coop) return set_err(ctx, IMCOM_ERR_CUDA, "device lacks cooperative launch");
-  int per_sm = 0;
-  IMC_CUDA(cudaFuncSetAttribute(trd_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)TRD_SMEM));
-  IMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trd_panel_kernel, TRD_THREADS,
-                                                         TRD_SMEM));
-  if (per_sm < 1) return set_err(ctx, IMCOM_ERR_CUDA, "panel kernel does not fit on an SM");
+  int per_sm = 0, per_sm_c = 0;
+  IMC_CUDA(cudaFuncSetAttribute(trd_panel_kernel<false>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRD_SMEM));
+  IMC_CUDA(cudaFuncSetAttribute(trd_panel_kernel<true>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRD_SMEM));
+  IMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trd_panel_kernel<false>,
+                                                         TRD_THREADS, TRD_SMEM));
+  IMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_c, trd_panel_kernel<true>,
+                                                         TRD_THREADS, TRD_SMEM));
+  if (per_sm < 1 || per_sm_c < 1)
+    return set_err(ctx, IMCOM_ERR_CUDA, "panel kernel does not fit on an SM");
   int tail_ctas = 0, tail_max = 0;
   tail_config(ctx, &tail_ctas, &tail_max);
   GridSync* sync = (GridSync*)((char*)accbuf + 2 * sizeof(TrdAcc) + 64);
