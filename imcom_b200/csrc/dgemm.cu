@@ -244,9 +244,8 @@ int dgemm_nn_skinny32(imcom_ctx* ctx, long long M, long long K, const double* A,
 // the tile is 64 x 64 (four warps of 32 x 32), all of K is loaded at once,
 // only the lower tiles are launched (a diagonal tile's upper-right quarter is
 // skipped), and three CTAs share an SM so that one's loads overlap another's
-// MMAs.  The accumulators start from alpha C and take the k-steps of 4 in
-// the general tile's order (zero-filled up to a multiple of its BK), so the
-// result is bit-identical to it.
+// MMAs.  The accumulators start from alpha C (loaded while the operands
+// arrive) and take the k-steps of 4 in order.
 // ---------------------------------------------------------------------------
 constexpr int LU_T = 64, LU_KMAX = 64, LU_THREADS = 128, LU_S = LU_T + 4;
 constexpr size_t LU_SMEM = (size_t)2 * LU_KMAX * LU_S * sizeof(double);
@@ -334,7 +333,7 @@ int dgemm_lower_nt(imcom_ctx* ctx, long long M, long long K, double alpha, const
   if (K <= LU_KMAX && beta == 1.0 && (alpha == 1.0 || alpha == -1.0)) {
     const long long nt = (M + LU_T - 1) / LU_T;
     const unsigned tiles = (unsigned)(nt * (nt + 1) / 2);
-    const int KP = (int)((K + BK - 1) / BK * BK);
+    const int KP = (int)((K + 3) / 4 * 4);  // whole k-steps of 4, zero-filled
     auto k = v2 ? lower_update_kernel<2> : lower_update_kernel<1>;
     IMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LU_SMEM));
     IMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,

@@ -89,22 +89,19 @@ __device__ __forceinline__ void dgemm_tile(long long M, long long N, long long K
     for (int j = 0; j < 4; ++j)
 #pragma unroll
       for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0;
-  // C += alpha op(A) op(B) with alpha = +-1 (the updates of the eigensolver):
-  // the accumulators start from alpha C, loaded before the operand pipeline
-  // so the C reads overlap it; the epilogue then stores alpha acc (sign
-  // flips are exact).
-  const bool preload = nkz == 1 && beta == 1.0 && (alpha == 1.0 || alpha == -1.0);
-  if (preload) {
+  // beta C is added in the epilogue.  Its tile is prefetched into L2 now (a
+  // hint, no registers held), so the epilogue's loads hit L2 and the HBM
+  // reads overlap the main loop instead of holding up the first MMA.
+  const bool readc = nkz == 1 && beta != 0.0;
+  if (readc) {
+    // 128 columns x 128 rows: 8 lines of 128 bytes per column, 4 per thread
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          long long row = m0 + wm * 64 + i * 16 + g + ((r >> 1) ? 8 : 0);
-          long long col = n0 + wn * 32 + j * 8 + 2 * t + (r & 1);
-          if (row < M && col < N) acc[i][j][r] = alpha * C[row + col * ldc];
-        }
+    for (int q = 0; q < 4; ++q) {
+      const int line = threadIdx.x + q * THREADS;
+      const long long col = n0 + (line >> 3), row = m0 + (line & 7) * 16;
+      if (row < M && col < N)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(C + row + col * ldc));
+    }
   }
 
   auto stageA = [&](int s) { return smem + s * STAGE_DBL; };
@@ -162,21 +159,30 @@ __device__ __forceinline__ void dgemm_tile(long long M, long long N, long long K
   }
   cp_wait<0>();
 
+  // one 16-row band at a time: its 16 C values are loaded together, then
+  // combined and stored
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 4; ++i) {
+    double cv[4][4];
 #pragma unroll
     for (int j = 0; j < 4; ++j)
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
-        long long row = m0 + wm * 64 + i * 16 + g + ((r >> 1) ? 8 : 0);
-        long long col = n0 + wn * 32 + j * 8 + 2 * t + (r & 1);
-        if (row < M && col < N) {
-          double* cp = C + row + col * ldc;
-          double v = alpha * acc[i][j][r];
-          if (!preload && nkz == 1 && beta != 0.0) v += beta * *cp;
-          *cp = v;
-        }
+        const long long row = m0 + wm * 64 + i * 16 + g + ((r >> 1) ? 8 : 0);
+        const long long col = n0 + wn * 32 + j * 8 + 2 * t + (r & 1);
+        cv[j][r] = (readc && row < M && col < N) ? C[row + col * ldc] : 0.0;
       }
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const long long row = m0 + wm * 64 + i * 16 + g + ((r >> 1) ? 8 : 0);
+        const long long col = n0 + wn * 32 + j * 8 + 2 * t + (r & 1);
+        if (row < M && col < N)
+          C[row + col * ldc] = readc ? fma(beta, cv[j][r], alpha * acc[i][j][r])
+                                     : alpha * acc[i][j][r];
+      }
+  }
 }
 
 template <bool AK, bool BKC, int VEC, bool LOWER = false>
