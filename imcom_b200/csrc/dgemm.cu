@@ -244,8 +244,8 @@ int dgemm_nn_skinny32(imcom_ctx* ctx, long long M, long long K, const double* A,
 // the tile is 64 x 64 (four warps of 32 x 32), all of K is loaded at once,
 // only the lower tiles are launched (a diagonal tile's upper-right quarter is
 // skipped), and three CTAs share an SM so that one's loads overlap another's
-// MMAs.  The accumulators start from alpha C (loaded while the operands
-// arrive) and take the k-steps of 4 in order.
+// MMAs.  C's tile is prefetched into L2 while the operands arrive and added
+// in the epilogue (C + alpha A B^T, alpha = +-1 exact).
 // ---------------------------------------------------------------------------
 constexpr int LU_T = 64, LU_KMAX = 64, LU_THREADS = 128, LU_S = LU_T + 4;
 constexpr size_t LU_SMEM = (size_t)2 * LU_KMAX * LU_S * sizeof(double);
@@ -277,17 +277,22 @@ __global__ void __launch_bounds__(LU_THREADS, 3)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wm = warp & 1, wn = warp >> 1, g = lane >> 2, t = lane & 3;
   const bool skip = ti == tj && wm < wn;  // above the diagonal
+  // C's tile into L2 while the operands arrive (4 lines of 128 bytes per
+  // column, 2 per thread); the epilogue's loads of it then hit L2
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int line = threadIdx.x + q * LU_THREADS;
+    const long long col = n0 + (line >> 2), row = m0 + (line & 3) * 16;
+    if (row < M && col < M && !(ti == tj && row + 15 < col))
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(C + row + col * ldc));
+  }
   double acc[2][4][4];
 #pragma unroll
   for (int i = 0; i < 2; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j)
 #pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const long long row = m0 + wm * 32 + i * 16 + g + ((r >> 1) ? 8 : 0);
-        const long long col = n0 + wn * 32 + j * 8 + 2 * t + (r & 1);
-        acc[i][j][r] = (!skip && row < M && col < M) ? alpha * C[row + col * ldc] : 0.0;
-      }
+      for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0;
   cp_wait<0>();
   __syncthreads();
   if (skip) return;
@@ -313,15 +318,25 @@ __global__ void __launch_bounds__(LU_THREADS, 3)
             : "d"(af[i][0]), "d"(af[i][1]), "d"(bf[j]));
   }
 #pragma unroll
-  for (int i = 0; i < 2; ++i)
+  for (int i = 0; i < 2; ++i) {
+    double cv[4][4];
 #pragma unroll
     for (int j = 0; j < 4; ++j)
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
         const long long row = m0 + wm * 32 + i * 16 + g + ((r >> 1) ? 8 : 0);
         const long long col = n0 + wn * 32 + j * 8 + 2 * t + (r & 1);
-        if (row < M && col < M) C[row + col * ldc] = alpha * acc[i][j][r];
+        cv[j][r] = (row < M && col < M) ? C[row + col * ldc] : 0.0;
       }
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const long long row = m0 + wm * 32 + i * 16 + g + ((r >> 1) ? 8 : 0);
+        const long long col = n0 + wn * 32 + j * 8 + 2 * t + (r & 1);
+        if (row < M && col < M) C[row + col * ldc] = fma(alpha, acc[i][j][r], cv[j][r]);
+      }
+  }
 }
 
 int dgemm_lower_nt(imcom_ctx* ctx, long long M, long long K, double alpha, const double* A,
