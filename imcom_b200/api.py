@@ -36,7 +36,7 @@ STACKS_GEMM, STACKS_STREAM, STACKS_AUTO = 0, 1, 2
 OPT_TABLE_FFT = 13
 OPT_KAPPA_FEATURES = 14
 OPT_KAPPA_START = 17
-TABLE_FFT_CUFFT, TABLE_FFT_OWN = 0, 1
+TABLE_FFT_CUFFT, TABLE_FFT_OWN, TABLE_FFT_AUTO = 0, 1, 2
 SPLIT_INFO = ("slices_P", "slices_T", "fp64_pixels_P", "fp64_columns_T", "max_bound_US",
               "max_bound_T_from_P", "max_bound_T_product", "P_split")
 STAGES = ("spectra", "build_A", "eigen_A", "build_B", "build_P", "bisect", "build_T", "epilogue",

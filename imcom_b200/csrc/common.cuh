@@ -95,7 +95,7 @@ struct imcom_ctx {
   size_t tables_bytes = 0;
   double2* fftbuf = nullptr;
   size_t fftbuf_bytes = 0;
-  int table_fft = IMCOM_TABLE_FFT_CUFFT;  // inverse FFT of the lookup tables
+  int table_fft = IMCOM_TABLE_FFT_AUTO;  // inverse FFT of the lookup tables
   double2* fft_tw = nullptr;              // exp(2 pi i t / L) of the own table FFT
   size_t fft_tw_bytes = 0;
   int fft_tw_L = 0;
@@ -212,6 +212,8 @@ int ensure_mat(imcom_ctx* ctx, DMat& M, long long rows, long long cols);
 // (and nothing is launched) for sides the own line transforms do not cover.
 int psf_r2c_own(imcom_ctx* ctx, int n, int count, const double* in, double2* H, double2* half,
                 bool* done);
+// Whether table_fft_inverse takes its register path for these sides.
+bool table_fft_fast(int nps, int L);
 int table_fft_inverse(imcom_ctx* ctx, int nps, int L, int ntab, const int2* dpairs, double2* W,
                       double* tab, int isB, bool* done);
 int ensure_buf(imcom_ctx* ctx, void** p, size_t& have, size_t need);

@@ -407,7 +407,9 @@ int imcom_gpu_set_option(imcom_ctx* ctx, int option, long long value) {
       ctx->kappa_feat = (int)value;
       return 0;
     case IMCOM_OPT_TABLE_FFT:
-      if (value != IMCOM_TABLE_FFT_CUFFT && value != IMCOM_TABLE_FFT_OWN) return -3;
+      if (value != IMCOM_TABLE_FFT_CUFFT && value != IMCOM_TABLE_FFT_OWN &&
+          value != IMCOM_TABLE_FFT_AUTO)
+        return -3;
       ctx->table_fft = (int)value;
       return 0;
     case IMCOM_OPT_STACK_KERNEL:

@@ -359,6 +359,185 @@ r2c_pass2(FftPlan plan, const double2* __restrict__ H, const double2* __restrict
   }
 }
 
+// ---------------------------------------------------------------------------
+// Register path for nps = 576, npad = 3 (L = 1728), the n = 4096 workload's
+// sides.  The grid's non-zero block is the spectrum X(u1, u2) at signed
+// frequencies m(u) = u (u < nps/2) or u - nps, so with k = 3 j + b
+//   sum_u X(u) exp(2 pi i m(u) k / L) = DFT_nps[X(u) exp(2 pi i m(u) b / L)](j)
+// along each axis: three length-576 transforms of pre-twiddled copies
+// replace one length-1728 transform of a zero-padded line.  One warp holds a
+// line, 18 values per lane (element 32 n1 + lane), and transforms it in
+// registers by four steps (576 = 18 x 32): a DFT-18 per lane, the twiddles
+// exp(2 pi i lane k1 / 576), and a DFT-32 across the lanes by five radix-2
+// decimation-in-frequency stages on shuffles, after which lane L's value k1
+// is output k1 + 18 bitrev5(L).  Blocks of 16 (pass 1) or 8 (pass 2) lines
+// stage their outputs in shared memory and write them in row segments:
+//   pass 1  lines u2 of one table, along u1: W[t][3 j + b][u2]
+//   pass 2  columns k1 of W, along u2: the table's real part, shifted and
+//           scaled like the other paths, one 8-column row segment per j.
+// All twiddles come from the table of exp(2 pi i t / 1728) (those of 576 at
+// t multiple of 3).
+// ---------------------------------------------------------------------------
+constexpr int FX_N1 = 18, FX_N2 = 32, FX_N = FX_N1 * FX_N2, FX_L = 3 * FX_N;
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) {
+  return make_double2(a.x + b.x, a.y + b.y);
+}
+__device__ __forceinline__ double2 csub(double2 a, double2 b) {
+  return make_double2(a.x - b.x, a.y - b.y);
+}
+
+// In-place DFT-3 with the + sign: (a, b, c) <- (a + b + c, a + w b + w^2 c,
+// a + w^2 b + w c), w = exp(2 pi i / 3); h3 = sqrt(3) / 2.
+__device__ __forceinline__ void dft3p(double2& a, double2& b, double2& c, double h3) {
+  const double2 t1 = cadd(b, c);
+  const double2 d = csub(b, c);
+  const double2 t2 = make_double2(-d.y * h3, d.x * h3);  // i h3 (b - c)
+  const double2 m = make_double2(a.x - 0.5 * t1.x, a.y - 0.5 * t1.y);
+  a = cadd(a, t1);
+  b = cadd(m, t2);
+  c = csub(m, t2);
+}
+
+// DFT-9 (+ sign) of z[0..8] as 3 x 3; output s + 3 t is left in z[3 s + t].
+// tw: exp(2 pi i t / 1728) (w9^r = tw[192 r]).
+__device__ __forceinline__ void dft9p(double2 (&z)[9], const double2* __restrict__ tw, double h3) {
+#pragma unroll
+  for (int r = 0; r < 3; ++r) dft3p(z[r], z[r + 3], z[r + 6], h3);
+  z[4] = cmul(z[4], tw[192]);      // r = 1, s = 1: w9
+  z[7] = cmul(z[7], tw[384]);      // r = 1, s = 2: w9^2
+  z[5] = cmul(z[5], tw[384]);      // r = 2, s = 1: w9^2
+  z[8] = cmul(z[8], tw[768]);      // r = 2, s = 2: w9^4
+#pragma unroll
+  for (int s = 0; s < 3; ++s) dft3p(z[3 * s], z[3 * s + 1], z[3 * s + 2], h3);
+}
+
+// DFT-576 (+ sign) of the warp's line: lane holds y[n1] = x[32 n1 + lane];
+// on return y[k1] = X[k1 + 18 bitrev5(lane)].
+__device__ __forceinline__ void dft576_warp(double2 (&y)[FX_N1], const double2* __restrict__ tw,
+                                            int lane) {
+  const double h3 = tw[576].y;  // sin(2 pi / 3)
+  // DFT-18 per lane: even and odd halves by DFT-9, joined with w18^k
+  double2 e[9], o[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    e[i] = y[2 * i];
+    o[i] = y[2 * i + 1];
+  }
+  dft9p(e, tw, h3);
+  dft9p(o, tw, h3);
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    const int at = 3 * (k % 3) + k / 3;  // output k of dft9p
+    const double2 t = cmul(o[at], tw[96 * k]);  // w18^k
+    y[k] = cadd(e[at], t);
+    y[k + 9] = csub(e[at], t);
+  }
+  // twiddles exp(2 pi i lane k1 / 576)
+#pragma unroll
+  for (int k1 = 1; k1 < FX_N1; ++k1) y[k1] = cmul(y[k1], tw[3 * ((lane * k1) % FX_N)]);
+  // DFT-32 across the lanes (element index = lane), decimation in frequency
+#pragma unroll
+  for (int h = 16; h >= 1; h >>= 1) {
+    const bool upper = (lane & h) != 0;
+    const double2 w = tw[3 * 18 * (16 / h) * (lane & (h - 1))];  // w_{2h}^(lane mod h)
+#pragma unroll
+    for (int k1 = 0; k1 < FX_N1; ++k1) {
+      const double px = __shfl_xor_sync(0xffffffffu, y[k1].x, h);
+      const double py = __shfl_xor_sync(0xffffffffu, y[k1].y, h);
+      const double2 p = make_double2(px, py);
+      y[k1] = upper ? cmul(csub(p, y[k1]), w) : cadd(y[k1], p);
+    }
+  }
+}
+
+__device__ __forceinline__ int fx_brev5(int x) { return (int)(__brev((unsigned)x) >> 27); }
+
+// exp(2 pi i m(u) b / L) for spectrum index u (signed frequency m(u))
+__device__ __forceinline__ double2 fx_pretwiddle(const double2* __restrict__ tw, int u, int b) {
+  const int m = u < FX_N / 2 ? u : u - FX_N;
+  return tw[((m * b) % FX_L + FX_L) % FX_L];
+}
+
+constexpr int FX1_LINES = 8, FX2_LINES = 8;
+constexpr size_t FX1_SMEM = (size_t)FX_L * sizeof(double2) + (size_t)FX_N * FX1_LINES * sizeof(double2);
+constexpr size_t FX2_SMEM = (size_t)FX_L * sizeof(double2) + (size_t)FX_N * FX2_LINES * sizeof(double);
+
+// Pass 1: spectrum columns u2 = 16 blockIdx.x + warp of table blockIdx.y,
+// along u1, into W[t][k1][u2] (ld nps).
+__global__ void __launch_bounds__(FX1_LINES * 32, 1)
+fx_pass1(const double2* __restrict__ Gt, const double2* __restrict__ Gammat,
+         const int2* __restrict__ pairs, const double2* __restrict__ twg, double2* __restrict__ W) {
+  extern __shared__ double2 fx_smem[];
+  double2* tw = fx_smem;            // [FX_L]
+  double2* S = fx_smem + FX_L;      // [FX_N][FX1_LINES]
+  for (int i = threadIdx.x; i < FX_L; i += blockDim.x) tw[i] = twg[i];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int t = blockIdx.y, u2 = blockIdx.x * FX1_LINES + warp;
+  const int2 pr = pairs[t];
+  __syncthreads();  // twiddles in place
+  for (int b = 0; b < 3; ++b) {
+    // the line's values are formed again for each b (L1 hits after the
+    // first): holding them across the transforms would spill
+    double2 y[FX_N1];
+#pragma unroll
+    for (int n1 = 0; n1 < FX_N1; ++n1)
+      y[n1] = cmul(pair_product(Gt, Gammat, pr, (size_t)(32 * n1 + lane) + (size_t)u2 * FX_N, FX_N),
+                   fx_pretwiddle(tw, 32 * n1 + lane, b));
+    dft576_warp(y, tw, lane);
+    const int j0 = FX_N1 * fx_brev5(lane);
+#pragma unroll
+    for (int k1 = 0; k1 < FX_N1; ++k1) S[(j0 + k1) * FX1_LINES + warp] = y[k1];
+    __syncthreads();
+    double2* dst = W + ((size_t)t * FX_L + b) * FX_N + (size_t)blockIdx.x * FX1_LINES;
+    for (int e = threadIdx.x; e < FX_N * FX1_LINES; e += blockDim.x) {
+      const int j = e / FX1_LINES, c = e - j * FX1_LINES;
+      dst[(size_t)(3 * j) * FX_N + c] = S[e];
+    }
+    __syncthreads();
+  }
+}
+
+// Pass 2: columns k1 = 8 blockIdx.x + warp of W for table blockIdx.y, along
+// u2, written as tab(p, q) = scale Re F(cshift(p), cshift(q)).
+__global__ void __launch_bounds__(FX2_LINES * 32, 2)
+fx_pass2(const double2* __restrict__ W, const double2* __restrict__ twg, double* __restrict__ tab,
+         int isB) {
+  extern __shared__ double2 fx_smem[];
+  double2* tw = fx_smem;                                 // [FX_L]
+  double* R = reinterpret_cast<double*>(fx_smem + FX_L);  // [FX_N][FX2_LINES]
+  for (int i = threadIdx.x; i < FX_L; i += blockDim.x) tw[i] = twg[i];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int t = blockIdx.y, k1 = blockIdx.x * FX2_LINES + warp;
+  const double2* src = W + ((size_t)t * FX_L + k1) * FX_N;
+  __syncthreads();
+  constexpr int s = FX_L / 2;
+  // the block's 8 columns map to 8 consecutive p (s is a multiple of 8)
+  const int p0 = (blockIdx.x * FX2_LINES - s + FX_L) % FX_L;
+  double* tt = tab + (size_t)t * FX_L * FX_L;
+  for (int b = 0; b < 3; ++b) {
+    double2 y[FX_N1];
+#pragma unroll
+    for (int n1 = 0; n1 < FX_N1; ++n1)
+      y[n1] = cmul(__ldg(src + 32 * n1 + lane), fx_pretwiddle(tw, 32 * n1 + lane, b));
+    dft576_warp(y, tw, lane);
+    const int j0 = FX_N1 * fx_brev5(lane);
+#pragma unroll
+    for (int q = 0; q < FX_N1; ++q) {
+      double v = y[q].x;
+      if (isB) v = -2.0 * v;
+      R[(j0 + q) * FX2_LINES + warp] = v / (double)FX_N / (double)FX_N;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < FX_N * FX2_LINES; e += blockDim.x) {
+      const int j = e / FX2_LINES, c = e - j * FX2_LINES;
+      const int q0 = (3 * j + b - s + FX_L) % FX_L;
+      tt[(size_t)q0 * FX_L + p0 + c] = R[e];
+    }
+    __syncthreads();
+  }
+}
+
 // exp(2 pi i t / L), t < L, rounded from extended precision; the parts that
 // are exactly 0 (where 4t is a multiple of L) come out as exact zeros.
 std::vector<double2> twiddles(int L) {
@@ -407,6 +586,8 @@ int psf_r2c_own(imcom_ctx* ctx, int n, int count, const double* in, double2* H, 
   return 0;
 }
 
+bool table_fft_fast(int nps, int L) { return nps == FX_N && L == FX_L; }
+
 int table_fft_inverse(imcom_ctx* ctx, int nps, int L, int ntab, const int2* dpairs, double2* W,
                       double* tab, int isB, bool* done) {
   *done = false;
@@ -420,6 +601,20 @@ int table_fft_inverse(imcom_ctx* ctx, int nps, int L, int ntab, const int2* dpai
                              cudaMemcpyHostToDevice, ctx->stream));
     IMC_CUDA(cudaStreamSynchronize(ctx->stream));
     ctx->fft_tw_L = L;
+  }
+  if (table_fft_fast(nps, L)) {  // the register path
+    IMC_CUDA(cudaFuncSetAttribute(fx_pass1, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)FX1_SMEM));
+    IMC_CUDA(cudaFuncSetAttribute(fx_pass2, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)FX2_SMEM));
+    fx_pass1<<<dim3(FX_N / FX1_LINES, (unsigned)ntab), FX1_LINES * 32, FX1_SMEM, ctx->stream>>>(
+        ctx->Gt, ctx->Gammat, dpairs, ctx->fft_tw, W);
+    IMC_LAUNCH();
+    fx_pass2<<<dim3(FX_L / FX2_LINES, (unsigned)ntab), FX2_LINES * 32, FX2_SMEM, ctx->stream>>>(
+        W, ctx->fft_tw, tab, isB);
+    IMC_LAUNCH();
+    *done = true;
+    return 0;
   }
   const int smem = plan.TP * plan.LS * (int)sizeof(double2);
   constexpr int kMax = FFT_MAX_ELEMS * (int)sizeof(double2);  // see psf_r2c_own

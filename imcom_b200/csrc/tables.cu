@@ -381,7 +381,10 @@ static int build_tables_body(imcom_ctx* ctx, int npad, int isB) {
                                          big2 * ntab * sizeof(double2));
   IMC_CUDA(cudaMemcpyAsync(dpairs, pairs.data(), ntab * sizeof(int2), cudaMemcpyHostToDevice,
                            ctx->stream));
-  if (ctx->table_fft == IMCOM_TABLE_FFT_OWN) {
+  // the own transform: always when asked for, by default where it is faster
+  // than cuFFT (the register path, nps = 576 with npad = 3)
+  if (ctx->table_fft == IMCOM_TABLE_FFT_OWN ||
+      (ctx->table_fft == IMCOM_TABLE_FFT_AUTO && table_fft_fast(nps, nbig))) {
     bool done = false;
     IMC_TRY(table_fft_inverse(ctx, nps, nbig, ntab, dpairs, ctx->fftbuf, ctx->tables, isB, &done));
     if (done) return 0;

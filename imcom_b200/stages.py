@@ -24,8 +24,9 @@ Usage: python -m imcom_b200.stages [workload] [--library-eigensolver] [--twostag
                   bisection
 --table-features  learned-kappa features from the neighbour table and band
                   segments (IMCOM_OPT_KAPPA_FEATURES = 1)
---own-table-fft   the library's own inverse FFT for the lookup tables
-                  (IMCOM_OPT_TABLE_FFT = 1)
+--own-table-fft   the library's own inverse FFT for the lookup tables at every
+                  side it covers (IMCOM_OPT_TABLE_FFT = 1; default 2: own
+                  where faster than cuFFT)
 --repeat-bisect N run the bisection N more times and print each one's time
 --compare-features  after the solve, time 5 learned bisections with the scanned
                   features and 5 with the table-built ones (committed weights),
@@ -94,7 +95,7 @@ def main(argv):
                           EIGH_TWOSTAGE if "--twostage" in argv else EIGH_DC)
         s.set_precision("--split" in argv)
         s.set_option(OPT_KAPPA_FEATURES, 1 if "--table-features" in argv else 0)
-        s.set_option(OPT_TABLE_FFT, 1 if "--own-table-fft" in argv else 0)
+        s.set_option(OPT_TABLE_FFT, 1 if "--own-table-fft" in argv else 2)
         compare = "--compare-features" in argv
         learned = "--learned" in argv or compare
         if learned:

@@ -108,15 +108,18 @@ typedef struct imcom_ctx imcom_ctx;
                                    stacks, the GEMM above (measured crossover) */
 #define IMCOM_STACKS_STREAM_MAX 32
 /* Inverse 2-D FFT of the lookup tables (imcom_build_Alookup/Blookup): 0 =
- * embedding, cuFFT and shift as separate steps (default); 1 = the library's
- * own transform in two passes that skip the grid's zero lines and fuse the
+ * embedding, cuFFT and shift as separate steps; 1 = the library's own
+ * transform in two passes that skip the grid's zero lines and fuse the
  * embedding and the shift (sides L = npad nps whose prime factors are 2, 3, 5,
  * 7, 11 and 13, up to 8191, 6143 with a factor 3, 5119 with a 5, 3583 with a
- * 7, 5631 with an 11, 6655 with a 13; other sides keep cuFFT).  Same tables to
- * rounding. */
+ * 7, 5631 with an 11, 6655 with a 13; other sides keep cuFFT; nps = 576 with
+ * npad = 3 takes a register path, three length-576 transforms per line);
+ * 2 (default) = the own transform where it is faster than cuFFT (the
+ * register path), cuFFT elsewhere.  Same tables to rounding. */
 #define IMCOM_OPT_TABLE_FFT 13
 #define IMCOM_TABLE_FFT_CUFFT 0
 #define IMCOM_TABLE_FFT_OWN 1
+#define IMCOM_TABLE_FFT_AUTO 2
 /* Features of the learned-kappa bracket: 0 = every pixel scans all inputs
  * for its neighbours and bins P^2 by eigenmode band element by element;
  * 1 (default) = the neighbour features come from a per-pixel table built

@@ -62,3 +62,16 @@ def test_side_with_large_prime_stays_on_cufft():
     A1, B1 = build_AB(prob, TABLE_FFT_OWN)
     A0, B0 = build_AB(prob, TABLE_FFT_CUFFT)
     assert np.array_equal(A1, A0) and np.array_equal(B1, B0)
+
+
+def test_register_path_matches_cufft_at_nps_576():
+    """nps = 576, L = 1728 (the n = 4096 workload's sides) takes the register
+    path: three length-576 transforms of pre-twiddled copies per line, one
+    warp per line.  A and B against the cuFFT path at the same bar."""
+    prob = synth.make("n4096", 0)
+    assert prob.nps == 576
+    A1, B1 = build_AB(prob, TABLE_FFT_OWN)
+    A0, B0 = build_AB(prob, TABLE_FFT_CUFFT)
+    assert np.array_equal(A1, A1.T)
+    assert rel(A1, A0) < 1e-12
+    assert rel(B1, B0) < 1e-12
