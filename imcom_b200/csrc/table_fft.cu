@@ -399,24 +399,33 @@ __device__ __forceinline__ void dft3p(double2& a, double2& b, double2& c, double
   c = csub(m, t2);
 }
 
+// The register path's twiddles in shared memory, laid out so that a warp's
+// reads are consecutive (no bank conflicts) or one broadcast address:
+//   pre[b nps + u]    exp(2 pi i m(u) b / L)
+//   lt[k1 32 + lane]  exp(2 pi i lane k1 / 576)
+//   st[i 32 + lane]   exp(2 pi i (lane mod h) / (2 h)), h = 16 >> i (i < 3)
+//   cst[k] = w18^k (k < 9), cst[9 + i] = w9^(1, 2, 4), cst[12].y = sin(2 pi / 3)
+constexpr int FX_TW = 3 * FX_N + FX_N1 * 32 + 3 * 32 + 16;  // double2 entries
+struct FxTw {
+  const double2 *pre, *lt, *st, *cst;
+};
+
 // DFT-9 (+ sign) of z[0..8] as 3 x 3; output s + 3 t is left in z[3 s + t].
-// tw: exp(2 pi i t / 1728) (w9^r = tw[192 r]).
-__device__ __forceinline__ void dft9p(double2 (&z)[9], const double2* __restrict__ tw, double h3) {
+__device__ __forceinline__ void dft9p(double2 (&z)[9], const double2* __restrict__ cst, double h3) {
 #pragma unroll
   for (int r = 0; r < 3; ++r) dft3p(z[r], z[r + 3], z[r + 6], h3);
-  z[4] = cmul(z[4], tw[192]);      // r = 1, s = 1: w9
-  z[7] = cmul(z[7], tw[384]);      // r = 1, s = 2: w9^2
-  z[5] = cmul(z[5], tw[384]);      // r = 2, s = 1: w9^2
-  z[8] = cmul(z[8], tw[768]);      // r = 2, s = 2: w9^4
+  z[4] = cmul(z[4], cst[9]);       // r = 1, s = 1: w9
+  z[7] = cmul(z[7], cst[10]);      // r = 1, s = 2: w9^2
+  z[5] = cmul(z[5], cst[10]);      // r = 2, s = 1: w9^2
+  z[8] = cmul(z[8], cst[11]);      // r = 2, s = 2: w9^4
 #pragma unroll
   for (int s = 0; s < 3; ++s) dft3p(z[3 * s], z[3 * s + 1], z[3 * s + 2], h3);
 }
 
 // DFT-576 (+ sign) of the warp's line: lane holds y[n1] = x[32 n1 + lane];
 // on return y[k1] = X[k1 + 18 bitrev5(lane)].
-__device__ __forceinline__ void dft576_warp(double2 (&y)[FX_N1], const double2* __restrict__ tw,
-                                            int lane) {
-  const double h3 = tw[576].y;  // sin(2 pi / 3)
+__device__ __forceinline__ void dft576_warp(double2 (&y)[FX_N1], const FxTw& tw, int lane) {
+  const double h3 = tw.cst[12].y;  // sin(2 pi / 3)
   // DFT-18 per lane: even and odd halves by DFT-9, joined with w18^k
   double2 e[9], o[9];
 #pragma unroll
@@ -424,54 +433,80 @@ __device__ __forceinline__ void dft576_warp(double2 (&y)[FX_N1], const double2* 
     e[i] = y[2 * i];
     o[i] = y[2 * i + 1];
   }
-  dft9p(e, tw, h3);
-  dft9p(o, tw, h3);
+  dft9p(e, tw.cst, h3);
+  dft9p(o, tw.cst, h3);
 #pragma unroll
   for (int k = 0; k < 9; ++k) {
     const int at = 3 * (k % 3) + k / 3;  // output k of dft9p
-    const double2 t = cmul(o[at], tw[96 * k]);  // w18^k
+    const double2 t = cmul(o[at], tw.cst[k]);  // w18^k
     y[k] = cadd(e[at], t);
     y[k + 9] = csub(e[at], t);
   }
   // twiddles exp(2 pi i lane k1 / 576)
 #pragma unroll
-  for (int k1 = 1; k1 < FX_N1; ++k1) y[k1] = cmul(y[k1], tw[3 * ((lane * k1) % FX_N)]);
-  // DFT-32 across the lanes (element index = lane), decimation in frequency
+  for (int k1 = 1; k1 < FX_N1; ++k1) y[k1] = cmul(y[k1], tw.lt[k1 * 32 + lane]);
+  // DFT-32 across the lanes (element index = lane), decimation in frequency:
+  // lower lane y + p, upper lane (p - y) w_{2h}^(lane mod h), formed as
+  // (s y + p) w with s = -1 and w = 1 on the lower lanes; the last two
+  // stages' twiddles are 1 and i (a swap), so they need no product.
 #pragma unroll
   for (int h = 16; h >= 1; h >>= 1) {
     const bool upper = (lane & h) != 0;
-    const double2 w = tw[3 * 18 * (16 / h) * (lane & (h - 1))];  // w_{2h}^(lane mod h)
+    const double sgn = upper ? -1.0 : 1.0;
+    const double2 w =
+        (upper && h >= 4) ? tw.st[(h == 16 ? 0 : h == 8 ? 1 : 2) * 32 + lane] : make_double2(1.0, 0.0);
+    const bool rot = h == 2 && upper && (lane & 1);  // w_4^1 = i
 #pragma unroll
     for (int k1 = 0; k1 < FX_N1; ++k1) {
       const double px = __shfl_xor_sync(0xffffffffu, y[k1].x, h);
       const double py = __shfl_xor_sync(0xffffffffu, y[k1].y, h);
-      const double2 p = make_double2(px, py);
-      y[k1] = upper ? cmul(csub(p, y[k1]), w) : cadd(y[k1], p);
+      const double2 r = make_double2(fma(sgn, y[k1].x, px), fma(sgn, y[k1].y, py));
+      if (h >= 4) y[k1] = cmul(r, w);
+      else if (h == 2) y[k1] = rot ? make_double2(-r.y, r.x) : r;
+      else y[k1] = r;
     }
   }
 }
 
 __device__ __forceinline__ int fx_brev5(int x) { return (int)(__brev((unsigned)x) >> 27); }
 
-// exp(2 pi i m(u) b / L) for spectrum index u (signed frequency m(u))
-__device__ __forceinline__ double2 fx_pretwiddle(const double2* __restrict__ tw, int u, int b) {
-  const int m = u < FX_N / 2 ? u : u - FX_N;
-  return tw[((m * b) % FX_L + FX_L) % FX_L];
+// The shared twiddle tables from the global table g[t] = exp(2 pi i t / L),
+// by every thread of the block (FX_TW entries at sm).
+__device__ __forceinline__ FxTw fx_fill(const double2* __restrict__ g, double2* sm) {
+  double2 *pre = sm, *lt = pre + 3 * FX_N, *st = lt + FX_N1 * 32, *cst = st + 3 * 32;
+  for (int i = threadIdx.x; i < 3 * FX_N; i += blockDim.x) {
+    const int b = i / FX_N, u = i - b * FX_N;
+    // m(u) b mod L with |m(u) b| < L (b <= 2, |m| <= nps / 2)
+    int k = b * u - (u >= FX_N / 2 ? b * FX_N : 0);
+    if (k < 0) k += FX_L;
+    pre[i] = g[k];
+  }
+  for (int i = threadIdx.x; i < FX_N1 * 32; i += blockDim.x)
+    lt[i] = g[3 * (i & 31) * (i >> 5)];  // lane (i & 31), k1 (i >> 5): lane k1 < 576
+  for (int i = threadIdx.x; i < 3 * 32; i += blockDim.x) {
+    const int h = 16 >> (i >> 5), L = i & 31;
+    st[i] = g[54 * (16 / h) * (L & (h - 1))];  // w_{2h}^(L mod h) = w_32^((16/h)(L mod h))
+  }
+  if (threadIdx.x < 9) cst[threadIdx.x] = g[96 * threadIdx.x];  // w18^k
+  if (threadIdx.x == 9) cst[9] = g[192];                        // w9
+  if (threadIdx.x == 10) cst[10] = g[384];                      // w9^2
+  if (threadIdx.x == 11) cst[11] = g[768];                      // w9^4
+  if (threadIdx.x == 12) cst[12] = g[576];                      // w3: (-1/2, sin(2 pi / 3))
+  return FxTw{pre, lt, st, cst};
 }
 
 constexpr int FX1_LINES = 8, FX2_LINES = 8;
-constexpr size_t FX1_SMEM = (size_t)FX_L * sizeof(double2) + (size_t)FX_N * FX1_LINES * sizeof(double2);
-constexpr size_t FX2_SMEM = (size_t)FX_L * sizeof(double2) + (size_t)FX_N * FX2_LINES * sizeof(double);
+constexpr size_t FX1_SMEM = ((size_t)FX_TW + (size_t)FX_N * FX1_LINES) * sizeof(double2);
+constexpr size_t FX2_SMEM = (size_t)FX_TW * sizeof(double2) + (size_t)FX_N * FX2_LINES * sizeof(double);
 
-// Pass 1: spectrum columns u2 = 16 blockIdx.x + warp of table blockIdx.y,
+// Pass 1: spectrum columns u2 = 8 blockIdx.x + warp of table blockIdx.y,
 // along u1, into W[t][k1][u2] (ld nps).
 __global__ void __launch_bounds__(FX1_LINES * 32, 1)
 fx_pass1(const double2* __restrict__ Gt, const double2* __restrict__ Gammat,
          const int2* __restrict__ pairs, const double2* __restrict__ twg, double2* __restrict__ W) {
   extern __shared__ double2 fx_smem[];
-  double2* tw = fx_smem;            // [FX_L]
-  double2* S = fx_smem + FX_L;      // [FX_N][FX1_LINES]
-  for (int i = threadIdx.x; i < FX_L; i += blockDim.x) tw[i] = twg[i];
+  const FxTw tw = fx_fill(twg, fx_smem);
+  double2* S = fx_smem + FX_TW;  // [FX_N][FX1_LINES]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int t = blockIdx.y, u2 = blockIdx.x * FX1_LINES + warp;
   const int2 pr = pairs[t];
@@ -483,7 +518,7 @@ fx_pass1(const double2* __restrict__ Gt, const double2* __restrict__ Gammat,
 #pragma unroll
     for (int n1 = 0; n1 < FX_N1; ++n1)
       y[n1] = cmul(pair_product(Gt, Gammat, pr, (size_t)(32 * n1 + lane) + (size_t)u2 * FX_N, FX_N),
-                   fx_pretwiddle(tw, 32 * n1 + lane, b));
+                   tw.pre[b * FX_N + 32 * n1 + lane]);
     dft576_warp(y, tw, lane);
     const int j0 = FX_N1 * fx_brev5(lane);
 #pragma unroll
@@ -504,9 +539,8 @@ __global__ void __launch_bounds__(FX2_LINES * 32, 2)
 fx_pass2(const double2* __restrict__ W, const double2* __restrict__ twg, double* __restrict__ tab,
          int isB) {
   extern __shared__ double2 fx_smem[];
-  double2* tw = fx_smem;                                 // [FX_L]
-  double* R = reinterpret_cast<double*>(fx_smem + FX_L);  // [FX_N][FX2_LINES]
-  for (int i = threadIdx.x; i < FX_L; i += blockDim.x) tw[i] = twg[i];
+  const FxTw tw = fx_fill(twg, fx_smem);
+  double* R = reinterpret_cast<double*>(fx_smem + FX_TW);  // [FX_N][FX2_LINES]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int t = blockIdx.y, k1 = blockIdx.x * FX2_LINES + warp;
   const double2* src = W + ((size_t)t * FX_L + k1) * FX_N;
@@ -519,7 +553,7 @@ fx_pass2(const double2* __restrict__ W, const double2* __restrict__ twg, double*
     double2 y[FX_N1];
 #pragma unroll
     for (int n1 = 0; n1 < FX_N1; ++n1)
-      y[n1] = cmul(__ldg(src + 32 * n1 + lane), fx_pretwiddle(tw, 32 * n1 + lane, b));
+      y[n1] = cmul(__ldg(src + 32 * n1 + lane), tw.pre[b * FX_N + 32 * n1 + lane]);
     dft576_warp(y, tw, lane);
     const int j0 = FX_N1 * fx_brev5(lane);
 #pragma unroll
