@@ -4,10 +4,11 @@
 // 467-480) embed conj(Gt_e) Gt_f (or conj(Gammat) Gt_e) in the middle of an
 // npad-times larger frequency grid (side L = npad nps), inverse-FFT the grid
 // (imcom_invft_c2c, imcom_proc.f90:498-512, an FFTW backward DFT) and keep the
-// cshifted, scaled real part as the table.  The default path does that as
+// cshifted, scaled real part as the table.  The cuFFT path does that as
 // embed_kernel -> cuFFT Z2Z -> shift_scale_kernel (tables.cu).  This file does
 // the same in two passes over HBM, using that only nps of the grid's L lines
-// are non-zero:
+// are non-zero (for nps = 576, npad = 3 by the register path further down,
+// the default there; elsewhere by the Stockham stages below, opt-in):
 //   pass 1  the nps non-zero lines, computed from the spectra straight into
 //           shared memory and transformed along p; the result W (nps x L per
 //           table) is 1/npad of the grid.

@@ -1,6 +1,8 @@
 """The lookup tables' inverse FFT: the library's own pruned, fused transform
-(IMCOM_OPT_TABLE_FFT = 1, csrc/table_fft.cu) against embedding + cuFFT +
-shift (the default), on one workload.
+(IMCOM_OPT_TABLE_FFT = 1, csrc/table_fft.cu: the register path at nps = 576,
+the Stockham path at other sides) against embedding + cuFFT + shift, on one
+workload.  By default (IMCOM_TABLE_FFT_AUTO) the library takes the register
+path where it applies and cuFFT elsewhere.
 
     python -m imcom_b200.table_fft [--workload n4096] [--reps 5]
 

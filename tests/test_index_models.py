@@ -876,3 +876,67 @@ def test_sum_by_binades_is_the_sequential_sum(case):
     else:
         t = rng.random(12000) * 1e-310
     assert seq_sum_by_binades(t) == _sequential(t)
+
+
+# ---- the register path of the table FFT (table_fft.cu, fx_pass1/2) ---------
+
+def _w(n, k):
+    return np.exp(2j * np.pi * (np.asarray(k) % n) / n)
+
+
+def _dft3p(a, b, c):
+    t1, t2 = b + c, (b - c) * (1j * math.sqrt(3) / 2)
+    m = a - 0.5 * t1
+    return a + t1, m + t2, m - t2
+
+
+def _dft9p(z):
+    z = list(z)
+    for r in range(3):
+        z[r], z[r + 3], z[r + 6] = _dft3p(z[r], z[r + 3], z[r + 6])
+    z[4] *= _w(9, 1); z[7] *= _w(9, 2); z[5] *= _w(9, 2); z[8] *= _w(9, 4)
+    for s in range(3):
+        z[3 * s], z[3 * s + 1], z[3 * s + 2] = _dft3p(z[3 * s], z[3 * s + 1], z[3 * s + 2])
+    return z  # output s + 3 t at z[3 s + t]
+
+
+def _dft576_warp(v):
+    """dft576_warp as written: lane L holds v[32 n1 + L]; returns X."""
+    reg = np.array([[v[32 * n1 + L] for n1 in range(18)] for L in range(32)])
+    for L in range(32):
+        e, o = _dft9p(reg[L][0::2]), _dft9p(reg[L][1::2])
+        y = np.zeros(18, complex)
+        for k in range(9):
+            at = 3 * (k % 3) + k // 3
+            t = o[at] * _w(18, k)
+            y[k], y[k + 9] = e[at] + t, e[at] - t
+        reg[L] = y * _w(576, L * np.arange(18))
+    for h in (16, 8, 4, 2, 1):
+        new = reg.copy()
+        for L in range(32):
+            upper = bool(L & h)
+            r = (-1.0 if upper else 1.0) * reg[L] + reg[L ^ h]
+            new[L] = r * (_w(2 * h, L % h) if upper else 1.0)
+        reg = new
+    X = np.zeros(576, complex)
+    for L in range(32):
+        j0 = 18 * int(f"{L:05b}"[::-1], 2)
+        X[j0:j0 + 18] = reg[L]
+    return X
+
+
+def test_register_dft576_model():
+    """The register path's line transform (DFT-18 per lane, lane twiddles,
+    DFT-32 across lanes, output k1 + 18 bitrev5(lane)) and its k = 3 j + b
+    split of the zero-padded length-1728 transform, against direct DFTs."""
+    rng = np.random.default_rng(3)
+    v = rng.standard_normal(576) + 1j * rng.standard_normal(576)
+    n = np.arange(576)
+    ref = np.array([np.sum(v * _w(576, n * k)) for k in range(576)])
+    assert np.abs(_dft576_warp(v) - ref).max() <= 1e-15 * np.abs(ref).max() * 10
+    m = np.where(n < 288, n, n - 576)
+    F_ref = np.array([np.sum(v * _w(1728, m * k)) for k in range(1728)])
+    F = np.zeros(1728, complex)
+    for b in range(3):
+        F[3 * n + b] = _dft576_warp(v * _w(1728, m * b))
+    assert np.abs(F - F_ref).max() <= 1e-14 * np.abs(F_ref).max()
