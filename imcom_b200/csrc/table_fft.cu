@@ -402,13 +402,15 @@ __device__ __forceinline__ void dft3p(double2& a, double2& b, double2& c, double
 
 // The register path's twiddles in shared memory, laid out so that a warp's
 // reads are consecutive (no bank conflicts) or one broadcast address:
-//   pre[b nps + u]    exp(2 pi i m(u) b / L)
-//   lt[k1 32 + lane]  exp(2 pi i lane k1 / 576)
+//   pl[b 32 + lane]   exp(2 pi i lane b / L)  (b < 3)
+//   lt[lane]          exp(2 pi i lane / 576)
 //   st[i 32 + lane]   exp(2 pi i (lane mod h) / (2 h)), h = 16 >> i (i < 3)
-//   cst[k] = w18^k (k < 9), cst[9 + i] = w9^(1, 2, 4), cst[12].y = sin(2 pi / 3)
-constexpr int FX_TW = 3 * FX_N + FX_N1 * 32 + 3 * 32 + 16;  // double2 entries
+//   cst[k] = w18^k (k < 9), cst[9 + i] = w9^(1, 2, 4), cst[12].y = sin(2 pi / 3),
+//   cst[13 + b] = exp(2 pi i 32 b / L)
+// The other twiddles are products of these (a few ulps at most).
+constexpr int FX_TW = 3 * 32 + 32 + 3 * 32 + 16;  // double2 entries
 struct FxTw {
-  const double2 *pre, *lt, *st, *cst;
+  const double2 *pl, *lt, *st, *cst;
 };
 
 // DFT-9 (+ sign) of z[0..8] as 3 x 3; output s + 3 t is left in z[3 s + t].
@@ -445,7 +447,17 @@ __device__ __forceinline__ void dft576_warp(double2 (&y)[FX_N1], const FxTw& tw,
   }
   // twiddles exp(2 pi i lane k1 / 576)
 #pragma unroll
-  for (int k1 = 1; k1 < FX_N1; ++k1) y[k1] = cmul(y[k1], tw.lt[k1 * 32 + lane]);
+  // as powers of w576^lane (one shared read instead of 17; 16 more products,
+  // ~2e-15 relative at k1 = 17)
+  {
+    const double2 w1 = tw.lt[lane];
+    double2 wk = w1;
+#pragma unroll
+    for (int k1 = 1; k1 < FX_N1; ++k1) {
+      y[k1] = cmul(y[k1], wk);
+      if (k1 + 1 < FX_N1) wk = cmul(wk, w1);
+    }
+  }
   // DFT-32 across the lanes (element index = lane), decimation in frequency:
   // lower lane y + p, upper lane (p - y) w_{2h}^(lane mod h), formed as
   // (s y + p) w with s = -1 and w = 1 on the lower lanes; the last two
@@ -474,16 +486,9 @@ __device__ __forceinline__ int fx_brev5(int x) { return (int)(__brev((unsigned)x
 // The shared twiddle tables from the global table g[t] = exp(2 pi i t / L),
 // by every thread of the block (FX_TW entries at sm).
 __device__ __forceinline__ FxTw fx_fill(const double2* __restrict__ g, double2* sm) {
-  double2 *pre = sm, *lt = pre + 3 * FX_N, *st = lt + FX_N1 * 32, *cst = st + 3 * 32;
-  for (int i = threadIdx.x; i < 3 * FX_N; i += blockDim.x) {
-    const int b = i / FX_N, u = i - b * FX_N;
-    // m(u) b mod L with |m(u) b| < L (b <= 2, |m| <= nps / 2)
-    int k = b * u - (u >= FX_N / 2 ? b * FX_N : 0);
-    if (k < 0) k += FX_L;
-    pre[i] = g[k];
-  }
-  for (int i = threadIdx.x; i < FX_N1 * 32; i += blockDim.x)
-    lt[i] = g[3 * (i & 31) * (i >> 5)];  // lane (i & 31), k1 (i >> 5): lane k1 < 576
+  double2 *pl = sm, *lt = pl + 3 * 32, *st = lt + 32, *cst = st + 3 * 32;
+  for (int i = threadIdx.x; i < 3 * 32; i += blockDim.x) pl[i] = g[(i >> 5) * (i & 31)];
+  for (int i = threadIdx.x; i < 32; i += blockDim.x) lt[i] = g[3 * i];
   for (int i = threadIdx.x; i < 3 * 32; i += blockDim.x) {
     const int h = 16 >> (i >> 5), L = i & 31;
     st[i] = g[54 * (16 / h) * (L & (h - 1))];  // w_{2h}^(L mod h) = w_32^((16/h)(L mod h))
@@ -493,11 +498,34 @@ __device__ __forceinline__ FxTw fx_fill(const double2* __restrict__ g, double2* 
   if (threadIdx.x == 10) cst[10] = g[384];                      // w9^2
   if (threadIdx.x == 11) cst[11] = g[768];                      // w9^4
   if (threadIdx.x == 12) cst[12] = g[576];                      // w3: (-1/2, sin(2 pi / 3))
-  return FxTw{pre, lt, st, cst};
+  if (threadIdx.x >= 13 && threadIdx.x < 16) cst[threadIdx.x] = g[32 * (threadIdx.x - 13)];
+  return FxTw{pl, lt, st, cst};
+}
+
+// y[n1] *= exp(2 pi i m(u) b / L), u = 32 n1 + lane: powers of w_L^(32 b)
+// from w_L^(lane b) up for n1 < 9 (m = u) and from w_L^((lane - 32) b) down
+// for n1 >= 9 (m = u - nps).
+__device__ __forceinline__ void fx_pretwiddle(double2 (&y)[FX_N1], const FxTw& tw, int lane,
+                                              int b) {
+  if (b == 0) return;
+  const double2 step = tw.cst[13 + b], stepm = make_double2(step.x, -step.y);
+  const double2 base = tw.pl[b * 32 + lane];
+  double2 c = base;
+#pragma unroll
+  for (int n1 = 0; n1 < FX_N1 / 2; ++n1) {
+    y[n1] = cmul(y[n1], c);
+    if (n1 + 1 < FX_N1 / 2) c = cmul(c, step);
+  }
+  c = cmul(base, stepm);
+#pragma unroll
+  for (int n1 = FX_N1 - 1; n1 >= FX_N1 / 2; --n1) {
+    y[n1] = cmul(y[n1], c);
+    if (n1 > FX_N1 / 2) c = cmul(c, stepm);
+  }
 }
 
 constexpr int FX1_LINES = 8, FX2_LINES = 8;
-constexpr size_t FX1_SMEM = ((size_t)FX_TW + (size_t)FX_N * FX1_LINES) * sizeof(double2);
+constexpr size_t FX1_SMEM = ((size_t)FX_TW + 2 * (size_t)FX_N * FX1_LINES) * sizeof(double2);
 constexpr size_t FX2_SMEM = (size_t)FX_TW * sizeof(double2) + (size_t)FX_N * FX2_LINES * sizeof(double);
 
 // Pass 1: spectrum columns u2 = 8 blockIdx.x + warp of table blockIdx.y,
@@ -507,19 +535,20 @@ fx_pass1(const double2* __restrict__ Gt, const double2* __restrict__ Gammat,
          const int2* __restrict__ pairs, const double2* __restrict__ twg, double2* __restrict__ W) {
   extern __shared__ double2 fx_smem[];
   const FxTw tw = fx_fill(twg, fx_smem);
-  double2* S = fx_smem + FX_TW;  // [FX_N][FX1_LINES]
+  double2* S = fx_smem + FX_TW;               // [FX_N][FX1_LINES]
+  double2* X = S + (size_t)FX_N * FX1_LINES;  // [FX1_LINES][FX_N]: the lines' values
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int t = blockIdx.y, u2 = blockIdx.x * FX1_LINES + warp;
   const int2 pr = pairs[t];
-  __syncthreads();  // twiddles in place
+  double2* xl = X + (size_t)warp * FX_N;
+  for (int u = lane; u < FX_N; u += 32)
+    xl[u] = pair_product(Gt, Gammat, pr, (size_t)u + (size_t)u2 * FX_N, FX_N);
+  __syncthreads();  // twiddles and the lines in place
   for (int b = 0; b < 3; ++b) {
-    // the line's values are formed again for each b (L1 hits after the
-    // first): holding them across the transforms would spill
     double2 y[FX_N1];
 #pragma unroll
-    for (int n1 = 0; n1 < FX_N1; ++n1)
-      y[n1] = cmul(pair_product(Gt, Gammat, pr, (size_t)(32 * n1 + lane) + (size_t)u2 * FX_N, FX_N),
-                   tw.pre[b * FX_N + 32 * n1 + lane]);
+    for (int n1 = 0; n1 < FX_N1; ++n1) y[n1] = xl[32 * n1 + lane];
+    fx_pretwiddle(y, tw, lane, b);
     dft576_warp(y, tw, lane);
     const int j0 = FX_N1 * fx_brev5(lane);
 #pragma unroll
@@ -554,7 +583,8 @@ fx_pass2(const double2* __restrict__ W, const double2* __restrict__ twg, double*
     double2 y[FX_N1];
 #pragma unroll
     for (int n1 = 0; n1 < FX_N1; ++n1)
-      y[n1] = cmul(__ldg(src + 32 * n1 + lane), tw.pre[b * FX_N + 32 * n1 + lane]);
+      y[n1] = __ldg(src + 32 * n1 + lane);
+    fx_pretwiddle(y, tw, lane, b);
     dft576_warp(y, tw, lane);
     const int j0 = FX_N1 * fx_brev5(lane);
 #pragma unroll
