@@ -78,7 +78,13 @@ int launch(imcom_ctx* ctx, long long M, long long N, long long K, double alpha, 
   }
   dim3 grd((unsigned)gm, (unsigned)gn, (unsigned)splits);
   double a1 = splits > 1 ? 1.0 : alpha;
-  if (vec == 2) {
+  if (ctx->sm_share > 0 && gm * gn * splits > sms) {
+    // a context on a share of the SMs: at most one CTA per SM of its share
+    auto k = vec == 2 ? dgemm_persist_kernel<AK, BKC, 2> : dgemm_persist_kernel<AK, BKC, 1>;
+    IMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES));
+    k<<<sms, THREADS, SMEM_BYTES, ctx->stream>>>(M, N, K, a1, A, lda, B, ldb, beta, out, ldo,
+                                                 kchunk, (int)gm, (int)gn, splits);
+  } else if (vec == 2) {
     auto k = dgemm_kernel<AK, BKC, 2>;
     IMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES));
     k<<<grd, THREADS, SMEM_BYTES, ctx->stream>>>(M, N, K, a1, A, lda, B, ldb, beta, out, ldo, kchunk);
@@ -254,88 +260,91 @@ template <int VEC>
 __global__ void __launch_bounds__(LU_THREADS, 3)
     lower_update_kernel(long long M, int K, int KP, double alpha, const double* __restrict__ A,
                         long long lda, const double* __restrict__ B, long long ldb,
-                        double* __restrict__ C, long long ldc) {
+                        double* __restrict__ C, long long ldc, int ntiles) {
   extern __shared__ __align__(16) double lu[];
   double* sA = lu;                   // sA[k][r]
   double* sB = lu + LU_KMAX * LU_S;  // sB[k][c]
-  // lower tile (ti, tj), ti >= tj, from the linear block index
-  const int b = (int)blockIdx.x;
-  int ti = (int)((sqrtf(8.0f * (float)b + 1.0f) - 1.0f) * 0.5f);
-  while ((ti + 1) * (ti + 2) / 2 <= b) ++ti;
-  while (ti > 0 && ti * (ti + 1) / 2 > b) --ti;
-  const int tj = b - ti * (ti + 1) / 2;
-  const long long m0 = (long long)ti * LU_T, n0 = (long long)tj * LU_T;
-  for (int c = threadIdx.x; c < KP * (LU_T / VEC); c += LU_THREADS) {
-    const int kk = c / (LU_T / VEC), rr = (c % (LU_T / VEC)) * VEC;
-    const long long ra = m0 + rr, rb = n0 + rr;
-    const int va = kk < K ? (int)min((long long)VEC, max(0LL, M - ra)) : 0;
-    const int vb = kk < K ? (int)min((long long)VEC, max(0LL, M - rb)) : 0;
-    cp_async(sA + kk * LU_S + rr, va ? A + ra + (long long)kk * lda : A, va * 8, VEC);
-    cp_async(sB + kk * LU_S + rr, vb ? B + rb + (long long)kk * ldb : B, vb * 8, VEC);
-  }
-  cp_commit();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wm = warp & 1, wn = warp >> 1, g = lane >> 2, t = lane & 3;
-  const bool skip = ti == tj && wm < wn;  // above the diagonal
-  // C's tile into L2 while the operands arrive (4 lines of 128 bytes per
-  // column, 2 per thread); the epilogue's loads of it then hit L2
-#pragma unroll
-  for (int q = 0; q < 2; ++q) {
-    const int line = threadIdx.x + q * LU_THREADS;
-    const long long col = n0 + (line >> 2), row = m0 + (line & 3) * 16;
-    if (row < M && col < M && !(ti == tj && row + 15 < col))
-      asm volatile("prefetch.global.L2 [%0];" ::"l"(C + row + col * ldc));
-  }
-  double acc[2][4][4];
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0;
-  cp_wait<0>();
-  __syncthreads();
-  if (skip) return;
-#pragma unroll 4
-  for (int kk = 0; kk < KP; kk += 4) {
-    double af[2][2], bf[4];
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      const int mr = wm * 32 + i * 16 + g;
-      af[i][0] = sA[(kk + t) * LU_S + mr];
-      af[i][1] = sA[(kk + t) * LU_S + mr + 8];
+  // one tile per CTA, or (a context on a share of the SMs) tiles b, b + gridDim.x, ...
+  for (int b = (int)blockIdx.x; b < ntiles; b += (int)gridDim.x) {
+    __syncthreads();  // every warp is done with the previous tile's sA, sB
+    // lower tile (ti, tj), ti >= tj, from the linear index b
+    int ti = (int)((sqrtf(8.0f * (float)b + 1.0f) - 1.0f) * 0.5f);
+    while ((ti + 1) * (ti + 2) / 2 <= b) ++ti;
+    while (ti > 0 && ti * (ti + 1) / 2 > b) --ti;
+    const int tj = b - ti * (ti + 1) / 2;
+    const long long m0 = (long long)ti * LU_T, n0 = (long long)tj * LU_T;
+    for (int c = threadIdx.x; c < KP * (LU_T / VEC); c += LU_THREADS) {
+      const int kk = c / (LU_T / VEC), rr = (c % (LU_T / VEC)) * VEC;
+      const long long ra = m0 + rr, rb = n0 + rr;
+      const int va = kk < K ? (int)min((long long)VEC, max(0LL, M - ra)) : 0;
+      const int vb = kk < K ? (int)min((long long)VEC, max(0LL, M - rb)) : 0;
+      cp_async(sA + kk * LU_S + rr, va ? A + ra + (long long)kk * lda : A, va * 8, VEC);
+      cp_async(sB + kk * LU_S + rr, vb ? B + rb + (long long)kk * ldb : B, vb * 8, VEC);
     }
-#pragma unroll
-    for (int j = 0; j < 4; ++j) bf[j] = sB[(kk + t) * LU_S + wn * 32 + j * 8 + g];
-#pragma unroll
+    cp_commit();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wm = warp & 1, wn = warp >> 1, g = lane >> 2, t = lane & 3;
+    const bool skip = ti == tj && wm < wn;  // above the diagonal
+    // C's tile into L2 while the operands arrive (4 lines of 128 bytes per
+    // column, 2 per thread); the epilogue's loads of it then hit L2
+  #pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int line = threadIdx.x + q * LU_THREADS;
+      const long long col = n0 + (line >> 2), row = m0 + (line & 3) * 16;
+      if (row < M && col < M && !(ti == tj && row + 15 < col))
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(C + row + col * ldc));
+    }
+    double acc[2][4][4];
+  #pragma unroll
     for (int i = 0; i < 2; ++i)
-#pragma unroll
+  #pragma unroll
       for (int j = 0; j < 4; ++j)
-        asm volatile(
-            "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
-            "{%0,%1,%2,%3};\n"
-            : "+d"(acc[i][j][0]), "+d"(acc[i][j][1]), "+d"(acc[i][j][2]), "+d"(acc[i][j][3])
-            : "d"(af[i][0]), "d"(af[i][1]), "d"(bf[j]));
-  }
-#pragma unroll
-  for (int i = 0; i < 2; ++i) {
-    double cv[4][4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const long long row = m0 + wm * 32 + i * 16 + g + ((r >> 1) ? 8 : 0);
-        const long long col = n0 + wn * 32 + j * 8 + 2 * t + (r & 1);
-        cv[j][r] = (row < M && col < M) ? C[row + col * ldc] : 0.0;
+  #pragma unroll
+        for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0;
+    cp_wait<0>();
+    __syncthreads();
+    if (skip) continue;
+  #pragma unroll 4
+    for (int kk = 0; kk < KP; kk += 4) {
+      double af[2][2], bf[4];
+  #pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int mr = wm * 32 + i * 16 + g;
+        af[i][0] = sA[(kk + t) * LU_S + mr];
+        af[i][1] = sA[(kk + t) * LU_S + mr + 8];
       }
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const long long row = m0 + wm * 32 + i * 16 + g + ((r >> 1) ? 8 : 0);
-        const long long col = n0 + wn * 32 + j * 8 + 2 * t + (r & 1);
-        if (row < M && col < M) C[row + col * ldc] = fma(alpha, acc[i][j][r], cv[j][r]);
-      }
+  #pragma unroll
+      for (int j = 0; j < 4; ++j) bf[j] = sB[(kk + t) * LU_S + wn * 32 + j * 8 + g];
+  #pragma unroll
+      for (int i = 0; i < 2; ++i)
+  #pragma unroll
+        for (int j = 0; j < 4; ++j)
+          asm volatile(
+              "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+              "{%0,%1,%2,%3};\n"
+              : "+d"(acc[i][j][0]), "+d"(acc[i][j][1]), "+d"(acc[i][j][2]), "+d"(acc[i][j][3])
+              : "d"(af[i][0]), "d"(af[i][1]), "d"(bf[j]));
+    }
+  #pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      double cv[4][4];
+  #pragma unroll
+      for (int j = 0; j < 4; ++j)
+  #pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const long long row = m0 + wm * 32 + i * 16 + g + ((r >> 1) ? 8 : 0);
+          const long long col = n0 + wn * 32 + j * 8 + 2 * t + (r & 1);
+          cv[j][r] = (row < M && col < M) ? C[row + col * ldc] : 0.0;
+        }
+  #pragma unroll
+      for (int j = 0; j < 4; ++j)
+  #pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const long long row = m0 + wm * 32 + i * 16 + g + ((r >> 1) ? 8 : 0);
+          const long long col = n0 + wn * 32 + j * 8 + 2 * t + (r & 1);
+          if (row < M && col < M) C[row + col * ldc] = fma(alpha, acc[i][j][r], cv[j][r]);
+        }
+    }
   }
 }
 
@@ -353,7 +362,11 @@ int dgemm_lower_nt(imcom_ctx* ctx, long long M, long long K, double alpha, const
     IMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LU_SMEM));
     IMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
                                   (int)cudaSharedmemCarveoutMaxShared));
-    k<<<tiles, LU_THREADS, LU_SMEM, ctx->stream>>>(M, (int)K, KP, alpha, A, lda, B, ldb, C, ldc);
+    // a context on a share of the SMs keeps to about three CTAs per SM of it
+    const unsigned grid =
+        ctx->sm_share > 0 ? std::min(tiles, 3u * (unsigned)sm_count(ctx)) : tiles;
+    k<<<grid, LU_THREADS, LU_SMEM, ctx->stream>>>(M, (int)K, KP, alpha, A, lda, B, ldb, C, ldc,
+                                                  (int)tiles);
     IMC_LAUNCH();
     return 0;
   }

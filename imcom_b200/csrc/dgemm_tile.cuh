@@ -195,5 +195,24 @@ dgemm_kernel(long long M, long long N, long long K, double alpha, const double* 
                                   (int)blockIdx.z, (int)gridDim.z);
 }
 
+// The same gm x gn x nkz tiles from a grid of at most a context's SM share:
+// CTA b takes tiles b, b + gridDim.x, ... (row blocks fastest), so a context
+// that shares the GPU with others keeps to about its share of the SMs.
+template <bool AK, bool BKC, int VEC>
+__global__ void __launch_bounds__(THREADS, 1)
+dgemm_persist_kernel(long long M, long long N, long long K, double alpha,
+                     const double* __restrict__ A, long long lda, const double* __restrict__ B,
+                     long long ldb, double beta, double* __restrict__ C, long long ldc,
+                     long long kchunk, int gm, int gn, int nkz) {
+  const long long total = (long long)gm * gn * nkz;
+  for (long long tile = blockIdx.x; tile < total; tile += gridDim.x) {
+    __syncthreads();  // every warp is done with the previous tile's shared stages
+    const long long xy = tile % ((long long)gm * gn);
+    dgemm_tile<AK, BKC, VEC, false>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kchunk,
+                                    (xy % gm) * BM, (xy / gm) * BN,
+                                    (int)(tile / ((long long)gm * gn)), nkz);
+  }
+}
+
 }  // namespace gemm
 }  // namespace imcom
