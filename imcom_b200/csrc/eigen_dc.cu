@@ -1274,19 +1274,27 @@ __global__ void dc_gather_kernel(const Node* nodes, const double* Z, long long l
 
 // The merge products of one level in one launch: OUT(node) = G(node) U(node)
 // for node z = blockIdx.z, M = its size, N = K = its non-deflated count read
-// on the device, so the level needs no host synchronisation.  CTAs past a
-// node's extent return at once.
+// on the device, so the level needs no host synchronisation.  Tiles past a
+// node's extent are skipped at once.
 template <int VEC>
 __global__ void __launch_bounds__(gemm::THREADS, 1)
 dc_gemm_kernel(const Node* nodes, const int* kcnt, const double* G, const double* U, double* OUT,
-               long long ld) {
-  const Node nd = nodes[blockIdx.z];
-  const long long k = kcnt[blockIdx.z];
-  const long long m0 = (long long)blockIdx.x * gemm::BM, n0 = (long long)blockIdx.y * gemm::BN;
-  if (m0 >= nd.nm || n0 >= k) return;
-  const size_t off = (size_t)nd.s + (size_t)nd.s * ld;
-  gemm::dgemm_tile<false, true, VEC>(nd.nm, k, k, 1.0, G + off, ld, U + off, ld, 0.0, OUT + off,
-                                     ld, k, m0, n0, 0, 1);
+               long long ld, int tiles, int nn) {
+  // one tile per CTA, or (a context on a share of the SMs, grid.x below the
+  // tile count) tiles b, b + gridDim.x, ... of tiles x tiles x nn
+  const long long total = (long long)tiles * tiles * nn;
+  for (long long b = blockIdx.x; b < total; b += gridDim.x) {
+    const int z = (int)(b / ((long long)tiles * tiles));
+    const int xy = (int)(b - (long long)z * tiles * tiles);
+    const Node nd = nodes[z];
+    const long long k = kcnt[z];
+    const long long m0 = (long long)(xy % tiles) * gemm::BM, n0 = (long long)(xy / tiles) * gemm::BN;
+    if (m0 >= nd.nm || n0 >= k) continue;  // uniform over the CTA
+    __syncthreads();  // every warp is done with the previous tile's shared stages
+    const size_t off = (size_t)nd.s + (size_t)nd.s * ld;
+    gemm::dgemm_tile<false, true, VEC>(nd.nm, k, k, 1.0, G + off, ld, U + off, ld, 0.0,
+                                       OUT + off, ld, k, m0, n0, 0, 1);
+  }
 }
 
 // Rank of each new eigenvalue within its node (stable, O(nm) per element).
@@ -1775,19 +1783,21 @@ int eigen_dc(imcom_ctx* ctx, const DMat& A, DMat& Wout, double* wout) {
       bool even = (UO.ld % 2 == 0) && (((uintptr_t)UO.p & 15) == 0);
       for (const Node& x : nodes) even = even && (x.s % 2 == 0);
       const unsigned tiles = (unsigned)((maxnm + gemm::BM - 1) / gemm::BM);
-      dim3 gd(tiles, tiles, nn_);
+      const unsigned total = tiles * tiles * (unsigned)nn_;
+      // a context on a share of the SMs: at most one CTA per SM of its share
+      const unsigned gd = ctx->sm_share > 0 ? std::min(total, (unsigned)sm_count(ctx)) : total;
       if (even) {
         IMC_CUDA(cudaFuncSetAttribute(dc_gemm_kernel<2>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)gemm::SMEM_BYTES));
         dc_gemm_kernel<2><<<gd, gemm::THREADS, gemm::SMEM_BYTES, ctx->stream>>>(
-            dnodes, wk.kcnt, Gm, Ub, OUT, UO.ld);
+            dnodes, wk.kcnt, Gm, Ub, OUT, UO.ld, (int)tiles, nn_);
       } else {
         IMC_CUDA(cudaFuncSetAttribute(dc_gemm_kernel<1>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)gemm::SMEM_BYTES));
         dc_gemm_kernel<1><<<gd, gemm::THREADS, gemm::SMEM_BYTES, ctx->stream>>>(
-            dnodes, wk.kcnt, Gm, Ub, OUT, UO.ld);
+            dnodes, wk.kcnt, Gm, Ub, OUT, UO.ld, (int)tiles, nn_);
       }
       IMC_LAUNCH();
     }
