@@ -184,7 +184,7 @@ def cpu_baseline(prob, steps=1):
 BATCH_KW = dict(UnotS=True, US_max=1e-6, US_tol=1e-8, maxnits=40)
 
 
-def batched_patches(npatch=256, sample=16, rank=0, world=1, dist=None, device=None, repeats=5,
+def batched_patches(npatch=256, sample=48, rank=0, world=1, dist=None, device=None, repeats=5,
                     cpu_sample=8):
     """The batched-patch workload: `npatch` patches of 4 exposures of side
     U{16..24} with 2% of input pixels masked (n ~ 990-2270), per-exposure
