@@ -202,7 +202,7 @@ def batched_patches(npatch=256, sample=48, rank=0, world=1, dist=None, device=No
     mine = replicas.shard_by_cost([replicas.patch_cost(p) for p in problems], rank, world)
     local = [problems[i] for i in mine]
     if local:
-        tune = batch.autotune(local[:sample], candidates=(1, 2, 3, 4, 6), tails=(0, 8, -1),
+        tune = batch.autotune(local[:sample], candidates=(1, 2, 3, 4, 6, 8), tails=(0, 8, -1),
                               **BATCH_KW)
     else:  # more ranks than patches: this rank only joins the barrier and the MAX
         tune = batch.Tuning(1, 0, {})
