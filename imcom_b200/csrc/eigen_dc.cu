@@ -1298,19 +1298,23 @@ dc_gemm_kernel(const Node* nodes, const int* kcnt, const double* G, const double
 }
 
 // Rank of each new eigenvalue within its node (stable, O(nm) per element).
+// One warp per element: the lanes split the comparisons and add their counts.
 __global__ void dc_rank_kernel(const Node* nodes, DcWork wk) {
   const Node nd = nodes[blockIdx.y];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (i >= nd.nm) return;
   const int s = nd.s, k = wk.kcnt[blockIdx.y];
   auto val = [&](int q) { return q < k ? wk.lam[s + q] : wk.defd[s + (q - k)]; };
   const double v = val(i);
   int rank = 0;
-  for (int q = 0; q < nd.nm; ++q) {
-    double u = val(q);
+  for (int q = lane; q < nd.nm; q += 32) {
+    const double u = val(q);
     rank += (u < v) || (u == v && q < i);
   }
-  wk.rank[s + i] = rank;
+#pragma unroll
+  for (int o = 16; o; o >>= 1) rank += __shfl_xor_sync(0xffffffffu, rank, o);
+  if (lane == 0) wk.rank[s + i] = rank;
 }
 
 // New node block: column rank(q) <- OUT(:, q) (q < k) or Z_old(:, defcol).
@@ -1801,7 +1805,7 @@ int eigen_dc(imcom_ctx* ctx, const DMat& A, DMat& Wout, double* wout) {
       }
       IMC_LAUNCH();
     }
-    dc_rank_kernel<<<ge, 256, 0, ctx->stream>>>(dnodes, wk);
+    dc_rank_kernel<<<dim3((maxnm + 7) / 8, nn_), 256, 0, ctx->stream>>>(dnodes, wk);
     IMC_LAUNCH();
     // Znxt(node) = [OUT | rotated deflated columns of Zcur] in eigenvalue order
     dim3 ga((maxnm + 255) / 256, maxnm, nn_);
