@@ -1023,6 +1023,80 @@ __global__ void __launch_bounds__(256) dc_deflate_kernel(const Node* nodes, DcWo
     __syncthreads();
   }
   const double tol = 8.0 * EPS * fmax(sh_d[0], rho * sh_z[0]);
+  // Fast path: when the cheap test below keeps every non-deflated pair (no
+  // pair needs the exact rotation test), the scan keeps the non-deflated and
+  // the z-deflated entries each in their order, so the output positions are
+  // prefix counts and every thread writes its own chunk.  Otherwise the
+  // sequential scan further down.
+  {
+    __shared__ int s_last[256], s_nk[256], s_nz[256], s_slow;
+    const int per = (nm + (int)blockDim.x - 1) / (int)blockDim.x;
+    const int a0 = min(nm, (int)threadIdx.x * per), a1 = min(nm, a0 + per);
+    const double* ds = wk.ds + s;
+    const double* zs = wk.zs + s;
+    int last = -1, nk = 0, nz = 0;
+    for (int q = a0; q < a1; ++q) {
+      if (rho * fabs(zs[q]) <= tol) {
+        ++nz;
+      } else {
+        ++nk;
+        last = q;
+      }
+    }
+    s_last[threadIdx.x] = last;
+    s_nk[threadIdx.x] = nk;
+    s_nz[threadIdx.x] = nz;
+    if (threadIdx.x == 0) s_slow = 0;
+    __syncthreads();
+    // the previous non-deflated entry before this chunk and the chunk's
+    // output offsets
+    int prev = -1, ko = 0, zo = 0;
+    for (int u = 0; u < (int)threadIdx.x; ++u) {
+      if (s_last[u] >= 0) prev = s_last[u];
+      ko += s_nk[u];
+      zo += s_nz[u];
+    }
+    bool slow = false;
+    for (int q = a0; q < a1; ++q) {
+      const double zj = zs[q];
+      if (rho * fabs(zj) <= tol) continue;
+      if (prev >= 0) {  // the same test as the scan's, against the raw previous entry
+        const double zpv = zs[prev], t = ds[q] - ds[prev];
+        const double far = 4.0 * tol * fma(zj, zj, zpv * zpv);
+        if (!(far >= 2.2250738585072014e-308 && fabs(t * zj * zpv) > far)) slow = true;
+      }
+      prev = q;
+    }
+    if (slow) s_slow = 1;
+    __syncthreads();
+    if (!s_slow) {
+      const int* pm = wk.perm + s;
+      for (int q = a0; q < a1; ++q) {
+        const double zj = zs[q];
+        if (rho * fabs(zj) <= tol) {
+          wk.defd[s + zo] = ds[q];
+          wk.defcol[s + zo] = pm[q];
+          ++zo;
+        } else {
+          wk.dl[s + ko] = ds[q];
+          wk.zz[s + ko] = zj;
+          wk.ndcol[s + ko] = pm[q];
+          ++ko;
+        }
+      }
+      if (threadIdx.x == 0) {
+        int kt = 0, zt = 0;
+        for (int u = 0; u < (int)blockDim.x; ++u) {
+          kt += s_nk[u];
+          zt += s_nz[u];
+        }
+        wk.kcnt[blockIdx.x] = kt;
+        wk.ndef[blockIdx.x] = zt;
+        wk.nrot[blockIdx.x] = 0;
+      }
+      return;
+    }
+  }
   int k = 0, ndef = 0, nrot = 0;
   bool have = false;      // a previous non-deflated entry exists
   double dp = 0.0, zp = 0.0;

@@ -940,3 +940,87 @@ def test_register_dft576_model():
     for b in range(3):
         F[3 * n + b] = _dft576_warp(v * _w(1728, m * b))
     assert np.abs(F - F_ref).max() <= 1e-14 * np.abs(F_ref).max()
+
+
+# ---- the deflation scan's parallel path (eigen_dc.cu, dc_deflate_kernel) ---
+
+def _fma(a, b, c):
+    """a b + c rounded once (the device fma)."""
+    from fractions import Fraction
+    return float(Fraction(a) * Fraction(b) + Fraction(c))
+
+
+def _deflate_scan(d, z, perm, rho, tol):
+    """The sequential scan as written (LAPACK dlaed2's tests), returning the
+    non-deflated (d, z, column), deflated (d, column) lists and rotations."""
+    dl, dd, rot = [], [], 0
+    have, dp, zp, pp = False, 0.0, 0.0, 0
+    for dj, zj, pj in zip(d, z, perm):
+        if rho * abs(zj) <= tol:
+            dd.append((dj, pj))
+            continue
+        if not have:
+            have, dp, zp, pp = True, dj, zj, pj
+            continue
+        t = dj - dp
+        far = 4.0 * tol * _fma(zj, zj, zp * zp)
+        rotate = False
+        if not (far >= 2.2250738585072014e-308 and abs(t * zj * zp) > far):
+            tau = math.hypot(zj, zp)
+            c, s = zj / tau, -zp / tau
+            rotate = abs(t * c * s) <= tol
+        if rotate:
+            rot += 1
+            dd.append((dp * c * c + dj * s * s, pp))
+            dp, zp, pp = dp * s * s + dj * c * c, tau, pj
+        else:
+            dl.append((dp, zp, pp))
+            dp, zp, pp = dj, zj, pj
+    if have:
+        dl.append((dp, zp, pp))
+    return dl, dd, rot
+
+
+def _deflate_parallel(d, z, perm, rho, tol, threads=256):
+    """The fast path as written: per-thread chunks, the cheap test against
+    the raw previous entry, prefix offsets; None when a pair needs the scan."""
+    nm = len(d)
+    per = -(-nm // threads)
+    chunks = [(min(nm, u * per), min(nm, u * per + per)) for u in range(threads)]
+    zdef = [rho * abs(x) <= tol for x in z]
+    prev = -1
+    for a0, a1 in chunks:
+        for q in range(a0, a1):
+            if zdef[q]:
+                continue
+            if prev >= 0:
+                far = 4.0 * tol * _fma(z[q], z[q], z[prev] * z[prev])
+                if not (far >= 2.2250738585072014e-308 and abs((d[q] - d[prev]) * z[q] * z[prev]) > far):
+                    return None
+            prev = q
+    dl = [(d[q], z[q], perm[q]) for q in range(nm) if not zdef[q]]
+    dd = [(d[q], perm[q]) for q in range(nm) if zdef[q]]
+    return dl, dd, 0
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_deflation_fast_path_is_the_scan(seed):
+    """Wherever the parallel path applies it gives the scan's lists; it
+    declines exactly when some pair needs the exact test."""
+    rng = np.random.default_rng(seed)
+    nm = int(rng.integers(1, 3000))
+    d = np.sort(rng.standard_normal(nm) * 10.0 ** rng.integers(-2, 3))
+    if seed % 2:  # clusters: some pairs close enough to rotate
+        d[1::7] = d[0::7][: len(d[1::7])] + 1e-17
+        d = np.sort(d)
+    z = rng.standard_normal(nm)
+    z[rng.random(nm) < 0.2] *= 1e-20  # z-deflated entries
+    perm = rng.permutation(nm)
+    rho = 1.3
+    tol = 8.0 * 2.0 ** -53 * max(np.abs(d).max(), rho * np.abs(z).max())
+    fast = _deflate_parallel(list(d), list(z), list(perm), rho, tol)
+    slow = _deflate_scan(list(d), list(z), list(perm), rho, tol)
+    if fast is not None:
+        assert fast == slow
+    else:
+        assert seed % 2  # only the clustered cases need the scan
