@@ -1024,3 +1024,39 @@ def test_deflation_fast_path_is_the_scan(seed):
         assert fast == slow
     else:
         assert seed % 2  # only the clustered cases need the scan
+
+
+# ---- the trailing update's lower-tile enumeration (dgemm.cu) ---------------
+
+def _lower_tile(b):
+    """lower_update_kernel's (ti, tj) from the linear index b: a float32
+    square root as the first guess, corrected by integer steps."""
+    ti = int((np.sqrt(np.float32(8.0) * np.float32(b) + np.float32(1.0)) - np.float32(1.0))
+             * np.float32(0.5))
+    while (ti + 1) * (ti + 2) // 2 <= b:
+        ti += 1
+    while ti > 0 and ti * (ti + 1) // 2 > b:
+        ti -= 1
+    return ti, b - ti * (ti + 1) // 2
+
+
+@pytest.mark.parametrize("nt", [1, 2, 3, 10, 64, 254, 700])
+def test_lower_tiles_enumerate_the_lower_triangle(nt):
+    """Linear indices 0 .. nt(nt+1)/2 - 1 map one to one onto the tiles
+    (ti, tj) with tj <= ti < nt (nt = 254 is n = 16200 in 64-row tiles)."""
+    tiles = [_lower_tile(b) for b in range(nt * (nt + 1) // 2)]
+    assert len(set(tiles)) == len(tiles)
+    assert all(0 <= tj <= ti < nt for ti, tj in tiles)
+
+
+def test_persistent_tile_loops_cover_each_tile_once():
+    """dgemm_persist_kernel and dc_gemm_kernel: CTA b takes tiles b, b + grid,
+    ... of gm x gn x nkz (row blocks fastest); every tile exactly once."""
+    for gm, gn, nkz, grid in [(32, 32, 1, 24), (2, 32, 9, 18), (5, 3, 1, 148), (1, 1, 4, 3)]:
+        seen = []
+        for b in range(grid):
+            for tile in range(b, gm * gn * nkz, grid):
+                xy = tile % (gm * gn)
+                seen.append((xy % gm, xy // gm, tile // (gm * gn)))
+        assert sorted(seen) == sorted((x, y, z) for z in range(nkz) for y in range(gn)
+                                      for x in range(gm))
