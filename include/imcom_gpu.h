@@ -84,7 +84,10 @@ typedef struct imcom_ctx imcom_ctx;
 #define IMCOM_OPT_BISECT_CTAS_PER_SM 9
 /* Number of SMs this context sizes its persistent and cooperative grids for
  * (the tridiagonalisation panel kernel, the resident bisection, split-K
- * GEMMs); 0 = the whole device.  Contexts that solve independent patches at
+ * GEMMs; with a share set, the FP64 GEMMs, the trailing updates and the
+ * divide-and-conquer products also loop over their tiles on grids bounded by
+ * it, so that contexts side by side keep off each other's SMs); 0 = the
+ * whole device.  Contexts that solve independent patches at
  * the same time on one GPU each take a share.  Results agree to rounding
  * (the reduction order of the eigensolver follows the grid). */
 #define IMCOM_OPT_SM_SHARE 10
