@@ -1060,3 +1060,47 @@ def test_persistent_tile_loops_cover_each_tile_once():
                 seen.append((xy % gm, xy // gm, tile // (gm * gn)))
         assert sorted(seen) == sorted((x, y, z) for z in range(nkz) for y in range(gn)
                                       for x in range(gm))
+
+
+def table_register_model(Gt, Gammat, pairs, nps, isB):
+    """fx_pass1/2's composition for npad = 3 (L = 3 nps): along each axis
+    three length-nps transforms of copies pre-twiddled by exp(2 pi i m(u) b / L)
+    (m(u) the signed frequency of spectrum index u) give outputs 3 j + b; W is
+    kept as W[k1][u2]; pass 2 writes the real part through both cshifts."""
+    L, s = 3 * nps, 3 * nps // 2
+    u = np.arange(nps)
+    m = np.where(u < nps // 2, u, u - nps)
+    tabs = []
+    for pr in pairs:
+        if pr[1] > 0:
+            X = np.conj(Gt[:, :, pr[0] - 1]) * Gt[:, :, pr[1] - 1]  # X[u1, u2]
+        else:
+            X = np.conj(Gammat) * Gt[:, :, pr[0] - 1]
+        W = np.zeros((L, nps), complex)
+        for b in range(3):
+            tw = np.exp(2j * np.pi * ((m * b) % L) / L)
+            W[3 * u + b, :] = np.fft.ifft(X * tw[:, None], axis=0) * nps
+        tab = np.empty((L, L))
+        p0 = (np.arange(L) - s) % L
+        for b in range(3):
+            tw = np.exp(2j * np.pi * ((m * b) % L) / L)
+            v = (np.fft.ifft(W * tw[None, :], axis=1) * nps).real  # [k1][j]
+            v = (-2.0 * v if isB else v) / nps / nps
+            tab[np.ix_(p0, (3 * u + b - s) % L)] = v
+        tabs.append(tab)
+    return tabs
+
+
+@pytest.mark.parametrize("nps", [4, 6, 12, 20])
+def test_register_table_path_matches_embed_fft_shift(nps):
+    """The register path's layout and shifts against the embed, FFT and
+    shift of the cuFFT path (npad = 3; the kernels take nps = 576)."""
+    rng = np.random.default_rng(nps)
+    E = 2
+    Gt = rng.standard_normal((nps, nps, E)) + 1j * rng.standard_normal((nps, nps, E))
+    Gammat = rng.standard_normal((nps, nps)) + 1j * rng.standard_normal((nps, nps))
+    for isB, pairs in ((0, [(1, 1), (1, 2), (2, 2)]), (1, [(1, 0), (2, 0)])):
+        got = table_register_model(Gt, Gammat, pairs, nps, isB)
+        ref = table_reference(Gt, Gammat, pairs, nps, 3 * nps, isB)
+        for g, r in zip(got, ref):
+            assert np.max(np.abs(g - r)) <= 1e-12 * max(1.0, np.max(np.abs(r)))
